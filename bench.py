@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: gate-evals/s of path-delay-fault grading on B200.
+
+One gate-eval is one (vector pair x gate) through the whole pipeline:
+two-pattern simulation, robust marking, pruning, first-detect merge and
+exact path counting.  A step grades one batch of synthetic pairs as a fresh
+job (the state is reset inside the step).  The default workload is the plain
+drop-in configuration: a 20,000-gate synthetic netlist (1,500 PI, 1,500 PO,
+depth 60) and 32,768 random vector pairs.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  For N > 1 (torchrun), each rank grades its
+own 32,768 pairs of the same circuit; the ranks exchange first-detect ids
+(all-reduce MIN) before counting, so the job equals one grading of all
+N x 32,768 pairs (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def _load(name, path):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def pkg():
+    return _load("pdf_b200", os.path.join(ROOT, "gpu-path-delay-coverage_b200", "__init__.py"))
+
+
+def oracle():
+    return _load("pdf_oracle", os.path.join(ROOT, "oracle", "oracle.py"))
+
+
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_id}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, val in zip(names, f[4:8]):
+                if val.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_id_for_smi(torch, dev: int) -> str:
+    try:
+        bus = torch.cuda.get_device_properties(dev).pci_bus_id
+        if bus:
+            return str(bus)
+    except Exception:
+        pass
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    ids = [x for x in vis.split(",") if x.strip()]
+    return ids[dev] if dev < len(ids) else str(dev)
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def traffic_summary(workload: str):
+    p = os.path.join(ROOT, "profiles", f"k_forward_{workload}.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(P, O, nl, v, t, n_sample: int, threads: int) -> dict:
+    """The oracle (a restatement of the reference algorithm; the reference has
+    no CPU implementation) on a prefix of the workload's pairs."""
+    codes = P.codes_from_planes(v[:, :P.words(n_sample)], t[:, :P.words(n_sample)], n_sample)
+    t0 = time.perf_counter()
+    r = O.grade(nl, codes, n_sample, mark_mode=P.MARK_ROBUST, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": nl.n_gates * n_sample / dt, "unit": "gate-evals/s", "cores": threads, "kind": "port",
+            "sample": f"first {n_sample} of the workload's pairs, {nl.n_gates} gates, "
+                      f"{dt:.2f} s, count {r.total}"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU path (the oracle port) on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    P, O = pkg(), oracle()
+    w = P.WORKLOADS[args.workload]
+    nl = P.gen_netlist(w["gen"])
+    n = w["pairs"]
+    v, t = P.gen_pairs(P.pair_seed(w["gen"].seed), nl.n_pi, n)
+    threads = os.cpu_count() or 1
+    n_sample = min(n, args.ref_sample)
+    codes = P.codes_from_planes(v[:, :P.words(n_sample)], t[:, :P.words(n_sample)], n_sample)
+    for _ in range(args.warmup):
+        O.grade(nl, codes, n_sample, mark_mode=P.MARK_ROBUST, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.grade(nl, codes, n_sample, mark_mode=P.MARK_ROBUST, threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    val = nl.n_gates * n_sample / (ms / 1e3)
+    line = {
+        "impl": "reference", "metric": "gate-evals/s", "value": val, "unit": "gate-evals/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded)",
+        "config": workload_config(P, args.workload, nl, n_sample),
+        "cpu_baseline": {"value": val, "unit": "gate-evals/s", "cores": threads, "kind": "port",
+                         "sample": f"first {n_sample} of {n} pairs per step"},
+        "e2e": {"value": val, "unit": "gate-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(P, name, nl, n_pairs) -> dict:
+    return {"workload": f"{name}: {nl.n_gates} gates, {nl.n_pi} PI, {int(nl.po.sum())} PO, "
+                        f"depth {nl.n_levels - 1}, {n_pairs} pairs/rank",
+            "gates": nl.n_gates, "pairs_per_rank": n_pairs, "mark_mode": "robust (LUT_R)",
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    P = pkg()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    w = P.WORKLOADS[args.workload]
+    nl = P.gen_netlist(w["gen"])
+    n = w["pairs"]
+    G, W = nl.n_gates, P.words(n)
+    v, t = P.gen_pairs(P.pair_seed(w["gen"].seed) + rank, nl.n_pi, n)
+    base = rank * n
+
+    c = P.Circuit(nl, device=local, mark_mode=P.MARK_ROBUST, max_pairs=n)
+    s = P.State(c)
+    stream = torch.cuda.current_stream().cuda_stream
+    dv = torch.from_numpy(v.view(np.int32)).cuda()
+    dt_ = torch.from_numpy(t.view(np.int32)).cuda()
+    sv, st_, mk = (torch.empty((G, W), dtype=torch.int32, device="cuda") for _ in range(3))
+    pairs = P.make_pairs(dv, dt_, n)
+    out = P.make_outputs(sv, st_, mk)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        s.reset_async(stream)
+        P.grade_async(c, s, pairs, base, out, stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    ref_total = s.snapshot()[2].value
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(gpu_id_for_smi(torch, local))
+    sampler.start()
+    time.sleep(0.3)
+    s.profile(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        ev[i][0].record()
+        step()
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    prof_ms, prof_calls = s.profile_read()
+    s.profile(False)
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    totals_ok = s.snapshot()[2].value == ref_total
+
+    # e2e: the public synchronous call with pinned host pairs (H2D inside the
+    # call) and the batch count read back to the host, every step.
+    hv = torch.from_numpy(v.view(np.int32)).pin_memory()
+    ht = torch.from_numpy(t.view(np.int32)).pin_memory()
+    hpairs = P.Pairs_t(hv.data_ptr(), ht.data_ptr(), n, W, 0)
+    import ctypes as C
+    e2e_ms = []
+    for i in range(max(3, args.warmup) + args.steps):
+        flush.fill_(i & 0xFF)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.reset_async(stream)
+        tot = P.Totals_t()
+        P.check(P.lib().pdf_grade(c.h, s.h, C.byref(hpairs), base, C.byref(out), C.byref(tot),
+                                  C.c_void_p(stream)), "pdf_grade")
+        if i >= max(3, args.warmup):
+            e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_ms_mean = sum(e2e_ms) / len(e2e_ms)
+
+    # max over ranks
+    if dist:
+        tt = torch.tensor([ms, e2e_ms_mean], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_ms_mean = tt.tolist()
+
+    units = world * G * n
+    value = units / (ms / 1e3)
+    peaks = measured_peaks()
+    B = 0.375 + 0.25 * nl.n_pi / G  # algorithmic bytes per gate-eval
+    fwd_ms = prof_ms[0] / max(1, prof_calls)
+    achieved = B * G * n / (fwd_ms / 1e3) / 1e9
+    tr = traffic_summary(args.workload)
+    line = {
+        "metric": "gate-evals/s", "value": value, "unit": "gate-evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+        "config": workload_config(P, args.workload, nl, n),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "kernel": "k_forward",
+                     "kernel_ms": fwd_ms, "cover_ms": prof_ms[1] / max(1, prof_calls),
+                     "bytes_per_gate_eval": B, "peak_source": peaks["source"] + " (hbm_gbs)",
+                     "traffic": tr.get("dram_bytes_per_launch") if tr else None},
+        "e2e": {"value": units / (e2e_ms_mean / 1e3), "unit": "gate-evals/s",
+                "h2d_bytes_per_step": int(2 * nl.n_pi * W * 4), "d2h_bytes_per_step": 64},
+        "gpu_launches": 6 * args.steps,
+        "clocks": clocks,
+        "result_stable": bool(totals_ok),
+        "batch_count": ref_total,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        O = oracle()
+        line["cpu_baseline"] = cpu_baseline(P, O, nl, v, t, min(n, args.cpu_sample), os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--cpu-sample", type=int, default=1 << 30)
+    ap.add_argument("--ref-sample", type=int, default=1 << 30)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,768 @@
+// pdf_api.cpp -- the C ABI (include/pdf.h) over the sm_100a kernels.
+//
+// Every call returns a status and never exits: the reference's HANDLE_ERROR
+// exit(EXIT_FAILURE) (simkernel.cuh:32-39, markkernel.cuh:13-20,
+// mergekernel.cuh:17-24, coverkernel.cuh:15-25) becomes PDF_ECUDA / PDF_EINVAL.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "pdf.h"
+#include "pdf_internal.h"
+#include "pdf_kernels.cuh"
+
+namespace {
+
+
+#define PDF_CUDA(call)                                  \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) {                        \
+            (void)cudaGetLastError();                   \
+            return e_ == cudaErrorMemoryAllocation ? PDF_ENOMEM : PDF_ECUDA; \
+        }                                               \
+    } while (0)
+
+void set_msg(char *msg, size_t len, const char *fmt, unsigned long long a = 0,
+             unsigned long long b = 0) {
+    if (msg && len) std::snprintf(msg, len, fmt, a, b);
+}
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    // Grow to at least `need` bytes (contents are not kept).
+    cudaError_t ensure(size_t need) {
+        if (bytes >= need) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, need ? need : 16);
+        if (e == cudaSuccess) bytes = need;
+        return e;
+    }
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// Scoped device selection.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+// Per-batch device workspace (owned by a state, or by a circuit for the
+// stage calls).
+struct Workspace {
+    DevBuf nzb, maxlvl, active, active_list, active_count;
+    DevBuf planes;   // internal V, T, M planes when the caller gives none
+    DevBuf pi;       // staged host pairs
+    uint64_t plane_ld = 0, plane_words = 0;
+    void release() {
+        nzb.release();
+        maxlvl.release();
+        active.release();
+        active_list.release();
+        active_count.release();
+        planes.release();
+        pi.release();
+    }
+};
+
+struct pdf_circuit {
+    int device = 0;
+    int mark_mode = PDF_MARK_DEFAULT;
+    pdf_circuit_info info{};
+    DevBuf rec, edges, level_off;
+    DevCircuit dc{};
+    uint32_t bw = 4, threads = 512, ring = 0;
+    size_t fwd_smem = 0;
+    uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
+    Workspace stage;  // scratch of the stage calls
+    std::mutex mu;    // serialises the stage scratch
+};
+
+struct ProfEvents {
+    cudaEvent_t ev[4];  // call start, forward end, cover end, call end
+};
+
+struct pdf_state {
+    pdf_circuit *c = nullptr;
+    DevBuf first_x, first_y, acc;
+    DevAcc *host_acc = nullptr;  // pinned
+    Workspace ws;
+    std::mutex mu;
+    bool profiling = false;
+    std::vector<ProfEvents> prof;   // one entry per profiled call
+    std::vector<ProfEvents> pool;   // recycled events
+};
+
+namespace {
+void prof_release(std::vector<ProfEvents> &v) {
+    for (auto &p : v)
+        for (auto &e : p.ev) cudaEventDestroy(e);
+    v.clear();
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+extern "C" const char *pdf_status_string(int s) {
+    switch (s) {
+        case PDF_OK: return "ok";
+        case PDF_EINVAL: return "invalid argument";
+        case PDF_ENOMEM: return "out of memory";
+        case PDF_EOVERFLOW: return "path count overflow";
+        case PDF_ETIMEOUT: return "device wait timed out";
+        case PDF_ECUDA: return "CUDA error";
+        case PDF_ENOTSUP: return "not supported";
+        case PDF_EBUSY: return "busy";
+        case PDF_ENODEV: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int pdf_abi_version(void) { return PDF_ABI_VERSION; }
+
+extern "C" pdf_status pdf_netlist_check(const pdf_netlist *nl, char *msg, size_t len) {
+    if (!nl) {
+        set_msg(msg, len, "null netlist");
+        return PDF_EINVAL;
+    }
+    const uint32_t G = nl->n_gates, L = nl->n_levels;
+    if (G == 0 || G == 0xFFFFFFFFu || L == 0 || !nl->level_offsets || !nl->type || !nl->po ||
+        !nl->nfi || !nl->nfo || !nl->edge_offset || (!nl->edges && nl->n_edges)) {
+        set_msg(msg, len, "empty netlist or missing array");
+        return PDF_EINVAL;
+    }
+    if (nl->n_edges >= 0xFFFFFFFFull) {
+        set_msg(msg, len, "too many edges (%llu)", nl->n_edges);
+        return PDF_EINVAL;
+    }
+    if (nl->level_offsets[0] != 0 || nl->level_offsets[L] != G) {
+        set_msg(msg, len, "level_offsets must start at 0 and end at n_gates");
+        return PDF_EINVAL;
+    }
+    for (uint32_t l = 0; l < L; l++)
+        if (nl->level_offsets[l + 1] < nl->level_offsets[l]) {
+            set_msg(msg, len, "level_offsets decrease at level %llu", l);
+            return PDF_EINVAL;
+        }
+    const uint32_t npi = nl->level_offsets[1];
+    if (npi == 0) {
+        set_msg(msg, len, "level 0 (primary inputs) is empty");
+        return PDF_EINVAL;
+    }
+    std::vector<uint32_t> level(G);
+    for (uint32_t l = 0; l < L; l++)
+        for (uint32_t g = nl->level_offsets[l]; g < nl->level_offsets[l + 1]; g++) level[g] = l;
+    for (uint32_t g = 0; g < G; g++) {
+        const uint32_t t = nl->type[g];
+        if (t >= PDF_NTYPES) {
+            set_msg(msg, len, "gate %llu: unknown type code %llu", g, t);
+            return PDF_EINVAL;
+        }
+        if (nl->po[g] > 1) {
+            set_msg(msg, len, "gate %llu: po must be 0 or 1", g);
+            return PDF_EINVAL;
+        }
+        if ((t == PDF_INPT) != (g < npi)) {
+            set_msg(msg, len, "gate %llu: INPT gates must be exactly level 0", g);
+            return PDF_EINVAL;
+        }
+        if (t == PDF_INPT ? nl->nfi[g] != 0 : (nl->nfi[g] == 0 || nl->nfi[g] > 255)) {
+            set_msg(msg, len, "gate %llu: bad fan-in count %llu", g, nl->nfi[g]);
+            return PDF_EINVAL;
+        }
+        const uint64_t end = nl->edge_offset[g] + (uint64_t)nl->nfi[g] + nl->nfo[g];
+        if (end > nl->n_edges || end < nl->edge_offset[g]) {
+            set_msg(msg, len, "gate %llu: edge range out of bounds", g);
+            return PDF_EINVAL;
+        }
+        for (uint32_t j = 0; j < nl->nfi[g]; j++) {
+            const uint32_t f = nl->edges[nl->edge_offset[g] + j];
+            if (f >= G || level[f] >= level[g]) {
+                set_msg(msg, len, "gate %llu: fan-in %llu not on a lower level", g, f);
+                return PDF_EINVAL;
+            }
+        }
+        for (uint32_t k = 0; k < nl->nfo[g]; k++) {
+            const uint32_t f = nl->edges[nl->edge_offset[g] + nl->nfi[g] + k];
+            if (f >= G || level[f] <= level[g]) {
+                set_msg(msg, len, "gate %llu: fan-out %llu not on a higher level", g, f);
+                return PDF_EINVAL;
+            }
+        }
+    }
+    // Fan-out lists must be the transpose of the fan-in lists (as multisets).
+    std::vector<uint64_t> cnt(G, 0);
+    for (uint32_t g = 0; g < G; g++)
+        for (uint32_t j = 0; j < nl->nfi[g]; j++) cnt[nl->edges[nl->edge_offset[g] + j]]++;
+    for (uint32_t g = 0; g < G; g++)
+        if (cnt[g] != nl->nfo[g]) {
+            set_msg(msg, len, "gate %llu: fan-out count %llu differs from its fan-in uses", g,
+                    nl->nfo[g]);
+            return PDF_EINVAL;
+        }
+    // Multiset comparison: count (source, consumer) occurrences both ways.
+    {
+        std::vector<std::pair<uint32_t, uint32_t>> in, out;
+        in.reserve(nl->n_edges / 2 + 1);
+        out.reserve(nl->n_edges / 2 + 1);
+        for (uint32_t g = 0; g < G; g++) {
+            for (uint32_t j = 0; j < nl->nfi[g]; j++) in.emplace_back(nl->edges[nl->edge_offset[g] + j], g);
+            for (uint32_t k = 0; k < nl->nfo[g]; k++)
+                out.emplace_back(g, nl->edges[nl->edge_offset[g] + nl->nfi[g] + k]);
+        }
+        std::sort(in.begin(), in.end());
+        std::sort(out.begin(), out.end());
+        if (in != out) {
+            set_msg(msg, len, "fan-out lists are not the transpose of the fan-in lists");
+            return PDF_EINVAL;
+        }
+    }
+    set_msg(msg, len, "ok");
+    return PDF_OK;
+}
+
+// ---------------------------------------------------------------------------
+
+extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circuit_opts *opts,
+                                         pdf_circuit **out) {
+    if (!out) return PDF_EINVAL;
+    *out = nullptr;
+    pdf_status st = pdf_netlist_check(nl, nullptr, 0);
+    if (st != PDF_OK) return st;
+    pdf_circuit_opts o{};
+    if (opts) o = *opts;
+    if (o.mark_mode != PDF_MARK_DEFAULT && o.mark_mode != PDF_MARK_ROBUST) return PDF_EINVAL;
+    if (o.tile_words && o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8)
+        return PDF_EINVAL;
+    if (o.threads && (o.threads < 64 || o.threads > 1024 || o.threads % 32)) return PDF_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        (void)cudaGetLastError();
+        return PDF_ENODEV;
+    }
+    if (o.device < 0 || o.device >= ndev) return PDF_EINVAL;
+    DeviceGuard dg(o.device);
+    if (!dg.ok) return PDF_ECUDA;
+
+    pdf_circuit *c = new (std::nothrow) pdf_circuit();
+    if (!c) return PDF_ENOMEM;
+    c->device = o.device;
+    c->mark_mode = o.mark_mode;
+    const uint32_t G = nl->n_gates, L = nl->n_levels;
+    pdf_circuit_info &inf = c->info;
+    inf.n_gates = G;
+    inf.n_levels = L;
+    inf.n_pi = nl->level_offsets[1];
+    inf.n_edges = nl->n_edges;
+    for (uint32_t g = 0; g < G; g++) {
+        inf.n_po += nl->po[g] ? 1 : 0;
+        inf.max_nfi = std::max(inf.max_nfi, nl->nfi[g]);
+        inf.max_nfo = std::max(inf.max_nfo, nl->nfo[g]);
+    }
+    for (uint32_t l = 0; l < L; l++)
+        inf.max_level_width = std::max(inf.max_level_width, nl->level_offsets[l + 1] - nl->level_offsets[l]);
+
+    std::vector<GateRec> recs(G);
+    for (uint32_t g = 0; g < G; g++) {
+        GateRec &r = recs[g];
+        std::memset(&r, 0, sizeof r);
+        r.w[0] = (uint32_t)nl->type[g] | ((uint32_t)(nl->po[g] ? 1 : 0) << 4) | (nl->nfi[g] << 8);
+        r.w[1] = nl->nfo[g];
+        r.w[2] = (uint32_t)nl->edge_offset[g];
+        for (uint32_t j = 0; j < nl->nfi[g] && j < (uint32_t)kInlineFanins; j++)
+            r.w[3 + j] = nl->edges[nl->edge_offset[g] + j];
+    }
+    auto fail = [&](pdf_status s) {
+        c->rec.release();
+        c->edges.release();
+        c->level_off.release();
+        delete c;
+        return s;
+    };
+    if (c->rec.ensure(sizeof(GateRec) * G) != cudaSuccess ||
+        c->edges.ensure(sizeof(uint32_t) * std::max<uint64_t>(nl->n_edges, 1)) != cudaSuccess ||
+        c->level_off.ensure(sizeof(uint32_t) * (L + 1)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(PDF_ENOMEM);
+    }
+    if (cudaMemcpy(c->rec.p, recs.data(), sizeof(GateRec) * G, cudaMemcpyHostToDevice) != cudaSuccess ||
+        (nl->n_edges && cudaMemcpy(c->edges.p, nl->edges, sizeof(uint32_t) * nl->n_edges,
+                                   cudaMemcpyHostToDevice) != cudaSuccess) ||
+        cudaMemcpy(c->level_off.p, nl->level_offsets, sizeof(uint32_t) * (L + 1),
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(PDF_ECUDA);
+    }
+    c->dc.rec = c->rec.as<GateRec>();
+    c->dc.edges = c->edges.as<uint32_t>();
+    c->dc.level_off = c->level_off.as<uint32_t>();
+    c->dc.n_gates = G;
+    c->dc.n_levels = L;
+    c->dc.n_pi = inf.n_pi;
+
+    // Launch plan.
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess) return fail(PDF_ECUDA);
+    c->bw = o.tile_words ? o.tile_words : 4;
+    c->threads = o.threads ? o.threads : 512;
+    // Two CTAs per SM: each gets just under half of the SM's shared memory.
+    const size_t budget = std::min<size_t>(prop.sharedMemPerBlockOptin, prop.sharedMemPerMultiprocessor / 2 - 2048);
+    uint32_t ring = 1;
+    while ((size_t)ring * 2 * c->bw * 12 <= budget) ring *= 2;
+    if ((size_t)ring * c->bw * 12 > budget) ring = 0;
+    c->ring = ring;
+    c->fwd_smem = forward_smem_bytes(c->bw, ring);
+    c->hash_cap = 4096;
+    c->cover_threads = 256;
+    c->cover_grid = (uint32_t)prop.multiProcessorCount;
+    inf.tile_words = c->bw;
+    inf.threads = c->threads;
+    inf.max_pairs = o.max_pairs ? o.max_pairs : 65536;
+    inf.device_bytes = c->rec.bytes + c->edges.bytes + c->level_off.bytes;
+    *out = c;
+    return PDF_OK;
+}
+
+extern "C" void pdf_circuit_destroy(pdf_circuit *c) {
+    if (!c) return;
+    DeviceGuard dg(c->device);
+    c->stage.release();
+    c->rec.release();
+    c->edges.release();
+    c->level_off.release();
+    delete c;
+}
+
+extern "C" pdf_status pdf_circuit_query(const pdf_circuit *c, pdf_circuit_info *info) {
+    if (!c || !info) return PDF_EINVAL;
+    *info = c->info;
+    return PDF_OK;
+}
+
+// ---------------------------------------------------------------------------
+
+extern "C" pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out) {
+    if (!c || !out) return PDF_EINVAL;
+    *out = nullptr;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    pdf_state *s = new (std::nothrow) pdf_state();
+    if (!s) return PDF_ENOMEM;
+    s->c = c;
+    const size_t G = c->info.n_gates;
+    if (s->first_x.ensure(4 * G) != cudaSuccess || s->first_y.ensure(4 * G) != cudaSuccess ||
+        s->acc.ensure(sizeof(DevAcc)) != cudaSuccess ||
+        cudaMallocHost(&s->host_acc, sizeof(DevAcc)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        pdf_state_destroy(s);
+        return PDF_ENOMEM;
+    }
+    pdf_status st = pdf_state_reset(s);
+    if (st != PDF_OK) {
+        pdf_state_destroy(s);
+        return st;
+    }
+    *out = s;
+    return PDF_OK;
+}
+
+extern "C" void pdf_state_destroy(pdf_state *s) {
+    if (!s) return;
+    DeviceGuard dg(s->c ? s->c->device : 0);
+    prof_release(s->prof);
+    prof_release(s->pool);
+    s->ws.release();
+    s->first_x.release();
+    s->first_y.release();
+    s->acc.release();
+    if (s->host_acc) cudaFreeHost(s->host_acc);
+    delete s;
+}
+
+extern "C" pdf_status pdf_state_reset(pdf_state *s) {
+    if (!s) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    const size_t G = s->c->info.n_gates;
+    PDF_CUDA(cudaDeviceSynchronize());
+    PDF_CUDA(cudaMemset(s->first_x.p, 0xFF, 4 * G));
+    PDF_CUDA(cudaMemset(s->first_y.p, 0xFF, 4 * G));
+    PDF_CUDA(cudaMemset(s->acc.p, 0, sizeof(DevAcc)));
+    PDF_CUDA(cudaDeviceSynchronize());
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_state_reset_async(pdf_state *s, void *stream) {
+    if (!s) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    const size_t G = s->c->info.n_gates;
+    PDF_CUDA(cudaMemsetAsync(s->first_x.p, 0xFF, 4 * G, cs));
+    PDF_CUDA(cudaMemsetAsync(s->first_y.p, 0xFF, 4 * G, cs));
+    PDF_CUDA(cudaMemsetAsync(s->acc.p, 0, sizeof(DevAcc), cs));
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_state_profile(pdf_state *s, int enable) {
+    if (!s) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    std::lock_guard<std::mutex> lk(s->mu);
+    PDF_CUDA(cudaDeviceSynchronize());
+    for (auto &p : s->prof) s->pool.push_back(p);
+    s->prof.clear();
+    s->profiling = enable != 0;
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_state_profile_read(pdf_state *s, double *ms, uint32_t *calls) {
+    if (!s || !ms) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    std::lock_guard<std::mutex> lk(s->mu);
+    ms[0] = ms[1] = ms[2] = 0;
+    for (auto &p : s->prof) {
+        PDF_CUDA(cudaEventSynchronize(p.ev[3]));
+        float a = 0, b = 0, c = 0;
+        PDF_CUDA(cudaEventElapsedTime(&a, p.ev[0], p.ev[1]));
+        PDF_CUDA(cudaEventElapsedTime(&b, p.ev[1], p.ev[2]));
+        PDF_CUDA(cudaEventElapsedTime(&c, p.ev[0], p.ev[3]));
+        ms[0] += a;
+        ms[1] += b;
+        ms[2] += c;
+    }
+    if (calls) *calls = (uint32_t)s->prof.size();
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_state_snapshot(pdf_state *s, uint32_t *first_x, uint32_t *first_y,
+                                         pdf_totals *tot) {
+    if (!s) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    const size_t G = s->c->info.n_gates;
+    PDF_CUDA(cudaDeviceSynchronize());
+    if (first_x) PDF_CUDA(cudaMemcpy(first_x, s->first_x.p, 4 * G, cudaMemcpyDeviceToHost));
+    if (first_y) PDF_CUDA(cudaMemcpy(first_y, s->first_y.p, 4 * G, cudaMemcpyDeviceToHost));
+    DevAcc h{};
+    PDF_CUDA(cudaMemcpy(&h, s->acc.p, sizeof h, cudaMemcpyDeviceToHost));
+    if (tot) {
+        tot->lo = h.total_lo;
+        tot->hi = h.total_hi;
+        tot->pairs = h.pairs;
+        tot->flags = h.flags;
+        tot->reserved = 0;
+    }
+    if (h.err) return PDF_ENOMEM;
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_state_restore(pdf_state *s, const uint32_t *first_x,
+                                        const uint32_t *first_y, const pdf_totals *tot) {
+    if (!s || !first_x || !first_y || !tot) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    const size_t G = s->c->info.n_gates;
+    PDF_CUDA(cudaDeviceSynchronize());
+    PDF_CUDA(cudaMemcpy(s->first_x.p, first_x, 4 * G, cudaMemcpyHostToDevice));
+    PDF_CUDA(cudaMemcpy(s->first_y.p, first_y, 4 * G, cudaMemcpyHostToDevice));
+    DevAcc h{};
+    h.total_lo = tot->lo;
+    h.total_hi = tot->hi;
+    h.pairs = tot->pairs;
+    h.flags = tot->flags;
+    PDF_CUDA(cudaMemcpy(s->acc.p, &h, sizeof h, cudaMemcpyHostToDevice));
+    PDF_CUDA(cudaDeviceSynchronize());
+    return PDF_OK;
+}
+
+// ---------------------------------------------------------------------------
+
+namespace {
+
+pdf_status check_pairs(const pdf_circuit *c, const pdf_pairs *pr, uint64_t pair_base) {
+    if (!pr || !pr->v || !pr->t) return PDF_EINVAL;
+    if (pr->n_pairs == 0) return PDF_EINVAL;
+    if (pr->ld < (pr->n_pairs + 31) / 32) return PDF_EINVAL;
+    if (pair_base + pr->n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;  // pair ids are uint32, ~0 = none
+    (void)c;
+    return PDF_OK;
+}
+
+// Sizes the workspace for W words of pairs.
+pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes) {
+    const uint64_t n_blocks = (W + c->bw - 1) / c->bw;
+    const uint64_t bm_words = (c->info.n_gates + 31) / 32;
+    PDF_CUDA(ws.nzb.ensure(n_blocks * bm_words * 4));
+    PDF_CUDA(ws.maxlvl.ensure(n_blocks * 4));
+    PDF_CUDA(ws.active.ensure(W * 4));
+    PDF_CUDA(ws.active_list.ensure(W * 32 * 4));
+    PDF_CUDA(ws.active_count.ensure(16));
+    if (need_planes) {
+        const uint64_t ld = n_blocks * c->bw;
+        if (ws.plane_ld < ld || !ws.planes.p) {
+            PDF_CUDA(ws.planes.ensure(3 * (uint64_t)c->info.n_gates * ld * 4));
+            ws.plane_ld = ld;
+        }
+    }
+    return PDF_OK;
+}
+
+FwdArgs base_fwd(pdf_circuit *c, uint64_t n_pairs) {
+    FwdArgs a{};
+    a.c = c->dc;
+    a.n_pairs = n_pairs;
+    a.W = (uint32_t)((n_pairs + 31) / 32);
+    a.bm_words = (c->info.n_gates + 31) / 32;
+    a.ring_gates = c->ring;
+    return a;
+}
+
+CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t ld, uint64_t n_pairs,
+                     uint32_t pair_base, const uint32_t *fx, const uint32_t *fy, DevAcc *acc) {
+    CoverArgs a{};
+    a.c = c->dc;
+    a.M = M;
+    a.ld = ld;
+    a.nzb = ws.nzb.as<uint32_t>();
+    a.blk_maxlvl = ws.maxlvl.as<uint32_t>();
+    a.bm_words = (c->info.n_gates + 31) / 32;
+    a.bw = c->bw;
+    a.first_x = fx;
+    a.first_y = fy;
+    a.n_pairs = n_pairs;
+    a.pair_base = pair_base;
+    a.active = ws.active.as<uint32_t>();
+    a.active_list = ws.active_list.as<uint32_t>();
+    a.active_count = ws.active_count.as<uint32_t>();
+    a.acc = acc;
+    a.hash_cap = c->hash_cap;
+    return a;
+}
+
+// Device pointers of the pairs (staging host pairs through the workspace).
+pdf_status stage_pairs(pdf_circuit *c, Workspace &ws, const pdf_pairs *pr, const uint32_t **v,
+                       const uint32_t **t, uint64_t *ld, cudaStream_t st) {
+    if (pr->on_device) {
+        *v = pr->v;
+        *t = pr->t;
+        *ld = pr->ld;
+        return PDF_OK;
+    }
+    const uint64_t W = (pr->n_pairs + 31) / 32, npi = c->info.n_pi;
+    PDF_CUDA(ws.pi.ensure(2 * npi * W * 4));
+    uint32_t *dv = ws.pi.as<uint32_t>(), *dt = dv + npi * W;
+    PDF_CUDA(cudaMemcpy2DAsync(dv, W * 4, pr->v, pr->ld * 4, W * 4, npi, cudaMemcpyHostToDevice, st));
+    PDF_CUDA(cudaMemcpy2DAsync(dt, W * 4, pr->t, pr->ld * 4, W * 4, npi, cudaMemcpyHostToDevice, st));
+    *v = dv;
+    *t = dt;
+    *ld = W;
+    return PDF_OK;
+}
+
+pdf_status copy_plane_out(uint32_t *dst, uint64_t dst_ld, int dst_dev, const uint32_t *src,
+                          uint64_t src_ld, uint64_t W, uint64_t G, cudaStream_t st) {
+    if (!dst) return PDF_OK;
+    if (dst_ld < W) return PDF_EINVAL;
+    PDF_CUDA(cudaMemcpy2DAsync(dst, dst_ld * 4, src, src_ld * 4, W * 4, G,
+                               dst_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    return PDF_OK;
+}
+
+}  // namespace
+
+extern "C" pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr,
+                                      uint64_t pair_base, const pdf_outputs *out, void *stream) {
+    if (!c || !s || s->c != c) return PDF_EINVAL;
+    pdf_status st = check_pairs(c, pr, pair_base);
+    if (st != PDF_OK) return st;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(s->mu);
+    const uint64_t n = pr->n_pairs, W = (n + 31) / 32, G = c->info.n_gates;
+    const bool direct = out && out->on_device && out->sim_v && out->sim_t && out->mark && out->ld >= W;
+    st = ensure_ws(c, s->ws, W, !direct);
+    if (st != PDF_OK) return st;
+    const uint32_t *pv, *pt;
+    uint64_t pld;
+    st = stage_pairs(c, s->ws, pr, &pv, &pt, &pld, cs);
+    if (st != PDF_OK) return st;
+
+    FwdArgs a = base_fwd(c, n);
+    a.pi_v = pv;
+    a.pi_t = pt;
+    a.pi_ld = pld;
+    if (direct) {
+        a.V = out->sim_v;
+        a.T = out->sim_t;
+        a.M = out->mark;
+        a.ld = out->ld;
+    } else {
+        a.ld = s->ws.plane_ld;
+        a.V = s->ws.planes.as<uint32_t>();
+        a.T = a.V + G * a.ld;
+        a.M = a.T + G * a.ld;
+    }
+    a.nzb = s->ws.nzb.as<uint32_t>();
+    a.blk_maxlvl = s->ws.maxlvl.as<uint32_t>();
+    a.first_x = s->first_x.as<uint32_t>();
+    a.first_y = s->first_y.as<uint32_t>();
+    a.pair_base = (uint32_t)pair_base;
+    DevAcc *acc = s->acc.as<DevAcc>();
+    ProfEvents *pe = nullptr;
+    if (s->profiling) {
+        ProfEvents p{};
+        if (!s->pool.empty()) {
+            p = s->pool.back();
+            s->pool.pop_back();
+        } else {
+            for (auto &e : p.ev) PDF_CUDA(cudaEventCreate(&e));
+        }
+        s->prof.push_back(p);
+        pe = &s->prof.back();
+        PDF_CUDA(cudaEventRecord(pe->ev[0], cs));
+    }
+    PDF_CUDA(launch_batch_begin(acc, cs));
+    PDF_CUDA(launch_forward(a, FWD_FUSED, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
+    if (pe) PDF_CUDA(cudaEventRecord(pe->ev[1], cs));
+    CoverArgs ca = base_cover(c, s->ws, a.M, a.ld, n, (uint32_t)pair_base, a.first_x, a.first_y, acc);
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
+    PDF_CUDA(launch_batch_end(acc, n, cs));
+    if (pe) PDF_CUDA(cudaEventRecord(pe->ev[2], cs));
+    if (out && !direct) {
+        st = copy_plane_out(out->sim_v, out->ld, out->on_device, a.V, a.ld, W, G, cs);
+        if (st == PDF_OK) st = copy_plane_out(out->sim_t, out->ld, out->on_device, a.T, a.ld, W, G, cs);
+        if (st == PDF_OK) st = copy_plane_out(out->mark, out->ld, out->on_device, a.M, a.ld, W, G, cs);
+        if (st != PDF_OK) return st;
+    }
+    if (pe) PDF_CUDA(cudaEventRecord(pe->ev[3], cs));
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_grade(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr, uint64_t pair_base,
+                                const pdf_outputs *out, pdf_totals *batch, void *stream) {
+    pdf_status st = pdf_grade_async(c, s, pr, pair_base, out, stream);
+    if (st != PDF_OK) return st;
+    DeviceGuard dg(c->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
+    PDF_CUDA(cudaStreamSynchronize(cs));
+    const DevAcc &h = *s->host_acc;
+    if (batch) {
+        batch->lo = h.batch_lo;
+        batch->hi = h.batch_hi;
+        batch->pairs = pr->n_pairs;
+        batch->flags = h.batch_flags;
+        batch->reserved = 0;
+    }
+    if (h.err) return PDF_ENOMEM;
+    return PDF_OK;
+}
+
+// ---- stage calls ----------------------------------------------------------
+
+extern "C" pdf_status pdf_sim(pdf_circuit *c, const pdf_pairs *pr, uint32_t *sim_v, uint32_t *sim_t,
+                              uint64_t ld, void *stream) {
+    if (!c || !sim_v || !sim_t) return PDF_EINVAL;
+    pdf_status st = check_pairs(c, pr, 0);
+    if (st != PDF_OK) return st;
+    if (ld < (pr->n_pairs + 31) / 32) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(c->mu);
+    const uint32_t *pv, *pt;
+    uint64_t pld;
+    st = stage_pairs(c, c->stage, pr, &pv, &pt, &pld, cs);
+    if (st != PDF_OK) return st;
+    FwdArgs a = base_fwd(c, pr->n_pairs);
+    a.pi_v = pv;
+    a.pi_t = pt;
+    a.pi_ld = pld;
+    a.V = sim_v;
+    a.T = sim_t;
+    a.ld = ld;
+    PDF_CUDA(launch_forward(a, FWD_SIM, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
+    if (!pr->on_device) PDF_CUDA(cudaStreamSynchronize(cs));  // staging buffer reuse
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_mark(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t,
+                               uint32_t *mark, uint64_t n_pairs, uint64_t ld, void *stream) {
+    if (!c || !sim_v || !sim_t || !mark || n_pairs == 0 || ld < (n_pairs + 31) / 32) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(c->mu);
+    const uint64_t W = (n_pairs + 31) / 32;
+    pdf_status st = ensure_ws(c, c->stage, W, false);
+    if (st != PDF_OK) return st;
+    FwdArgs a = base_fwd(c, n_pairs);
+    a.V = const_cast<uint32_t *>(sim_v);
+    a.T = const_cast<uint32_t *>(sim_t);
+    a.M = mark;
+    a.ld = ld;
+    a.nzb = c->stage.nzb.as<uint32_t>();
+    a.blk_maxlvl = c->stage.maxlvl.as<uint32_t>();
+    PDF_CUDA(launch_forward(a, FWD_MARK, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_merge(pdf_circuit *c, pdf_state *s, const uint32_t *sim_v, const uint32_t *mark,
+                                uint64_t n_pairs, uint64_t ld, uint64_t pair_base, void *stream) {
+    if (!c || !s || s->c != c || !sim_v || !mark || n_pairs == 0 || ld < (n_pairs + 31) / 32)
+        return PDF_EINVAL;
+    if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    PDF_CUDA(launch_merge_dense(c->dc, sim_v, mark, ld, n_pairs, (uint32_t)pair_base,
+                                s->first_x.as<uint32_t>(), s->first_y.as<uint32_t>(), cs));
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark, uint64_t n_pairs,
+                                uint64_t ld, uint64_t pair_base, pdf_totals *chunk, void *stream) {
+    if (!c || !s || s->c != c || !mark || n_pairs == 0 || ld < (n_pairs + 31) / 32) return PDF_EINVAL;
+    if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(s->mu);
+    const uint64_t W = (n_pairs + 31) / 32;
+    pdf_status st = ensure_ws(c, s->ws, W, false);
+    if (st != PDF_OK) return st;
+    DevAcc *acc = s->acc.as<DevAcc>();
+    PDF_CUDA(launch_batch_begin(acc, cs));
+    PDF_CUDA(launch_bitmap_from_marks(c->dc, mark, ld, n_pairs, c->bw, s->ws.nzb.as<uint32_t>(),
+                                      s->ws.maxlvl.as<uint32_t>(), (c->info.n_gates + 31) / 32, cs));
+    CoverArgs ca = base_cover(c, s->ws, mark, ld, n_pairs, (uint32_t)pair_base, s->first_x.as<uint32_t>(),
+                              s->first_y.as<uint32_t>(), acc);
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
+    PDF_CUDA(launch_batch_end(acc, n_pairs, cs));
+    PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
+    PDF_CUDA(cudaStreamSynchronize(cs));
+    const DevAcc &h = *s->host_acc;
+    if (chunk) {
+        chunk->lo = h.batch_lo;
+        chunk->hi = h.batch_hi;
+        chunk->pairs = n_pairs;
+        chunk->flags = h.batch_flags;
+        chunk->reserved = 0;
+    }
+    if (h.err) return PDF_ENOMEM;
+    return PDF_OK;
+}

@@ -1,0 +1,85 @@
+// pdf_kernels.cuh -- launch interface between the host API and the kernels.
+#ifndef PDF_KERNELS_CUH
+#define PDF_KERNELS_CUH
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pdf_device.cuh"
+
+struct DevCircuit {
+    const GateRec *rec;         // [n_gates]
+    const uint32_t *edges;      // fan-ins then fan-outs per gate
+    const uint32_t *level_off;  // [n_levels + 1]
+    uint32_t n_gates, n_levels, n_pi;
+};
+
+// Kernel stage selection for the forward kernel.
+enum FwdMode {
+    FWD_FUSED = 0,   // sim from the PI planes, forward mark, prune, merge
+    FWD_SIM = 1,     // sim only (pdf_sim)
+    FWD_MARK = 2     // sim planes given; forward mark + prune (pdf_mark)
+};
+
+struct FwdArgs {
+    DevCircuit c;
+    const uint32_t *pi_v, *pi_t;  // [n_pi][pi_ld]
+    uint64_t pi_ld;
+    uint32_t *V, *T, *M;          // planes [n_gates][ld]
+    uint64_t ld;
+    uint32_t *nzb;                // [n_blocks][bm_words] gates with a nonzero mark
+    uint32_t *blk_maxlvl;         // [n_blocks] highest level holding a mark (+1), 0 = none
+    uint32_t bm_words;
+    uint32_t *first_x, *first_y;  // [n_gates] (FWD_FUSED only)
+    uint64_t n_pairs;
+    uint32_t W;                   // ceil(n_pairs / 32)
+    uint32_t pair_base;
+    uint32_t ring_gates;          // power of two, or 0 (no ring)
+};
+
+// Batch accumulators kept in device memory by a pdf_state.
+struct DevAcc {
+    unsigned long long batch_lo, batch_hi;  // this batch's count
+    unsigned long long total_lo, total_hi;  // running total
+    unsigned long long pairs;
+    unsigned int flags;                     // PDF_FLAG_*
+    unsigned int batch_flags;
+    unsigned int err;                       // device-side error code (0 = none)
+    unsigned int pad[3];
+};
+
+struct CoverArgs {
+    DevCircuit c;
+    const uint32_t *M;            // pruned marks [n_gates][ld]
+    uint64_t ld;
+    const uint32_t *nzb;          // per column block bitmaps
+    const uint32_t *blk_maxlvl;
+    uint32_t bm_words;
+    uint32_t bw;                  // words per column block
+    const uint32_t *first_x, *first_y;
+    uint64_t n_pairs;
+    uint32_t pair_base;
+    uint32_t *active;             // [W] bitmap of first-detecting pairs
+    uint32_t *active_list;        // [max_pairs]
+    uint32_t *active_count;       // [1]
+    DevAcc *acc;
+    uint32_t hash_cap;            // entries of the per-CTA shared-memory hash (power of two)
+};
+
+// Host-side launchers (pdf_kernels.cu).  All return cudaError_t of the launch.
+cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
+                           size_t smem, cudaStream_t st);
+size_t forward_smem_bytes(uint32_t bw, uint32_t ring_gates);
+cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st);
+size_t cover_smem_bytes(uint32_t hash_cap);
+cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M,
+                               uint64_t ld, uint64_t n_pairs, uint32_t pair_base,
+                               uint32_t *first_x, uint32_t *first_y, cudaStream_t st);
+cudaError_t launch_bitmap_from_marks(const DevCircuit &c, const uint32_t *M, uint64_t ld,
+                                     uint64_t n_pairs, uint32_t bw, uint32_t *nzb,
+                                     uint32_t *blk_maxlvl, uint32_t bm_words, cudaStream_t st);
+cudaError_t launch_batch_begin(DevAcc *acc, cudaStream_t st);
+cudaError_t launch_batch_end(DevAcc *acc, uint64_t n_pairs, cudaStream_t st);
+
+#endif

@@ -1,0 +1,282 @@
+/*
+ * pdf.h -- C ABI of the B200 path-delay-fault grader.
+ *
+ * The grader takes a levelized combinational netlist and a batch of two-pattern
+ * vector pairs and produces, per (net, pair), a 2-bit transition code and a
+ * robust path mark, per net the first pair index that marks it with a falling
+ * and with a rising transition, and the exact number of covered paths.
+ *
+ * Every entry point returns a pdf_status and never exits or traps.  Host
+ * buffers are caller-owned; device memory behind a pdf_circuit / pdf_state is
+ * library-owned.  Streams are passed as `void *` (a cudaStream_t, NULL = the
+ * legacy default stream) so that no CUDA or torch type appears here.
+ *
+ * Reference interface replaced (lordofhyphens/gpu-path-delay-coverage):
+ *   gpuRunSimulation   simkernel.cuh:16,200     -> pdf_sim
+ *   gpuMarkPaths       markkernel.cuh:31,295    -> pdf_mark
+ *   gpuMergeSegments<1> mergekernel.cuh:200-201 -> pdf_merge
+ *   gpuCountPaths<1>   coverkernel.cuh:233-235  -> pdf_cover
+ *   the chunk loop     main.cu:171-231          -> pdf_grade
+ *   GPU_Circuit::copy  main.cu:137              -> pdf_circuit_create
+ *   dc_seglist + totals main.cu:141,169,224     -> pdf_state_*
+ */
+#ifndef PDF_H
+#define PDF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDF_ABI_VERSION 1
+
+typedef enum pdf_status {
+    PDF_OK = 0,
+    PDF_EINVAL = 1,     /* malformed argument or netlist */
+    PDF_ENOMEM = 2,     /* device or host allocation failed / admission refused */
+    PDF_EOVERFLOW = 3,  /* a path count does not fit in 128 bits */
+    PDF_ETIMEOUT = 4,   /* a bounded device-side wait gave up */
+    PDF_ECUDA = 5,      /* a CUDA runtime call failed */
+    PDF_ENOTSUP = 6,    /* feature not available in this build / on this device */
+    PDF_EBUSY = 7,      /* resource in use (serving queue full, job still running) */
+    PDF_ENODEV = 8      /* no CUDA device */
+} pdf_status;
+
+/* Gate type codes.  AND..XNOR must be 2..7: the reference indexes its robust
+ * sensitisation table with (type - 2) (markkernel.cuh:36-37,49). */
+enum {
+    PDF_UNKN = 0,
+    PDF_INPT = 1,
+    PDF_AND = 2,
+    PDF_NAND = 3,
+    PDF_OR = 4,
+    PDF_NOR = 5,
+    PDF_XOR = 6,
+    PDF_XNOR = 7,
+    PDF_BUFF = 8,
+    PDF_NOT = 9,
+    PDF_FROM = 10,
+    PDF_DFF = 11,
+    PDF_NTYPES = 12
+};
+
+/* 2-bit transition codes: bit0 = value under the second vector, bit1 = the
+ * value changed (simkernel.cuh:164, markkernel.cuh:230, mergekernel.cuh:141-146).
+ * T0 is a falling transition, T1 a rising one. */
+enum { PDF_S0 = 0, PDF_S1 = 1, PDF_T0 = 2, PDF_T1 = 3 };
+
+/* Result flags (pdf_totals.flags). */
+#define PDF_FLAG_OVERFLOW 0x1u   /* some count exceeded 2^128 - 1; totals are saturated */
+
+/*
+ * A levelized netlist (the data contract of the reference's GPU_Circuit:
+ * GPUNODE{type,nfi,nfo,offset,po} and the FIN edge array,
+ * simkernel.cuh:108-145, markkernel.cuh:220-223,277, coverkernel.cuh:205).
+ *
+ * Gate ids are in level order: level l holds gates
+ * [level_offsets[l], level_offsets[l+1]).  Level 0 holds the primary inputs
+ * (type PDF_INPT) and nothing else.  Every fan-in of a gate lies on a lower
+ * level.  For gate g, edges[edge_offset[g] + j] (j < nfi[g]) are its fan-ins
+ * in order (fan-in 0 first) and edges[edge_offset[g] + nfi[g] + k]
+ * (k < nfo[g]) its fan-outs.  The fan-out lists must be exactly the transpose
+ * of the fan-in lists (as multisets).  po[g] != 0 marks a primary output.
+ */
+typedef struct pdf_netlist {
+    uint32_t n_gates;
+    uint32_t n_levels;              /* number of levels, >= 1 */
+    const uint32_t *level_offsets;  /* n_levels + 1 entries */
+    const uint8_t *type;            /* n_gates */
+    const uint8_t *po;              /* n_gates */
+    const uint32_t *nfi;            /* n_gates */
+    const uint32_t *nfo;            /* n_gates */
+    const uint64_t *edge_offset;    /* n_gates */
+    const uint32_t *edges;
+    uint64_t n_edges;               /* length of edges[] */
+} pdf_netlist;
+
+/*
+ * Vector pairs as two bit-planes per primary input.  For PI i (the i-th gate
+ * of level 0) and pair p, bit (p % 32) of v[i * ld + p / 32] is the value
+ * under the second vector (code bit 0) and the same bit of t[] is the
+ * transition flag (code bit 1).  Bits at pair indices >= n_pairs are ignored.
+ */
+typedef struct pdf_pairs {
+    const uint32_t *v;
+    const uint32_t *t;
+    uint64_t n_pairs;
+    uint64_t ld;        /* words per PI row, >= ceil(n_pairs / 32) */
+    int on_device;      /* 1: v, t are device pointers on the circuit's device */
+} pdf_pairs;
+
+/*
+ * Optional per-(net, pair) outputs, gate-major bit-planes: bit (p % 32) of
+ * word [g * ld + p / 32].  sim_v / sim_t are the two code bits of the
+ * simulated transition value, mark the robust mark after pruning.  Any pointer
+ * may be NULL.  Bits at pair indices >= n_pairs are written as 0.
+ */
+typedef struct pdf_outputs {
+    uint32_t *sim_v;
+    uint32_t *sim_t;
+    uint32_t *mark;
+    uint64_t ld;        /* words per gate row, >= ceil(n_pairs / 32) */
+    int on_device;
+} pdf_outputs;
+
+/* 128-bit path totals. */
+typedef struct pdf_totals {
+    uint64_t lo;
+    uint64_t hi;
+    uint64_t pairs;     /* pairs graded */
+    uint32_t flags;     /* PDF_FLAG_* */
+    uint32_t reserved;
+} pdf_totals;
+
+typedef struct pdf_circuit pdf_circuit;
+typedef struct pdf_state pdf_state;
+
+/* Robust mode.  The reference reads one of two sensitisation tables
+ * (markkernel.cuh:36-37, selected at :255-259 by --robust, main.cu:53). */
+enum {
+    PDF_MARK_DEFAULT = 0,  /* LUT_NR: {0x2A00,0x2A00,0x5100,0x5100,0,0} (no --robust) */
+    PDF_MARK_ROBUST = 1    /* LUT_R:  {0x2200,0x2200,0x1100,0x1100,0,0} (--robust)    */
+};
+
+typedef struct pdf_circuit_opts {
+    int device;          /* CUDA device ordinal */
+    int mark_mode;       /* PDF_MARK_DEFAULT or PDF_MARK_ROBUST */
+    uint32_t max_pairs;  /* largest batch this circuit will grade (sizes scratch); 0 = 65536 */
+    uint32_t tile_words; /* 0 = autotune; else words (32 pairs) per CTA column block: 1,2,4,8 */
+    uint32_t threads;    /* 0 = autotune; else threads per CTA: 128..1024 */
+    uint32_t reserved[3];
+} pdf_circuit_opts;
+
+typedef struct pdf_circuit_info {
+    uint32_t n_gates, n_levels, n_pi, n_po;
+    uint32_t max_level_width;
+    uint32_t max_nfi, max_nfo;
+    uint32_t tile_words, threads;
+    uint64_t n_edges;
+    uint64_t device_bytes;   /* netlist + plan + scratch */
+    uint64_t max_pairs;
+} pdf_circuit_info;
+
+const char *pdf_status_string(int status);
+int pdf_abi_version(void);
+
+/* Host-side structural check of a netlist (no device needed).  On failure a
+ * one-line reason is written to msg (if msg_len > 0). */
+pdf_status pdf_netlist_check(const pdf_netlist *nl, char *msg, size_t msg_len);
+
+/* Upload a netlist to a device (GPU_Circuit::copy, main.cu:137). */
+pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circuit_opts *opts,
+                              pdf_circuit **out);
+void pdf_circuit_destroy(pdf_circuit *c);
+pdf_status pdf_circuit_query(const pdf_circuit *c, pdf_circuit_info *info);
+
+/* Per-circuit first-detect state and running total: the reference keeps the
+ * per-segment first pair ids in dc_seglist across chunks and the total in
+ * *totals (main.cu:141,169,224; mergekernel.cuh:205-222).  first_x = first
+ * pair marking the net with a falling (T0) transition, first_y = rising (T1);
+ * 0xFFFFFFFF = none yet. */
+pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out);
+void pdf_state_destroy(pdf_state *s);
+pdf_status pdf_state_reset(pdf_state *s);
+/* Synchronises with the state's last grading call. Any pointer may be NULL. */
+pdf_status pdf_state_snapshot(pdf_state *s, uint32_t *first_x, uint32_t *first_y,
+                              pdf_totals *totals);
+pdf_status pdf_state_restore(pdf_state *s, const uint32_t *first_x,
+                             const uint32_t *first_y, const pdf_totals *totals);
+
+/* Stream-ordered reset: clears the state on `stream` without waiting. */
+pdf_status pdf_state_reset_async(pdf_state *s, void *stream);
+
+/* Device timing of grading calls with CUDA events on the grading stream.
+ * enable = 1 clears and starts recording, 0 stops.  pdf_state_profile_read
+ * waits for the recorded calls and returns, summed over them, ms[0] = the
+ * forward kernel (sim + mark + prune + merge), ms[1] = the cover kernels,
+ * ms[2] = the whole call; *calls = calls recorded. */
+pdf_status pdf_state_profile(pdf_state *s, int enable);
+pdf_status pdf_state_profile_read(pdf_state *s, double *ms, uint32_t *calls);
+
+/*
+ * Grade one batch of pairs with global pair indices pair_base .. pair_base +
+ * n_pairs - 1 (the chunk loop body, main.cu:171-231): simulate, mark, prune,
+ * fold the first-detecting pairs into the state and add the batch's covered
+ * path count to the state's total.  Batches of one state must come in
+ * increasing pair order for the result to be independent of the batching.
+ *
+ * pdf_grade_async only enqueues work on `stream`; pdf_grade also waits and
+ * returns this batch's count in *batch (may be NULL).
+ */
+pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pairs *pairs,
+                           uint64_t pair_base, const pdf_outputs *out, void *stream);
+pdf_status pdf_grade(pdf_circuit *c, pdf_state *s, const pdf_pairs *pairs,
+                     uint64_t pair_base, const pdf_outputs *out, pdf_totals *batch,
+                     void *stream);
+
+/*
+ * Stage calls, one per reference host function, over device buffers in the
+ * pdf_outputs plane layout (gate-major, ld words per row).  They compose to
+ * exactly what pdf_grade computes.
+ */
+/* gpuRunSimulation (simkernel.cuh:200-249): transition codes of every net. */
+pdf_status pdf_sim(pdf_circuit *c, const pdf_pairs *pairs, uint32_t *sim_v,
+                   uint32_t *sim_t, uint64_t ld, void *stream);
+/* gpuMarkPaths (markkernel.cuh:295-355): forward robust marks, then removal of
+ * marks that reach no primary output. */
+pdf_status pdf_mark(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t,
+                    uint32_t *mark, uint64_t n_pairs, uint64_t ld, void *stream);
+/* gpuMergeSegments<1> (mergekernel.cuh:200-267): fold the first marking pair
+ * of every net (split by transition direction) into the state. */
+pdf_status pdf_merge(pdf_circuit *c, pdf_state *s, const uint32_t *sim_v,
+                     const uint32_t *mark, uint64_t n_pairs, uint64_t ld,
+                     uint64_t pair_base, void *stream);
+/* gpuCountPaths<1> (coverkernel.cuh:233-333): count covered paths of this
+ * chunk against the state's first-detect ids, add them to the state's total
+ * and (synchronously) return the chunk's count in *chunk_total. */
+pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark,
+                     uint64_t n_pairs, uint64_t ld, uint64_t pair_base,
+                     pdf_totals *chunk_total, void *stream);
+
+/* ---- synthetic inputs (seeded, host-side) ---- */
+
+typedef struct pdf_gen_params {
+    uint64_t seed;
+    uint32_t n_gates;     /* total, including the primary inputs */
+    uint32_t n_pi;
+    uint32_t n_po;
+    uint32_t depth;       /* levels above the inputs; n_levels = depth + 1 */
+    uint32_t fanin_min;   /* for AND..XNOR; NOT/BUFF take exactly 1 */
+    uint32_t fanin_max;
+    uint32_t fanout_dist; /* 0 = geometric, 1 = Zipf */
+    double zipf_s;
+    uint32_t fanout_max;  /* cap on fan-out (0 = none) */
+    uint32_t type_mask;   /* bit per gate code drawn uniformly; 0 = AND..XNOR,NOT,BUFF */
+    uint32_t reserved[4];
+} pdf_gen_params;
+
+typedef struct pdf_netbuf pdf_netbuf;  /* a library-owned host netlist */
+
+pdf_status pdf_gen_netlist(const pdf_gen_params *p, pdf_netbuf **out);
+pdf_status pdf_netbuf_from(const pdf_netlist *nl, pdf_netbuf **out);  /* deep copy */
+void pdf_netbuf_view(const pdf_netbuf *b, pdf_netlist *view);
+void pdf_netbuf_free(pdf_netbuf *b);
+
+/* Uniform random pairs: every code bit of every (PI, pair) independent and
+ * uniform.  Writes n_pi rows of ld words into v and t (host memory); bits at
+ * pair indices >= n_pairs are 0. */
+pdf_status pdf_gen_pairs(uint64_t seed, uint32_t n_pi, uint64_t n_pairs, uint64_t ld,
+                         uint32_t *v, uint32_t *t);
+
+/* Reference-compatible pair formation from one vector stream
+ * (simkernel.cuh:115-124): pair p = (vector p, vector p+1); the last pair wraps
+ * to vector 0.  vec is n_pi rows of n_vec bytes (0/1).  Produces n_vec pairs. */
+pdf_status pdf_pairs_from_vectors(const uint8_t *vec, uint32_t n_pi, uint64_t n_vec,
+                                  uint64_t ld, uint32_t *v, uint32_t *t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDF_H */

@@ -1,0 +1,125 @@
+"""A second, independent restatement of the reference semantics in pure
+Python, per pair, for tiny circuits: it checks the C oracle, and its cover
+counts paths by explicit enumeration instead of the reference's dynamic
+program (coverkernel.cuh:171-230), so it also checks that program.
+
+Tables are the reference's constants (simkernel.cuh:158-165,
+markkernel.cuh:36-37).
+"""
+from __future__ import annotations
+
+INPT, AND, NAND, OR, NOR, XOR, XNOR, BUFF, NOT, FROM, DFF = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+S0, S1, T0, T1 = 0, 1, 2, 3
+
+LUT2 = {
+    NAND: [S1, S1, S1, S1, S1, S0, T1, T0, S1, T1, T1, S1, S1, T0, S1, T0],
+    AND: [S0, S0, S0, S0, S0, S1, T0, T1, S0, T0, T0, S0, S0, T1, S0, T1],
+    NOR: [S1, S0, T1, T0, S0, S0, S0, S0, T1, S0, T1, S0, T0, S0, S0, T0],
+    OR: [S0, S1, T0, T1, S1, S1, S1, S1, T0, S1, T0, S1, T1, S1, S1, T1],
+    XNOR: [S1, S0, T1, T0, S0, S1, T0, T1, T1, T0, S1, S0, T0, T1, S0, S1],
+    XOR: [S0, S1, T0, T1, S1, S0, T1, T0, T0, T1, S0, S1, T1, T0, S1, S0],
+}
+STABLE = [S0, T0, T1, S1]
+NOT_LUT = [S1, S0, T1, T0]
+SENS = {  # mark_mode -> table indexed by type - 2
+    0: [0x2A00, 0x2A00, 0x5100, 0x5100, 0, 0],
+    1: [0x2200, 0x2200, 0x1100, 0x1100, 0, 0],
+}
+
+
+def per_vector(op, a: int, b: int) -> int:
+    """Code of op applied to each of the two vectors of codes a and b."""
+    a2, b2 = a & 1, b & 1
+    a1, b1 = a2 ^ (a >> 1), b2 ^ (b >> 1)
+    v1, v2 = op(a1, b1) & 1, op(a2, b2) & 1
+    return v2 | ((v1 ^ v2) << 1)
+
+
+def sim_pair(nl, pi_codes, p):
+    G = nl.n_gates
+    val = [0] * G
+    for g in range(G):
+        t = int(nl.type[g])
+        fi = [int(x) for x in nl.fanins(g)]
+        if t == INPT:
+            val[g] = int(pi_codes[g][p])
+        elif t in (BUFF, FROM, DFF):
+            val[g] = val[fi[0]]
+        else:
+            v = val[fi[0]]
+            if t == NOT:
+                v = NOT_LUT[v]
+            for f in fi[1:]:
+                # the coalesced simLUT evaluates only AND/NAND/OR/NOR; else 0
+                v = LUT2[t][val[f] * 4 + v] if t in (AND, NAND, OR, NOR) else 0
+            val[g] = v
+    return val
+
+
+def mark_pair(nl, val, mode: int, prune: bool = True):
+    G = nl.n_gates
+    m = [0] * G
+    for g in range(G):
+        t = int(nl.type[g])
+        fi = [int(x) for x in nl.fanins(g)]
+        trans = 1 if val[g] > 1 else 0
+        if t == INPT:
+            r = trans
+        elif t in (FROM, BUFF, DFF, NOT):
+            r = m[fi[0]]
+        elif AND <= t <= XNOR:
+            r = 0
+            for i in range(len(fi)):
+                ok = all((SENS[mode][t - 2] >> (val[fi[i]] * 4 + val[fi[j]])) & 1
+                         for j in range(len(fi)) if j != i)
+                r |= int(ok) & m[fi[0]]
+        else:
+            r = 0
+        m[g] = r & trans
+    if prune:
+        for g in reversed(range(G)):
+            keep = 1 if nl.po[g] else 0
+            for fo in nl.fanouts(g):
+                keep |= m[int(fo)]
+            m[g] &= keep
+    return m
+
+
+def grade(nl, pi_codes, n_pairs: int, mode: int = 0, pair_base: int = 0, first_x=None, first_y=None):
+    """Returns (vals[p][g], marks[p][g], first_x, first_y, total) with the cover
+    counted by enumerating every marked input-to-output path per pair."""
+    G = nl.n_gates
+    fx = [0xFFFFFFFF] * G if first_x is None else list(first_x)
+    fy = [0xFFFFFFFF] * G if first_y is None else list(first_y)
+    vals, marks = [], []
+    for p in range(n_pairs):
+        v = sim_pair(nl, pi_codes, p)
+        m = mark_pair(nl, v, mode)
+        vals.append(v)
+        marks.append(m)
+        for g in range(G):
+            if m[g]:
+                pid = pair_base + p
+                if v[g] & 1:
+                    fy[g] = min(fy[g], pid)
+                else:
+                    fx[g] = min(fx[g], pid)
+    total = 0
+    lvl0 = int(nl.level_offsets[1])
+    for p in range(n_pairs):
+        pid = pair_base + p
+        m = marks[p]
+
+        def paths(g, credited):
+            if not m[g]:
+                return 0
+            cr = credited or fx[g] == pid or fy[g] == pid
+            n = 1 if (nl.po[g] == 1 and cr) else 0
+            for fo in nl.fanouts(g):
+                n += paths(int(fo), cr)
+            return n
+
+        for g in range(lvl0):
+            if nl.type[g] == INPT:
+                total += paths(g, False)
+    return vals, marks, fx, fy, total

@@ -1,0 +1,99 @@
+"""Known-answer tests of the reference's lookup tables.
+
+The reference's tables (simkernel.cuh:158-165, markkernel.cuh:36-41) are
+the only fixed data of the algorithm.  These tests pin (1) that each 2-input
+table is the exact per-vector boolean function, (2) that the oracle holds
+those tables, and (3) that the bit-plane forms the kernels use
+(pdf_device.cuh) equal them on every entry.
+"""
+import operator
+import subprocess
+
+import numpy as np
+import pytest
+
+import helpers
+import refmodel as R
+
+OPS = {R.AND: operator.and_, R.NAND: lambda a, b: 1 - (a & b), R.OR: operator.or_,
+       R.NOR: lambda a, b: 1 - (a | b), R.XOR: operator.xor, R.XNOR: lambda a, b: 1 - (a ^ b)}
+
+
+@pytest.mark.parametrize("t", sorted(OPS))
+def test_reference_tables_are_per_vector_boolean(t):
+    for r in range(4):
+        for v in range(4):
+            assert R.LUT2[t][r * 4 + v] == R.per_vector(OPS[t], v, r)
+
+
+def test_stable_and_not_tables():
+    # stable[v2 * 2 + v1]: S0 (0,0), T0 (1->0), T1 (0->1), S1 (1,1)
+    for v1 in (0, 1):
+        for v2 in (0, 1):
+            code = R.STABLE[v2 * 2 + v1]
+            assert code & 1 == v2 and (code >> 1) == (v1 ^ v2)
+    for c in range(4):
+        assert R.NOT_LUT[c] == (c ^ 1)
+
+
+def test_oracle_holds_the_tables():
+    o = helpers.oracle().lib()
+    for t in list(OPS) + [0, 1, 8, 9, 10, 11]:
+        for r in range(4):
+            for v in range(4):
+                want = R.LUT2[t][r * 4 + v] if t in OPS else 0
+                assert o.pdfo_lut2(t, v, r) == want
+    for v1 in (0, 1):
+        for v2 in (0, 1):
+            assert o.pdfo_stable(v1, v2) == R.STABLE[v2 * 2 + v1]
+    for c in range(4):
+        assert o.pdfo_not(c) == R.NOT_LUT[c]
+    for mode in (0, 1):
+        for t in range(12):
+            for on in range(4):
+                for off in range(4):
+                    want = (R.SENS[mode][t - 2] >> (on * 4 + off)) & 1 if 2 <= t <= 7 else 0
+                    assert o.pdfo_sens(mode, t, on, off) == want
+
+
+def test_sensitisation_tables_decode():
+    # LUT_NR (default): AND/NAND on=T0 & side in {S1,T1}; on=T1 & side=S1.
+    nr, r = R.SENS[0], R.SENS[1]
+    bits = lambda m: {(i >> 2, i & 3) for i in range(16) if (m >> i) & 1}
+    assert bits(nr[0]) == {(R.T0, R.S1), (R.T0, R.T1), (R.T1, R.S1)}
+    assert bits(nr[2]) == {(R.T0, R.S0), (R.T1, R.S0), (R.T1, R.T0)}
+    assert bits(r[0]) == {(R.T0, R.S1), (R.T1, R.S1)}
+    assert bits(r[2]) == {(R.T0, R.S0), (R.T1, R.S0)}
+    assert nr[4] == nr[5] == r[4] == r[5] == 0
+
+
+@pytest.fixture(scope="module")
+def probe(tmp_path_factory):
+    exe = tmp_path_factory.mktemp("probe") / "lut_probe"
+    src = helpers.ROOT / "tests" / "lut_probe.cpp"
+    subprocess.run(["g++", "-std=c++17", "-O1", f"-I{helpers.ROOT / 'include'}",
+                    f"-I{helpers.PKG_DIR / 'csrc'}", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    rows = {}
+    for line in out.splitlines():
+        k, *vals = line.split()
+        rows.setdefault(k, []).append(tuple(int(x) for x in vals))
+    return rows
+
+
+def test_device_fold_equals_reference_simlut(probe):
+    for t, a, b, code in probe["fold"]:
+        # fold step val = simLUT(type, val=a, r=b) of the coalesced overload
+        want = R.LUT2[t][b * 4 + a] if t in (R.AND, R.NAND, R.OR, R.NOR) else 0
+        assert code == want, (t, a, b)
+
+
+def test_device_not_equals_reference(probe):
+    for a, code in probe["not"]:
+        assert code == R.NOT_LUT[a]
+
+
+def test_device_sens_equals_reference(probe):
+    for mode, t, on, off, s in probe["sens"]:
+        want = (R.SENS[mode][t - 2] >> (on * 4 + off)) & 1 if 2 <= t <= 7 else 0
+        assert s == want, (mode, t, on, off)
