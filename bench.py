@@ -107,10 +107,18 @@ class ClockSampler:
 
 
 def gpu_id_for_smi(torch, dev: int) -> str:
+    """nvidia-smi index of CUDA device `dev`, matched by PCI bus/device id."""
     try:
-        bus = torch.cuda.get_device_properties(dev).pci_bus_id
-        if bus:
-            return str(bus)
+        pr = torch.cuda.get_device_properties(dev)
+        want = (int(pr.pci_domain_id), int(pr.pci_bus_id), int(pr.pci_device_id))
+        out = subprocess.run(["nvidia-smi", "--query-gpu=index,pci.bus_id", "--format=csv,noheader"],
+                             capture_output=True, text=True, timeout=20).stdout
+        for ln in out.splitlines():
+            idx, bus = [x.strip() for x in ln.split(",")]
+            dom, b, rest = bus.split(":")
+            d = rest.split(".")[0]
+            if (int(dom, 16), int(b, 16), int(d, 16)) == want:
+                return idx
     except Exception:
         pass
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")

@@ -59,21 +59,17 @@ __device__ __forceinline__ void bitmap_set_aggregated(uint32_t *bm, uint32_t g) 
 // Prune (markkernel.cuh:271-293) and, when fused, merge
 // (mergekernel.cuh:116-198), levels descending, only over gates whose mark in
 // this column block is nonzero.
+// Returns the highest level holding a surviving mark, plus one (0 = none).
 template <int BW, int MODE>
-__device__ __forceinline__ void prune_merge(const FwdArgs &a, uint32_t *nzb, uint32_t w0,
-                                            uint32_t *s_maxlvl) {
+__device__ __forceinline__ uint32_t prune_merge(const FwdArgs &a, uint32_t *nzb, uint32_t w0, uint32_t top) {
     const uint32_t *edges = a.c.edges;
-    for (int l = (int)a.c.n_levels - 1; l >= 0; l--) {
+    uint32_t maxlvl = 0;
+    for (int l = (int)top - 1; l >= 0; l--) {
         const uint32_t s = a.c.level_off[l], e = a.c.level_off[l + 1];
-        if (e == s) continue;
-        const uint32_t q0 = s >> 5, q1 = (e - 1) >> 5;
-        for (uint32_t q = q0 + threadIdx.x; q <= q1; q += blockDim.x) {
-            uint32_t bits = nzb[q];
-            if (q == q0) bits &= 0xFFFFFFFFu << (s & 31);
-            if (q == q1) bits &= 0xFFFFFFFFu >> (31 - ((e - 1) & 31));
-            while (bits) {
-                const uint32_t g = q * 32 + (__ffs(bits) - 1);
-                bits &= bits - 1;
+        bool lvl_any = false;
+        for (uint32_t g = s + threadIdx.x; g < e; g += blockDim.x) {
+            {
+                if (!((nzb[g >> 5] >> (g & 31)) & 1u)) continue;
                 const GateRec r = load_rec(a.c.rec + g);
                 uint32_t mk[BW], keep[BW];
 #pragma unroll
@@ -103,7 +99,7 @@ __device__ __forceinline__ void prune_merge(const FwdArgs &a, uint32_t *nzb, uin
                     atomicAnd(nzb + (g >> 5), ~(1u << (g & 31)));
                     continue;
                 }
-                atomicMax(s_maxlvl, (uint32_t)l + 1);
+                lvl_any = true;
                 if (MODE == FWD_FUSED) {
                     uint32_t cx = kEmpty, cy = kEmpty;
 #pragma unroll
@@ -125,8 +121,9 @@ __device__ __forceinline__ void prune_merge(const FwdArgs &a, uint32_t *nzb, uin
                 }
             }
         }
-        __syncthreads();
+        if (__syncthreads_or(lvl_any) && maxlvl == 0) maxlvl = (uint32_t)l + 1;
     }
+    return maxlvl;
 }
 
 // ---------------------------------------------------------------------------
@@ -142,7 +139,6 @@ __device__ __forceinline__ void prune_merge(const FwdArgs &a, uint32_t *nzb, uin
 template <int BW, int ROBUST, int MODE>
 __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
     extern __shared__ uint32_t sm[];
-    __shared__ uint32_t s_maxlvl;
     const uint32_t R = a.ring_gates, Rm = R - 1;
     uint32_t *rV = sm, *rT = sm + (size_t)R * BW, *rM = sm + 2 * (size_t)R * BW;
     const uint32_t blk = blockIdx.x;
@@ -153,13 +149,14 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
 
     if (MODE != FWD_SIM) {
         for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) nzb[q] = 0;
-        if (threadIdx.x == 0) s_maxlvl = 0;
         __syncthreads();
     }
 
+    uint32_t fwd_top = 0;  // highest level holding a forward mark, plus one
     for (uint32_t l = 0; l < a.c.n_levels; l++) {
         const uint32_t s = a.c.level_off[l], e = a.c.level_off[l + 1];
         const uint32_t ring_lo = R ? (e > R ? e - R : 0) : e;
+        bool lvl_any = false;
         const uint32_t ntask = (e - s) * BW;
         for (uint32_t k = threadIdx.x; k < ntask; k += blockDim.x) {
             const uint32_t g = s + k / BW, j = k % BW, w = w0 + j;
@@ -248,13 +245,16 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
                 rT[slot] = T;
                 rM[slot] = M;
             }
-            if (MODE != FWD_SIM && M) bitmap_set_aggregated(nzb, g);
+            if (MODE != FWD_SIM && M) {
+                bitmap_set_aggregated(nzb, g);
+                lvl_any = true;
+            }
         }
-        __syncthreads();
+        if (__syncthreads_or(lvl_any)) fwd_top = l + 1;
     }
     if (MODE == FWD_SIM) return;
-    prune_merge<BW, MODE>(a, nzb, w0, &s_maxlvl);
-    if (threadIdx.x == 0) a.blk_maxlvl[blk] = s_maxlvl;
+    const uint32_t maxlvl = prune_merge<BW, MODE>(a, nzb, w0, fwd_top);
+    if (threadIdx.x == 0) a.blk_maxlvl[blk] = maxlvl;
 }
 
 // ---------------------------------------------------------------------------
