@@ -28,6 +28,12 @@ namespace {
         }                                               \
     } while (0)
 
+pdf_status err_status(unsigned int err) {
+    if (err & kErrHashFull) return PDF_ENOMEM;
+    if (err & kErrTimeout) return PDF_ETIMEOUT;
+    return PDF_OK;
+}
+
 void set_msg(char *msg, size_t len, const char *fmt, unsigned long long a = 0,
              unsigned long long b = 0) {
     if (msg && len) std::snprintf(msg, len, fmt, a, b);
@@ -90,9 +96,11 @@ struct pdf_circuit {
     int device = 0;
     int mark_mode = PDF_MARK_DEFAULT;
     pdf_circuit_info info{};
-    DevBuf rec, edges, level_off;
+    DevBuf rec, edges, level_off, pieces, err;
     DevCircuit dc{};
-    uint32_t bw = 4, threads = 512, ring = 0;
+    uint32_t bw = 4, threads = 512, ring = 0, ring2 = 0;
+    uint32_t cap = 512, ecap = 2048, n_pieces = 0, bm_shared = 0;
+    uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
     size_t fwd_smem = 0;
     uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
     Workspace stage;  // scratch of the stage calls
@@ -283,34 +291,122 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     for (uint32_t l = 0; l < L; l++)
         inf.max_level_width = std::max(inf.max_level_width, nl->level_offsets[l + 1] - nl->level_offsets[l]);
 
+    // Canonical edge array: each gate's fan-ins then fan-outs, gates in id
+    // order, so that a run of gates owns one contiguous slice (staged into
+    // shared memory by a bulk copy).  Padded so 16-byte rounding stays inside.
+    std::vector<uint32_t> edges;
+    std::vector<uint64_t> eoff(G + 1);
+    edges.reserve(nl->n_edges + 8);
+    for (uint32_t g = 0; g < G; g++) {
+        eoff[g] = edges.size();
+        const uint32_t *e = nl->edges + nl->edge_offset[g];
+        edges.insert(edges.end(), e, e + nl->nfi[g] + nl->nfo[g]);
+    }
+    eoff[G] = edges.size();
+    while (edges.size() % 4) edges.push_back(0);
+    for (int i = 0; i < 4; i++) edges.push_back(0);
+
     std::vector<GateRec> recs(G);
     for (uint32_t g = 0; g < G; g++) {
         GateRec &r = recs[g];
         std::memset(&r, 0, sizeof r);
-        r.w[0] = (uint32_t)nl->type[g] | ((uint32_t)(nl->po[g] ? 1 : 0) << 4) | (nl->nfi[g] << 8);
+        r.w[0] = make_rec_header(nl->type[g], nl->po[g], nl->nfi[g]);
         r.w[1] = nl->nfo[g];
-        r.w[2] = (uint32_t)nl->edge_offset[g];
-        for (uint32_t j = 0; j < nl->nfi[g] && j < (uint32_t)kInlineFanins; j++)
-            r.w[3 + j] = nl->edges[nl->edge_offset[g] + j];
+        r.w[2] = (uint32_t)eoff[g];
+        for (uint32_t j = 0; j < nl->nfi[g] && j < (uint32_t)kInlineFanins; j++) r.w[3 + j] = edges[eoff[g] + j];
     }
-    auto fail = [&](pdf_status s) {
+
+    // Launch plan: CTAs of `threads` threads own `bw` words of pairs; two
+    // CTAs per SM share its shared memory.
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess) {
+        delete c;
+        return PDF_ECUDA;
+    }
+    c->bw = o.tile_words ? o.tile_words : 4;
+    c->threads = o.threads ? o.threads : 512;
+    const size_t budget = std::min<size_t>(prop.sharedMemPerBlockOptin, prop.sharedMemPerMultiprocessor / 2 - 2048);
+    auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
+    const uint32_t bm_words = (G + 31) / 32;
+    c->cap = std::min<uint32_t>(512, (inf.max_level_width + 7) & ~7u);
+    c->ecap = 2048;
+    // pieces: runs of one level, <= cap gates, edge slice <= ecap words
+    std::vector<Piece> pieces;
+    auto f4 = [](uint64_t x) { return x & ~(uint64_t)3; };
+    auto c4 = [](uint64_t x) { return (x + 3) & ~(uint64_t)3; };
+    for (uint32_t l = 0; l < L; l++) {
+        const uint32_t s0 = nl->level_offsets[l], e0 = nl->level_offsets[l + 1];
+        for (uint32_t a = s0; a < e0;) {
+            uint32_t b = a + 1;
+            while (b < e0 && b - a < c->cap && c4(eoff[b + 1]) - f4(eoff[a]) <= c->ecap) b++;
+            Piece p{};
+            p.a = a;
+            p.b = b;
+            p.level = l;
+            if (c4(eoff[b]) - f4(eoff[a]) <= c->ecap) {
+                p.ea = (uint32_t)f4(eoff[a]);
+                p.eb = (uint32_t)c4(eoff[b]);
+            } else {
+                p.ea = p.eb = 0xFFFFFFFFu;  // one gate with a huge edge list: read in place
+            }
+            pieces.push_back(p);
+            a = b;
+        }
+    }
+    c->n_pieces = (uint32_t)pieces.size();
+    if (c->n_pieces > 65536) {
+        delete c;
+        return PDF_ENOTSUP;
+    }
+    size_t off = 0;
+    c->off_rec = (uint32_t)off;
+    off += al(2 * (size_t)c->cap * sizeof(GateRec));
+    c->off_edge = (uint32_t)off;
+    off += al(2 * (size_t)c->ecap * 4);
+    c->bm_shared = (size_t)bm_words * 4 <= 16384 ? 1u : 0u;
+    c->off_bm = (uint32_t)off;
+    if (c->bm_shared) off += al((size_t)bm_words * 4);
+    c->off_pbits = (uint32_t)off;
+    off += al(((size_t)c->n_pieces + 31) / 32 * 4);
+    c->off_mbar = (uint32_t)off;
+    off += 128;
+    c->off_ring = (uint32_t)off;
+    uint32_t ring = 0;
+    if (budget > off)
+        for (uint32_t r = 1; (size_t)r * c->bw * 12 <= budget - off; r *= 2) ring = r;
+    c->ring = ring;
+    uint32_t ring2 = 0;
+    for (uint32_t r = 1; ring && (size_t)r * c->bw * 4 <= (size_t)ring * c->bw * 12; r *= 2) ring2 = r;
+    c->ring2 = ring2;
+    c->fwd_smem = off + (size_t)ring * c->bw * 12;
+    c->hash_cap = 4096;
+    c->cover_threads = 256;
+    c->cover_grid = (uint32_t)prop.multiProcessorCount;
+
+    auto fail = [&](pdf_status st2) {
         c->rec.release();
         c->edges.release();
         c->level_off.release();
+        c->pieces.release();
+        c->err.release();
         delete c;
-        return s;
+        return st2;
     };
     if (c->rec.ensure(sizeof(GateRec) * G) != cudaSuccess ||
-        c->edges.ensure(sizeof(uint32_t) * std::max<uint64_t>(nl->n_edges, 1)) != cudaSuccess ||
-        c->level_off.ensure(sizeof(uint32_t) * (L + 1)) != cudaSuccess) {
+        c->edges.ensure(sizeof(uint32_t) * edges.size()) != cudaSuccess ||
+        c->level_off.ensure(sizeof(uint32_t) * (L + 1)) != cudaSuccess ||
+        c->pieces.ensure(sizeof(Piece) * pieces.size()) != cudaSuccess || c->err.ensure(16) != cudaSuccess) {
         (void)cudaGetLastError();
         return fail(PDF_ENOMEM);
     }
     if (cudaMemcpy(c->rec.p, recs.data(), sizeof(GateRec) * G, cudaMemcpyHostToDevice) != cudaSuccess ||
-        (nl->n_edges && cudaMemcpy(c->edges.p, nl->edges, sizeof(uint32_t) * nl->n_edges,
-                                   cudaMemcpyHostToDevice) != cudaSuccess) ||
-        cudaMemcpy(c->level_off.p, nl->level_offsets, sizeof(uint32_t) * (L + 1),
-                   cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(c->edges.p, edges.data(), sizeof(uint32_t) * edges.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(c->level_off.p, nl->level_offsets, sizeof(uint32_t) * (L + 1), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(c->pieces.p, pieces.data(), sizeof(Piece) * pieces.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemset(c->err.p, 0, 16) != cudaSuccess) {
         (void)cudaGetLastError();
         return fail(PDF_ECUDA);
     }
@@ -320,26 +416,10 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->dc.n_gates = G;
     c->dc.n_levels = L;
     c->dc.n_pi = inf.n_pi;
-
-    // Launch plan.
-    cudaDeviceProp prop{};
-    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess) return fail(PDF_ECUDA);
-    c->bw = o.tile_words ? o.tile_words : 4;
-    c->threads = o.threads ? o.threads : 512;
-    // Two CTAs per SM: each gets just under half of the SM's shared memory.
-    const size_t budget = std::min<size_t>(prop.sharedMemPerBlockOptin, prop.sharedMemPerMultiprocessor / 2 - 2048);
-    uint32_t ring = 1;
-    while ((size_t)ring * 2 * c->bw * 12 <= budget) ring *= 2;
-    if ((size_t)ring * c->bw * 12 > budget) ring = 0;
-    c->ring = ring;
-    c->fwd_smem = forward_smem_bytes(c->bw, ring);
-    c->hash_cap = 4096;
-    c->cover_threads = 256;
-    c->cover_grid = (uint32_t)prop.multiProcessorCount;
     inf.tile_words = c->bw;
     inf.threads = c->threads;
     inf.max_pairs = o.max_pairs ? o.max_pairs : 65536;
-    inf.device_bytes = c->rec.bytes + c->edges.bytes + c->level_off.bytes;
+    inf.device_bytes = c->rec.bytes + c->edges.bytes + c->level_off.bytes + c->pieces.bytes;
     *out = c;
     return PDF_OK;
 }
@@ -351,6 +431,8 @@ extern "C" void pdf_circuit_destroy(pdf_circuit *c) {
     c->rec.release();
     c->edges.release();
     c->level_off.release();
+    c->pieces.release();
+    c->err.release();
     delete c;
 }
 
@@ -470,8 +552,7 @@ extern "C" pdf_status pdf_state_snapshot(pdf_state *s, uint32_t *first_x, uint32
         tot->flags = h.flags;
         tot->reserved = 0;
     }
-    if (h.err) return PDF_ENOMEM;
-    return PDF_OK;
+    return err_status(h.err);
 }
 
 extern "C" pdf_status pdf_state_restore(pdf_state *s, const uint32_t *first_x,
@@ -527,10 +608,23 @@ pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes
 FwdArgs base_fwd(pdf_circuit *c, uint64_t n_pairs) {
     FwdArgs a{};
     a.c = c->dc;
+    a.pieces = c->pieces.as<Piece>();
+    a.n_pieces = c->n_pieces;
+    a.cap = c->cap;
+    a.ecap = c->ecap;
     a.n_pairs = n_pairs;
     a.W = (uint32_t)((n_pairs + 31) / 32);
     a.bm_words = (c->info.n_gates + 31) / 32;
+    a.bm_shared = c->bm_shared;
     a.ring_gates = c->ring;
+    a.ring2_gates = c->ring2;
+    a.off_ring = c->off_ring;
+    a.off_rec = c->off_rec;
+    a.off_edge = c->off_edge;
+    a.off_bm = c->off_bm;
+    a.off_pbits = c->off_pbits;
+    a.off_mbar = c->off_mbar;
+    a.err = c->err.as<uint32_t>();
     return a;
 }
 
@@ -626,6 +720,7 @@ extern "C" pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pa
     a.first_y = s->first_y.as<uint32_t>();
     a.pair_base = (uint32_t)pair_base;
     DevAcc *acc = s->acc.as<DevAcc>();
+    a.err = &acc->err;
     ProfEvents *pe = nullptr;
     if (s->profiling) {
         ProfEvents p{};
@@ -672,8 +767,7 @@ extern "C" pdf_status pdf_grade(pdf_circuit *c, pdf_state *s, const pdf_pairs *p
         batch->flags = h.batch_flags;
         batch->reserved = 0;
     }
-    if (h.err) return PDF_ENOMEM;
-    return PDF_OK;
+    return err_status(h.err);
 }
 
 // ---- stage calls ----------------------------------------------------------
@@ -763,6 +857,8 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
         chunk->flags = h.batch_flags;
         chunk->reserved = 0;
     }
-    if (h.err) return PDF_ENOMEM;
-    return PDF_OK;
+    unsigned int cerr = 0;
+    PDF_CUDA(cudaMemcpy(&cerr, c->err.p, sizeof cerr, cudaMemcpyDeviceToHost));
+    pdf_status st2 = err_status(h.err | cerr);
+    return st2;
 }

@@ -24,7 +24,7 @@
 typedef unsigned __int128 pdf_u128;
 
 // Gate record, 32 bytes, one per gate, built at circuit upload.
-//   w[0] = type | po << 4 | nfi << 8
+//   w[0] = type | po << 4 | nfi << 8 | RF_* flags (bits 16..22) | nfold << 24
 //   w[1] = nfo
 //   w[2] = edge offset: fan-ins at edges[w2 + j], fan-outs at edges[w2 + nfi + k]
 //   w[3..7] = fan-ins 0..4 inline (the rest only in edges[])
@@ -33,9 +33,70 @@ struct __align__(16) GateRec {
 };
 static constexpr int kInlineFanins = 5;
 
+// Per-gate evaluation flags, derived once from (type, nfi) so that the
+// kernels evaluate every gate with the same branch-free instruction sequence
+// (simkernel.cuh:111-149, markkernel.cuh:233-264):
+enum : uint32_t {
+    RF_NOT = 1u << 16,     // fan-in 0 enters inverted (NOT with one fan-in)
+    RF_IM = 1u << 17,      // fold inputs inverted: OR/NOR as AND of complements
+    RF_OM = 1u << 18,      // each fold step inverts its result (NAND, NOR)
+    RF_KILL = 1u << 19,    // the value is S0: a multi-input gate whose fold the
+                           // coalesced simLUT sends to 0 (XOR, XNOR, NOT, others)
+    RF_SENS = 1u << 20,    // the mark needs the side-input test (AND..XNOR, nfi >= 2)
+    RF_MARKF0 = 1u << 21,  // mark = transition & mark of fan-in 0
+    RF_INPT = 1u << 22,    // primary input: mark = transition
+};
+
 PDF_HD uint32_t rec_type(const GateRec &r) { return r.w[0] & 0xFu; }
 PDF_HD uint32_t rec_po(const GateRec &r) { return (r.w[0] >> 4) & 1u; }
 PDF_HD uint32_t rec_nfi(const GateRec &r) { return (r.w[0] >> 8) & 0xFFu; }
+PDF_HD uint32_t hdr_nfold(uint32_t h) { return h >> 24; }
+
+// Header word of a gate (w[0]).
+PDF_HD uint32_t make_rec_header(uint32_t type, uint32_t po, uint32_t nfi) {
+    uint32_t f = 0, nfold = 0;
+    const bool two_input = type >= PDF_AND && type <= PDF_XNOR;
+    const bool copy = type == PDF_BUFF || type == PDF_FROM || type == PDF_DFF;
+    if (type == PDF_INPT) {
+        f |= RF_INPT;
+    } else if (copy) {
+        f |= RF_MARKF0;  // :126-130 copy fan-in 0; mark follows fan-in 0 (:242-246)
+    } else if (nfi >= 2 && !(type >= PDF_AND && type <= PDF_NOR)) {
+        f |= RF_KILL;  // the fold step yields 0 (:89-92)
+        if (type == PDF_NOT || two_input) f |= RF_MARKF0;
+    } else {
+        if (type == PDF_NOT) f |= RF_NOT | RF_MARKF0;
+        if (two_input) f |= RF_MARKF0;
+        if (type == PDF_OR || type == PDF_NOR) f |= RF_IM;
+        if (type == PDF_NAND || type == PDF_NOR) f |= RF_OM;
+        if (two_input && nfi >= 2) f |= RF_SENS;
+        if (type >= PDF_AND && type <= PDF_NOR) nfold = nfi - 1;
+    }
+    return type | (po ? 1u : 0u) << 4 | (nfi & 0xFFu) << 8 | f | nfold << 24;
+}
+
+PDF_HD uint32_t flagmask(uint32_t h, uint32_t f) { return (h & f) ? 0xFFFFFFFFu : 0u; }
+
+// Gate evaluation on bit-planes, tracking the values under both vectors
+// (V = vector 2, v1 = vector 1).  The reference folds the 2-input table left
+// over the fan-ins (simkernel.cuh:142-148); every table is an exact
+// per-vector function, so one step is AND with optional input/output
+// inversion (De Morgan for OR/NOR).  NOT inverts both vectors.
+PDF_HD void eval_first(uint32_t h, uint32_t fV, uint32_t fT, uint32_t &V, uint32_t &v1) {
+    const uint32_t n = flagmask(h, RF_NOT);
+    V = fV ^ n;
+    v1 = fV ^ fT ^ n;
+}
+PDF_HD void eval_fold(uint32_t h, uint32_t &V, uint32_t &v1, uint32_t rV, uint32_t rT) {
+    const uint32_t im = flagmask(h, RF_IM), x = im ^ flagmask(h, RF_OM);
+    V = ((V ^ im) & (rV ^ im)) ^ x;
+    v1 = ((v1 ^ im) & (rV ^ rT ^ im)) ^ x;
+}
+PDF_HD void eval_finish(uint32_t h, uint32_t &V, uint32_t v1, uint32_t &T) {
+    const uint32_t keep = ~flagmask(h, RF_KILL);
+    T = (V ^ v1) & keep;
+    V &= keep;
+}
 
 // Two-input fold step val = OP2(val, r) on bit-planes (simkernel.cuh:146 via
 // the coalesce_t simLUT, :62-95): AND/NAND/OR/NOR evaluate per vector;
@@ -73,25 +134,35 @@ PDF_HD void fold2(uint32_t type, uint32_t &V, uint32_t &T, uint32_t rV, uint32_t
 PDF_HD void not1(uint32_t &V, uint32_t &T) { V = ~V; (void)T; }
 
 // Sensitisation test LUT_16(LUT[type - 2], on, off) (markkernel.cuh:36-41)
-// on 32 (on, off) code pairs at once.  robust selects LUT_R, else LUT_NR.
+// on 32 (on, off) code pairs at once.  ROBUST selects LUT_R, else LUT_NR.
 //   AND/NAND LUT_NR 0x2A00: on=T0 & off in {S1,T1}  |  on=T1 & off=S1
-//   AND/NAND LUT_R  0x2200: off=S1
+//   AND/NAND LUT_R  0x2200: on in {T0,T1} & off=S1
 //   OR/NOR   LUT_NR 0x5100: on=T0 & off=S0  |  on=T1 & off in {S0,T0}
-//   OR/NOR   LUT_R  0x1100: off=S0
+//   OR/NOR   LUT_R  0x1100: on in {T0,T1} & off=S0
 //   XOR/XNOR 0x0000: never
+template <int ROBUST>
+PDF_HD uint32_t sens_class(bool or_like, uint32_t onV, uint32_t onT, uint32_t offV, uint32_t offT) {
+    if (or_like) return ROBUST ? (onT & ~offV & ~offT) : (onT & ~offV & (~offT | onV));
+    return ROBUST ? (onT & offV & ~offT) : (onT & offV & (~onV | ~offT));
+}
 template <int ROBUST>
 PDF_HD uint32_t sens(uint32_t type, uint32_t onV, uint32_t onT, uint32_t offV, uint32_t offT) {
     switch (type) {
         case PDF_AND:
-        case PDF_NAND:
-            return ROBUST ? (onT & offV & ~offT) : (onT & offV & (~onV | ~offT));
+        case PDF_NAND: return sens_class<ROBUST>(false, onV, onT, offV, offT);
         case PDF_OR:
-        case PDF_NOR:
-            return ROBUST ? (onT & ~offV & ~offT) : (onT & ~offV & (~offT | onV));
-        default:
-            return 0;
+        case PDF_NOR: return sens_class<ROBUST>(true, onV, onT, offV, offT);
+        default: return 0;
     }
 }
+
+// A run of gates of one level, the unit of staging and of synchronisation.
+struct __align__(16) Piece {
+    uint32_t a, b;     // gates [a, b)
+    uint32_t ea, eb;   // edge slice [ea, eb) to stage (16-byte aligned), or ea = eb = ~0: not staged
+    uint32_t level;
+    uint32_t pad[3];
+};
 
 // Saturating 128-bit add; sets *ovf on overflow.
 PDF_HD pdf_u128 add_sat(pdf_u128 a, pdf_u128 b, bool &ovf) {

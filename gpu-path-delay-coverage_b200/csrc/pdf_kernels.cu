@@ -56,115 +56,174 @@ __device__ __forceinline__ void bitmap_set_aggregated(uint32_t *bm, uint32_t g) 
     if ((threadIdx.x & 31) == (uint32_t)(__ffs(grp) - 1)) atomicOr(bm + word, bits);
 }
 
-// Prune (markkernel.cuh:271-293) and, when fused, merge
-// (mergekernel.cuh:116-198), levels descending, only over gates whose mark in
-// this column block is nonzero.
-// Returns the highest level holding a surviving mark, plus one (0 = none).
-template <int BW, int MODE>
-__device__ __forceinline__ uint32_t prune_merge(const FwdArgs &a, uint32_t *nzb, uint32_t w0, uint32_t top) {
-    const uint32_t *edges = a.c.edges;
-    uint32_t maxlvl = 0;
-    for (int l = (int)top - 1; l >= 0; l--) {
-        const uint32_t s = a.c.level_off[l], e = a.c.level_off[l + 1];
-        bool lvl_any = false;
-        for (uint32_t g = s + threadIdx.x; g < e; g += blockDim.x) {
-            {
-                if (!((nzb[g >> 5] >> (g & 31)) & 1u)) continue;
-                const GateRec r = load_rec(a.c.rec + g);
-                uint32_t mk[BW], keep[BW];
-#pragma unroll
-                for (int j = 0; j < BW; j++) {
-                    mk[j] = (w0 + j < a.W) ? a.M[(size_t)g * a.ld + w0 + j] : 0u;
-                    keep[j] = rec_po(r) ? 0xFFFFFFFFu : 0u;
-                }
-                if (!rec_po(r)) {
-                    const uint32_t nfo = r.w[1], base = r.w[2] + rec_nfi(r);
-                    for (uint32_t k = 0; k < nfo; k++) {
-                        const uint32_t fo = __ldg(edges + base + k);
-                        if (!((nzb[fo >> 5] >> (fo & 31)) & 1u)) continue;
-#pragma unroll
-                        for (int j = 0; j < BW; j++)
-                            if (w0 + j < a.W) keep[j] |= a.M[(size_t)fo * a.ld + w0 + j];
-                    }
-                }
-                bool any = false;
-#pragma unroll
-                for (int j = 0; j < BW; j++) {
-                    const uint32_t nm = mk[j] & keep[j];
-                    if (nm != mk[j]) a.M[(size_t)g * a.ld + w0 + j] = nm;
-                    mk[j] = nm;
-                    any |= nm != 0;
-                }
-                if (!any) {
-                    atomicAnd(nzb + (g >> 5), ~(1u << (g & 31)));
-                    continue;
-                }
-                lvl_any = true;
-                if (MODE == FWD_FUSED) {
-                    uint32_t cx = kEmpty, cy = kEmpty;
-#pragma unroll
-                    for (int j = 0; j < BW; j++) {
-                        if (!mk[j] || (cx != kEmpty && cy != kEmpty)) continue;
-                        const uint32_t v = a.V[(size_t)g * a.ld + w0 + j];
-                        const uint32_t x = mk[j] & ~v, y = mk[j] & v;
-                        if (cx == kEmpty && x) cx = (w0 + j) * 32 + (__ffs(x) - 1);
-                        if (cy == kEmpty && y) cy = (w0 + j) * 32 + (__ffs(y) - 1);
-                    }
-                    if (cx != kEmpty) {
-                        const uint32_t id = a.pair_base + cx;
-                        if (id < *(volatile uint32_t *)(a.first_x + g)) atomicMin(a.first_x + g, id);
-                    }
-                    if (cy != kEmpty) {
-                        const uint32_t id = a.pair_base + cy;
-                        if (id < *(volatile uint32_t *)(a.first_y + g)) atomicMin(a.first_y + g, id);
-                    }
-                }
-            }
+__device__ __forceinline__ bool bit_test(const uint32_t *bm, uint32_t g) { return (bm[g >> 5] >> (g & 31)) & 1u; }
+
+// ---- TMA bulk copies and mbarriers (inline PTX, sm_90+ / sm_100a) ----
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *m, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes)
+                 : "memory");
+}
+// One untiled bulk copy global -> shared; both addresses 16-byte aligned,
+// bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *m) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(m))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *m, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Every wait is bounded: on expiry the caller reports PDF_ETIMEOUT.
+constexpr uint32_t kSpinLimit = 1u << 24;
+__device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t phase) {
+    for (uint32_t i = 0; i < kSpinLimit; i++)
+        if (mbar_try_wait(m, phase)) return true;
+    return false;
+}
+
+// Shared-memory layout of k_forward (byte offsets from the host plan).
+struct FwdSmem {
+    uint32_t *ring;      // forward: [R][3][BW] (V, T, M); reverse: [R2][BW] pruned marks
+    GateRec *rec;        // [2][cap] staged gate records of a piece
+    uint32_t *edge;      // [2][ecap] staged edge slices (reverse pass)
+    uint32_t *bm;        // nonzero-mark bitmap (shared or global)
+    uint32_t *pbits;     // pieces that hold a forward mark
+    uint64_t *mbar;      // [2]
+};
+
+// Stage piece `p` into buffer `buf`: its gate records and, for the reverse
+// pass, its edge slice.  Called by one thread.
+__device__ __forceinline__ void stage_piece(const FwdArgs &a, const FwdSmem &S, const Piece &p, int buf,
+                                            bool edges) {
+    const uint32_t rb = (p.b - p.a) * (uint32_t)sizeof(GateRec);
+    const bool e = edges && p.ea != 0xFFFFFFFFu;
+    const uint32_t eb = e ? (p.eb - p.ea) * 4u : 0u;
+    fence_proxy_async();
+    mbar_expect_tx(S.mbar + buf, rb + eb);
+    bulk_g2s(S.rec + (size_t)buf * a.cap, a.c.rec + p.a, rb, S.mbar + buf);
+    if (e) bulk_g2s(S.edge + (size_t)buf * a.ecap, a.c.edges + p.ea, eb, S.mbar + buf);
+}
+
+// Rarely needed: OR over on-path candidates i of AND over side inputs x != i
+// of the sensitisation test (markkernel.cuh:253-261 with robust()/
+// nonrobust(), :43-72), restricted to the pairs in `need`.
+template <int ROBUST, class Fetch>
+__device__ __forceinline__ uint32_t sens_any(const GateRec &r, const uint32_t *edges, uint32_t nfi,
+                                          uint32_t need, Fetch fetch) {
+    const bool or_like = (r.w[0] & RF_IM) != 0;
+    uint32_t acc = 0;
+    for (uint32_t i = 0; i < nfi && (need & ~acc); i++) {
+        uint32_t iv, it;
+        fetch(fanin_id(r, edges, i), iv, it);
+        uint32_t term = 0xFFFFFFFFu;
+        for (uint32_t x = 0; x < nfi && term; x++) {
+            if (x == i) continue;
+            uint32_t xv, xt;
+            fetch(fanin_id(r, edges, x), xv, xt);
+            term &= sens_class<ROBUST>(or_like, iv, it, xv, xt);
         }
-        if (__syncthreads_or(lvl_any) && maxlvl == 0) maxlvl = (uint32_t)l + 1;
+        acc |= term;
     }
-    return maxlvl;
+    return acc;
 }
 
 // ---------------------------------------------------------------------------
-// Forward kernel.
+// Forward kernel: one CTA per column block of BW words (32 * BW pairs).
 //
-// Shared memory: a ring of the last R gates' V, T, M words for this CTA's
-// column block (slot = gate & (R - 1)).  While level [s, e) is computed, a
-// fan-in f is read from the ring iff f >= e - R, and only gates g >= e - R
-// write the ring; within that window no two gates share a slot, so every ring
-// read sees its own gate.  Older fan-ins come from the global planes (written
-// by this CTA, ordered by __syncthreads).
+// Gates are walked in pieces (runs of one level, <= cap gates) whose records
+// are staged into shared memory by a TMA bulk copy issued one piece ahead.
+//
+// Forward (sim + forward mark, simkernel.cuh:96-156, markkernel.cuh:215-270):
+// a ring of the last R gates' V, T, M words sits in shared memory
+// (slot = gate & (R - 1)).  During piece [a, b) a fan-in f is read from the
+// ring iff f >= b - R and only gates g >= b - R write it; within that window
+// no two gates share a slot, so a ring read always sees its own gate.  Older
+// fan-ins come from the global planes (written by this CTA and ordered by
+// __syncthreads).
+//
+// Reverse (prune, markkernel.cuh:271-293): only pieces that hold a forward
+// mark, descending, only gates whose bitmap bit is set.  Pruned marks of
+// recent gates sit in a second ring (the same memory, R2 slots of BW words):
+// during piece [a, b) a fan-out fo is read from it iff fo < a + R2 and only
+// gates g < a + R2 write it.
+//
+// Merge (mergekernel.cuh:116-198) needs no level order: one sweep over the
+// surviving marks folds the first falling / rising pair of every net into
+// first_x / first_y with atomicMin.
 // ---------------------------------------------------------------------------
 template <int BW, int ROBUST, int MODE>
 __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
-    extern __shared__ uint32_t sm[];
-    const uint32_t R = a.ring_gates, Rm = R - 1;
-    uint32_t *rV = sm, *rT = sm + (size_t)R * BW, *rM = sm + 2 * (size_t)R * BW;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    FwdSmem S;
+    S.ring = reinterpret_cast<uint32_t *>(smraw + a.off_ring);
+    S.rec = reinterpret_cast<GateRec *>(smraw + a.off_rec);
+    S.edge = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
+    S.pbits = reinterpret_cast<uint32_t *>(smraw + a.off_pbits);
+    S.mbar = reinterpret_cast<uint64_t *>(smraw + a.off_mbar);
     const uint32_t blk = blockIdx.x;
     const uint32_t w0 = blk * BW;
+    S.bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
+    uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
     const uint32_t *edges = a.c.edges;
-    uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
     const uint32_t tailmask = (a.n_pairs & 31) ? ((1u << (a.n_pairs & 31)) - 1u) : 0xFFFFFFFFu;
+    const uint32_t R = a.ring_gates, Rm = R - 1;
+    uint32_t *rV = S.ring, *rT = S.ring + (size_t)R * BW, *rM = S.ring + 2 * (size_t)R * BW;
 
-    if (MODE != FWD_SIM) {
-        for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) nzb[q] = 0;
-        __syncthreads();
+    if (MODE != FWD_SIM)
+        for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) S.bm[q] = 0;
+    for (uint32_t q = threadIdx.x; q < (a.n_pieces + 31) / 32; q += blockDim.x) S.pbits[q] = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(S.mbar, 1);
+        mbar_init(S.mbar + 1, 1);
+        fence_mbar_init();
     }
+    __syncthreads();
 
-    uint32_t fwd_top = 0;  // highest level holding a forward mark, plus one
-    for (uint32_t l = 0; l < a.c.n_levels; l++) {
-        const uint32_t s = a.c.level_off[l], e = a.c.level_off[l + 1];
-        const uint32_t ring_lo = R ? (e > R ? e - R : 0) : e;
-        bool lvl_any = false;
-        const uint32_t ntask = (e - s) * BW;
+    uint32_t phase = 0;  // bit b: parity of the next wait on mbar[b]
+    bool failed = false;
+    // ------------------------------------------------------------- forward
+    if (threadIdx.x == 0) stage_piece(a, S, a.pieces[0], 0, false);
+    for (uint32_t i = 0; i < a.n_pieces; i++) {
+        const Piece P = a.pieces[i];
+        const int buf = i & 1;
+        if (threadIdx.x == 0 && i + 1 < a.n_pieces) stage_piece(a, S, a.pieces[i + 1], buf ^ 1, false);
+        const bool ok = mbar_wait(S.mbar + buf, (phase >> buf) & 1u);
+        phase ^= 1u << buf;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            if (i + 1 < a.n_pieces) (void)mbar_wait(S.mbar + (buf ^ 1), (phase >> (buf ^ 1)) & 1u);
+            break;
+        }
+        const GateRec *recs = S.rec + (size_t)buf * a.cap;
+        const uint32_t ring_lo = R ? (P.b > R ? P.b - R : 0) : P.b;
+        const uint32_t ntask = (P.b - P.a) * BW;
+        bool any = false;
         for (uint32_t k = threadIdx.x; k < ntask; k += blockDim.x) {
-            const uint32_t g = s + k / BW, j = k % BW, w = w0 + j;
+            const uint32_t gi = k / BW, j = k % BW, g = P.a + gi, w = w0 + j;
             if (w >= a.W) continue;
             const uint32_t wmask = (w == a.W - 1) ? tailmask : 0xFFFFFFFFu;
-            const GateRec r = load_rec(a.c.rec + g);
-            const uint32_t type = rec_type(r), nfi = rec_nfi(r);
-            auto fetchVT = [&](uint32_t f, uint32_t &fv, uint32_t &ft) {
+            auto fetch = [&](uint32_t f, uint32_t &fv, uint32_t &ft) {
                 if (f >= ring_lo) {
                     fv = rV[(f & Rm) * BW + j];
                     ft = rT[(f & Rm) * BW + j];
@@ -173,64 +232,51 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
                     ft = a.T[(size_t)f * a.ld + w];
                 }
             };
-            auto fetchM = [&](uint32_t f) -> uint32_t {
-                return f >= ring_lo ? rM[(f & Rm) * BW + j] : a.M[(size_t)f * a.ld + w];
-            };
-            uint32_t V, T;
+            const GateRec &r = recs[gi];
+            const uint32_t h = r.w[0];
+            uint32_t V, T, M = 0;
             if (MODE == FWD_MARK) {
                 V = a.V[(size_t)g * a.ld + w] & wmask;
                 T = a.T[(size_t)g * a.ld + w] & wmask;
-            } else if (type == PDF_INPT) {  // simkernel.cuh:112-125 (pairs already formed)
+            } else if (h & RF_INPT) {  // simkernel.cuh:112-125, pairs already formed
                 V = __ldg(a.pi_v + (size_t)g * a.pi_ld + w) & wmask;
                 T = __ldg(a.pi_t + (size_t)g * a.pi_ld + w) & wmask;
             } else {
-                fetchVT(fanin_id(r, edges, 0), V, T);  // :129, :135
-                if (type != PDF_BUFF && type != PDF_FROM && type != PDF_DFF) {
-                    if (type == PDF_NOT) not1(V, T);  // :136-141
-                    for (uint32_t jj = 1; jj < nfi; jj++) {  // :142-148
-                        uint32_t fv, ft;
-                        fetchVT(fanin_id(r, edges, jj), fv, ft);
-                        fold2(type, V, T, fv, ft);
+                uint32_t fv, ft, v1;
+                fetch(r.w[3], fv, ft);
+                eval_first(h, fv, ft, V, v1);
+                const uint32_t nfold = hdr_nfold(h);
+                if (nfold >= 1) {
+                    fetch(r.w[4], fv, ft);
+                    eval_fold(h, V, v1, fv, ft);
+                    if (nfold >= 2) {
+                        fetch(r.w[5], fv, ft);
+                        eval_fold(h, V, v1, fv, ft);
+                        if (nfold >= 3) {
+                            fetch(r.w[6], fv, ft);
+                            eval_fold(h, V, v1, fv, ft);
+                            if (nfold >= 4) {
+                                fetch(r.w[7], fv, ft);
+                                eval_fold(h, V, v1, fv, ft);
+                                for (uint32_t jj = 5; jj <= nfold; jj++) {
+                                    fetch(__ldg(edges + r.w[2] + jj), fv, ft);
+                                    eval_fold(h, V, v1, fv, ft);
+                                }
+                            }
+                        }
                     }
                 }
+                eval_finish(h, V, v1, T);
                 V &= wmask;
                 T &= wmask;
             }
-            uint32_t M = 0;
             if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
-                switch (type) {
-                    case PDF_INPT: M = T; break;
-                    case PDF_FROM:
-                    case PDF_BUFF:
-                    case PDF_DFF:
-                    case PDF_NOT: M = T ? (T & fetchM(fanin_id(r, edges, 0))) : 0u; break;
-                    case PDF_AND:
-                    case PDF_NAND:
-                    case PDF_OR:
-                    case PDF_NOR:
-                    case PDF_XOR:
-                    case PDF_XNOR: {
-                        uint32_t base = T ? (T & fetchM(fanin_id(r, edges, 0))) : 0u;
-                        if (base && nfi > 1) {
-                            uint32_t acc = 0;
-                            for (uint32_t i = 0; i < nfi && (base & ~acc); i++) {
-                                uint32_t iv, it;
-                                fetchVT(fanin_id(r, edges, i), iv, it);
-                                uint32_t term = 0xFFFFFFFFu;
-                                for (uint32_t x = 0; x < nfi && term; x++) {
-                                    if (x == i) continue;
-                                    uint32_t xv, xt;
-                                    fetchVT(fanin_id(r, edges, x), xv, xt);
-                                    term &= sens<ROBUST>(type, iv, it, xv, xt);
-                                }
-                                acc |= term;
-                            }
-                            base &= acc;
-                        }
-                        M = base;
-                        break;
-                    }
-                    default: break;
+                if (h & RF_INPT) {
+                    M = T;
+                } else if ((h & RF_MARKF0) && T) {
+                    const uint32_t f0 = r.w[3];
+                    M = T & (f0 >= ring_lo ? rM[(f0 & Rm) * BW + j] : a.M[(size_t)f0 * a.ld + w]);
+                    if (M && (h & RF_SENS)) M &= sens_any<ROBUST>(r, edges, rec_nfi(r), M, fetch);
                 }
             }
             const size_t o = (size_t)g * a.ld + w;
@@ -246,14 +292,118 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
                 rM[slot] = M;
             }
             if (MODE != FWD_SIM && M) {
-                bitmap_set_aggregated(nzb, g);
-                lvl_any = true;
+                bitmap_set_aggregated(S.bm, g);
+                any = true;
             }
         }
-        if (__syncthreads_or(lvl_any)) fwd_top = l + 1;
+        if (__syncthreads_or(any) && threadIdx.x == 0) S.pbits[i >> 5] |= 1u << (i & 31);
+    }
+    if (failed) {
+        if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
+        return;
     }
     if (MODE == FWD_SIM) return;
-    const uint32_t maxlvl = prune_merge<BW, MODE>(a, nzb, w0, fwd_top);
+    __syncthreads();
+
+    // ------------------------------------------------------------- reverse
+    const uint32_t R2 = a.ring2_gates, R2m = R2 - 1;
+    uint32_t *ring2 = S.ring;
+    auto prev_marked = [&](int from) -> int {  // highest marked piece index < from
+        for (int q = (from - 1) >> 5; q >= 0 && from > 0; q--) {
+            uint32_t bits = S.pbits[q];
+            if (q == (from - 1) >> 5) bits &= (from & 31) ? ((1u << (from & 31)) - 1u) : 0xFFFFFFFFu;
+            if (bits) return q * 32 + 31 - __clz(bits);
+        }
+        return -1;
+    };
+    int cur = prev_marked((int)a.n_pieces);
+    uint32_t maxlvl = 0;
+    int sbuf = 0;
+    if (cur >= 0 && threadIdx.x == 0) stage_piece(a, S, a.pieces[cur], 0, true);
+    while (cur >= 0) {
+        const int nxt = prev_marked(cur);
+        const Piece P = a.pieces[cur];
+        if (threadIdx.x == 0 && nxt >= 0) stage_piece(a, S, a.pieces[nxt], sbuf ^ 1, true);
+        const bool ok = mbar_wait(S.mbar + sbuf, (phase >> sbuf) & 1u);
+        phase ^= 1u << sbuf;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            if (nxt >= 0) (void)mbar_wait(S.mbar + (sbuf ^ 1), (phase >> (sbuf ^ 1)) & 1u);
+            break;
+        }
+        const GateRec *recs = S.rec + (size_t)sbuf * a.cap;
+        const uint32_t *es = S.edge + (size_t)sbuf * a.ecap;
+        const bool staged = P.ea != 0xFFFFFFFFu;
+        const uint32_t win = P.a + R2;  // fan-outs below this are in ring2
+        bool any = false;
+        for (uint32_t gi = threadIdx.x; gi < P.b - P.a; gi += blockDim.x) {
+            const uint32_t g = P.a + gi;
+            if (!bit_test(S.bm, g)) continue;
+            const GateRec &r = recs[gi];
+            uint32_t mk[BW], keep[BW];
+#pragma unroll
+            for (int j = 0; j < BW; j++) {
+                mk[j] = (w0 + j < a.W) ? a.M[(size_t)g * a.ld + w0 + j] : 0u;
+                keep[j] = rec_po(r) ? 0xFFFFFFFFu : 0u;
+            }
+            if (!rec_po(r)) {
+                const uint32_t nfo = r.w[1], base = r.w[2] + rec_nfi(r);
+                for (uint32_t k = 0; k < nfo; k++) {
+                    const uint32_t fo = staged ? es[base + k - P.ea] : __ldg(edges + base + k);
+                    if (!bit_test(S.bm, fo)) continue;
+                    if (fo < win) {
+#pragma unroll
+                        for (int j = 0; j < BW; j++) keep[j] |= ring2[(fo & R2m) * BW + j];
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < BW; j++)
+                            if (w0 + j < a.W) keep[j] |= a.M[(size_t)fo * a.ld + w0 + j];
+                    }
+                }
+            }
+            bool nz = false;
+#pragma unroll
+            for (int j = 0; j < BW; j++) {
+                const uint32_t nm = mk[j] & keep[j];
+                if (nm != mk[j]) a.M[(size_t)g * a.ld + w0 + j] = nm;
+                if (g < win) ring2[(g & R2m) * BW + j] = nm;
+                nz |= nm != 0;
+            }
+            if (!nz) atomicAnd(S.bm + (g >> 5), ~(1u << (g & 31)));
+            any |= nz;
+        }
+        if (__syncthreads_or(any) && P.level + 1 > maxlvl) maxlvl = P.level + 1;
+        cur = nxt;
+        sbuf ^= 1;
+    }
+    if (failed) {
+        if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
+        return;
+    }
+
+    // ------------------------------------------------------------- merge
+    const uint32_t gend = a.c.level_off[maxlvl];
+    if (MODE == FWD_FUSED) {
+        for (uint32_t g = threadIdx.x; g < gend; g += blockDim.x) {
+            if (!bit_test(S.bm, g)) continue;
+            uint32_t cx = kEmpty, cy = kEmpty;
+#pragma unroll
+            for (int j = 0; j < BW; j++) {
+                if (w0 + j >= a.W || (cx != kEmpty && cy != kEmpty)) continue;
+                const uint32_t m = a.M[(size_t)g * a.ld + w0 + j];
+                if (!m) continue;
+                const uint32_t v = a.V[(size_t)g * a.ld + w0 + j];
+                const uint32_t x = m & ~v, y = m & v;
+                if (cx == kEmpty && x) cx = (w0 + j) * 32 + (__ffs(x) - 1);
+                if (cy == kEmpty && y) cy = (w0 + j) * 32 + (__ffs(y) - 1);
+            }
+            if (cx != kEmpty) atomicMin(a.first_x + g, a.pair_base + cx);
+            if (cy != kEmpty) atomicMin(a.first_y + g, a.pair_base + cy);
+        }
+    }
+    // publish the bitmap of surviving marks for the cover kernels
+    if (a.bm_shared && gbm)
+        for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) gbm[q] = S.bm[q];
     if (threadIdx.x == 0) a.blk_maxlvl[blk] = maxlvl;
 }
 
@@ -334,7 +484,7 @@ __device__ void atomic_add_u128(unsigned long long *lo, unsigned long long *hi, 
 // shared-memory open-addressing table keyed by net id.  Level-0 INPT c values
 // are summed into the batch count (kernSumSingle, coverkernel.cuh:77-105).
 __global__ void __launch_bounds__(512) k_cover(const CoverArgs a) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+    extern __shared__ __align__(128) unsigned char smraw[];
     const uint32_t cap = a.hash_cap, cmask = cap - 1;
     pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw);
     pdf_u128 *cv = hv + cap;
@@ -403,7 +553,7 @@ __global__ void __launch_bounds__(512) k_cover(const CoverArgs a) {
                                 sl = (sl + 1) & cmask;
                             }
                             if (probe == cap) {
-                                atomicOr(&a.acc->err, 1u);  // table full
+                                atomicOr(&a.acc->err, kErrHashFull);  // table full
                             } else {
                                 hv[sl] = h;
                                 cv[sl] = c;
@@ -510,6 +660,7 @@ cudaError_t launch_fwd_t(const FwdArgs &a, uint32_t threads, size_t smem, cudaSt
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const uint32_t blocks = (a.W + BW - 1) / BW;
+    if (blocks == 0 || a.n_pieces == 0) return cudaErrorInvalidValue;
     kern<<<blocks, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
@@ -533,9 +684,6 @@ cudaError_t launch_fwd_bw(const FwdArgs &a, int mode, int robust, uint32_t threa
 
 }  // namespace
 
-size_t forward_smem_bytes(uint32_t bw, uint32_t ring_gates) {
-    return (size_t)ring_gates * bw * 3 * sizeof(uint32_t);
-}
 
 cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st) {

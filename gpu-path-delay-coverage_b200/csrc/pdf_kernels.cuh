@@ -24,6 +24,9 @@ enum FwdMode {
 
 struct FwdArgs {
     DevCircuit c;
+    const Piece *pieces;          // level-ordered runs of gates (the staging unit)
+    uint32_t n_pieces;
+    uint32_t cap, ecap;           // gates / edge words per staging buffer
     const uint32_t *pi_v, *pi_t;  // [n_pi][pi_ld]
     uint64_t pi_ld;
     uint32_t *V, *T, *M;          // planes [n_gates][ld]
@@ -31,12 +34,21 @@ struct FwdArgs {
     uint32_t *nzb;                // [n_blocks][bm_words] gates with a nonzero mark
     uint32_t *blk_maxlvl;         // [n_blocks] highest level holding a mark (+1), 0 = none
     uint32_t bm_words;
+    uint32_t bm_shared;           // 1: the bitmap lives in shared memory during the kernel
     uint32_t *first_x, *first_y;  // [n_gates] (FWD_FUSED only)
+    uint32_t *err;                // device error word (PDF_ETIMEOUT on a wait that expired)
     uint64_t n_pairs;
     uint32_t W;                   // ceil(n_pairs / 32)
     uint32_t pair_base;
-    uint32_t ring_gates;          // power of two, or 0 (no ring)
+    uint32_t ring_gates;          // forward ring slots (power of two, or 0)
+    uint32_t ring2_gates;         // reverse ring slots (power of two, or 0)
+    // shared-memory byte offsets
+    uint32_t off_ring, off_rec, off_edge, off_bm, off_pbits, off_mbar;
 };
+
+// Device error bits (DevAcc::err and the circuit's error word).
+constexpr unsigned int kErrTimeout = 0x4u;     // a bounded wait expired (PDF_ETIMEOUT)
+constexpr unsigned int kErrHashFull = 0x100u;  // a pair marked more nets than the cover table holds
 
 // Batch accumulators kept in device memory by a pdf_state.
 struct DevAcc {
@@ -70,7 +82,6 @@ struct CoverArgs {
 // Host-side launchers (pdf_kernels.cu).  All return cudaError_t of the launch.
 cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st);
-size_t forward_smem_bytes(uint32_t bw, uint32_t ring_gates);
 cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st);
 size_t cover_smem_bytes(uint32_t hash_cap);
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M,

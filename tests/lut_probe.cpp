@@ -24,5 +24,25 @@ int main() {
         not1(V, T);
         std::printf("not %u %u\n", a, (V & 1) | ((T & 1) << 1));
     }
+    // Header-driven gate evaluation (what the kernels run) for every type,
+    // fan-in count 1..3 and input codes.
+    for (uint32_t type = 0; type < PDF_NTYPES; type++) {
+        if (type == PDF_INPT) continue;
+        for (uint32_t nfi = 1; nfi <= 3; nfi++) {
+            const uint32_t h = make_rec_header(type, 0, nfi);
+            std::printf("flags %u %u %u %u %u\n", type, nfi, (h & RF_MARKF0) ? 1 : 0, (h & RF_INPT) ? 1 : 0,
+                        (h & RF_SENS) ? 1 : 0);
+            const uint32_t combos = 1u << (2 * nfi);
+            for (uint32_t cmb = 0; cmb < combos; cmb++) {
+                uint32_t c[3] = {cmb & 3, (cmb >> 2) & 3, (cmb >> 4) & 3};
+                uint32_t V, v1, T;
+                eval_first(h, (c[0] & 1) << 7, (c[0] >> 1) << 7, V, v1);
+                for (uint32_t j = 1; j <= hdr_nfold(h); j++) eval_fold(h, V, v1, (c[j] & 1) << 7, (c[j] >> 1) << 7);
+                eval_finish(h, V, v1, T);
+                const uint32_t code = ((V >> 7) & 1) | (((T >> 7) & 1) << 1);
+                std::printf("gate %u %u %u %u %u %u\n", type, nfi, c[0], c[1], c[2], code);
+            }
+        }
+    }
     return 0;
 }

@@ -97,3 +97,35 @@ def test_device_sens_equals_reference(probe):
     for mode, t, on, off, s in probe["sens"]:
         want = (R.SENS[mode][t - 2] >> (on * 4 + off)) & 1 if 2 <= t <= 7 else 0
         assert s == want, (mode, t, on, off)
+
+
+def _ref_gate(t, codes):
+    """Value of one gate under the reference's kernSimulateP1 (simkernel.cuh:111-149)."""
+    if t in (R.BUFF, R.FROM, R.DFF):
+        return codes[0]
+    v = codes[0]
+    if t == R.NOT:
+        v = R.NOT_LUT[v]
+    for c in codes[1:]:
+        v = R.LUT2[t][c * 4 + v] if t in (R.AND, R.NAND, R.OR, R.NOR) else 0
+    return v
+
+
+def test_device_gate_evaluation_equals_reference(probe):
+    seen = 0
+    for t, nfi, c0, c1, c2, code in probe["gate"]:
+        assert code == _ref_gate(t, [c0, c1, c2][:nfi]), (t, nfi, c0, c1, c2)
+        seen += 1
+    assert seen == 11 * (4 + 16 + 64)
+
+
+def test_device_mark_flags_equal_reference(probe):
+    # markkernel.cuh:233-264: INPT marks on a transition; FROM/BUFF/DFF/NOT and
+    # AND..XNOR follow fan-in 0; the side-input test only matters with >= 2 inputs
+    for t, nfi, markf0, inpt, sens in probe["flags"]:
+        assert inpt == 0
+        assert markf0 == int(t in (R.FROM, R.BUFF, R.DFF, R.NOT) or R.AND <= t <= R.XNOR), (t, nfi)
+        if sens:
+            assert R.AND <= t <= R.NOR and nfi >= 2
+        if R.AND <= t <= R.NOR and nfi >= 2:
+            assert sens
