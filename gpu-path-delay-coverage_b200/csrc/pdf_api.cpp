@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -324,7 +325,11 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         return PDF_ECUDA;
     }
     c->bw = o.tile_words ? o.tile_words : 4;
-    c->threads = o.threads ? o.threads : 512;
+    // one thread per gate of a piece; 8-word tiles need twice the registers
+    const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
+    const uint32_t cap_guess = std::min<uint32_t>(512, (inf.max_level_width + 7) & ~7u);
+    c->threads = o.threads ? std::min(o.threads, max_threads)
+                           : std::min(max_threads, std::max<uint32_t>(128, (cap_guess + 31) & ~31u));
     const size_t budget = std::min<size_t>(prop.sharedMemPerBlockOptin, prop.sharedMemPerMultiprocessor / 2 - 2048);
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
@@ -651,22 +656,37 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
 }
 
 // Device pointers of the pairs (staging host pairs through the workspace).
+// True when (ptr, ld) can be used by the kernels directly: rows of ld words,
+// ld a multiple of the tile width, every row long enough for whole tiles, and
+// 16-byte aligned base addresses.
+bool planes_fit(const pdf_circuit *c, uint64_t W, uint64_t ld, std::initializer_list<const void *> ptrs) {
+    const uint64_t Wp = (W + c->bw - 1) / c->bw * c->bw;
+    if (ld < Wp || ld % c->bw) return false;
+    for (const void *p : ptrs)
+        if (!p || (reinterpret_cast<uintptr_t>(p) & 15)) return false;
+    return true;
+}
+
+// Device pointers of the pairs, staging them through the workspace when
+// they are host memory or not in the kernels' layout.
 pdf_status stage_pairs(pdf_circuit *c, Workspace &ws, const pdf_pairs *pr, const uint32_t **v,
                        const uint32_t **t, uint64_t *ld, cudaStream_t st) {
-    if (pr->on_device) {
+    const uint64_t W = (pr->n_pairs + 31) / 32, npi = c->info.n_pi;
+    if (pr->on_device && planes_fit(c, W, pr->ld, {pr->v, pr->t})) {
         *v = pr->v;
         *t = pr->t;
         *ld = pr->ld;
         return PDF_OK;
     }
-    const uint64_t W = (pr->n_pairs + 31) / 32, npi = c->info.n_pi;
-    PDF_CUDA(ws.pi.ensure(2 * npi * W * 4));
-    uint32_t *dv = ws.pi.as<uint32_t>(), *dt = dv + npi * W;
-    PDF_CUDA(cudaMemcpy2DAsync(dv, W * 4, pr->v, pr->ld * 4, W * 4, npi, cudaMemcpyHostToDevice, st));
-    PDF_CUDA(cudaMemcpy2DAsync(dt, W * 4, pr->t, pr->ld * 4, W * 4, npi, cudaMemcpyHostToDevice, st));
+    const uint64_t Wp = (W + c->bw - 1) / c->bw * c->bw;
+    PDF_CUDA(ws.pi.ensure(2 * npi * Wp * 4));
+    uint32_t *dv = ws.pi.as<uint32_t>(), *dt = dv + npi * Wp;
+    const cudaMemcpyKind k = pr->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    PDF_CUDA(cudaMemcpy2DAsync(dv, Wp * 4, pr->v, pr->ld * 4, W * 4, npi, k, st));
+    PDF_CUDA(cudaMemcpy2DAsync(dt, Wp * 4, pr->t, pr->ld * 4, W * 4, npi, k, st));
     *v = dv;
     *t = dt;
-    *ld = W;
+    *ld = Wp;
     return PDF_OK;
 }
 
@@ -691,7 +711,7 @@ extern "C" pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pa
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
     std::lock_guard<std::mutex> lk(s->mu);
     const uint64_t n = pr->n_pairs, W = (n + 31) / 32, G = c->info.n_gates;
-    const bool direct = out && out->on_device && out->sim_v && out->sim_t && out->mark && out->ld >= W;
+    const bool direct = out && out->on_device && planes_fit(c, W, out->ld, {out->sim_v, out->sim_t, out->mark});
     st = ensure_ws(c, s->ws, W, !direct);
     if (st != PDF_OK) return st;
     const uint32_t *pv, *pt;
@@ -777,10 +797,14 @@ extern "C" pdf_status pdf_sim(pdf_circuit *c, const pdf_pairs *pr, uint32_t *sim
     if (!c || !sim_v || !sim_t) return PDF_EINVAL;
     pdf_status st = check_pairs(c, pr, 0);
     if (st != PDF_OK) return st;
-    if (ld < (pr->n_pairs + 31) / 32) return PDF_EINVAL;
+    const uint64_t W = (pr->n_pairs + 31) / 32, G = c->info.n_gates;
+    if (ld < W) return PDF_EINVAL;
     DeviceGuard dg(c->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
     std::lock_guard<std::mutex> lk(c->mu);
+    const bool direct = planes_fit(c, W, ld, {sim_v, sim_t});
+    st = ensure_ws(c, c->stage, W, !direct);
+    if (st != PDF_OK) return st;
     const uint32_t *pv, *pt;
     uint64_t pld;
     st = stage_pairs(c, c->stage, pr, &pv, &pt, &pld, cs);
@@ -789,11 +813,21 @@ extern "C" pdf_status pdf_sim(pdf_circuit *c, const pdf_pairs *pr, uint32_t *sim
     a.pi_v = pv;
     a.pi_t = pt;
     a.pi_ld = pld;
-    a.V = sim_v;
-    a.T = sim_t;
-    a.ld = ld;
+    if (direct) {
+        a.V = sim_v;
+        a.T = sim_t;
+        a.ld = ld;
+    } else {
+        a.ld = c->stage.plane_ld;
+        a.V = c->stage.planes.as<uint32_t>();
+        a.T = a.V + G * a.ld;
+    }
     PDF_CUDA(launch_forward(a, FWD_SIM, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
-    if (!pr->on_device) PDF_CUDA(cudaStreamSynchronize(cs));  // staging buffer reuse
+    if (!direct) {
+        PDF_CUDA(cudaMemcpy2DAsync(sim_v, ld * 4, a.V, a.ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
+        PDF_CUDA(cudaMemcpy2DAsync(sim_t, ld * 4, a.T, a.ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
+    }
+    PDF_CUDA(cudaStreamSynchronize(cs));  // the stage scratch is reused by the next stage call
     return PDF_OK;
 }
 
@@ -803,17 +837,30 @@ extern "C" pdf_status pdf_mark(pdf_circuit *c, const uint32_t *sim_v, const uint
     DeviceGuard dg(c->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
     std::lock_guard<std::mutex> lk(c->mu);
-    const uint64_t W = (n_pairs + 31) / 32;
-    pdf_status st = ensure_ws(c, c->stage, W, false);
+    const uint64_t W = (n_pairs + 31) / 32, G = c->info.n_gates;
+    const bool direct = planes_fit(c, W, ld, {sim_v, sim_t, mark});
+    pdf_status st = ensure_ws(c, c->stage, W, !direct);
     if (st != PDF_OK) return st;
     FwdArgs a = base_fwd(c, n_pairs);
-    a.V = const_cast<uint32_t *>(sim_v);
-    a.T = const_cast<uint32_t *>(sim_t);
-    a.M = mark;
-    a.ld = ld;
+    if (direct) {
+        a.V = const_cast<uint32_t *>(sim_v);
+        a.T = const_cast<uint32_t *>(sim_t);
+        a.M = mark;
+        a.ld = ld;
+    } else {
+        a.ld = c->stage.plane_ld;
+        a.V = c->stage.planes.as<uint32_t>();
+        a.T = a.V + G * a.ld;
+        a.M = a.T + G * a.ld;
+        PDF_CUDA(cudaMemcpy2DAsync(a.V, a.ld * 4, sim_v, ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
+        PDF_CUDA(cudaMemcpy2DAsync(a.T, a.ld * 4, sim_t, ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
+    }
     a.nzb = c->stage.nzb.as<uint32_t>();
     a.blk_maxlvl = c->stage.maxlvl.as<uint32_t>();
     PDF_CUDA(launch_forward(a, FWD_MARK, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
+    if (!direct)
+        PDF_CUDA(cudaMemcpy2DAsync(mark, ld * 4, a.M, a.ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
+    PDF_CUDA(cudaStreamSynchronize(cs));
     return PDF_OK;
 }
 

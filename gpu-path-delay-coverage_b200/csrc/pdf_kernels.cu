@@ -125,31 +125,110 @@ __device__ __forceinline__ void stage_piece(const FwdArgs &a, const FwdSmem &S, 
     if (e) bulk_g2s(S.edge + (size_t)buf * a.ecap, a.c.edges + p.ea, eb, S.mbar + buf);
 }
 
+// BW consecutive words of one plane row, moved with 16-byte (or 8-byte)
+// vector accesses.  Every address passed here is a multiple of BW words.
+template <int BW>
+struct Vec {
+    uint32_t x[BW];
+};
+template <int BW>
+__device__ __forceinline__ Vec<BW> vld(const uint32_t *p) {
+    Vec<BW> v;
+    if constexpr (BW == 1) {
+        v.x[0] = *p;
+    } else if constexpr (BW == 2) {
+        const uint2 q = *reinterpret_cast<const uint2 *>(p);
+        v.x[0] = q.x;
+        v.x[1] = q.y;
+    } else {
+#pragma unroll
+        for (int i = 0; i < BW; i += 4) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(p + i);
+            v.x[i] = q.x;
+            v.x[i + 1] = q.y;
+            v.x[i + 2] = q.z;
+            v.x[i + 3] = q.w;
+        }
+    }
+    return v;
+}
+template <int BW>
+__device__ __forceinline__ Vec<BW> vldg(const uint32_t *p) {  // read-only data (pairs)
+    Vec<BW> v;
+    if constexpr (BW == 1) {
+        v.x[0] = __ldg(p);
+    } else if constexpr (BW == 2) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2 *>(p));
+        v.x[0] = q.x;
+        v.x[1] = q.y;
+    } else {
+#pragma unroll
+        for (int i = 0; i < BW; i += 4) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p + i));
+            v.x[i] = q.x;
+            v.x[i + 1] = q.y;
+            v.x[i + 2] = q.z;
+            v.x[i + 3] = q.w;
+        }
+    }
+    return v;
+}
+template <int BW>
+__device__ __forceinline__ void vst(uint32_t *p, const Vec<BW> &v) {
+    if constexpr (BW == 1) {
+        *p = v.x[0];
+    } else if constexpr (BW == 2) {
+        *reinterpret_cast<uint2 *>(p) = make_uint2(v.x[0], v.x[1]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < BW; i += 4)
+            *reinterpret_cast<uint4 *>(p + i) = make_uint4(v.x[i], v.x[i + 1], v.x[i + 2], v.x[i + 3]);
+    }
+}
+template <int BW>
+__device__ __forceinline__ bool vany(const Vec<BW> &v) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int i = 0; i < BW; i++) o |= v.x[i];
+    return o != 0;
+}
+
 // Rarely needed: OR over on-path candidates i of AND over side inputs x != i
 // of the sensitisation test (markkernel.cuh:253-261 with robust()/
 // nonrobust(), :43-72), restricted to the pairs in `need`.
-template <int ROBUST, class Fetch>
-__device__ __forceinline__ uint32_t sens_any(const GateRec &r, const uint32_t *edges, uint32_t nfi,
-                                          uint32_t need, Fetch fetch) {
+template <int BW, int ROBUST, class Fetch>
+__device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, const uint32_t *edges, uint32_t nfi,
+                                            const Vec<BW> &need, Fetch fetch) {
     const bool or_like = (r.w[0] & RF_IM) != 0;
-    uint32_t acc = 0;
-    for (uint32_t i = 0; i < nfi && (need & ~acc); i++) {
-        uint32_t iv, it;
+    Vec<BW> acc;
+#pragma unroll
+    for (int j = 0; j < BW; j++) acc.x[j] = 0;
+    for (uint32_t i = 0; i < nfi; i++) {
+        uint32_t left = 0;
+#pragma unroll
+        for (int j = 0; j < BW; j++) left |= need.x[j] & ~acc.x[j];
+        if (!left) break;
+        Vec<BW> iv, it;
         fetch(fanin_id(r, edges, i), iv, it);
-        uint32_t term = 0xFFFFFFFFu;
-        for (uint32_t x = 0; x < nfi && term; x++) {
+        Vec<BW> term;
+#pragma unroll
+        for (int j = 0; j < BW; j++) term.x[j] = 0xFFFFFFFFu;
+        for (uint32_t x = 0; x < nfi; x++) {
             if (x == i) continue;
-            uint32_t xv, xt;
+            Vec<BW> xv, xt;
             fetch(fanin_id(r, edges, x), xv, xt);
-            term &= sens_class<ROBUST>(or_like, iv, it, xv, xt);
+#pragma unroll
+            for (int j = 0; j < BW; j++) term.x[j] &= sens_class<ROBUST>(or_like, iv.x[j], it.x[j], xv.x[j], xt.x[j]);
         }
-        acc |= term;
+#pragma unroll
+        for (int j = 0; j < BW; j++) acc.x[j] |= term.x[j];
     }
     return acc;
 }
 
 // ---------------------------------------------------------------------------
-// Forward kernel: one CTA per column block of BW words (32 * BW pairs).
+// Forward kernel: one CTA per column block of BW words (32 * BW pairs); one
+// thread per gate, carrying all BW words of the block.
 //
 // Gates are walked in pieces (runs of one level, <= cap gates) whose records
 // are staged into shared memory by a TMA bulk copy issued one piece ahead.
@@ -171,9 +250,13 @@ __device__ __forceinline__ uint32_t sens_any(const GateRec &r, const uint32_t *e
 // Merge (mergekernel.cuh:116-198) needs no level order: one sweep over the
 // surviving marks folds the first falling / rising pair of every net into
 // first_x / first_y with atomicMin.
+//
+// Plane rows are read and written BW words at a time: ld and pi_ld are
+// multiples of BW and every row holds all n_blocks * BW words; words at or
+// past ceil(n_pairs / 32) are masked to zero.
 // ---------------------------------------------------------------------------
 template <int BW, int ROBUST, int MODE>
-__global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
+__global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     FwdSmem S;
     S.ring = reinterpret_cast<uint32_t *>(smraw + a.off_ring);
@@ -186,9 +269,15 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
     S.bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
     uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
     const uint32_t *edges = a.c.edges;
-    const uint32_t tailmask = (a.n_pairs & 31) ? ((1u << (a.n_pairs & 31)) - 1u) : 0xFFFFFFFFu;
     const uint32_t R = a.ring_gates, Rm = R - 1;
     uint32_t *rV = S.ring, *rT = S.ring + (size_t)R * BW, *rM = S.ring + 2 * (size_t)R * BW;
+    Vec<BW> wm;  // valid bits of each word of this block
+#pragma unroll
+    for (int j = 0; j < BW; j++) {
+        const uint32_t w = w0 + j;
+        wm.x[j] = w + 1 < a.W ? 0xFFFFFFFFu
+                              : (w + 1 == a.W ? ((a.n_pairs & 31) ? (1u << (a.n_pairs & 31)) - 1u : 0xFFFFFFFFu) : 0u);
+    }
 
     if (MODE != FWD_SIM)
         for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) S.bm[q] = 0;
@@ -217,81 +306,86 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
         }
         const GateRec *recs = S.rec + (size_t)buf * a.cap;
         const uint32_t ring_lo = R ? (P.b > R ? P.b - R : 0) : P.b;
-        const uint32_t ntask = (P.b - P.a) * BW;
         bool any = false;
-        for (uint32_t k = threadIdx.x; k < ntask; k += blockDim.x) {
-            const uint32_t gi = k / BW, j = k % BW, g = P.a + gi, w = w0 + j;
-            if (w >= a.W) continue;
-            const uint32_t wmask = (w == a.W - 1) ? tailmask : 0xFFFFFFFFu;
-            auto fetch = [&](uint32_t f, uint32_t &fv, uint32_t &ft) {
+        for (uint32_t gi = threadIdx.x; gi < P.b - P.a; gi += blockDim.x) {
+            const uint32_t g = P.a + gi;
+            auto fetch = [&](uint32_t f, Vec<BW> &fv, Vec<BW> &ft) {
                 if (f >= ring_lo) {
-                    fv = rV[(f & Rm) * BW + j];
-                    ft = rT[(f & Rm) * BW + j];
+                    fv = vld<BW>(rV + (f & Rm) * BW);
+                    ft = vld<BW>(rT + (f & Rm) * BW);
                 } else {
-                    fv = a.V[(size_t)f * a.ld + w];
-                    ft = a.T[(size_t)f * a.ld + w];
+                    fv = vld<BW>(a.V + (size_t)f * a.ld + w0);
+                    ft = vld<BW>(a.T + (size_t)f * a.ld + w0);
                 }
             };
-            const GateRec &r = recs[gi];
+            const GateRec r = recs[gi];
             const uint32_t h = r.w[0];
-            uint32_t V, T, M = 0;
+            Vec<BW> V, T, M;
             if (MODE == FWD_MARK) {
-                V = a.V[(size_t)g * a.ld + w] & wmask;
-                T = a.T[(size_t)g * a.ld + w] & wmask;
-            } else if (h & RF_INPT) {  // simkernel.cuh:112-125, pairs already formed
-                V = __ldg(a.pi_v + (size_t)g * a.pi_ld + w) & wmask;
-                T = __ldg(a.pi_t + (size_t)g * a.pi_ld + w) & wmask;
-            } else {
-                uint32_t fv, ft, v1;
-                fetch(r.w[3], fv, ft);
-                eval_first(h, fv, ft, V, v1);
-                const uint32_t nfold = hdr_nfold(h);
-                if (nfold >= 1) {
-                    fetch(r.w[4], fv, ft);
-                    eval_fold(h, V, v1, fv, ft);
-                    if (nfold >= 2) {
-                        fetch(r.w[5], fv, ft);
-                        eval_fold(h, V, v1, fv, ft);
-                        if (nfold >= 3) {
-                            fetch(r.w[6], fv, ft);
-                            eval_fold(h, V, v1, fv, ft);
-                            if (nfold >= 4) {
-                                fetch(r.w[7], fv, ft);
-                                eval_fold(h, V, v1, fv, ft);
-                                for (uint32_t jj = 5; jj <= nfold; jj++) {
-                                    fetch(__ldg(edges + r.w[2] + jj), fv, ft);
-                                    eval_fold(h, V, v1, fv, ft);
-                                }
-                            }
-                        }
-                    }
+                V = vld<BW>(a.V + (size_t)g * a.ld + w0);
+                T = vld<BW>(a.T + (size_t)g * a.ld + w0);
+#pragma unroll
+                for (int j = 0; j < BW; j++) {
+                    V.x[j] &= wm.x[j];
+                    T.x[j] &= wm.x[j];
                 }
-                eval_finish(h, V, v1, T);
-                V &= wmask;
-                T &= wmask;
+            } else if (h & RF_INPT) {  // simkernel.cuh:112-125, pairs already formed
+                V = vldg<BW>(a.pi_v + (size_t)g * a.pi_ld + w0);
+                T = vldg<BW>(a.pi_t + (size_t)g * a.pi_ld + w0);
+#pragma unroll
+                for (int j = 0; j < BW; j++) {
+                    V.x[j] &= wm.x[j];
+                    T.x[j] &= wm.x[j];
+                }
+            } else {
+                Vec<BW> fv, ft, v1;
+                fetch(r.w[3], fv, ft);
+#pragma unroll
+                for (int j = 0; j < BW; j++) eval_first(h, fv.x[j], ft.x[j], V.x[j], v1.x[j]);
+                const uint32_t nfold = hdr_nfold(h);
+                for (uint32_t jj = 1; jj <= nfold; jj++) {
+                    fetch(fanin_id(r, edges, jj), fv, ft);
+#pragma unroll
+                    for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < BW; j++) {
+                    eval_finish(h, V.x[j], v1.x[j], T.x[j]);
+                    V.x[j] &= wm.x[j];
+                    T.x[j] &= wm.x[j];
+                }
             }
+#pragma unroll
+            for (int j = 0; j < BW; j++) M.x[j] = 0;
             if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
                 if (h & RF_INPT) {
                     M = T;
-                } else if ((h & RF_MARKF0) && T) {
+                } else if ((h & RF_MARKF0) && vany(T)) {
                     const uint32_t f0 = r.w[3];
-                    M = T & (f0 >= ring_lo ? rM[(f0 & Rm) * BW + j] : a.M[(size_t)f0 * a.ld + w]);
-                    if (M && (h & RF_SENS)) M &= sens_any<ROBUST>(r, edges, rec_nfi(r), M, fetch);
+                    const Vec<BW> m0 =
+                        f0 >= ring_lo ? vld<BW>(rM + (f0 & Rm) * BW) : vld<BW>(a.M + (size_t)f0 * a.ld + w0);
+#pragma unroll
+                    for (int j = 0; j < BW; j++) M.x[j] = T.x[j] & m0.x[j];
+                    if ((h & RF_SENS) && vany(M)) {
+                        const Vec<BW> sv = sens_any<BW, ROBUST>(r, edges, rec_nfi(r), M, fetch);
+#pragma unroll
+                        for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
+                    }
                 }
             }
-            const size_t o = (size_t)g * a.ld + w;
+            const size_t o = (size_t)g * a.ld + w0;
             if (MODE != FWD_MARK) {
-                a.V[o] = V;
-                a.T[o] = T;
+                vst<BW>(a.V + o, V);
+                vst<BW>(a.T + o, T);
             }
-            if (MODE != FWD_SIM) a.M[o] = M;
+            if (MODE != FWD_SIM) vst<BW>(a.M + o, M);
             if (g >= ring_lo) {
-                const uint32_t slot = (g & Rm) * BW + j;
-                rV[slot] = V;
-                rT[slot] = T;
-                rM[slot] = M;
+                const uint32_t slot = (g & Rm) * BW;
+                vst<BW>(rV + slot, V);
+                vst<BW>(rT + slot, T);
+                vst<BW>(rM + slot, M);
             }
-            if (MODE != FWD_SIM && M) {
+            if (MODE != FWD_SIM && vany(M)) {
                 bitmap_set_aggregated(S.bm, g);
                 any = true;
             }
@@ -340,35 +434,31 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
             const uint32_t g = P.a + gi;
             if (!bit_test(S.bm, g)) continue;
             const GateRec &r = recs[gi];
-            uint32_t mk[BW], keep[BW];
+            const Vec<BW> mk = vld<BW>(a.M + (size_t)g * a.ld + w0);
+            Vec<BW> keep;
 #pragma unroll
-            for (int j = 0; j < BW; j++) {
-                mk[j] = (w0 + j < a.W) ? a.M[(size_t)g * a.ld + w0 + j] : 0u;
-                keep[j] = rec_po(r) ? 0xFFFFFFFFu : 0u;
-            }
+            for (int j = 0; j < BW; j++) keep.x[j] = rec_po(r) ? 0xFFFFFFFFu : 0u;
             if (!rec_po(r)) {
                 const uint32_t nfo = r.w[1], base = r.w[2] + rec_nfi(r);
                 for (uint32_t k = 0; k < nfo; k++) {
                     const uint32_t fo = staged ? es[base + k - P.ea] : __ldg(edges + base + k);
                     if (!bit_test(S.bm, fo)) continue;
-                    if (fo < win) {
+                    const Vec<BW> fm =
+                        fo < win ? vld<BW>(ring2 + (fo & R2m) * BW) : vld<BW>(a.M + (size_t)fo * a.ld + w0);
 #pragma unroll
-                        for (int j = 0; j < BW; j++) keep[j] |= ring2[(fo & R2m) * BW + j];
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < BW; j++)
-                            if (w0 + j < a.W) keep[j] |= a.M[(size_t)fo * a.ld + w0 + j];
-                    }
+                    for (int j = 0; j < BW; j++) keep.x[j] |= fm.x[j];
                 }
             }
-            bool nz = false;
+            Vec<BW> nm;
+            bool changed = false;
 #pragma unroll
             for (int j = 0; j < BW; j++) {
-                const uint32_t nm = mk[j] & keep[j];
-                if (nm != mk[j]) a.M[(size_t)g * a.ld + w0 + j] = nm;
-                if (g < win) ring2[(g & R2m) * BW + j] = nm;
-                nz |= nm != 0;
+                nm.x[j] = mk.x[j] & keep.x[j];
+                changed |= nm.x[j] != mk.x[j];
             }
+            if (changed) vst<BW>(a.M + (size_t)g * a.ld + w0, nm);
+            if (g < win) vst<BW>(ring2 + (g & R2m) * BW, nm);
+            const bool nz = vany(nm);
             if (!nz) atomicAnd(S.bm + (g >> 5), ~(1u << (g & 31)));
             any |= nz;
         }
@@ -386,16 +476,14 @@ __global__ void __launch_bounds__(1024) k_forward(const FwdArgs a) {
     if (MODE == FWD_FUSED) {
         for (uint32_t g = threadIdx.x; g < gend; g += blockDim.x) {
             if (!bit_test(S.bm, g)) continue;
+            const Vec<BW> m = vld<BW>(a.M + (size_t)g * a.ld + w0);
+            const Vec<BW> v = vld<BW>(a.V + (size_t)g * a.ld + w0);
             uint32_t cx = kEmpty, cy = kEmpty;
 #pragma unroll
-            for (int j = 0; j < BW; j++) {
-                if (w0 + j >= a.W || (cx != kEmpty && cy != kEmpty)) continue;
-                const uint32_t m = a.M[(size_t)g * a.ld + w0 + j];
-                if (!m) continue;
-                const uint32_t v = a.V[(size_t)g * a.ld + w0 + j];
-                const uint32_t x = m & ~v, y = m & v;
-                if (cx == kEmpty && x) cx = (w0 + j) * 32 + (__ffs(x) - 1);
-                if (cy == kEmpty && y) cy = (w0 + j) * 32 + (__ffs(y) - 1);
+            for (int j = BW - 1; j >= 0; j--) {  // lowest word wins
+                const uint32_t x = m.x[j] & ~v.x[j], y = m.x[j] & v.x[j];
+                if (x) cx = (w0 + j) * 32 + (__ffs(x) - 1);
+                if (y) cy = (w0 + j) * 32 + (__ffs(y) - 1);
             }
             if (cx != kEmpty) atomicMin(a.first_x + g, a.pair_base + cx);
             if (cy != kEmpty) atomicMin(a.first_y + g, a.pair_base + cy);
