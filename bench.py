@@ -233,14 +233,28 @@ def run_ours(args):
     out = P.make_outputs(sv, st_, mk)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    D = _load("pdf_b200_dist", os.path.join(ROOT, "gpu-path-delay-coverage_b200", "dist.py")) if dist else None
+    fx_t = torch.empty(G, dtype=torch.int32, device="cuda")
+    fy_t = torch.empty(G, dtype=torch.int32, device="cuda")
+
     def step():
         s.reset_async(stream)
-        P.grade_async(c, s, pairs, base, out, stream)
+        if dist is None:
+            P.grade_async(c, s, pairs, base, out, stream)
+            return
+        # pairs sharded over ranks: mark locally, MIN-reduce the first-detect
+        # ids over NVLink (NCCL), then count locally
+        P.grade_mark_async(c, s, pairs, base, out, stream)
+        P.first_copy(s, fx_t, fy_t, False, stream)
+        D.exchange_first_(fx_t, fy_t)
+        P.first_copy(s, fx_t, fy_t, True, stream)
+        P.grade_cover_async(c, s, stream)
 
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
     ref_total = s.snapshot()[2].value
+    job_total = D.sum_u128(ref_total, "cuda") if dist else ref_total
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     sampler = ClockSampler(gpu_id_for_smi(torch, local))
@@ -264,8 +278,8 @@ def run_ours(args):
     ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
     totals_ok = s.snapshot()[2].value == ref_total
 
-    # e2e: the public synchronous call with pinned host pairs (H2D inside the
-    # call) and the batch count read back to the host, every step.
+    # e2e: the public calls with pinned host pairs (H2D inside the call) and
+    # the batch count read back to the host, every step.
     hv = torch.from_numpy(v.view(np.int32)).pin_memory()
     ht = torch.from_numpy(t.view(np.int32)).pin_memory()
     hpairs = P.Pairs_t(hv.data_ptr(), ht.data_ptr(), n, W, 0)
@@ -274,11 +288,21 @@ def run_ours(args):
     for i in range(max(3, args.warmup) + args.steps):
         flush.fill_(i & 0xFF)
         torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
         s.reset_async(stream)
         tot = P.Totals_t()
-        P.check(P.lib().pdf_grade(c.h, s.h, C.byref(hpairs), base, C.byref(out), C.byref(tot),
-                                  C.c_void_p(stream)), "pdf_grade")
+        if dist is None:
+            P.check(P.lib().pdf_grade(c.h, s.h, C.byref(hpairs), base, C.byref(out), C.byref(tot),
+                                      C.c_void_p(stream)), "pdf_grade")
+        else:
+            P.grade_mark_async(c, s, hpairs, base, out, stream)
+            P.first_copy(s, fx_t, fy_t, False, stream)
+            D.exchange_first_(fx_t, fy_t)
+            P.first_copy(s, fx_t, fy_t, True, stream)
+            P.grade_cover_async(c, s, stream)
+            s.snapshot()
         if i >= max(3, args.warmup):
             e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_ms_mean = sum(e2e_ms) / len(e2e_ms)
@@ -308,10 +332,10 @@ def run_ours(args):
                      "traffic": tr.get("dram_bytes_per_launch") if tr else None},
         "e2e": {"value": units / (e2e_ms_mean / 1e3), "unit": "gate-evals/s",
                 "h2d_bytes_per_step": int(2 * nl.n_pi * W * 4), "d2h_bytes_per_step": 64},
-        "gpu_launches": 6 * args.steps,
+        "gpu_launches": 5 * args.steps,  # batch_begin, k_forward, k_active, k_cover, batch_end
         "clocks": clocks,
         "result_stable": bool(totals_ok),
-        "batch_count": ref_total,
+        "batch_count": job_total,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         O = oracle()

@@ -107,6 +107,10 @@ ABI = [
                                   C.POINTER(Outputs_t), C.c_void_p]),
     ("pdf_grade", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Pairs_t), C.c_uint64,
                             C.POINTER(Outputs_t), C.POINTER(Totals_t), C.c_void_p]),
+    ("pdf_grade_mark_async", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Pairs_t), C.c_uint64,
+                                       C.POINTER(Outputs_t), C.c_void_p]),
+    ("pdf_grade_cover_async", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pdf_state_first_copy", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     ("pdf_sim", C.c_int, [C.c_void_p, C.POINTER(Pairs_t), C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     ("pdf_mark", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
                            C.c_void_p]),
@@ -434,6 +438,21 @@ def grade_async(c: Circuit, s: State, pairs: Pairs_t, pair_base: int, out: Outpu
                 stream: int = 0) -> None:
     check(lib().pdf_grade_async(c.h, s.h, C.byref(pairs), pair_base, C.byref(out) if out else None,
                                 C.c_void_p(stream)), "pdf_grade_async")
+
+
+def grade_mark_async(c: Circuit, s: State, pairs: Pairs_t, pair_base: int, out: Outputs_t | None,
+                     stream: int = 0) -> None:
+    check(lib().pdf_grade_mark_async(c.h, s.h, C.byref(pairs), pair_base, C.byref(out) if out else None,
+                                     C.c_void_p(stream)), "pdf_grade_mark_async")
+
+
+def grade_cover_async(c: Circuit, s: State, stream: int = 0) -> None:
+    check(lib().pdf_grade_cover_async(c.h, s.h, C.c_void_p(stream)), "pdf_grade_cover_async")
+
+
+def first_copy(s: State, fx, fy, to_state: bool, stream: int = 0) -> None:
+    check(lib().pdf_state_first_copy(s.h, _addr(fx), _addr(fy), int(to_state), C.c_void_p(stream)),
+          "pdf_state_first_copy")
 
 
 def stage_sim(c: Circuit, v, t, n_pairs, sim_v, sim_t, stream: int = 0):

@@ -78,7 +78,7 @@ struct DeviceGuard {
 // Per-batch device workspace (owned by a state, or by a circuit for the
 // stage calls).
 struct Workspace {
-    DevBuf nzb, maxlvl, active, active_list, active_count;
+    DevBuf nzb, maxlvl, active;
     DevBuf planes;   // internal V, T, M planes when the caller gives none
     DevBuf pi;       // staged host pairs
     uint64_t plane_ld = 0, plane_words = 0;
@@ -86,8 +86,6 @@ struct Workspace {
         nzb.release();
         maxlvl.release();
         active.release();
-        active_list.release();
-        active_count.release();
         planes.release();
         pi.release();
     }
@@ -103,7 +101,7 @@ struct pdf_circuit {
     uint32_t cap = 512, ecap = 2048, n_pieces = 0, bm_shared = 0;
     uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
     size_t fwd_smem = 0;
-    uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
+    uint32_t hash_cap = 4096, cover_threads = 256;
     Workspace stage;  // scratch of the stage calls
     std::mutex mu;    // serialises the stage scratch
 };
@@ -121,6 +119,11 @@ struct pdf_state {
     bool profiling = false;
     std::vector<ProfEvents> prof;   // one entry per profiled call
     std::vector<ProfEvents> pool;   // recycled events
+    ProfEvents *pe = nullptr;       // events of the call in progress
+    // the batch marked by pdf_grade_mark_async and not yet counted
+    bool pending = false;
+    const uint32_t *pend_M = nullptr;
+    uint64_t pend_ld = 0, pend_n = 0, pend_base = 0;
 };
 
 namespace {
@@ -385,8 +388,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->ring2 = ring2;
     c->fwd_smem = off + (size_t)ring * c->bw * 12;
     c->hash_cap = 4096;
+    while (c->hash_cap > 64 && cover_smem_bytes(c->hash_cap) > prop.sharedMemPerBlockOptin) c->hash_cap /= 2;
     c->cover_threads = 256;
-    c->cover_grid = (uint32_t)prop.multiProcessorCount;
 
     auto fail = [&](pdf_status st2) {
         c->rec.release();
@@ -530,7 +533,7 @@ extern "C" pdf_status pdf_state_profile_read(pdf_state *s, double *ms, uint32_t 
         PDF_CUDA(cudaEventSynchronize(p.ev[3]));
         float a = 0, b = 0, c = 0;
         PDF_CUDA(cudaEventElapsedTime(&a, p.ev[0], p.ev[1]));
-        PDF_CUDA(cudaEventElapsedTime(&b, p.ev[1], p.ev[2]));
+        PDF_CUDA(cudaEventElapsedTime(&b, p.ev[2], p.ev[3]));
         PDF_CUDA(cudaEventElapsedTime(&c, p.ev[0], p.ev[3]));
         ms[0] += a;
         ms[1] += b;
@@ -598,8 +601,6 @@ pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes
     PDF_CUDA(ws.nzb.ensure(n_blocks * bm_words * 4));
     PDF_CUDA(ws.maxlvl.ensure(n_blocks * 4));
     PDF_CUDA(ws.active.ensure(W * 4));
-    PDF_CUDA(ws.active_list.ensure(W * 32 * 4));
-    PDF_CUDA(ws.active_count.ensure(16));
     if (need_planes) {
         const uint64_t ld = n_blocks * c->bw;
         if (ws.plane_ld < ld || !ws.planes.p) {
@@ -648,8 +649,6 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
     a.n_pairs = n_pairs;
     a.pair_base = pair_base;
     a.active = ws.active.as<uint32_t>();
-    a.active_list = ws.active_list.as<uint32_t>();
-    a.active_count = ws.active_count.as<uint32_t>();
     a.acc = acc;
     a.hash_cap = c->hash_cap;
     return a;
@@ -701,18 +700,15 @@ pdf_status copy_plane_out(uint32_t *dst, uint64_t dst_ld, int dst_dev, const uin
 
 }  // namespace
 
-extern "C" pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr,
-                                      uint64_t pair_base, const pdf_outputs *out, void *stream) {
-    if (!c || !s || s->c != c) return PDF_EINVAL;
-    pdf_status st = check_pairs(c, pr, pair_base);
-    if (st != PDF_OK) return st;
-    DeviceGuard dg(c->device);
-    if (!dg.ok) return PDF_ECUDA;
-    cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    std::lock_guard<std::mutex> lk(s->mu);
+namespace {
+
+// First half of a grading call: sim, mark, prune and merge into the state.
+// Records what the second half needs in the state.
+pdf_status grade_mark_locked(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr, uint64_t pair_base,
+                             const pdf_outputs *out, cudaStream_t cs) {
     const uint64_t n = pr->n_pairs, W = (n + 31) / 32, G = c->info.n_gates;
     const bool direct = out && out->on_device && planes_fit(c, W, out->ld, {out->sim_v, out->sim_t, out->mark});
-    st = ensure_ws(c, s->ws, W, !direct);
+    pdf_status st = ensure_ws(c, s->ws, W, !direct);
     if (st != PDF_OK) return st;
     const uint32_t *pv, *pt;
     uint64_t pld;
@@ -741,7 +737,7 @@ extern "C" pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pa
     a.pair_base = (uint32_t)pair_base;
     DevAcc *acc = s->acc.as<DevAcc>();
     a.err = &acc->err;
-    ProfEvents *pe = nullptr;
+    s->pe = nullptr;
     if (s->profiling) {
         ProfEvents p{};
         if (!s->pool.empty()) {
@@ -751,23 +747,93 @@ extern "C" pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pa
             for (auto &e : p.ev) PDF_CUDA(cudaEventCreate(&e));
         }
         s->prof.push_back(p);
-        pe = &s->prof.back();
-        PDF_CUDA(cudaEventRecord(pe->ev[0], cs));
+        s->pe = &s->prof.back();
+        PDF_CUDA(cudaEventRecord(s->pe->ev[0], cs));
     }
     PDF_CUDA(launch_batch_begin(acc, cs));
     PDF_CUDA(launch_forward(a, FWD_FUSED, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
-    if (pe) PDF_CUDA(cudaEventRecord(pe->ev[1], cs));
-    CoverArgs ca = base_cover(c, s->ws, a.M, a.ld, n, (uint32_t)pair_base, a.first_x, a.first_y, acc);
-    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
-    PDF_CUDA(launch_batch_end(acc, n, cs));
-    if (pe) PDF_CUDA(cudaEventRecord(pe->ev[2], cs));
+    if (s->pe) PDF_CUDA(cudaEventRecord(s->pe->ev[1], cs));
     if (out && !direct) {
         st = copy_plane_out(out->sim_v, out->ld, out->on_device, a.V, a.ld, W, G, cs);
         if (st == PDF_OK) st = copy_plane_out(out->sim_t, out->ld, out->on_device, a.T, a.ld, W, G, cs);
         if (st == PDF_OK) st = copy_plane_out(out->mark, out->ld, out->on_device, a.M, a.ld, W, G, cs);
         if (st != PDF_OK) return st;
     }
-    if (pe) PDF_CUDA(cudaEventRecord(pe->ev[3], cs));
+    s->pend_M = a.M;
+    s->pend_ld = a.ld;
+    s->pend_n = n;
+    s->pend_base = pair_base;
+    s->pending = true;
+    return PDF_OK;
+}
+
+// Second half: count the covered paths of the marked batch against the
+// state's first-detect ids and add them to the total.
+pdf_status grade_cover_locked(pdf_circuit *c, pdf_state *s, cudaStream_t cs) {
+    if (!s->pending) return PDF_EINVAL;
+    s->pending = false;
+    DevAcc *acc = s->acc.as<DevAcc>();
+    const uint32_t base = (uint32_t)s->pend_base;
+    CoverArgs ca = base_cover(c, s->ws, s->pend_M, s->pend_ld, s->pend_n, base, s->first_x.as<uint32_t>(),
+                              s->first_y.as<uint32_t>(), acc);
+    if (s->pe) PDF_CUDA(cudaEventRecord(s->pe->ev[2], cs));  // cover starts (after any exchange)
+    PDF_CUDA(launch_cover(ca, c->cover_threads, cs));
+    PDF_CUDA(launch_batch_end(acc, s->pend_n, cs));
+    if (s->pe) {
+        PDF_CUDA(cudaEventRecord(s->pe->ev[3], cs));
+        s->pe = nullptr;
+    }
+    return PDF_OK;
+}
+
+}  // namespace
+
+extern "C" pdf_status pdf_grade_mark_async(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr,
+                                           uint64_t pair_base, const pdf_outputs *out, void *stream) {
+    if (!c || !s || s->c != c) return PDF_EINVAL;
+    pdf_status st = check_pairs(c, pr, pair_base);
+    if (st != PDF_OK) return st;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    std::lock_guard<std::mutex> lk(s->mu);
+    return grade_mark_locked(c, s, pr, pair_base, out, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" pdf_status pdf_grade_cover_async(pdf_circuit *c, pdf_state *s, void *stream) {
+    if (!c || !s || s->c != c) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    std::lock_guard<std::mutex> lk(s->mu);
+    return grade_cover_locked(c, s, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" pdf_status pdf_grade_async(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr,
+                                      uint64_t pair_base, const pdf_outputs *out, void *stream) {
+    if (!c || !s || s->c != c) return PDF_EINVAL;
+    pdf_status st = check_pairs(c, pr, pair_base);
+    if (st != PDF_OK) return st;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(s->mu);
+    st = grade_mark_locked(c, s, pr, pair_base, out, cs);
+    if (st != PDF_OK) return st;
+    return grade_cover_locked(c, s, cs);
+}
+
+extern "C" pdf_status pdf_state_first_copy(pdf_state *s, uint32_t *first_x, uint32_t *first_y, int to_state,
+                                           void *stream) {
+    if (!s || !first_x || !first_y) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    const size_t bytes = 4 * (size_t)s->c->info.n_gates;
+    if (to_state) {
+        PDF_CUDA(cudaMemcpyAsync(s->first_x.p, first_x, bytes, cudaMemcpyDeviceToDevice, cs));
+        PDF_CUDA(cudaMemcpyAsync(s->first_y.p, first_y, bytes, cudaMemcpyDeviceToDevice, cs));
+    } else {
+        PDF_CUDA(cudaMemcpyAsync(first_x, s->first_x.p, bytes, cudaMemcpyDeviceToDevice, cs));
+        PDF_CUDA(cudaMemcpyAsync(first_y, s->first_y.p, bytes, cudaMemcpyDeviceToDevice, cs));
+    }
     return PDF_OK;
 }
 
@@ -892,7 +958,7 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
                                       s->ws.maxlvl.as<uint32_t>(), (c->info.n_gates + 31) / 32, cs));
     CoverArgs ca = base_cover(c, s->ws, mark, ld, n_pairs, (uint32_t)pair_base, s->first_x.as<uint32_t>(),
                               s->first_y.as<uint32_t>(), acc);
-    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
+    PDF_CUDA(launch_cover(ca, c->cover_threads, cs));
     PDF_CUDA(launch_batch_end(acc, n_pairs, cs));
     PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));

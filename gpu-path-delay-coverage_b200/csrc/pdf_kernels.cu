@@ -255,6 +255,8 @@ __device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, const uint32_t *ed
 // multiples of BW and every row holds all n_blocks * BW words; words at or
 // past ceil(n_pairs / 32) are masked to zero.
 // ---------------------------------------------------------------------------
+constexpr int kEagerFanins = 3;  // fan-ins loaded up front (fan-in 0 and two fold steps)
+
 template <int BW, int ROBUST, int MODE>
 __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -292,11 +294,15 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
     uint32_t phase = 0;  // bit b: parity of the next wait on mbar[b]
     bool failed = false;
     // ------------------------------------------------------------- forward
-    if (threadIdx.x == 0) stage_piece(a, S, a.pieces[0], 0, false);
+    Piece Pn = a.pieces[0];
+    if (threadIdx.x == 0) stage_piece(a, S, Pn, 0, false);
     for (uint32_t i = 0; i < a.n_pieces; i++) {
-        const Piece P = a.pieces[i];
+        const Piece P = Pn;
         const int buf = i & 1;
-        if (threadIdx.x == 0 && i + 1 < a.n_pieces) stage_piece(a, S, a.pieces[i + 1], buf ^ 1, false);
+        if (i + 1 < a.n_pieces) {
+            Pn = a.pieces[i + 1];
+            if (threadIdx.x == 0) stage_piece(a, S, Pn, buf ^ 1, false);
+        }
         const bool ok = mbar_wait(S.mbar + buf, (phase >> buf) & 1u);
         phase ^= 1u << buf;
         if (__syncthreads_or(!ok)) {
@@ -338,39 +344,68 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
                     T.x[j] &= wm.x[j];
                 }
             } else {
-                Vec<BW> fv, ft, v1;
-                fetch(r.w[3], fv, ft);
-#pragma unroll
-                for (int j = 0; j < BW; j++) eval_first(h, fv.x[j], ft.x[j], V.x[j], v1.x[j]);
+                // Issue every load of the gate before using any (generic
+                // pointers into the ring or the planes), so a piece waits for
+                // at most one round trip to L2.
                 const uint32_t nfold = hdr_nfold(h);
-                for (uint32_t jj = 1; jj <= nfold; jj++) {
-                    fetch(fanin_id(r, edges, jj), fv, ft);
+                Vec<BW> fv[kEagerFanins], ft[kEagerFanins], m0;
 #pragma unroll
-                    for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
+                for (int q = 0; q < kEagerFanins; q++) {
+                    if ((uint32_t)q <= nfold) {
+                        const uint32_t f = r.w[3 + q];
+                        const bool in_ring = f >= ring_lo;
+                        const uint32_t *pv = in_ring ? rV + (f & Rm) * BW : a.V + (size_t)f * a.ld + w0;
+                        const uint32_t *pt = in_ring ? rT + (f & Rm) * BW : a.T + (size_t)f * a.ld + w0;
+                        fv[q] = vld<BW>(pv);
+                        ft[q] = vld<BW>(pt);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < BW; j++) m0.x[j] = 0;
+                if (MODE == FWD_FUSED && (h & RF_MARKF0)) {
+                    const uint32_t f0 = r.w[3];
+                    m0 = vld<BW>(f0 >= ring_lo ? rM + (f0 & Rm) * BW : a.M + (size_t)f0 * a.ld + w0);
+                }
+                Vec<BW> v1;
+#pragma unroll
+                for (int j = 0; j < BW; j++) eval_first(h, fv[0].x[j], ft[0].x[j], V.x[j], v1.x[j]);
+#pragma unroll
+                for (int q = 1; q < kEagerFanins; q++)
+                    if ((uint32_t)q <= nfold)
+#pragma unroll
+                        for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv[q].x[j], ft[q].x[j]);
+                for (uint32_t jj = kEagerFanins; jj <= nfold; jj++) {
+                    Vec<BW> xv, xt;
+                    fetch(fanin_id(r, edges, jj), xv, xt);
+#pragma unroll
+                    for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], xv.x[j], xt.x[j]);
                 }
 #pragma unroll
                 for (int j = 0; j < BW; j++) {
                     eval_finish(h, V.x[j], v1.x[j], T.x[j]);
                     V.x[j] &= wm.x[j];
                     T.x[j] &= wm.x[j];
+                    M.x[j] = (h & RF_MARKF0) ? (T.x[j] & m0.x[j]) : 0u;
                 }
             }
+            if (MODE == FWD_SIM || (h & RF_INPT) || MODE == FWD_MARK) {
 #pragma unroll
-            for (int j = 0; j < BW; j++) M.x[j] = 0;
+                for (int j = 0; j < BW; j++) M.x[j] = 0;
+            }
             if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
                 if (h & RF_INPT) {
                     M = T;
-                } else if ((h & RF_MARKF0) && vany(T)) {
+                } else if (MODE == FWD_MARK && (h & RF_MARKF0) && vany(T)) {
                     const uint32_t f0 = r.w[3];
                     const Vec<BW> m0 =
                         f0 >= ring_lo ? vld<BW>(rM + (f0 & Rm) * BW) : vld<BW>(a.M + (size_t)f0 * a.ld + w0);
 #pragma unroll
                     for (int j = 0; j < BW; j++) M.x[j] = T.x[j] & m0.x[j];
-                    if ((h & RF_SENS) && vany(M)) {
-                        const Vec<BW> sv = sens_any<BW, ROBUST>(r, edges, rec_nfi(r), M, fetch);
+                }
+                if (!(h & RF_INPT) && (h & RF_SENS) && vany(M)) {
+                    const Vec<BW> sv = sens_any<BW, ROBUST>(r, edges, rec_nfi(r), M, fetch);
 #pragma unroll
-                        for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
-                    }
+                    for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
                 }
             }
             const size_t o = (size_t)g * a.ld + w0;
@@ -509,32 +544,6 @@ __global__ void k_active(const CoverArgs a) {
     if (fy != kEmpty && dy < a.n_pairs) atomicOr(a.active + (dy >> 5), 1u << (dy & 31));
 }
 
-// Ordered list of the active pairs (one CTA).
-__global__ void __launch_bounds__(1024) k_active_compact(const CoverArgs a, uint32_t W) {
-    __shared__ uint32_t s_cnt[1024];
-    const uint32_t per = (W + blockDim.x - 1) / blockDim.x;
-    const uint32_t q0 = threadIdx.x * per, q1 = min(W, q0 + per);
-    uint32_t cnt = 0;
-    for (uint32_t q = q0; q < q1; q++) cnt += __popc(a.active[q]);
-    s_cnt[threadIdx.x] = cnt;
-    __syncthreads();
-    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {  // inclusive scan
-        const uint32_t v = threadIdx.x >= off ? s_cnt[threadIdx.x - off] : 0u;
-        __syncthreads();
-        s_cnt[threadIdx.x] += v;
-        __syncthreads();
-    }
-    uint32_t pos = s_cnt[threadIdx.x] - cnt;
-    for (uint32_t q = q0; q < q1; q++) {
-        uint32_t bits = a.active[q];
-        while (bits) {
-            a.active_list[pos++] = q * 32 + (__ffs(bits) - 1);
-            bits &= bits - 1;
-        }
-    }
-    if (threadIdx.x == blockDim.x - 1) *a.active_count = s_cnt[threadIdx.x];
-}
-
 __device__ __forceinline__ uint32_t hash_slot(uint32_t g, uint32_t mask) {
     return (g * 2654435761u) & mask;
 }
@@ -563,110 +572,146 @@ __device__ void atomic_add_u128(unsigned long long *lo, unsigned long long *hi, 
     }
 }
 
-// One CTA per active pair (persistent over the list).  Walks the levels that
-// hold marks in the pair's column block, from the top down, over the nets
-// the pair marks (kernCover, coverkernel.cuh:193-229):
+// Path counting (kernCover, coverkernel.cuh:171-230, and kernSumSingle,
+// :77-105) for the pairs of one column block that first-detect some net.
+// One CTA per column block; up to kCoverSlots such pairs per pass.  Levels
+// descending from the block's highest marked level, over the nets with a
+// surviving mark in the block that one of the pass's pairs marks:
 //   H = [po] + sum h(fo);  C = sum c(fo);  first = pid is first_x or first_y
 //   c = C + (first ? H : 0);  h = first ? 0 : H;  h = 0 on INPT
-// (unmarked nets hold h = c = 0 and are never stored).  (h, c) live in a
-// shared-memory open-addressing table keyed by net id.  Level-0 INPT c values
-// are summed into the batch count (kernSumSingle, coverkernel.cuh:77-105).
-__global__ void __launch_bounds__(512) k_cover(const CoverArgs a) {
+// (a net a pair does not mark has h = c = 0).  (h, c) of each net, one per
+// slot, sit in a shared-memory open-addressing table keyed by net id.  The
+// level-0 INPT c values are the pairs' counts, summed into the batch count.
+constexpr int kCoverSlots = 4;
+__global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const uint32_t cap = a.hash_cap, cmask = cap - 1;
-    pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw);
-    pdf_u128 *cv = hv + cap;
-    uint32_t *keys = reinterpret_cast<uint32_t *>(cv + cap);
-    __shared__ pdf_u128 s_red[32];
+    uint32_t *keys = reinterpret_cast<uint32_t *>(smraw);
+    pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw + (((size_t)cap * 4 + 127) & ~(size_t)127));
+    pdf_u128 *cv = hv + (size_t)cap * kCoverSlots;
+    __shared__ uint32_t s_pairs[256];
+    __shared__ uint32_t s_na;
+    __shared__ pdf_u128 s_red[8];
     __shared__ unsigned int s_flags;
 
-    const uint32_t n_active = *a.active_count;
-    for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) {
-        const uint32_t p = a.active_list[ai];
-        const uint32_t pid = a.pair_base + p;
-        const uint32_t wp = p >> 5, bit = p & 31, blk = wp / a.bw;
-        const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
-        const uint32_t top = a.blk_maxlvl[blk];
+    const uint32_t blk = blockIdx.x, w0 = blk * a.bw;
+    const uint32_t W = (uint32_t)((a.n_pairs + 31) / 32);
+    if (threadIdx.x == 0) {
+        uint32_t n = 0;
+        for (uint32_t j = 0; j < a.bw && w0 + j < W; j++) {
+            uint32_t bits = a.active[w0 + j];
+            while (bits) {
+                s_pairs[n++] = (w0 + j) * 32 + (__ffs(bits) - 1);
+                bits &= bits - 1;
+            }
+        }
+        s_na = n;
+        s_flags = 0;
+    }
+    __syncthreads();
+    const uint32_t na = s_na;
+    if (na == 0) return;
+    const uint32_t top = a.blk_maxlvl[blk];
+    const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
+    pdf_u128 total = 0;
+    bool ovf = false;
+    for (uint32_t g0 = 0; g0 < na; g0 += kCoverSlots) {
+        const uint32_t ns = min((uint32_t)kCoverSlots, na - g0);
+        uint32_t pw[kCoverSlots], pb[kCoverSlots], pid[kCoverSlots];
+#pragma unroll
+        for (int k = 0; k < kCoverSlots; k++) {
+            const uint32_t p = s_pairs[g0 + min((uint32_t)k, ns - 1)];
+            pw[k] = p >> 5;
+            pb[k] = p & 31;
+            pid[k] = a.pair_base + p;
+        }
         for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) keys[i] = kEmpty;
-        if (threadIdx.x == 0) s_flags = 0;
         __syncthreads();
-        pdf_u128 total = 0;
-        bool ovf = false;
         for (int l = (int)top - 1; l >= 0; l--) {
             const uint32_t s = a.c.level_off[l], e = a.c.level_off[l + 1];
-            if (e > s) {
-                const uint32_t q0 = s >> 5, q1 = (e - 1) >> 5;
-                for (uint32_t q = q0 + threadIdx.x; q <= q1; q += blockDim.x) {
-                    uint32_t bits = nzb[q];
-                    if (q == q0) bits &= 0xFFFFFFFFu << (s & 31);
-                    if (q == q1) bits &= 0xFFFFFFFFu >> (31 - ((e - 1) & 31));
-                    while (bits) {
-                        const uint32_t g = q * 32 + (__ffs(bits) - 1);
-                        bits &= bits - 1;
-                        if (!((a.M[(size_t)g * a.ld + wp] >> bit) & 1u)) continue;
-                        const GateRec r = load_rec(a.c.rec + g);
-                        pdf_u128 H = rec_po(r) ? 1 : 0, C = 0;
-                        const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
-                        for (uint32_t k = 0; k < nfo; k++) {
-                            const uint32_t fo = __ldg(a.c.edges + eb + k);
-                            uint32_t sl = hash_slot(fo, cmask);
-                            for (uint32_t probe = 0; probe < cap; probe++) {
-                                const uint32_t key = keys[sl];
-                                if (key == fo) {
-                                    bool dummy = false;
-                                    C = add_sat(C, cv[sl], ovf);
-                                    H = add_sat(H, hv[sl], dummy);
-                                    break;
-                                }
-                                if (key == kEmpty) break;
-                                sl = (sl + 1) & cmask;
+            for (uint32_t g = s + threadIdx.x; g < e; g += blockDim.x) {
+                if (!((nzb[g >> 5] >> (g & 31)) & 1u)) continue;
+                uint32_t smask = 0;
+#pragma unroll
+                for (int k = 0; k < kCoverSlots; k++)
+                    if ((uint32_t)k < ns && ((a.M[(size_t)g * a.ld + pw[k]] >> pb[k]) & 1u)) smask |= 1u << k;
+                if (!smask) continue;
+                const GateRec r = load_rec(a.c.rec + g);
+                const uint32_t fx = a.first_x[g], fy = a.first_y[g];
+                pdf_u128 H[kCoverSlots], Cc[kCoverSlots];
+#pragma unroll
+                for (int k = 0; k < kCoverSlots; k++) {
+                    H[k] = rec_po(r) ? 1 : 0;
+                    Cc[k] = 0;
+                }
+                const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
+                for (uint32_t q = 0; q < nfo; q++) {
+                    const uint32_t fo = __ldg(a.c.edges + eb + q);
+                    uint32_t sl = hash_slot(fo, cmask);
+                    for (uint32_t probe = 0; probe < cap; probe++) {
+                        const uint32_t key = keys[sl];
+                        if (key == fo) {
+                            bool hovf = false;
+#pragma unroll
+                            for (int k = 0; k < kCoverSlots; k++) {
+                                Cc[k] = add_sat(Cc[k], cv[(size_t)sl * kCoverSlots + k], ovf);
+                                H[k] = add_sat(H[k], hv[(size_t)sl * kCoverSlots + k], hovf);
                             }
+                            break;
                         }
-                        const bool first = a.first_x[g] == pid || a.first_y[g] == pid;
-                        pdf_u128 c = C, h = H;
-                        if (first) {
-                            c = add_sat(C, H, ovf);
-                            h = 0;
-                        }
-                        if (c == ~(pdf_u128)0) ovf = true;
-                        if (rec_type(r) == PDF_INPT) {
-                            h = 0;
-                            if (l == 0) total = add_sat(total, c, ovf);
-                        }
-                        if (l > 0) {  // level-0 values are never read
-                            uint32_t sl = hash_slot(g, cmask);
-                            uint32_t probe = 0;
-                            for (; probe < cap; probe++) {
-                                if (atomicCAS(keys + sl, kEmpty, g) == kEmpty) break;
-                                sl = (sl + 1) & cmask;
-                            }
-                            if (probe == cap) {
-                                atomicOr(&a.acc->err, kErrHashFull);  // table full
-                            } else {
-                                hv[sl] = h;
-                                cv[sl] = c;
-                            }
+                        if (key == kEmpty) break;
+                        sl = (sl + 1) & cmask;
+                    }
+                }
+                pdf_u128 hs[kCoverSlots], cs[kCoverSlots];
+#pragma unroll
+                for (int k = 0; k < kCoverSlots; k++) {
+                    hs[k] = 0;
+                    cs[k] = 0;
+                    if (!((smask >> k) & 1u)) continue;
+                    const bool first = fx == pid[k] || fy == pid[k];
+                    cs[k] = first ? add_sat(Cc[k], H[k], ovf) : Cc[k];
+                    hs[k] = first ? 0 : H[k];
+                    if (cs[k] == ~(pdf_u128)0) ovf = true;
+                    if (rec_type(r) == PDF_INPT) {
+                        hs[k] = 0;
+                        if (l == 0) total = add_sat(total, cs[k], ovf);
+                    }
+                }
+                if (l > 0) {  // level-0 values are never read
+                    uint32_t sl = hash_slot(g, cmask);
+                    uint32_t probe = 0;
+                    for (; probe < cap; probe++) {
+                        if (atomicCAS(keys + sl, kEmpty, g) == kEmpty) break;
+                        sl = (sl + 1) & cmask;
+                    }
+                    if (probe == cap) {
+                        atomicOr(&a.acc->err, kErrHashFull);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < kCoverSlots; k++) {
+                            hv[(size_t)sl * kCoverSlots + k] = hs[k];
+                            cv[(size_t)sl * kCoverSlots + k] = cs[k];
                         }
                     }
                 }
             }
             __syncthreads();
         }
-        // Block sum of the pair's count.
-        for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
-        if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
-        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            pdf_u128 t = threadIdx.x < (blockDim.x + 31) / 32 ? s_red[threadIdx.x] : 0;
-            bool o2 = false;
-            for (int d = 16; d > 0; d >>= 1) t = add_sat(t, shfl_down_u128(t, d), o2);
-            if (threadIdx.x == 0) {
-                if (o2 || s_flags) atomicOr(&a.acc->batch_flags, PDF_FLAG_OVERFLOW);
-                if (t) atomic_add_u128(&a.acc->batch_lo, &a.acc->batch_hi, &a.acc->batch_flags, t);
-            }
+    }
+    // Block sum of the counts.
+    for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
+    if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        pdf_u128 t = threadIdx.x < (blockDim.x + 31) / 32 ? s_red[threadIdx.x] : 0;
+        bool o2 = false;
+        for (int d = 16; d > 0; d >>= 1) t = add_sat(t, shfl_down_u128(t, d), o2);
+        if (threadIdx.x == 0) {
+            if (o2 || s_flags) atomicOr(&a.acc->batch_flags, PDF_FLAG_OVERFLOW);
+            if (t) atomic_add_u128(&a.acc->batch_lo, &a.acc->batch_hi, &a.acc->batch_flags, t);
         }
-        __syncthreads();
     }
 }
 
@@ -785,19 +830,18 @@ cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, 
 }
 
 size_t cover_smem_bytes(uint32_t hash_cap) {
-    return (size_t)hash_cap * (2 * sizeof(pdf_u128) + sizeof(uint32_t));
+    return (((size_t)hash_cap * 4 + 127) & ~(size_t)127) + (size_t)hash_cap * kCoverSlots * 2 * sizeof(pdf_u128);
 }
 
-cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st) {
+cudaError_t launch_cover(const CoverArgs &a, uint32_t threads, cudaStream_t st) {
     const uint32_t W = (uint32_t)((a.n_pairs + 31) / 32);
     cudaError_t e = cudaMemsetAsync(a.active, 0, (size_t)W * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     k_active<<<(a.c.n_gates + 255) / 256, 256, 0, st>>>(a);
-    k_active_compact<<<1, 1024, 0, st>>>(a, W);
     const size_t smem = cover_smem_bytes(a.hash_cap);
     e = cudaFuncSetAttribute(k_cover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_cover<<<grid, threads, smem, st>>>(a);
+    k_cover<<<(W + a.bw - 1) / a.bw, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

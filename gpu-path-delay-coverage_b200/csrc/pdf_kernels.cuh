@@ -73,16 +73,14 @@ struct CoverArgs {
     uint64_t n_pairs;
     uint32_t pair_base;
     uint32_t *active;             // [W] bitmap of first-detecting pairs
-    uint32_t *active_list;        // [max_pairs]
-    uint32_t *active_count;       // [1]
     DevAcc *acc;
-    uint32_t hash_cap;            // entries of the per-CTA shared-memory hash (power of two)
+    uint32_t hash_cap;            // entries of the per-CTA shared-memory table (power of two)
 };
 
 // Host-side launchers (pdf_kernels.cu).  All return cudaError_t of the launch.
 cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st);
-cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st);
+cudaError_t launch_cover(const CoverArgs &a, uint32_t threads, cudaStream_t st);
 size_t cover_smem_bytes(uint32_t hash_cap);
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M,
                                uint64_t ld, uint64_t n_pairs, uint32_t pair_base,

@@ -217,6 +217,24 @@ pdf_status pdf_grade(pdf_circuit *c, pdf_state *s, const pdf_pairs *pairs,
                      void *stream);
 
 /*
+ * The two halves of pdf_grade_async, for callers that combine first-detect
+ * ids of several states between them (pairs sharded over GPUs: each rank
+ * marks its own pairs, the ranks reduce first_x/first_y with an unsigned MIN,
+ * then each rank counts its pairs).  pdf_grade_mark_async runs sim, mark,
+ * prune and merge into the state and writes the outputs;
+ * pdf_grade_cover_async counts the paths of that batch against the state's
+ * current first-detect ids.  No reference counterpart: the reference is
+ * single-GPU (main.cu:34).
+ */
+pdf_status pdf_grade_mark_async(pdf_circuit *c, pdf_state *s, const pdf_pairs *pairs,
+                                uint64_t pair_base, const pdf_outputs *out, void *stream);
+pdf_status pdf_grade_cover_async(pdf_circuit *c, pdf_state *s, void *stream);
+/* Stream-ordered copy of the state's first-detect ids to (to_state = 0) or
+ * from (to_state = 1) device buffers of n_gates uint32 each. */
+pdf_status pdf_state_first_copy(pdf_state *s, uint32_t *first_x, uint32_t *first_y, int to_state,
+                                void *stream);
+
+/*
  * Stage calls, one per reference host function, over device buffers in the
  * pdf_outputs plane layout (gate-major, ld words per row).  They compose to
  * exactly what pdf_grade computes.

@@ -111,3 +111,25 @@ def mark(nl, sim_codes: np.ndarray, n_pairs: int, mark_mode: int = 0, prune: boo
     s = np.ascontiguousarray(sim_codes, dtype=np.uint8)
     lib().pdfo_mark(_nl(nl), s.ctypes.data, n_pairs, mark_mode, out.ctypes.data, int(prune), threads)
     return out
+
+
+def merge(nl, sim_codes, mark_bits, n_pairs: int, pair_base: int, first_x, first_y) -> None:
+    """kernSegmentReduce2<1> restated: folds first ids into first_x/first_y (uint32, in place)."""
+    s = np.ascontiguousarray(sim_codes, dtype=np.uint8)
+    m = np.ascontiguousarray(mark_bits, dtype=np.uint8)
+    assert first_x.dtype == np.uint32 and first_y.dtype == np.uint32
+    lib().pdfo_merge(_nl(nl), s.ctypes.data, m.ctypes.data, n_pairs, pair_base, first_x.ctypes.data,
+                     first_y.ctypes.data, 0)
+
+
+def cover(nl, mark_bits, n_pairs: int, pair_base: int, first_x, first_y, threads: int = 0):
+    """kernCover<1> + kernSumSingle restated: returns (count, flags) of one chunk."""
+    m = np.ascontiguousarray(mark_bits, dtype=np.uint8)
+    fx = np.ascontiguousarray(first_x, dtype=np.uint32)
+    fy = np.ascontiguousarray(first_y, dtype=np.uint32)
+    lo, hi, fl = C.c_uint64(0), C.c_uint64(0), C.c_uint32(0)
+    rc = lib().pdfo_cover(_nl(nl), m.ctypes.data, n_pairs, pair_base, fx.ctypes.data, fy.ctypes.data,
+                          C.addressof(lo), C.addressof(hi), C.addressof(fl), threads)
+    if rc:
+        raise MemoryError("oracle allocation failed")
+    return (hi.value << 64) | lo.value, fl.value
