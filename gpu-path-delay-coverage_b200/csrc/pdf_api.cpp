@@ -99,7 +99,8 @@ struct pdf_circuit {
     DevCircuit dc{};
     uint32_t bw = 4, threads = 512, ring = 0, ring2 = 0;
     uint32_t cap = 512, ecap = 2048, n_pieces = 0, bm_shared = 0;
-    uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
+    uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_slot = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
+    uint32_t farcap = 0;
     size_t fwd_smem = 0;
     uint32_t hash_cap = 4096, cover_threads = 256;
     Workspace stage;  // scratch of the stage calls
@@ -330,13 +331,23 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->bw = o.tile_words ? o.tile_words : 4;
     // one thread per gate of a piece; 8-word tiles need twice the registers
     const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
-    const uint32_t cap_guess = std::min<uint32_t>(512, (inf.max_level_width + 7) & ~7u);
+    uint32_t widest_g = 1;
+    for (uint32_t l = 1; l < L; l++) widest_g = std::max(widest_g, nl->level_offsets[l + 1] - nl->level_offsets[l]);
+    if (L == 1) widest_g = inf.max_level_width;
+    const uint32_t cap_guess = std::min<uint32_t>(512, (widest_g + 31) & ~31u);
     c->threads = o.threads ? std::min(o.threads, max_threads)
                            : std::min(max_threads, std::max<uint32_t>(128, (cap_guess + 31) & ~31u));
-    const size_t budget = std::min<size_t>(prop.sharedMemPerBlockOptin, prop.sharedMemPerMultiprocessor / 2 - 2048);
+    const size_t budget = c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
+                                      : std::min<size_t>(prop.sharedMemPerBlockOptin,
+                                                         prop.sharedMemPerMultiprocessor / 2 - 2048);
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
-    c->cap = std::min<uint32_t>(512, (inf.max_level_width + 7) & ~7u);
+    // piece size from the widest level above the inputs (the inputs' level,
+    // often the widest, just splits into more pieces)
+    uint32_t widest = 1;
+    for (uint32_t l = 1; l < L; l++) widest = std::max(widest, nl->level_offsets[l + 1] - nl->level_offsets[l]);
+    if (L == 1) widest = inf.max_level_width;
+    c->cap = std::min<uint32_t>(512, (widest + 31) & ~31u);
     c->ecap = 2048;
     // pieces: runs of one level, <= cap gates, edge slice <= ecap words
     std::vector<Piece> pieces;
@@ -366,11 +377,55 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         delete c;
         return PDF_ENOTSUP;
     }
+    // Shared memory of k_forward: 3 record buffers; one region shared by the
+    // reverse pass's 2 edge buffers and the forward pass's 2 far-fan-in
+    // buffers (+ their slot table); bitmap; piece bits; barriers; the ring.
     size_t off = 0;
     c->off_rec = (uint32_t)off;
-    off += al(2 * (size_t)c->cap * sizeof(GateRec));
+    off += al(3 * (size_t)c->cap * sizeof(GateRec));
+    // Ring size and far-buffer capacity from the netlist: for each candidate
+    // ring (largest first), the most far fan-ins any piece prefetches; take
+    // the largest ring whose far buffer fits beside it.
+    auto far_bytes = [&](uint32_t fc) { return 2 * 3 * (size_t)fc * c->bw * 4; };
+    const size_t fixed = al(3 * (size_t)c->cap * sizeof(GateRec)) + al(2 * (size_t)c->cap * 4 * sizeof(uint16_t)) +
+                         ((size_t)bm_words * 4 <= 16384 ? al((size_t)bm_words * 4) : 0) +
+                         al(((size_t)c->n_pieces + 31) / 32 * 4) + 128;
+    auto far_count = [&](uint32_t R) {
+        uint32_t worst = 0;
+        for (size_t i = 1; i < pieces.size(); i++) {
+            const Piece &p = pieces[i];
+            const uint32_t lo = R ? (p.b > R ? p.b - R : 0) : p.b, fin = pieces[i - 1].a;
+            uint32_t n = 0;
+            for (uint32_t g = p.a; g < p.b; g++) {
+                const uint32_t h = make_rec_header(nl->type[g], nl->po[g], nl->nfi[g]);
+                if (h & RF_INPT) continue;
+                const uint32_t nq = std::min<uint32_t>(hdr_nfold(h) + 1, 4);
+                for (uint32_t q = 0; q < nq; q++) {
+                    const uint32_t f = edges[eoff[g] + q];
+                    n += (f < lo && f < fin) ? 1 : 0;
+                }
+            }
+            worst = std::max(worst, n);
+        }
+        return worst;
+    };
+    uint32_t ring = 0, farcap = 0;
+    uint32_t rmax = 1;
+    while ((size_t)rmax * 2 * c->bw * 12 <= budget) rmax *= 2;
+    for (uint32_t R = rmax; R >= 32; R /= 2) {
+        const uint32_t fc = std::min<uint32_t>((far_count(R) + 31) & ~31u, 4096);
+        const size_t need = fixed + al(std::max(2 * (size_t)c->ecap * 4, far_bytes(fc))) + (size_t)R * c->bw * 12;
+        if (need <= budget) {
+            ring = R;
+            farcap = fc;
+            break;
+        }
+    }
+    c->farcap = farcap;
     c->off_edge = (uint32_t)off;
-    off += al(2 * (size_t)c->ecap * 4);
+    off += al(std::max(2 * (size_t)c->ecap * 4, far_bytes(c->farcap)));
+    c->off_slot = (uint32_t)off;
+    off += al(2 * (size_t)c->cap * 4 * sizeof(uint16_t));
     c->bm_shared = (size_t)bm_words * 4 <= 16384 ? 1u : 0u;
     c->off_bm = (uint32_t)off;
     if (c->bm_shared) off += al((size_t)bm_words * 4);
@@ -379,9 +434,6 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->off_mbar = (uint32_t)off;
     off += 128;
     c->off_ring = (uint32_t)off;
-    uint32_t ring = 0;
-    if (budget > off)
-        for (uint32_t r = 1; (size_t)r * c->bw * 12 <= budget - off; r *= 2) ring = r;
     c->ring = ring;
     uint32_t ring2 = 0;
     for (uint32_t r = 1; ring && (size_t)r * c->bw * 4 <= (size_t)ring * c->bw * 12; r *= 2) ring2 = r;
@@ -627,6 +679,8 @@ FwdArgs base_fwd(pdf_circuit *c, uint64_t n_pairs) {
     a.off_ring = c->off_ring;
     a.off_rec = c->off_rec;
     a.off_edge = c->off_edge;
+    a.off_slot = c->off_slot;
+    a.farcap = c->farcap;
     a.off_bm = c->off_bm;
     a.off_pbits = c->off_pbits;
     a.off_mbar = c->off_mbar;
@@ -975,3 +1029,4 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
     pdf_status st2 = err_status(h.err | cerr);
     return st2;
 }
+

@@ -102,14 +102,35 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t phase) {
     return false;
 }
 
+// Asynchronous global -> shared copies of BW words (cp.async, completed by
+// cp.async.wait_all in the issuing thread).
+template <int BW>
+__device__ __forceinline__ void cp_async_vec(uint32_t *dst, const uint32_t *src) {
+    if constexpr (BW == 1) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+    } else if constexpr (BW == 2) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+    } else {
+#pragma unroll
+        for (int i = 0; i < BW; i += 4)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + i)), "l"(src + i)
+                         : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Shared-memory layout of k_forward (byte offsets from the host plan).
 struct FwdSmem {
     uint32_t *ring;      // forward: [R][3][BW] (V, T, M); reverse: [R2][BW] pruned marks
-    GateRec *rec;        // [2][cap] staged gate records of a piece
-    uint32_t *edge;      // [2][ecap] staged edge slices (reverse pass)
+    GateRec *rec;        // [3][cap] staged gate records of a piece
+    uint32_t *edge;      // [2][ecap] staged edge slices (reverse pass; shares memory with far)
+    uint32_t *far;       // [2][3][farcap][BW] prefetched far fan-in V, T, M (forward pass)
+    uint16_t *slot;      // [2][cap][kPrefetchFanins] far-buffer slot of each fan-in (0xFFFF: none)
     uint32_t *bm;        // nonzero-mark bitmap (shared or global)
     uint32_t *pbits;     // pieces that hold a forward mark
-    uint64_t *mbar;      // [2]
+    uint32_t *farcnt;    // [2] far slots handed out
+    uint64_t *mbar;      // [3]
 };
 
 // Stage piece `p` into buffer `buf`: its gate records and, for the reverse
@@ -255,7 +276,7 @@ __device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, const uint32_t *ed
 // multiples of BW and every row holds all n_blocks * BW words; words at or
 // past ceil(n_pairs / 32) are masked to zero.
 // ---------------------------------------------------------------------------
-constexpr int kEagerFanins = 3;  // fan-ins loaded up front (fan-in 0 and two fold steps)
+constexpr int kPrefetchFanins = 4;  // fan-ins per gate eligible for the far-buffer prefetch
 
 template <int BW, int ROBUST, int MODE>
 __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
@@ -264,7 +285,10 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
     S.ring = reinterpret_cast<uint32_t *>(smraw + a.off_ring);
     S.rec = reinterpret_cast<GateRec *>(smraw + a.off_rec);
     S.edge = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
+    S.far = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
+    S.slot = reinterpret_cast<uint16_t *>(smraw + a.off_slot);
     S.pbits = reinterpret_cast<uint32_t *>(smraw + a.off_pbits);
+    S.farcnt = reinterpret_cast<uint32_t *>(smraw + a.off_mbar + 64);
     S.mbar = reinterpret_cast<uint64_t *>(smraw + a.off_mbar);
     const uint32_t blk = blockIdx.x;
     const uint32_t w0 = blk * BW;
@@ -273,6 +297,7 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
     const uint32_t *edges = a.c.edges;
     const uint32_t R = a.ring_gates, Rm = R - 1;
     uint32_t *rV = S.ring, *rT = S.ring + (size_t)R * BW, *rM = S.ring + 2 * (size_t)R * BW;
+    const uint32_t farcap = a.farcap;
     Vec<BW> wm;  // valid bits of each word of this block
 #pragma unroll
     for (int j = 0; j < BW; j++) {
@@ -280,6 +305,10 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
         wm.x[j] = w + 1 < a.W ? 0xFFFFFFFFu
                               : (w + 1 == a.W ? ((a.n_pairs & 31) ? (1u << (a.n_pairs & 31)) - 1u : 0xFFFFFFFFu) : 0u);
     }
+    // far buffer of parity p, plane k (0 V, 1 T, 2 M), slot s
+    auto farp = [&](uint32_t p, uint32_t k, uint32_t sl) -> uint32_t * {
+        return S.far + (((size_t)p * 3 + k) * farcap + sl) * BW;
+    };
 
     if (MODE != FWD_SIM)
         for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) S.bm[q] = 0;
@@ -287,30 +316,93 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
     if (threadIdx.x == 0) {
         mbar_init(S.mbar, 1);
         mbar_init(S.mbar + 1, 1);
+        mbar_init(S.mbar + 2, 1);
         fence_mbar_init();
+        S.farcnt[0] = S.farcnt[1] = 0;
     }
     __syncthreads();
 
-    uint32_t phase = 0;  // bit b: parity of the next wait on mbar[b]
+    uint32_t phase = 0;     // bit b: parity of the next wait on mbar[b]
+    uint32_t inflight = 0;  // bit b: a copy on mbar[b] not yet waited for (uniform)
     bool failed = false;
-    // ------------------------------------------------------------- forward
-    Piece Pn = a.pieces[0];
-    if (threadIdx.x == 0) stage_piece(a, S, Pn, 0, false);
-    for (uint32_t i = 0; i < a.n_pieces; i++) {
-        const Piece P = Pn;
-        const int buf = i & 1;
-        if (i + 1 < a.n_pieces) {
-            Pn = a.pieces[i + 1];
-            if (threadIdx.x == 0) stage_piece(a, S, Pn, buf ^ 1, false);
+
+    // Prefetch the fan-ins of piece P (records in `recs`) that lie outside
+    // its ring window into far buffer `fb`: issued one piece ahead, so the
+    // piece then reads them from shared memory.  Only gates below
+    // `final_below` (the start of the piece now running) are copied: they
+    // are already written.
+    auto prefetch = [&](const Piece &P, const GateRec *recs, uint32_t fb, uint32_t final_below) {
+        if (!farcap) return;
+        const uint32_t lo = R ? (P.b > R ? P.b - R : 0) : P.b;
+        for (uint32_t gi = threadIdx.x; gi < P.b - P.a; gi += blockDim.x) {
+            const GateRec &r = recs[gi];
+            const uint32_t h = r.w[0];
+            if (h & RF_INPT) continue;
+            const uint32_t nfold = hdr_nfold(h);
+#pragma unroll
+            for (int q = 0; q < kPrefetchFanins; q++) {
+                if ((uint32_t)q > nfold) break;
+                const uint32_t f = r.w[3 + q];
+                if (f >= lo) continue;
+                // only gates already written are copied; the rest are read
+                // from the planes when the piece runs
+                uint32_t sl = f < final_below ? atomicAdd(S.farcnt + fb, 1u) : 0xFFFFu;
+                if (sl < farcap) {
+                    cp_async_vec<BW>(farp(fb, 0, sl), a.V + (size_t)f * a.ld + w0);
+                    cp_async_vec<BW>(farp(fb, 1, sl), a.T + (size_t)f * a.ld + w0);
+                    if (MODE != FWD_SIM && q == 0 && (h & RF_MARKF0))
+                        cp_async_vec<BW>(farp(fb, 2, sl), a.M + (size_t)f * a.ld + w0);
+                } else {
+                    sl = 0xFFFFu;
+                }
+                S.slot[((size_t)fb * a.cap + gi) * kPrefetchFanins + q] = (uint16_t)sl;
+            }
         }
-        const bool ok = mbar_wait(S.mbar + buf, (phase >> buf) & 1u);
-        phase ^= 1u << buf;
+        cp_async_commit();
+    };
+
+    // ------------------------------------------------------------- forward
+    // Records are staged two pieces ahead (three buffers, mbar[i % 3]); far
+    // fan-ins one piece ahead (two buffers).
+    Piece P0 = a.pieces[0], P1 = a.n_pieces > 1 ? a.pieces[1] : P0, P2 = P1;
+    if (threadIdx.x == 0) {
+        stage_piece(a, S, P0, 0, false);
+        if (a.n_pieces > 1) stage_piece(a, S, P1, 1, false);
+    }
+    inflight = a.n_pieces > 1 ? 3u : 1u;
+    {
+        const bool ok = mbar_wait(S.mbar, 0);
+        phase ^= 1u;
+        inflight &= ~1u;
+        if (__syncthreads_or(!ok)) failed = true;
+    }
+    if (!failed) prefetch(P0, S.rec, 0, P0.a);
+    for (uint32_t i = 0; i < a.n_pieces && !failed; i++) {
+        const Piece P = P0;
+        const uint32_t rb = i % 3, fb = i & 1;
+        const bool has_next = i + 1 < a.n_pieces;
+        if (i + 2 < a.n_pieces) P2 = a.pieces[i + 2];
+        if (threadIdx.x == 0) S.farcnt[fb ^ 1] = 0;
+        bool ok = true;
+        if (has_next) {
+            const uint32_t nb = (i + 1) % 3;
+            ok = mbar_wait(S.mbar + nb, (phase >> nb) & 1u);
+            phase ^= 1u << nb;
+            inflight &= ~(1u << nb);
+        }
+        cp_async_wait_all();  // this thread's prefetch for piece i
         if (__syncthreads_or(!ok)) {
             failed = true;
-            if (i + 1 < a.n_pieces) (void)mbar_wait(S.mbar + (buf ^ 1), (phase >> (buf ^ 1)) & 1u);
             break;
         }
-        const GateRec *recs = S.rec + (size_t)buf * a.cap;
+        if (i + 2 < a.n_pieces) {
+            if (threadIdx.x == 0) stage_piece(a, S, P2, (i + 2) % 3, false);
+            inflight |= 1u << ((i + 2) % 3);
+        }
+        if (has_next) prefetch(P1, S.rec + (size_t)((i + 1) % 3) * a.cap, fb ^ 1, P.a);
+
+        const GateRec *recs = S.rec + (size_t)rb * a.cap;
+        const uint16_t *slots = S.slot + (size_t)fb * a.cap * kPrefetchFanins;
         const uint32_t ring_lo = R ? (P.b > R ? P.b - R : 0) : P.b;
         bool any = false;
         for (uint32_t gi = threadIdx.x; gi < P.b - P.a; gi += blockDim.x) {
@@ -343,69 +435,61 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
                     V.x[j] &= wm.x[j];
                     T.x[j] &= wm.x[j];
                 }
-            } else {
-                // Issue every load of the gate before using any (generic
-                // pointers into the ring or the planes), so a piece waits for
-                // at most one round trip to L2.
-                const uint32_t nfold = hdr_nfold(h);
-                Vec<BW> fv[kEagerFanins], ft[kEagerFanins], m0;
+            }
+            Vec<BW> m0;
 #pragma unroll
-                for (int q = 0; q < kEagerFanins; q++) {
-                    if ((uint32_t)q <= nfold) {
-                        const uint32_t f = r.w[3 + q];
-                        const bool in_ring = f >= ring_lo;
-                        const uint32_t *pv = in_ring ? rV + (f & Rm) * BW : a.V + (size_t)f * a.ld + w0;
-                        const uint32_t *pt = in_ring ? rT + (f & Rm) * BW : a.T + (size_t)f * a.ld + w0;
-                        fv[q] = vld<BW>(pv);
-                        ft[q] = vld<BW>(pt);
+            for (int j = 0; j < BW; j++) m0.x[j] = 0;
+            if (!(h & RF_INPT)) {
+                // Fan-in q < kPrefetchFanins comes from the ring, the far
+                // buffer prefetched one piece ahead, or (far-buffer overflow)
+                // the planes; later fan-ins from the ring or the planes.
+                auto src = [&](uint32_t q, uint32_t f, uint32_t k) -> const uint32_t * {
+                    const uint32_t *ring_k = k == 0 ? rV : (k == 1 ? rT : rM);
+                    if (f >= ring_lo) return ring_k + (f & Rm) * BW;
+                    // the slot table is written only while the prefetch is on
+                    const uint32_t sl =
+                        (farcap && q < (uint32_t)kPrefetchFanins) ? slots[gi * kPrefetchFanins + q] : 0xFFFFu;
+                    if (sl != 0xFFFFu) return farp(fb, k, sl);
+                    const uint32_t *plane = k == 0 ? a.V : (k == 1 ? a.T : a.M);
+                    return plane + (size_t)f * a.ld + w0;
+                };
+                const uint32_t nfold = hdr_nfold(h);
+                const uint32_t f0 = r.w[3];
+                if (MODE != FWD_SIM && (h & RF_MARKF0)) m0 = vld<BW>(src(0, f0, 2));
+                if (MODE != FWD_MARK) {
+                    Vec<BW> v1;
+                    {
+                        const Vec<BW> fv = vld<BW>(src(0, f0, 0)), ft = vld<BW>(src(0, f0, 1));
+#pragma unroll
+                        for (int j = 0; j < BW; j++) eval_first(h, fv.x[j], ft.x[j], V.x[j], v1.x[j]);
+                    }
+                    for (uint32_t q = 1; q <= nfold; q++) {
+                        const uint32_t f = fanin_id(r, edges, q);
+                        const Vec<BW> fv = vld<BW>(src(q, f, 0)), ft = vld<BW>(src(q, f, 1));
+#pragma unroll
+                        for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < BW; j++) {
+                        eval_finish(h, V.x[j], v1.x[j], T.x[j]);
+                        V.x[j] &= wm.x[j];
+                        T.x[j] &= wm.x[j];
                     }
                 }
-#pragma unroll
-                for (int j = 0; j < BW; j++) m0.x[j] = 0;
-                if (MODE == FWD_FUSED && (h & RF_MARKF0)) {
-                    const uint32_t f0 = r.w[3];
-                    m0 = vld<BW>(f0 >= ring_lo ? rM + (f0 & Rm) * BW : a.M + (size_t)f0 * a.ld + w0);
-                }
-                Vec<BW> v1;
-#pragma unroll
-                for (int j = 0; j < BW; j++) eval_first(h, fv[0].x[j], ft[0].x[j], V.x[j], v1.x[j]);
-#pragma unroll
-                for (int q = 1; q < kEagerFanins; q++)
-                    if ((uint32_t)q <= nfold)
-#pragma unroll
-                        for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv[q].x[j], ft[q].x[j]);
-                for (uint32_t jj = kEagerFanins; jj <= nfold; jj++) {
-                    Vec<BW> xv, xt;
-                    fetch(fanin_id(r, edges, jj), xv, xt);
-#pragma unroll
-                    for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], xv.x[j], xt.x[j]);
-                }
-#pragma unroll
-                for (int j = 0; j < BW; j++) {
-                    eval_finish(h, V.x[j], v1.x[j], T.x[j]);
-                    V.x[j] &= wm.x[j];
-                    T.x[j] &= wm.x[j];
-                    M.x[j] = (h & RF_MARKF0) ? (T.x[j] & m0.x[j]) : 0u;
-                }
             }
-            if (MODE == FWD_SIM || (h & RF_INPT) || MODE == FWD_MARK) {
 #pragma unroll
-                for (int j = 0; j < BW; j++) M.x[j] = 0;
-            }
+            for (int j = 0; j < BW; j++) M.x[j] = 0;
             if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
                 if (h & RF_INPT) {
                     M = T;
-                } else if (MODE == FWD_MARK && (h & RF_MARKF0) && vany(T)) {
-                    const uint32_t f0 = r.w[3];
-                    const Vec<BW> m0 =
-                        f0 >= ring_lo ? vld<BW>(rM + (f0 & Rm) * BW) : vld<BW>(a.M + (size_t)f0 * a.ld + w0);
+                } else if (h & RF_MARKF0) {
 #pragma unroll
                     for (int j = 0; j < BW; j++) M.x[j] = T.x[j] & m0.x[j];
-                }
-                if (!(h & RF_INPT) && (h & RF_SENS) && vany(M)) {
-                    const Vec<BW> sv = sens_any<BW, ROBUST>(r, edges, rec_nfi(r), M, fetch);
+                    if ((h & RF_SENS) && vany(M)) {
+                        const Vec<BW> sv = sens_any<BW, ROBUST>(r, edges, rec_nfi(r), M, fetch);
 #pragma unroll
-                    for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
+                        for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
+                    }
                 }
             }
             const size_t o = (size_t)g * a.ld + w0;
@@ -426,6 +510,14 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
             }
         }
         if (__syncthreads_or(any) && threadIdx.x == 0) S.pbits[i >> 5] |= 1u << (i & 31);
+        P0 = P1;
+        P1 = P2;
+    }
+    if (failed) {
+        // wait (bounded) for the record copies still in flight, then report
+        for (uint32_t b = 0; b < 3; b++)
+            if ((inflight >> b) & 1u) (void)mbar_wait(S.mbar + b, (phase >> b) & 1u);
+        cp_async_wait_all();
     }
     if (failed) {
         if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
@@ -878,3 +970,4 @@ cudaError_t launch_batch_end(DevAcc *acc, uint64_t n_pairs, cudaStream_t st) {
     k_batch_end<<<1, 1, 0, st>>>(acc, n_pairs);
     return cudaGetLastError();
 }
+

@@ -27,6 +27,7 @@ struct FwdArgs {
     const Piece *pieces;          // level-ordered runs of gates (the staging unit)
     uint32_t n_pieces;
     uint32_t cap, ecap;           // gates / edge words per staging buffer
+    uint32_t farcap;              // far fan-in slots per prefetch buffer (0: no prefetch)
     const uint32_t *pi_v, *pi_t;  // [n_pi][pi_ld]
     uint64_t pi_ld;
     uint32_t *V, *T, *M;          // planes [n_gates][ld]
@@ -43,7 +44,7 @@ struct FwdArgs {
     uint32_t ring_gates;          // forward ring slots (power of two, or 0)
     uint32_t ring2_gates;         // reverse ring slots (power of two, or 0)
     // shared-memory byte offsets
-    uint32_t off_ring, off_rec, off_edge, off_bm, off_pbits, off_mbar;
+    uint32_t off_ring, off_rec, off_edge, off_slot, off_bm, off_pbits, off_mbar;
 };
 
 // Device error bits (DevAcc::err and the circuit's error word).
