@@ -30,7 +30,7 @@ FLAG_OVERFLOW = 1
 NONE = 0xFFFFFFFF
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "EOVERFLOW", 4: "ETIMEOUT", 5: "ECUDA",
-          6: "ENOTSUP", 7: "EBUSY", 8: "ENODEV"}
+          6: "ENOTSUP", 7: "EBUSY", 8: "ENODEV", 9: "ELIMIT"}
 
 
 class PdfError(RuntimeError):
@@ -118,6 +118,8 @@ ABI = [
                             C.c_uint64, C.c_void_p]),
     ("pdf_cover", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,
                             C.POINTER(Totals_t), C.c_void_p]),
+    ("pdf_cover_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
+                                    C.c_void_p, C.POINTER(Totals_t), C.c_void_p]),
     ("pdf_gen_netlist", C.c_int, [C.POINTER(GenParams_t), C.POINTER(C.c_void_p)]),
     ("pdf_netbuf_from", C.c_int, [C.POINTER(Netlist_t), C.POINTER(C.c_void_p)]),
     ("pdf_netbuf_view", None, [C.c_void_p, C.POINTER(Netlist_t)]),
@@ -475,6 +477,14 @@ def stage_cover(c: Circuit, s: State, mark, n_pairs, pair_base, stream: int = 0)
     tot = Totals_t()
     check(lib().pdf_cover(c.h, s.h, _addr(mark), n_pairs, mark.shape[1], pair_base, C.byref(tot),
                           C.c_void_p(stream)), "pdf_cover")
+    return tot
+
+
+def stage_cover_noalloc(c: Circuit, mark, n_pairs, pair_base, first_x, first_y, stream: int = 0) -> Totals_t:
+    """pdf_cover_noalloc: the chunk count with no allocation (fixed device scratch)."""
+    tot = Totals_t()
+    check(lib().pdf_cover_noalloc(c.h, _addr(mark), n_pairs, mark.shape[1], pair_base, _addr(first_x),
+                                  _addr(first_y), C.byref(tot), C.c_void_p(stream)), "pdf_cover_noalloc")
     return tot
 
 

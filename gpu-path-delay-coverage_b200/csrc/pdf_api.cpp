@@ -148,6 +148,7 @@ extern "C" const char *pdf_status_string(int s) {
         case PDF_ENOTSUP: return "not supported";
         case PDF_EBUSY: return "busy";
         case PDF_ENODEV: return "no CUDA device";
+        case PDF_ELIMIT: return "request exceeds the fixed scratch of an allocation-free call";
         default: return "unknown status";
     }
 }
@@ -1030,3 +1031,61 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
     return st2;
 }
 
+// Allocation-free variant of pdf_cover: the same kernels, with their scratch
+// carved from the fixed array g_cover_scratch (pdf_kernels.cu) instead of a
+// workspace.  Allocates nothing, frees nothing.  The first call on a device
+// looks the array's address up (noalloc_scratch).
+extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, uint64_t n_pairs, uint64_t ld,
+                                        uint64_t pair_base, const uint32_t *first_x, const uint32_t *first_y,
+                                        pdf_totals *chunk_total, void *stream) {
+    if (!c || !mark || !first_x || !first_y || !chunk_total || n_pairs == 0 || ld < (n_pairs + 31) / 32)
+        return PDF_EINVAL;
+    if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
+    const uint64_t W = (n_pairs + 31) / 32, n_blocks = (W + c->bw - 1) / c->bw;
+    const uint64_t bm_words = (c->info.n_gates + 31) / 32;
+    auto a256 = [](uint64_t x) { return (x + 255) & ~(uint64_t)255; };
+    const uint64_t o_maxlvl = a256(n_blocks * bm_words * 4);
+    const uint64_t o_active = o_maxlvl + a256(n_blocks * 4);
+    const uint64_t o_acc = o_active + a256(W * 4);
+    const uint64_t need = o_acc + a256(sizeof(DevAcc));
+    if (need > kNoAllocScratchBytes) return PDF_ELIMIT;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    unsigned char *base = nullptr;
+    PDF_CUDA(noalloc_scratch(c->device, &base));
+    uint32_t *nzb = reinterpret_cast<uint32_t *>(base);
+    uint32_t *maxlvl = reinterpret_cast<uint32_t *>(base + o_maxlvl);
+    uint32_t *active = reinterpret_cast<uint32_t *>(base + o_active);
+    DevAcc *acc = reinterpret_cast<DevAcc *>(base + o_acc);
+    // the array keeps the previous call's contents: clear the accumulator
+    PDF_CUDA(cudaMemsetAsync(acc, 0, sizeof(DevAcc), cs));
+    PDF_CUDA(launch_batch_begin(acc, cs));
+    PDF_CUDA(launch_bitmap_from_marks(c->dc, mark, ld, n_pairs, c->bw, nzb, maxlvl, (uint32_t)bm_words, cs));
+    CoverArgs ca{};
+    ca.c = c->dc;
+    ca.M = mark;
+    ca.ld = ld;
+    ca.nzb = nzb;
+    ca.blk_maxlvl = maxlvl;
+    ca.bm_words = (uint32_t)bm_words;
+    ca.bw = c->bw;
+    ca.first_x = first_x;
+    ca.first_y = first_y;
+    ca.n_pairs = n_pairs;
+    ca.pair_base = (uint32_t)pair_base;
+    ca.active = active;
+    ca.acc = acc;
+    ca.hash_cap = c->hash_cap;
+    PDF_CUDA(launch_cover(ca, c->cover_threads, cs));
+    PDF_CUDA(launch_batch_end(acc, n_pairs, cs));
+    DevAcc h{};
+    PDF_CUDA(cudaMemcpyAsync(&h, acc, sizeof h, cudaMemcpyDeviceToHost, cs));
+    PDF_CUDA(cudaStreamSynchronize(cs));
+    chunk_total->lo = h.batch_lo;
+    chunk_total->hi = h.batch_hi;
+    chunk_total->pairs = n_pairs;
+    chunk_total->flags = h.batch_flags;
+    chunk_total->reserved = 0;
+    return err_status(h.err);
+}

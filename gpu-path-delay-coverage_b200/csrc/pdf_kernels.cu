@@ -16,6 +16,8 @@
 //               pairs mark, in exact 128-bit integers.
 #include "pdf_kernels.cuh"
 
+#include <mutex>
+
 namespace {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
@@ -971,3 +973,37 @@ cudaError_t launch_batch_end(DevAcc *acc, uint64_t n_pairs, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Fixed scratch of pdf_cover_noalloc.
+//
+// Callers that may not enter the CUDA allocator (a host framework that owns
+// every device byte through its own pool, or a latency-bound loop where a
+// cudaMalloc could synchronise the device or fail under memory pressure) get
+// a cover call whose scratch is this file-scope array instead of memory
+// allocated per call.  Every GPU that loads the library holds it until the
+// process exits.  All calls on a device share it, so calls that overlap on
+// the GPU race.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_cover_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+unsigned char *g_scratch_addr[kMaxDevices] = {};
+}  // namespace
+
+// Device address of g_cover_scratch on `device`, which the caller has made
+// current.  In host code the array's name is only a host-side stand-in, so
+// its device address is looked up once per device and cached.
+cudaError_t noalloc_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_addr[device]) {
+        unsigned char *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_cover_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[device] = p;
+    }
+    *out = g_scratch_addr[device];
+    return cudaSuccess;
+}

@@ -89,6 +89,10 @@ cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uin
 cudaError_t launch_bitmap_from_marks(const DevCircuit &c, const uint32_t *M, uint64_t ld,
                                      uint64_t n_pairs, uint32_t bw, uint32_t *nzb,
                                      uint32_t *blk_maxlvl, uint32_t bm_words, cudaStream_t st);
+// Fixed scratch of pdf_cover_noalloc (a file-scope __device__ array).
+constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
+cudaError_t noalloc_scratch(int device, unsigned char **out);
+
 cudaError_t launch_batch_begin(DevAcc *acc, cudaStream_t st);
 cudaError_t launch_batch_end(DevAcc *acc, uint64_t n_pairs, cudaStream_t st);
 

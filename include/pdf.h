@@ -41,7 +41,8 @@ typedef enum pdf_status {
     PDF_ECUDA = 5,      /* a CUDA runtime call failed */
     PDF_ENOTSUP = 6,    /* feature not available in this build / on this device */
     PDF_EBUSY = 7,      /* resource in use (serving queue full, job still running) */
-    PDF_ENODEV = 8      /* no CUDA device */
+    PDF_ENODEV = 8,     /* no CUDA device */
+    PDF_ELIMIT = 9      /* request larger than the fixed scratch of pdf_cover_noalloc */
 } pdf_status;
 
 /* Gate type codes.  AND..XNOR must be 2..7: the reference indexes its robust
@@ -257,6 +258,30 @@ pdf_status pdf_merge(pdf_circuit *c, pdf_state *s, const uint32_t *sim_v,
 pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark,
                      uint64_t n_pairs, uint64_t ld, uint64_t pair_base,
                      pdf_totals *chunk_total, void *stream);
+
+/*
+ * pdf_cover without any allocation.  No counterpart in the reference (whose
+ * gpuCountPaths allocates per chunk, coverkernel.cuh:256-275).
+ *
+ * For callers that may not enter the CUDA allocator while they grade: a host
+ * framework that owns all device memory through its own pool, or a
+ * latency-bound loop in which a cudaMalloc could synchronise the device or
+ * fail under memory pressure.  The circuit is created once beforehand
+ * (pdf_circuit_create allocates); this call then allocates and frees nothing.
+ * Its scratch is one fixed array of 8 MiB in device memory, held by every GPU
+ * that loads the library until the process exits; a chunk needs
+ * ceil(ceil(n_pairs/32)/tile_words) * ceil(n_gates/32) * 4 bytes of it plus a
+ * few KiB, and larger requests return PDF_ELIMIT.  The caller passes the
+ * pruned mark plane (as pdf_cover) and the first-detect ids as device arrays
+ * of n_gates uint32 (for example copied out with pdf_state_first_copy); the
+ * chunk's count is returned in *chunk_total (the call waits for it).
+ * The first call on each device looks up the array's device address; make
+ * that first call before any stream capture.  All calls on a device share the
+ * array, so calls that overlap on the GPU race: serialise them.
+ */
+pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, uint64_t n_pairs, uint64_t ld,
+                             uint64_t pair_base, const uint32_t *first_x, const uint32_t *first_y,
+                             pdf_totals *chunk_total, void *stream);
 
 /* ---- synthetic inputs (seeded, host-side) ---- */
 
