@@ -78,7 +78,7 @@ struct DeviceGuard {
 // Per-batch device workspace (owned by a state, or by a circuit for the
 // stage calls).
 struct Workspace {
-    DevBuf nzb, maxlvl, active;
+    DevBuf nzb, maxlvl, active, active_list;
     DevBuf planes;   // internal V, T, M planes when the caller gives none
     DevBuf pi;       // staged host pairs
     uint64_t plane_ld = 0, plane_words = 0;
@@ -86,6 +86,7 @@ struct Workspace {
         nzb.release();
         maxlvl.release();
         active.release();
+        active_list.release();
         planes.release();
         pi.release();
     }
@@ -95,14 +96,13 @@ struct pdf_circuit {
     int device = 0;
     int mark_mode = PDF_MARK_DEFAULT;
     pdf_circuit_info info{};
-    DevBuf rec, edges, level_off, pieces, err;
+    DevBuf rec, edges, level_off, pieces, far, err;
     DevCircuit dc{};
-    uint32_t bw = 4, threads = 512, ring = 0, ring2 = 0;
+    uint32_t bw = 4, threads = 512, ring = 0, ring2 = 0, farcap = 0;
     uint32_t cap = 512, ecap = 2048, n_pieces = 0, bm_shared = 0;
-    uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_slot = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
-    uint32_t farcap = 0;
+    uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
     size_t fwd_smem = 0;
-    uint32_t hash_cap = 4096, cover_threads = 256;
+    uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
     Workspace stage;  // scratch of the stage calls
     std::mutex mu;    // serialises the stage scratch
 };
@@ -279,6 +279,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     DeviceGuard dg(o.device);
     if (!dg.ok) return PDF_ECUDA;
 
+    // source words address gates with 31 bits and slots with 30 (pdf_device.cuh)
+    if (nl->n_gates >= SRC_FAR) return PDF_ENOTSUP;
     pdf_circuit *c = new (std::nothrow) pdf_circuit();
     if (!c) return PDF_ENOMEM;
     c->device = o.device;
@@ -318,8 +320,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         std::memset(&r, 0, sizeof r);
         r.w[0] = make_rec_header(nl->type[g], nl->po[g], nl->nfi[g]);
         r.w[1] = nl->nfo[g];
-        r.w[2] = (uint32_t)eoff[g];
-        for (uint32_t j = 0; j < nl->nfi[g] && j < (uint32_t)kInlineFanins; j++) r.w[3 + j] = edges[eoff[g] + j];
+        r.w[2] = (uint32_t)eoff[g];  // w[3..6]: source words, set with the launch plan below
     }
 
     // Launch plan: CTAs of `threads` threads own `bw` words of pairs; two
@@ -330,27 +331,22 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         return PDF_ECUDA;
     }
     c->bw = o.tile_words ? o.tile_words : 4;
-    // one thread per gate of a piece; 8-word tiles need twice the registers
     const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
-    uint32_t widest_g = 1;
-    for (uint32_t l = 1; l < L; l++) widest_g = std::max(widest_g, nl->level_offsets[l + 1] - nl->level_offsets[l]);
-    if (L == 1) widest_g = inf.max_level_width;
-    const uint32_t cap_guess = std::min<uint32_t>(512, (widest_g + 31) & ~31u);
-    c->threads = o.threads ? std::min(o.threads, max_threads)
-                           : std::min(max_threads, std::max<uint32_t>(128, (cap_guess + 31) & ~31u));
+    c->threads = o.threads ? std::min(o.threads, max_threads) : 512;
     const size_t budget = c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
                                       : std::min<size_t>(prop.sharedMemPerBlockOptin,
                                                          prop.sharedMemPerMultiprocessor / 2 - 2048);
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
-    // piece size from the widest level above the inputs (the inputs' level,
-    // often the widest, just splits into more pieces)
+    // Pieces (the kernels' unit of staging and of synchronisation), sized
+    // from the widest level above the inputs (the inputs' level, often the
+    // widest, just splits into more pieces): runs of one level, <= cap gates,
+    // edge slice <= ecap words.
     uint32_t widest = 1;
     for (uint32_t l = 1; l < L; l++) widest = std::max(widest, nl->level_offsets[l + 1] - nl->level_offsets[l]);
     if (L == 1) widest = inf.max_level_width;
     c->cap = std::min<uint32_t>(512, (widest + 31) & ~31u);
     c->ecap = 2048;
-    // pieces: runs of one level, <= cap gates, edge slice <= ecap words
     std::vector<Piece> pieces;
     auto f4 = [](uint64_t x) { return x & ~(uint64_t)3; };
     auto c4 = [](uint64_t x) { return (x + 3) & ~(uint64_t)3; };
@@ -378,77 +374,102 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         delete c;
         return PDF_ENOTSUP;
     }
-    // Shared memory of k_forward: 3 record buffers; one region shared by the
-    // reverse pass's 2 edge buffers and the forward pass's 2 far-fan-in
-    // buffers (+ their slot table); bitmap; piece bits; barriers; the ring.
-    size_t off = 0;
-    c->off_rec = (uint32_t)off;
-    off += al(3 * (size_t)c->cap * sizeof(GateRec));
-    // Ring size and far-buffer capacity from the netlist: for each candidate
-    // ring (largest first), the most far fan-ins any piece prefetches; take
-    // the largest ring whose far buffer fits beside it.
-    auto far_bytes = [&](uint32_t fc) { return 2 * 3 * (size_t)fc * c->bw * 4; };
-    const size_t fixed = al(3 * (size_t)c->cap * sizeof(GateRec)) + al(2 * (size_t)c->cap * 4 * sizeof(uint16_t)) +
-                         ((size_t)bm_words * 4 <= 16384 ? al((size_t)bm_words * 4) : 0) +
-                         al(((size_t)c->n_pieces + 31) / 32 * 4) + 128;
-    auto far_count = [&](uint32_t R) {
+    // Far fan-ins of piece i (ring of R slots): fan-ins 0..3 of its gates
+    // below b_i - R.  Those below a_{i-1} (complete when piece i - 1 starts)
+    // go to the piece's deduplicated far list, up to `limit` entries; the rest
+    // are read from their plane rows.  Fills the source words w[3..6].
+    std::vector<uint32_t> far_ids;
+    auto far_lists = [&](uint32_t R, uint32_t limit) -> uint32_t {
         uint32_t worst = 0;
-        for (size_t i = 1; i < pieces.size(); i++) {
-            const Piece &p = pieces[i];
-            const uint32_t lo = R ? (p.b > R ? p.b - R : 0) : p.b, fin = pieces[i - 1].a;
-            uint32_t n = 0;
+        far_ids.clear();
+        std::vector<uint32_t> seen(G, 0xFFFFFFFFu);  // gate -> slot in the current piece's list
+        std::vector<uint32_t> list;
+        for (size_t i = 0; i < pieces.size(); i++) {
+            Piece &p = pieces[i];
+            const uint32_t lo = p.b > R ? p.b - R : 0;
+            const uint32_t done = i ? pieces[i - 1].a : 0;
+            list.clear();
             for (uint32_t g = p.a; g < p.b; g++) {
-                const uint32_t h = make_rec_header(nl->type[g], nl->po[g], nl->nfi[g]);
-                if (h & RF_INPT) continue;
-                const uint32_t nq = std::min<uint32_t>(hdr_nfold(h) + 1, 4);
+                const uint32_t nq = std::min<uint32_t>(nl->nfi[g], kInlineFanins);
                 for (uint32_t q = 0; q < nq; q++) {
                     const uint32_t f = edges[eoff[g] + q];
-                    n += (f < lo && f < fin) ? 1 : 0;
+                    uint32_t sw = f & (R - 1);
+                    if (f < lo) {
+                        sw = SRC_PLANE | f;
+                        if (f < done) {
+                            if (seen[f] == 0xFFFFFFFFu && list.size() < limit) {
+                                seen[f] = (uint32_t)list.size();
+                                list.push_back(f);
+                            }
+                            if (seen[f] != 0xFFFFFFFFu) sw = SRC_FAR | seen[f];
+                        }
+                    }
+                    recs[g].w[3 + q] = sw;
                 }
             }
-            worst = std::max(worst, n);
+            for (uint32_t f : list) seen[f] = 0xFFFFFFFFu;
+            worst = std::max<uint32_t>(worst, (uint32_t)list.size());
+            p.far_off = (uint32_t)far_ids.size();
+            p.far_n = (uint32_t)list.size();
+            far_ids.insert(far_ids.end(), list.begin(), list.end());
         }
         return worst;
     };
-    uint32_t ring = 0, farcap = 0;
-    uint32_t rmax = 1;
-    while ((size_t)rmax * 2 * c->bw * 12 <= budget) rmax *= 2;
-    for (uint32_t R = rmax; R >= 32; R /= 2) {
-        const uint32_t fc = std::min<uint32_t>((far_count(R) + 31) & ~31u, 4096);
-        const size_t need = fixed + al(std::max(2 * (size_t)c->ecap * 4, far_bytes(fc))) + (size_t)R * c->bw * 12;
-        if (need <= budget) {
-            ring = R;
-            farcap = fc;
-            break;
-        }
+    // Shared memory of k_forward: 2 record buffers; one region holding the
+    // reverse pass's 2 edge buffers or the forward pass's 2 far buffers;
+    // bitmap; piece bits; barriers; the ring.  The ring: the largest power of
+    // two (>= cap, <= 2 * n_gates) that leaves room for far lists of 64
+    // entries; the far lists then get the rest of the budget.
+    const size_t rec_bytes = al(2 * (size_t)c->cap * sizeof(GateRec));
+    const size_t bm_bytes = (size_t)bm_words * 4 <= 16384 ? al((size_t)bm_words * 4) : 0;
+    const size_t fixed = rec_bytes + bm_bytes + al(((size_t)c->n_pieces + 31) / 32 * 4) + 128;
+    const size_t edge_bytes = 2 * (size_t)c->ecap * 4;
+    const size_t far_entry = (size_t)2 * 3 * c->bw * 4;  // one far slot in both buffers, 3 planes
+    uint32_t rmin = 32;
+    while (rmin < c->cap) rmin *= 2;
+    uint32_t rmax = rmin;
+    while ((uint64_t)rmax < 2 * (uint64_t)G && fixed + (size_t)rmax * 2 * c->bw * 12 <= budget) rmax *= 2;
+    uint32_t ring = 0;
+    for (uint32_t R = rmax; R >= rmin && !ring; R /= 2)
+        if (fixed + al(std::max(edge_bytes, 64 * far_entry)) + (size_t)R * c->bw * 12 <= budget) ring = R;
+    if (!ring) {
+        delete c;
+        return PDF_ENOTSUP;
     }
+    const size_t far_room = budget - fixed - (size_t)ring * c->bw * 12;
+    const uint32_t far_limit = (uint32_t)std::min<size_t>(kMaxFar, (far_room & ~(size_t)127) / far_entry) & ~3u;
+    const uint32_t farcap = std::max<uint32_t>(4, (far_lists(ring, far_limit) + 3) & ~3u);
+    if (far_ids.empty()) far_ids.push_back(0);
+    c->ring = ring;
     c->farcap = farcap;
+    size_t off = 0;
+    c->off_rec = (uint32_t)off;
+    off += rec_bytes;
     c->off_edge = (uint32_t)off;
-    off += al(std::max(2 * (size_t)c->ecap * 4, far_bytes(c->farcap)));
-    c->off_slot = (uint32_t)off;
-    off += al(2 * (size_t)c->cap * 4 * sizeof(uint16_t));
-    c->bm_shared = (size_t)bm_words * 4 <= 16384 ? 1u : 0u;
+    off += al(std::max(edge_bytes, farcap * far_entry));
+    c->bm_shared = bm_bytes ? 1u : 0u;
     c->off_bm = (uint32_t)off;
-    if (c->bm_shared) off += al((size_t)bm_words * 4);
+    off += bm_bytes;
     c->off_pbits = (uint32_t)off;
     off += al(((size_t)c->n_pieces + 31) / 32 * 4);
     c->off_mbar = (uint32_t)off;
     off += 128;
     c->off_ring = (uint32_t)off;
-    c->ring = ring;
     uint32_t ring2 = 0;
-    for (uint32_t r = 1; ring && (size_t)r * c->bw * 4 <= (size_t)ring * c->bw * 12; r *= 2) ring2 = r;
+    for (uint32_t r = 1; (size_t)r * c->bw * 4 <= (size_t)ring * c->bw * 12; r *= 2) ring2 = r;
     c->ring2 = ring2;
     c->fwd_smem = off + (size_t)ring * c->bw * 12;
     c->hash_cap = 4096;
     while (c->hash_cap > 64 && cover_smem_bytes(c->hash_cap) > prop.sharedMemPerBlockOptin) c->hash_cap /= 2;
     c->cover_threads = 256;
+    c->cover_grid = (uint32_t)prop.multiProcessorCount;
 
     auto fail = [&](pdf_status st2) {
         c->rec.release();
         c->edges.release();
         c->level_off.release();
         c->pieces.release();
+        c->far.release();
         c->err.release();
         delete c;
         return st2;
@@ -456,7 +477,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     if (c->rec.ensure(sizeof(GateRec) * G) != cudaSuccess ||
         c->edges.ensure(sizeof(uint32_t) * edges.size()) != cudaSuccess ||
         c->level_off.ensure(sizeof(uint32_t) * (L + 1)) != cudaSuccess ||
-        c->pieces.ensure(sizeof(Piece) * pieces.size()) != cudaSuccess || c->err.ensure(16) != cudaSuccess) {
+        c->pieces.ensure(sizeof(Piece) * pieces.size()) != cudaSuccess ||
+        c->far.ensure(sizeof(uint32_t) * far_ids.size()) != cudaSuccess || c->err.ensure(16) != cudaSuccess) {
         (void)cudaGetLastError();
         return fail(PDF_ENOMEM);
     }
@@ -466,6 +488,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         cudaMemcpy(c->level_off.p, nl->level_offsets, sizeof(uint32_t) * (L + 1), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMemcpy(c->pieces.p, pieces.data(), sizeof(Piece) * pieces.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(c->far.p, far_ids.data(), sizeof(uint32_t) * far_ids.size(), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMemset(c->err.p, 0, 16) != cudaSuccess) {
         (void)cudaGetLastError();
@@ -480,7 +504,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     inf.tile_words = c->bw;
     inf.threads = c->threads;
     inf.max_pairs = o.max_pairs ? o.max_pairs : 65536;
-    inf.device_bytes = c->rec.bytes + c->edges.bytes + c->level_off.bytes + c->pieces.bytes;
+    inf.device_bytes = c->rec.bytes + c->edges.bytes + c->level_off.bytes + c->pieces.bytes + c->far.bytes;
     *out = c;
     return PDF_OK;
 }
@@ -493,6 +517,7 @@ extern "C" void pdf_circuit_destroy(pdf_circuit *c) {
     c->edges.release();
     c->level_off.release();
     c->pieces.release();
+    c->far.release();
     c->err.release();
     delete c;
 }
@@ -653,7 +678,9 @@ pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes
     const uint64_t bm_words = (c->info.n_gates + 31) / 32;
     PDF_CUDA(ws.nzb.ensure(n_blocks * bm_words * 4));
     PDF_CUDA(ws.maxlvl.ensure(n_blocks * 4));
-    PDF_CUDA(ws.active.ensure(W * 4));
+    // active bitmap [W], then the count; the list holds <= 2 pairs per gate
+    PDF_CUDA(ws.active.ensure(W * 4 + 16));
+    PDF_CUDA(ws.active_list.ensure(std::min<uint64_t>(W * 32, 2 * (uint64_t)c->info.n_gates) * 4));
     if (need_planes) {
         const uint64_t ld = n_blocks * c->bw;
         if (ws.plane_ld < ld || !ws.planes.p) {
@@ -675,13 +702,13 @@ FwdArgs base_fwd(pdf_circuit *c, uint64_t n_pairs) {
     a.W = (uint32_t)((n_pairs + 31) / 32);
     a.bm_words = (c->info.n_gates + 31) / 32;
     a.bm_shared = c->bm_shared;
+    a.far_ids = c->far.as<uint32_t>();
+    a.farcap = c->farcap;
     a.ring_gates = c->ring;
     a.ring2_gates = c->ring2;
     a.off_ring = c->off_ring;
     a.off_rec = c->off_rec;
     a.off_edge = c->off_edge;
-    a.off_slot = c->off_slot;
-    a.farcap = c->farcap;
     a.off_bm = c->off_bm;
     a.off_pbits = c->off_pbits;
     a.off_mbar = c->off_mbar;
@@ -704,6 +731,8 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
     a.n_pairs = n_pairs;
     a.pair_base = pair_base;
     a.active = ws.active.as<uint32_t>();
+    a.active_count = a.active + (n_pairs + 31) / 32;
+    a.active_list = ws.active_list.as<uint32_t>();
     a.acc = acc;
     a.hash_cap = c->hash_cap;
     return a;
@@ -832,7 +861,7 @@ pdf_status grade_cover_locked(pdf_circuit *c, pdf_state *s, cudaStream_t cs) {
     CoverArgs ca = base_cover(c, s->ws, s->pend_M, s->pend_ld, s->pend_n, base, s->first_x.as<uint32_t>(),
                               s->first_y.as<uint32_t>(), acc);
     if (s->pe) PDF_CUDA(cudaEventRecord(s->pe->ev[2], cs));  // cover starts (after any exchange)
-    PDF_CUDA(launch_cover(ca, c->cover_threads, cs));
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
     PDF_CUDA(launch_batch_end(acc, s->pend_n, cs));
     if (s->pe) {
         PDF_CUDA(cudaEventRecord(s->pe->ev[3], cs));
@@ -1013,7 +1042,7 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
                                       s->ws.maxlvl.as<uint32_t>(), (c->info.n_gates + 31) / 32, cs));
     CoverArgs ca = base_cover(c, s->ws, mark, ld, n_pairs, (uint32_t)pair_base, s->first_x.as<uint32_t>(),
                               s->first_y.as<uint32_t>(), acc);
-    PDF_CUDA(launch_cover(ca, c->cover_threads, cs));
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
     PDF_CUDA(launch_batch_end(acc, n_pairs, cs));
     PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));
@@ -1046,7 +1075,8 @@ extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, ui
     auto a256 = [](uint64_t x) { return (x + 255) & ~(uint64_t)255; };
     const uint64_t o_maxlvl = a256(n_blocks * bm_words * 4);
     const uint64_t o_active = o_maxlvl + a256(n_blocks * 4);
-    const uint64_t o_acc = o_active + a256(W * 4);
+    const uint64_t o_list = o_active + a256(W * 4 + 16);
+    const uint64_t o_acc = o_list + a256(std::min<uint64_t>(W * 32, 2 * (uint64_t)c->info.n_gates) * 4);
     const uint64_t need = o_acc + a256(sizeof(DevAcc));
     if (need > kNoAllocScratchBytes) return PDF_ELIMIT;
     DeviceGuard dg(c->device);
@@ -1057,6 +1087,7 @@ extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, ui
     uint32_t *nzb = reinterpret_cast<uint32_t *>(base);
     uint32_t *maxlvl = reinterpret_cast<uint32_t *>(base + o_maxlvl);
     uint32_t *active = reinterpret_cast<uint32_t *>(base + o_active);
+    uint32_t *active_list = reinterpret_cast<uint32_t *>(base + o_list);
     DevAcc *acc = reinterpret_cast<DevAcc *>(base + o_acc);
     // the array keeps the previous call's contents: clear the accumulator
     PDF_CUDA(cudaMemsetAsync(acc, 0, sizeof(DevAcc), cs));
@@ -1075,9 +1106,11 @@ extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, ui
     ca.n_pairs = n_pairs;
     ca.pair_base = (uint32_t)pair_base;
     ca.active = active;
+    ca.active_count = active + W;
+    ca.active_list = active_list;
     ca.acc = acc;
     ca.hash_cap = c->hash_cap;
-    PDF_CUDA(launch_cover(ca, c->cover_threads, cs));
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
     PDF_CUDA(launch_batch_end(acc, n_pairs, cs));
     DevAcc h{};
     PDF_CUDA(cudaMemcpyAsync(&h, acc, sizeof h, cudaMemcpyDeviceToHost, cs));

@@ -27,11 +27,18 @@ typedef unsigned __int128 pdf_u128;
 //   w[0] = type | po << 4 | nfi << 8 | RF_* flags (bits 16..22) | nfold << 24
 //   w[1] = nfo
 //   w[2] = edge offset: fan-ins at edges[w2 + j], fan-outs at edges[w2 + nfi + k]
-//   w[3..7] = fan-ins 0..4 inline (the rest only in edges[])
+//   w[3..6] = where the forward kernel reads fan-ins 0..3 (source words):
+//          SRC_PLANE | f   the plane row of gate f in global memory
+//          SRC_FAR | s     slot s of the piece's far buffer (prefetched)
+//          s               slot s of the shared-memory ring of recent gates
+//   w[7] = 0
+// Fan-ins past the fourth are read from edges[] (ring or plane row).
 struct __align__(16) GateRec {
     uint32_t w[8];
 };
-static constexpr int kInlineFanins = 5;
+static constexpr int kInlineFanins = 4;
+static constexpr uint32_t SRC_PLANE = 0x80000000u, SRC_FAR = 0x40000000u, SRC_IDX = 0x3FFFFFFFu;
+static constexpr uint32_t kMaxFar = 1024;  // far-buffer slots per piece at most
 
 // Per-gate evaluation flags, derived once from (type, nfi) so that the
 // kernels evaluate every gate with the same branch-free instruction sequence
@@ -156,12 +163,62 @@ PDF_HD uint32_t sens(uint32_t type, uint32_t onV, uint32_t onT, uint32_t offV, u
     }
 }
 
+// The side-input test of a multi-input gate, OR over on-path candidates i
+// of AND over side inputs x != i of sens(on = i, off = x)
+// (markkernel.cuh:253-261 with robust()/nonrobust(), :43-72), in one pass
+// over the fan-ins.  Every table above factors as
+//   sens(i, x) = A1(i) & B1(x) | A2(i) & B2(x),   A1 & A2 = 0
+//   AND/NAND LUT_R : A1 = T,        B1 = V & ~T     (A2 = 0)
+//   OR/NOR   LUT_R : A1 = T,        B1 = ~V & ~T    (A2 = 0)
+//   AND/NAND LUT_NR: A1 = T & ~V,   B1 = V;         A2 = T & V,  B2 = V & ~T
+//   OR/NOR   LUT_NR: A1 = T & ~V,   B1 = ~V & ~T;   A2 = T & V,  B2 = ~V
+// so AND_{x != i} sens(i, x) = A1(i) & E1(i) | A2(i) & E2(i) with
+// Ek(i) = AND_{x != i} Bk(x) = Z0k | (Z1k & ~Bk(i)), where Z0k holds the
+// pairs with no zero among all Bk(x) and Z1k those with exactly one.  The
+// result is then Z0k & OR_i Ak(i) | Z1k & OR_i (Ak(i) & ~Bk(i)) over k.
+struct SensAcc {
+    uint32_t z0[2], z1[2], a[2], an[2];
+};
+PDF_HD void sens_init(SensAcc &s) {
+    for (int k = 0; k < 2; k++) {
+        s.z0[k] = 0xFFFFFFFFu;
+        s.z1[k] = 0;
+        s.a[k] = 0;
+        s.an[k] = 0;
+    }
+}
+PDF_HD void sens_term(SensAcc &s, int k, uint32_t A, uint32_t B) {
+    const uint32_t n = ~B;
+    s.z1[k] = (s.z1[k] & B) | (s.z0[k] & n);
+    s.z0[k] &= B;
+    s.a[k] |= A;
+    s.an[k] |= A & n;
+}
+// Fan-in with value bit-planes (V, T).
+template <int ROBUST>
+PDF_HD void sens_step(SensAcc &s, bool or_like, uint32_t V, uint32_t T) {
+    if (ROBUST) {
+        sens_term(s, 0, T, (or_like ? ~V : V) & ~T);
+    } else {
+        sens_term(s, 0, T & ~V, or_like ? (~V & ~T) : V);
+        sens_term(s, 1, T & V, or_like ? ~V : (V & ~T));
+    }
+}
+template <int ROBUST>
+PDF_HD uint32_t sens_result(const SensAcc &s) {
+    uint32_t r = (s.z0[0] & s.a[0]) | (s.z1[0] & s.an[0]);
+    if (!ROBUST) r |= (s.z0[1] & s.a[1]) | (s.z1[1] & s.an[1]);
+    return r;
+}
+
 // A run of gates of one level, the unit of staging and of synchronisation.
 struct __align__(16) Piece {
     uint32_t a, b;     // gates [a, b)
     uint32_t ea, eb;   // edge slice [ea, eb) to stage (16-byte aligned), or ea = eb = ~0: not staged
     uint32_t level;
-    uint32_t pad[3];
+    uint32_t far_off;  // its far fan-ins: far_ids[far_off .. far_off + far_n)
+    uint32_t far_n;    // <= kMaxFar
+    uint32_t pad;
 };
 
 // Saturating 128-bit add; sets *ovf on overflow.

@@ -6,10 +6,10 @@
 // the only dependency between pairs is the first-detect minimum, so column
 // blocks never wait on one another and no grid-wide barrier is needed.
 //
-//   k_forward   sim + forward robust mark (levels ascending, one
-//               __syncthreads per level), then, in the same CTA, the
-//               prune + first-detect merge over the gates whose marks are
-//               nonzero (levels descending).
+//   k_forward   sim + forward robust mark (levels ascending, warps as
+//               dataflow: each gate waits only for its own fan-ins), then,
+//               in the same CTA, the prune (levels descending) and the
+//               first-detect merge over the gates whose marks are nonzero.
 //   k_active / k_active_compact / k_cover
 //               path counting, only for pairs that first-detect some net
 //               (every other pair credits nothing), over only the nets those
@@ -35,17 +35,6 @@ __device__ __forceinline__ GateRec load_rec(const GateRec *p) {
     r.w[6] = b.z;
     r.w[7] = b.w;
     return r;
-}
-
-__device__ __forceinline__ uint32_t fanin_id(const GateRec &r, const uint32_t *edges, uint32_t j) {
-    switch (j) {
-        case 0: return r.w[3];
-        case 1: return r.w[4];
-        case 2: return r.w[5];
-        case 3: return r.w[6];
-        case 4: return r.w[7];
-        default: return __ldg(edges + r.w[2] + j);
-    }
 }
 
 // Set bit g of a bitmap with one atomic per distinct word among the calling
@@ -104,7 +93,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t phase) {
     return false;
 }
 
-// Asynchronous global -> shared copies of BW words (cp.async, completed by
+// Asynchronous global -> shared copy of BW words (cp.async, completed by
 // cp.async.wait_all in the issuing thread).
 template <int BW>
 __device__ __forceinline__ void cp_async_vec(uint32_t *dst, const uint32_t *src) {
@@ -119,20 +108,17 @@ __device__ __forceinline__ void cp_async_vec(uint32_t *dst, const uint32_t *src)
                          : "memory");
     }
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Shared-memory layout of k_forward (byte offsets from the host plan).
 struct FwdSmem {
-    uint32_t *ring;      // forward: [R][3][BW] (V, T, M); reverse: [R2][BW] pruned marks
-    GateRec *rec;        // [3][cap] staged gate records of a piece
-    uint32_t *edge;      // [2][ecap] staged edge slices (reverse pass; shares memory with far)
-    uint32_t *far;       // [2][3][farcap][BW] prefetched far fan-in V, T, M (forward pass)
-    uint16_t *slot;      // [2][cap][kPrefetchFanins] far-buffer slot of each fan-in (0xFFFF: none)
-    uint32_t *bm;        // nonzero-mark bitmap (shared or global)
-    uint32_t *pbits;     // pieces that hold a forward mark
-    uint32_t *farcnt;    // [2] far slots handed out
-    uint64_t *mbar;      // [3]
+    uint32_t *ring;   // forward: [3][R][BW] V, T, M; reverse: [R2][BW] pruned marks
+    GateRec *rec;     // [2][cap] staged gate records of a piece
+    uint32_t *edge;   // reverse: [2][ecap] staged edge slices
+    uint32_t *far;    // forward: [2][3][farcap][BW] far fan-in V, T, M (same memory as edge)
+    uint32_t *bm;     // nonzero-mark bitmap (shared or global)
+    uint32_t *pbits;  // pieces that hold a forward mark
+    uint64_t *mbar;   // [2]
 };
 
 // Stage piece `p` into buffer `buf`: its gate records and, for the reverse
@@ -196,6 +182,24 @@ __device__ __forceinline__ Vec<BW> vldg(const uint32_t *p) {  // read-only data 
     }
     return v;
 }
+// BW words from shared memory at byte address sa (ld.shared, 16-byte
+// vectors; sa a multiple of 4 * BW).
+template <int BW>
+__device__ __forceinline__ Vec<BW> vlds(uint32_t sa) {
+    Vec<BW> v;
+    if constexpr (BW == 1) {
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v.x[0]) : "r"(sa));
+    } else if constexpr (BW == 2) {
+        asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x[0]), "=r"(v.x[1]) : "r"(sa));
+    } else {
+#pragma unroll
+        for (int i = 0; i < BW; i += 4)
+            asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(v.x[i]), "=r"(v.x[i + 1]), "=r"(v.x[i + 2]), "=r"(v.x[i + 3])
+                         : "r"(sa + 4u * i));
+    }
+    return v;
+}
 template <int BW>
 __device__ __forceinline__ void vst(uint32_t *p, const Vec<BW> &v) {
     if constexpr (BW == 1) {
@@ -216,319 +220,34 @@ __device__ __forceinline__ bool vany(const Vec<BW> &v) {
     return o != 0;
 }
 
-// Rarely needed: OR over on-path candidates i of AND over side inputs x != i
-// of the sensitisation test (markkernel.cuh:253-261 with robust()/
-// nonrobust(), :43-72), restricted to the pairs in `need`.
+// The side-input test of a marked multi-input gate (markkernel.cuh:253-261
+// with robust()/nonrobust(), :43-72) in one pass over its nfi fan-ins
+// (sens_step, pdf_device.cuh).  fetch(q, V, T) reads fan-in q.
 template <int BW, int ROBUST, class Fetch>
-__device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, const uint32_t *edges, uint32_t nfi,
-                                            const Vec<BW> &need, Fetch fetch) {
+__device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, uint32_t nfi, Fetch fetch) {
     const bool or_like = (r.w[0] & RF_IM) != 0;
-    Vec<BW> acc;
+    SensAcc acc[BW];
 #pragma unroll
-    for (int j = 0; j < BW; j++) acc.x[j] = 0;
-    for (uint32_t i = 0; i < nfi; i++) {
-        uint32_t left = 0;
+    for (int j = 0; j < BW; j++) sens_init(acc[j]);
+    for (uint32_t q = 0; q < nfi; q++) {
+        Vec<BW> v, t;
+        fetch(q, v, t);
 #pragma unroll
-        for (int j = 0; j < BW; j++) left |= need.x[j] & ~acc.x[j];
-        if (!left) break;
-        Vec<BW> iv, it;
-        fetch(fanin_id(r, edges, i), iv, it);
-        Vec<BW> term;
-#pragma unroll
-        for (int j = 0; j < BW; j++) term.x[j] = 0xFFFFFFFFu;
-        for (uint32_t x = 0; x < nfi; x++) {
-            if (x == i) continue;
-            Vec<BW> xv, xt;
-            fetch(fanin_id(r, edges, x), xv, xt);
-#pragma unroll
-            for (int j = 0; j < BW; j++) term.x[j] &= sens_class<ROBUST>(or_like, iv.x[j], it.x[j], xv.x[j], xt.x[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < BW; j++) acc.x[j] |= term.x[j];
+        for (int j = 0; j < BW; j++) sens_step<ROBUST>(acc[j], or_like, v.x[j], t.x[j]);
     }
-    return acc;
+    Vec<BW> out;
+#pragma unroll
+    for (int j = 0; j < BW; j++) out.x[j] = sens_result<ROBUST>(acc[j]);
+    return out;
 }
 
-// ---------------------------------------------------------------------------
-// Forward kernel: one CTA per column block of BW words (32 * BW pairs); one
-// thread per gate, carrying all BW words of the block.
-//
-// Gates are walked in pieces (runs of one level, <= cap gates) whose records
-// are staged into shared memory by a TMA bulk copy issued one piece ahead.
-//
-// Forward (sim + forward mark, simkernel.cuh:96-156, markkernel.cuh:215-270):
-// a ring of the last R gates' V, T, M words sits in shared memory
-// (slot = gate & (R - 1)).  During piece [a, b) a fan-in f is read from the
-// ring iff f >= b - R and only gates g >= b - R write it; within that window
-// no two gates share a slot, so a ring read always sees its own gate.  Older
-// fan-ins come from the global planes (written by this CTA and ordered by
-// __syncthreads).
-//
-// Reverse (prune, markkernel.cuh:271-293): only pieces that hold a forward
-// mark, descending, only gates whose bitmap bit is set.  Pruned marks of
-// recent gates sit in a second ring (the same memory, R2 slots of BW words):
-// during piece [a, b) a fan-out fo is read from it iff fo < a + R2 and only
-// gates g < a + R2 write it.
-//
-// Merge (mergekernel.cuh:116-198) needs no level order: one sweep over the
-// surviving marks folds the first falling / rising pair of every net into
-// first_x / first_y with atomicMin.
-//
-// Plane rows are read and written BW words at a time: ld and pi_ld are
-// multiples of BW and every row holds all n_blocks * BW words; words at or
-// past ceil(n_pairs / 32) are masked to zero.
-// ---------------------------------------------------------------------------
-constexpr int kPrefetchFanins = 4;  // fan-ins per gate eligible for the far-buffer prefetch
-
-template <int BW, int ROBUST, int MODE>
-__global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
-    extern __shared__ __align__(128) unsigned char smraw[];
-    FwdSmem S;
-    S.ring = reinterpret_cast<uint32_t *>(smraw + a.off_ring);
-    S.rec = reinterpret_cast<GateRec *>(smraw + a.off_rec);
-    S.edge = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
-    S.far = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
-    S.slot = reinterpret_cast<uint16_t *>(smraw + a.off_slot);
-    S.pbits = reinterpret_cast<uint32_t *>(smraw + a.off_pbits);
-    S.farcnt = reinterpret_cast<uint32_t *>(smraw + a.off_mbar + 64);
-    S.mbar = reinterpret_cast<uint64_t *>(smraw + a.off_mbar);
-    const uint32_t blk = blockIdx.x;
+// Reverse pass (prune) and merge of k_forward, after its forward pass.
+// `phase` carries the parity bits of the two record mbarriers.
+template <int BW, int MODE>
+__device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem &S, uint32_t blk, uint32_t *gbm,
+                                                uint32_t phase) {
     const uint32_t w0 = blk * BW;
-    S.bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
-    uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
     const uint32_t *edges = a.c.edges;
-    const uint32_t R = a.ring_gates, Rm = R - 1;
-    uint32_t *rV = S.ring, *rT = S.ring + (size_t)R * BW, *rM = S.ring + 2 * (size_t)R * BW;
-    const uint32_t farcap = a.farcap;
-    Vec<BW> wm;  // valid bits of each word of this block
-#pragma unroll
-    for (int j = 0; j < BW; j++) {
-        const uint32_t w = w0 + j;
-        wm.x[j] = w + 1 < a.W ? 0xFFFFFFFFu
-                              : (w + 1 == a.W ? ((a.n_pairs & 31) ? (1u << (a.n_pairs & 31)) - 1u : 0xFFFFFFFFu) : 0u);
-    }
-    // far buffer of parity p, plane k (0 V, 1 T, 2 M), slot s
-    auto farp = [&](uint32_t p, uint32_t k, uint32_t sl) -> uint32_t * {
-        return S.far + (((size_t)p * 3 + k) * farcap + sl) * BW;
-    };
-
-    if (MODE != FWD_SIM)
-        for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) S.bm[q] = 0;
-    for (uint32_t q = threadIdx.x; q < (a.n_pieces + 31) / 32; q += blockDim.x) S.pbits[q] = 0;
-    if (threadIdx.x == 0) {
-        mbar_init(S.mbar, 1);
-        mbar_init(S.mbar + 1, 1);
-        mbar_init(S.mbar + 2, 1);
-        fence_mbar_init();
-        S.farcnt[0] = S.farcnt[1] = 0;
-    }
-    __syncthreads();
-
-    uint32_t phase = 0;     // bit b: parity of the next wait on mbar[b]
-    uint32_t inflight = 0;  // bit b: a copy on mbar[b] not yet waited for (uniform)
-    bool failed = false;
-
-    // Prefetch the fan-ins of piece P (records in `recs`) that lie outside
-    // its ring window into far buffer `fb`: issued one piece ahead, so the
-    // piece then reads them from shared memory.  Only gates below
-    // `final_below` (the start of the piece now running) are copied: they
-    // are already written.
-    auto prefetch = [&](const Piece &P, const GateRec *recs, uint32_t fb, uint32_t final_below) {
-        if (!farcap) return;
-        const uint32_t lo = R ? (P.b > R ? P.b - R : 0) : P.b;
-        for (uint32_t gi = threadIdx.x; gi < P.b - P.a; gi += blockDim.x) {
-            const GateRec &r = recs[gi];
-            const uint32_t h = r.w[0];
-            if (h & RF_INPT) continue;
-            const uint32_t nfold = hdr_nfold(h);
-#pragma unroll
-            for (int q = 0; q < kPrefetchFanins; q++) {
-                if ((uint32_t)q > nfold) break;
-                const uint32_t f = r.w[3 + q];
-                if (f >= lo) continue;
-                // only gates already written are copied; the rest are read
-                // from the planes when the piece runs
-                uint32_t sl = f < final_below ? atomicAdd(S.farcnt + fb, 1u) : 0xFFFFu;
-                if (sl < farcap) {
-                    cp_async_vec<BW>(farp(fb, 0, sl), a.V + (size_t)f * a.ld + w0);
-                    cp_async_vec<BW>(farp(fb, 1, sl), a.T + (size_t)f * a.ld + w0);
-                    if (MODE != FWD_SIM && q == 0 && (h & RF_MARKF0))
-                        cp_async_vec<BW>(farp(fb, 2, sl), a.M + (size_t)f * a.ld + w0);
-                } else {
-                    sl = 0xFFFFu;
-                }
-                S.slot[((size_t)fb * a.cap + gi) * kPrefetchFanins + q] = (uint16_t)sl;
-            }
-        }
-        cp_async_commit();
-    };
-
-    // ------------------------------------------------------------- forward
-    // Records are staged two pieces ahead (three buffers, mbar[i % 3]); far
-    // fan-ins one piece ahead (two buffers).
-    Piece P0 = a.pieces[0], P1 = a.n_pieces > 1 ? a.pieces[1] : P0, P2 = P1;
-    if (threadIdx.x == 0) {
-        stage_piece(a, S, P0, 0, false);
-        if (a.n_pieces > 1) stage_piece(a, S, P1, 1, false);
-    }
-    inflight = a.n_pieces > 1 ? 3u : 1u;
-    {
-        const bool ok = mbar_wait(S.mbar, 0);
-        phase ^= 1u;
-        inflight &= ~1u;
-        if (__syncthreads_or(!ok)) failed = true;
-    }
-    if (!failed) prefetch(P0, S.rec, 0, P0.a);
-    for (uint32_t i = 0; i < a.n_pieces && !failed; i++) {
-        const Piece P = P0;
-        const uint32_t rb = i % 3, fb = i & 1;
-        const bool has_next = i + 1 < a.n_pieces;
-        if (i + 2 < a.n_pieces) P2 = a.pieces[i + 2];
-        if (threadIdx.x == 0) S.farcnt[fb ^ 1] = 0;
-        bool ok = true;
-        if (has_next) {
-            const uint32_t nb = (i + 1) % 3;
-            ok = mbar_wait(S.mbar + nb, (phase >> nb) & 1u);
-            phase ^= 1u << nb;
-            inflight &= ~(1u << nb);
-        }
-        cp_async_wait_all();  // this thread's prefetch for piece i
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            break;
-        }
-        if (i + 2 < a.n_pieces) {
-            if (threadIdx.x == 0) stage_piece(a, S, P2, (i + 2) % 3, false);
-            inflight |= 1u << ((i + 2) % 3);
-        }
-        if (has_next) prefetch(P1, S.rec + (size_t)((i + 1) % 3) * a.cap, fb ^ 1, P.a);
-
-        const GateRec *recs = S.rec + (size_t)rb * a.cap;
-        const uint16_t *slots = S.slot + (size_t)fb * a.cap * kPrefetchFanins;
-        const uint32_t ring_lo = R ? (P.b > R ? P.b - R : 0) : P.b;
-        bool any = false;
-        for (uint32_t gi = threadIdx.x; gi < P.b - P.a; gi += blockDim.x) {
-            const uint32_t g = P.a + gi;
-            auto fetch = [&](uint32_t f, Vec<BW> &fv, Vec<BW> &ft) {
-                if (f >= ring_lo) {
-                    fv = vld<BW>(rV + (f & Rm) * BW);
-                    ft = vld<BW>(rT + (f & Rm) * BW);
-                } else {
-                    fv = vld<BW>(a.V + (size_t)f * a.ld + w0);
-                    ft = vld<BW>(a.T + (size_t)f * a.ld + w0);
-                }
-            };
-            const GateRec r = recs[gi];
-            const uint32_t h = r.w[0];
-            Vec<BW> V, T, M;
-            if (MODE == FWD_MARK) {
-                V = vld<BW>(a.V + (size_t)g * a.ld + w0);
-                T = vld<BW>(a.T + (size_t)g * a.ld + w0);
-#pragma unroll
-                for (int j = 0; j < BW; j++) {
-                    V.x[j] &= wm.x[j];
-                    T.x[j] &= wm.x[j];
-                }
-            } else if (h & RF_INPT) {  // simkernel.cuh:112-125, pairs already formed
-                V = vldg<BW>(a.pi_v + (size_t)g * a.pi_ld + w0);
-                T = vldg<BW>(a.pi_t + (size_t)g * a.pi_ld + w0);
-#pragma unroll
-                for (int j = 0; j < BW; j++) {
-                    V.x[j] &= wm.x[j];
-                    T.x[j] &= wm.x[j];
-                }
-            }
-            Vec<BW> m0;
-#pragma unroll
-            for (int j = 0; j < BW; j++) m0.x[j] = 0;
-            if (!(h & RF_INPT)) {
-                // Fan-in q < kPrefetchFanins comes from the ring, the far
-                // buffer prefetched one piece ahead, or (far-buffer overflow)
-                // the planes; later fan-ins from the ring or the planes.
-                auto src = [&](uint32_t q, uint32_t f, uint32_t k) -> const uint32_t * {
-                    const uint32_t *ring_k = k == 0 ? rV : (k == 1 ? rT : rM);
-                    if (f >= ring_lo) return ring_k + (f & Rm) * BW;
-                    // the slot table is written only while the prefetch is on
-                    const uint32_t sl =
-                        (farcap && q < (uint32_t)kPrefetchFanins) ? slots[gi * kPrefetchFanins + q] : 0xFFFFu;
-                    if (sl != 0xFFFFu) return farp(fb, k, sl);
-                    const uint32_t *plane = k == 0 ? a.V : (k == 1 ? a.T : a.M);
-                    return plane + (size_t)f * a.ld + w0;
-                };
-                const uint32_t nfold = hdr_nfold(h);
-                const uint32_t f0 = r.w[3];
-                if (MODE != FWD_SIM && (h & RF_MARKF0)) m0 = vld<BW>(src(0, f0, 2));
-                if (MODE != FWD_MARK) {
-                    Vec<BW> v1;
-                    {
-                        const Vec<BW> fv = vld<BW>(src(0, f0, 0)), ft = vld<BW>(src(0, f0, 1));
-#pragma unroll
-                        for (int j = 0; j < BW; j++) eval_first(h, fv.x[j], ft.x[j], V.x[j], v1.x[j]);
-                    }
-                    for (uint32_t q = 1; q <= nfold; q++) {
-                        const uint32_t f = fanin_id(r, edges, q);
-                        const Vec<BW> fv = vld<BW>(src(q, f, 0)), ft = vld<BW>(src(q, f, 1));
-#pragma unroll
-                        for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
-                    }
-#pragma unroll
-                    for (int j = 0; j < BW; j++) {
-                        eval_finish(h, V.x[j], v1.x[j], T.x[j]);
-                        V.x[j] &= wm.x[j];
-                        T.x[j] &= wm.x[j];
-                    }
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < BW; j++) M.x[j] = 0;
-            if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
-                if (h & RF_INPT) {
-                    M = T;
-                } else if (h & RF_MARKF0) {
-#pragma unroll
-                    for (int j = 0; j < BW; j++) M.x[j] = T.x[j] & m0.x[j];
-                    if ((h & RF_SENS) && vany(M)) {
-                        const Vec<BW> sv = sens_any<BW, ROBUST>(r, edges, rec_nfi(r), M, fetch);
-#pragma unroll
-                        for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
-                    }
-                }
-            }
-            const size_t o = (size_t)g * a.ld + w0;
-            if (MODE != FWD_MARK) {
-                vst<BW>(a.V + o, V);
-                vst<BW>(a.T + o, T);
-            }
-            if (MODE != FWD_SIM) vst<BW>(a.M + o, M);
-            if (g >= ring_lo) {
-                const uint32_t slot = (g & Rm) * BW;
-                vst<BW>(rV + slot, V);
-                vst<BW>(rT + slot, T);
-                vst<BW>(rM + slot, M);
-            }
-            if (MODE != FWD_SIM && vany(M)) {
-                bitmap_set_aggregated(S.bm, g);
-                any = true;
-            }
-        }
-        if (__syncthreads_or(any) && threadIdx.x == 0) S.pbits[i >> 5] |= 1u << (i & 31);
-        P0 = P1;
-        P1 = P2;
-    }
-    if (failed) {
-        // wait (bounded) for the record copies still in flight, then report
-        for (uint32_t b = 0; b < 3; b++)
-            if ((inflight >> b) & 1u) (void)mbar_wait(S.mbar + b, (phase >> b) & 1u);
-        cp_async_wait_all();
-    }
-    if (failed) {
-        if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
-        return;
-    }
-    if (MODE == FWD_SIM) return;
-    __syncthreads();
-
-    // ------------------------------------------------------------- reverse
     const uint32_t R2 = a.ring2_gates, R2m = R2 - 1;
     uint32_t *ring2 = S.ring;
     auto prev_marked = [&](int from) -> int {  // highest marked piece index < from
@@ -539,6 +258,7 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
         }
         return -1;
     };
+    bool failed = false;
     int cur = prev_marked((int)a.n_pieces);
     uint32_t maxlvl = 0;
     int sbuf = 0;
@@ -625,6 +345,225 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
 }
 
 // ---------------------------------------------------------------------------
+// Forward kernel: one CTA per column block of BW words (32 * BW pairs); one
+// thread per gate, carrying all BW words of the block.
+//
+// Gates are walked in pieces (runs of one level, <= cap gates), one
+// __syncthreads per piece; each piece's records are staged into shared
+// memory by a TMA bulk copy issued one piece ahead.
+//
+// Forward (sim + forward mark, simkernel.cuh:96-156, markkernel.cuh:215-270):
+// a ring of the last R gates' V, T, M words sits in shared memory
+// (slot = gate & (R - 1)); every gate writes its slot.  During piece [a, b)
+// a fan-in f >= b - R is read from the ring: no gate of [f + 1, b) shares its
+// slot.  Older fan-ins are the piece's far fan-ins, listed at circuit upload
+// (deduplicated, per piece) together with one source byte per fan-in in the
+// gate record.  While piece i runs, threads without a gate of piece i copy
+// the rows of piece i + 1's far fan-ins (gates below piece i, so complete)
+// into a far buffer with cp.async; piece i + 1 reads them from there.  A
+// far fan-in the list could not hold is read from its plane row.
+//
+// Reverse (prune, markkernel.cuh:271-293): only pieces that hold a forward
+// mark, descending, only gates whose bitmap bit is set.  Pruned marks of
+// recent gates sit in a second ring (the same memory, R2 slots of BW words):
+// during piece [a, b) a fan-out fo is read from it iff fo < a + R2 and only
+// gates g < a + R2 write it.
+//
+// Merge (mergekernel.cuh:116-198) needs no level order: one sweep over the
+// surviving marks folds the first falling / rising pair of every net into
+// first_x / first_y with atomicMin.
+//
+// Plane rows are read and written BW words at a time: ld and pi_ld are
+// multiples of BW and every row holds all n_blocks * BW words; words at or
+// past ceil(n_pairs / 32) are masked to zero.
+// ---------------------------------------------------------------------------
+template <int BW, int ROBUST, int MODE>
+__global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
+    extern __shared__ __align__(128) unsigned char smraw[];
+    FwdSmem S;
+    S.ring = reinterpret_cast<uint32_t *>(smraw + a.off_ring);
+    S.rec = reinterpret_cast<GateRec *>(smraw + a.off_rec);
+    S.edge = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
+    S.far = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
+    S.pbits = reinterpret_cast<uint32_t *>(smraw + a.off_pbits);
+    S.mbar = reinterpret_cast<uint64_t *>(smraw + a.off_mbar);
+    const uint32_t blk = blockIdx.x;
+    const uint32_t w0 = blk * BW;
+    S.bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
+    uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
+    const uint32_t *edges = a.c.edges;
+    const uint32_t R = a.ring_gates, Rm = R - 1;
+    uint32_t *rV = S.ring, *rT = S.ring + (size_t)R * BW, *rM = S.ring + 2 * (size_t)R * BW;
+    const size_t fplane = (size_t)a.farcap * BW;  // words per far-buffer plane
+    const uint32_t fplane_b = (uint32_t)fplane * 4u, ring_b = R * BW * 4u;
+    const uint32_t ring_sa = smem_u32(S.ring);
+    const bool tail = w0 + BW >= a.W;             // the block holds padding words
+    Vec<BW> wm;                                   // valid bits of each word of this block
+#pragma unroll
+    for (int j = 0; j < BW; j++) {
+        const uint32_t w = w0 + j;
+        wm.x[j] = w + 1 < a.W ? 0xFFFFFFFFu
+                              : (w + 1 == a.W ? ((a.n_pairs & 31) ? (1u << (a.n_pairs & 31)) - 1u : 0xFFFFFFFFu) : 0u);
+    }
+
+    if (MODE != FWD_SIM)
+        for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) S.bm[q] = 0;
+    for (uint32_t q = threadIdx.x; q < (a.n_pieces + 31) / 32; q += blockDim.x) S.pbits[q] = 0;
+    __shared__ uint32_t s_fail;
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        mbar_init(S.mbar, 1);
+        mbar_init(S.mbar + 1, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    // Copy the far fan-ins of piece Q into far buffer fb; entry e goes to
+    // thread blockDim - 1 - e, a thread without a gate when the piece
+    // running now is smaller than the CTA.
+    auto prefetch = [&](const Piece &Q, uint32_t fb) {
+        for (uint32_t e = blockDim.x - 1 - threadIdx.x; e < Q.far_n; e += blockDim.x) {
+            const uint32_t f = __ldg(a.far_ids + Q.far_off + e);
+            const size_t o = (size_t)f * a.ld + w0;
+            uint32_t *d = S.far + (size_t)fb * 3 * fplane + (size_t)e * BW;
+            cp_async_vec<BW>(d, a.V + o);
+            cp_async_vec<BW>(d + fplane, a.T + o);
+            if (MODE != FWD_SIM) cp_async_vec<BW>(d + 2 * fplane, a.M + o);
+        }
+    };
+
+    uint32_t phase = 0;  // bit b: parity of the next wait on mbar[b]
+    // ------------------------------------------------------------- forward
+    if (threadIdx.x == 0) stage_piece(a, S, a.pieces[0], 0, false);
+    Piece P1 = a.n_pieces > 1 ? a.pieces[1] : a.pieces[0];
+    for (uint32_t i = 0; i < a.n_pieces; i++) {
+        const Piece P = i == 0 ? a.pieces[0] : P1;
+        const int buf = i & 1;
+        const bool has_next = i + 1 < a.n_pieces;
+        if (has_next) P1 = a.pieces[i + 1];
+        if (threadIdx.x == 0 && has_next) stage_piece(a, S, P1, buf ^ 1, false);
+        if (has_next) prefetch(P1, buf ^ 1);
+        // every thread waits for the records itself; the piece's only
+        // barrier is at its end
+        const bool ok = mbar_wait(S.mbar + buf, (phase >> buf) & 1u);
+        phase ^= 1u << buf;
+        if (!ok) s_fail = 1;
+        const GateRec *recs = S.rec + (size_t)buf * a.cap;
+        const uint32_t far_sa = smem_u32(S.far) + (uint32_t)buf * 3u * fplane_b;
+        const uint32_t ring_lo = P.b - R;  // (wraps below 0: every fan-in is in the ring then)
+        bool any = false;
+        for (uint32_t gi = threadIdx.x; ok && gi < P.b - P.a; gi += blockDim.x) {
+            const uint32_t g = P.a + gi;
+            const GateRec r = recs[gi];
+            const uint32_t h = r.w[0];
+            // source word of fan-in q (pdf_device.cuh)
+            auto srcw = [&](uint32_t q) -> uint32_t {
+                if (q < (uint32_t)kInlineFanins) return r.w[3 + q];
+                const uint32_t f = __ldg(edges + r.w[2] + q);
+                return (P.b <= R || f >= ring_lo) ? (f & Rm) : (SRC_PLANE | f);
+            };
+            // plane k (0 V, 1 T, 2 M) of the gate behind source word sw
+            auto load = [&](uint32_t sw, uint32_t k) -> Vec<BW> {
+                if (sw & SRC_PLANE) {
+                    const uint32_t *pl = k == 0 ? a.V : (k == 1 ? a.T : a.M);
+                    return vld<BW>(pl + (size_t)(sw & ~SRC_PLANE) * a.ld + w0);
+                }
+                const uint32_t sa = (sw & SRC_FAR) ? far_sa + k * fplane_b + (sw & SRC_IDX) * (4u * BW)
+                                                   : ring_sa + k * ring_b + sw * (4u * BW);
+                return vlds<BW>(sa);
+            };
+            Vec<BW> V, T, M;
+            if (MODE == FWD_MARK) {
+                V = vld<BW>(a.V + (size_t)g * a.ld + w0);
+                T = vld<BW>(a.T + (size_t)g * a.ld + w0);
+            } else if (h & RF_INPT) {  // simkernel.cuh:112-125, pairs already formed
+                V = vldg<BW>(a.pi_v + (size_t)g * a.pi_ld + w0);
+                T = vldg<BW>(a.pi_t + (size_t)g * a.pi_ld + w0);
+            }
+            if (tail && (MODE == FWD_MARK || (h & RF_INPT))) {
+#pragma unroll
+                for (int j = 0; j < BW; j++) {
+                    V.x[j] &= wm.x[j];
+                    T.x[j] &= wm.x[j];
+                }
+            }
+            if (MODE != FWD_MARK && !(h & RF_INPT)) {
+                Vec<BW> v1;
+                {
+                    const uint32_t s0 = r.w[3];
+                    const Vec<BW> fv = load(s0, 0), ft = load(s0, 1);
+#pragma unroll
+                    for (int j = 0; j < BW; j++) eval_first(h, fv.x[j], ft.x[j], V.x[j], v1.x[j]);
+                }
+                const uint32_t nfold = hdr_nfold(h);
+                for (uint32_t q = 1; q <= nfold; q++) {
+                    const uint32_t sq = srcw(q);
+                    const Vec<BW> fv = load(sq, 0), ft = load(sq, 1);
+#pragma unroll
+                    for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < BW; j++) eval_finish(h, V.x[j], v1.x[j], T.x[j]);
+                if (tail) {
+#pragma unroll
+                    for (int j = 0; j < BW; j++) {
+                        V.x[j] &= wm.x[j];
+                        T.x[j] &= wm.x[j];
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < BW; j++) M.x[j] = 0;
+            if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
+                if (h & RF_INPT) {
+                    M = T;
+                } else if ((h & RF_MARKF0) && vany(T)) {
+                    const Vec<BW> m0 = load(r.w[3], 2);
+#pragma unroll
+                    for (int j = 0; j < BW; j++) M.x[j] = T.x[j] & m0.x[j];
+                    if ((h & RF_SENS) && vany(M)) {
+                        auto fetch = [&](uint32_t q, Vec<BW> &fv, Vec<BW> &ft) {
+                            const uint32_t sq = srcw(q);
+                            fv = load(sq, 0);
+                            ft = load(sq, 1);
+                        };
+                        const Vec<BW> sv = sens_any<BW, ROBUST>(r, rec_nfi(r), fetch);
+#pragma unroll
+                        for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
+                    }
+                }
+            }
+            const size_t o = (size_t)g * a.ld + w0;
+            if (MODE != FWD_MARK) {
+                vst<BW>(a.V + o, V);
+                vst<BW>(a.T + o, T);
+            }
+            if (MODE != FWD_SIM) vst<BW>(a.M + o, M);
+            const uint32_t slot = (g & Rm) * BW;
+            vst<BW>(rV + slot, V);
+            vst<BW>(rT + slot, T);
+            if (MODE != FWD_SIM) vst<BW>(rM + slot, M);
+            if (MODE != FWD_SIM && vany(M)) {
+                bitmap_set_aggregated(S.bm, g);
+                any = true;
+            }
+        }
+        cp_async_wait_all();  // this thread's copies for piece i + 1
+        if (__syncthreads_or(any) && threadIdx.x == 0) S.pbits[i >> 5] |= 1u << (i & 31);
+        if (s_fail) {
+            // the record copy still in flight, then report
+            if (has_next) (void)mbar_wait(S.mbar + (buf ^ 1), (phase >> (buf ^ 1)) & 1u);
+            if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
+            return;
+        }
+    }
+    if constexpr (MODE != FWD_SIM) {
+        __syncthreads();
+        prune_and_merge<BW, MODE>(a, S, blk, gbm, phase);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Cover.
 // ---------------------------------------------------------------------------
 
@@ -636,6 +575,32 @@ __global__ void k_active(const CoverArgs a) {
     const uint32_t dx = fx - a.pair_base, dy = fy - a.pair_base;
     if (fx != kEmpty && dx < a.n_pairs) atomicOr(a.active + (dx >> 5), 1u << (dx & 31));
     if (fy != kEmpty && dy < a.n_pairs) atomicOr(a.active + (dy >> 5), 1u << (dy & 31));
+}
+
+// Ordered list of the active pairs (one CTA).
+__global__ void __launch_bounds__(1024) k_active_compact(const CoverArgs a, uint32_t W) {
+    __shared__ uint32_t s_cnt[1024];
+    const uint32_t per = (W + blockDim.x - 1) / blockDim.x;
+    const uint32_t q0 = threadIdx.x * per, q1 = min(W, q0 + per);
+    uint32_t cnt = 0;
+    for (uint32_t q = q0; q < q1; q++) cnt += __popc(a.active[q]);
+    s_cnt[threadIdx.x] = cnt;
+    __syncthreads();
+    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {  // inclusive scan
+        const uint32_t v = threadIdx.x >= off ? s_cnt[threadIdx.x - off] : 0u;
+        __syncthreads();
+        s_cnt[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t pos = s_cnt[threadIdx.x] - cnt;
+    for (uint32_t q = q0; q < q1; q++) {
+        uint32_t bits = a.active[q];
+        while (bits) {
+            a.active_list[pos++] = q * 32 + (__ffs(bits) - 1);
+            bits &= bits - 1;
+        }
+    }
+    if (threadIdx.x == blockDim.x - 1) *a.active_count = s_cnt[threadIdx.x];
 }
 
 __device__ __forceinline__ uint32_t hash_slot(uint32_t g, uint32_t mask) {
@@ -666,146 +631,110 @@ __device__ void atomic_add_u128(unsigned long long *lo, unsigned long long *hi, 
     }
 }
 
-// Path counting (kernCover, coverkernel.cuh:171-230, and kernSumSingle,
-// :77-105) for the pairs of one column block that first-detect some net.
-// One CTA per column block; up to kCoverSlots such pairs per pass.  Levels
-// descending from the block's highest marked level, over the nets with a
-// surviving mark in the block that one of the pass's pairs marks:
+// One CTA per active pair (persistent over the list).  Walks the levels that
+// hold marks in the pair's column block, from the top down, over the nets
+// the pair marks (kernCover, coverkernel.cuh:193-229):
 //   H = [po] + sum h(fo);  C = sum c(fo);  first = pid is first_x or first_y
 //   c = C + (first ? H : 0);  h = first ? 0 : H;  h = 0 on INPT
-// (a net a pair does not mark has h = c = 0).  (h, c) of each net, one per
-// slot, sit in a shared-memory open-addressing table keyed by net id.  The
-// level-0 INPT c values are the pairs' counts, summed into the batch count.
-constexpr int kCoverSlots = 4;
-__global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
+// (unmarked nets hold h = c = 0 and are never stored).  (h, c) live in a
+// shared-memory open-addressing table keyed by net id.  Level-0 INPT c values
+// are summed into the batch count (kernSumSingle, coverkernel.cuh:77-105).
+__global__ void __launch_bounds__(512) k_cover(const CoverArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const uint32_t cap = a.hash_cap, cmask = cap - 1;
-    uint32_t *keys = reinterpret_cast<uint32_t *>(smraw);
-    pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw + (((size_t)cap * 4 + 127) & ~(size_t)127));
-    pdf_u128 *cv = hv + (size_t)cap * kCoverSlots;
-    __shared__ uint32_t s_pairs[256];
-    __shared__ uint32_t s_na;
-    __shared__ pdf_u128 s_red[8];
+    pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw);
+    pdf_u128 *cv = hv + cap;
+    uint32_t *keys = reinterpret_cast<uint32_t *>(cv + cap);
+    __shared__ pdf_u128 s_red[32];
     __shared__ unsigned int s_flags;
 
-    const uint32_t blk = blockIdx.x, w0 = blk * a.bw;
-    const uint32_t W = (uint32_t)((a.n_pairs + 31) / 32);
-    if (threadIdx.x == 0) {
-        uint32_t n = 0;
-        for (uint32_t j = 0; j < a.bw && w0 + j < W; j++) {
-            uint32_t bits = a.active[w0 + j];
-            while (bits) {
-                s_pairs[n++] = (w0 + j) * 32 + (__ffs(bits) - 1);
-                bits &= bits - 1;
-            }
-        }
-        s_na = n;
-        s_flags = 0;
-    }
-    __syncthreads();
-    const uint32_t na = s_na;
-    if (na == 0) return;
-    const uint32_t top = a.blk_maxlvl[blk];
-    const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
-    pdf_u128 total = 0;
-    bool ovf = false;
-    for (uint32_t g0 = 0; g0 < na; g0 += kCoverSlots) {
-        const uint32_t ns = min((uint32_t)kCoverSlots, na - g0);
-        uint32_t pw[kCoverSlots], pb[kCoverSlots], pid[kCoverSlots];
-#pragma unroll
-        for (int k = 0; k < kCoverSlots; k++) {
-            const uint32_t p = s_pairs[g0 + min((uint32_t)k, ns - 1)];
-            pw[k] = p >> 5;
-            pb[k] = p & 31;
-            pid[k] = a.pair_base + p;
-        }
+    const uint32_t n_active = *a.active_count;
+    for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) {
+        const uint32_t p = a.active_list[ai];
+        const uint32_t pid = a.pair_base + p;
+        const uint32_t wp = p >> 5, bit = p & 31, blk = wp / a.bw;
+        const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
+        const uint32_t top = a.blk_maxlvl[blk];
         for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) keys[i] = kEmpty;
+        if (threadIdx.x == 0) s_flags = 0;
         __syncthreads();
+        pdf_u128 total = 0;
+        bool ovf = false;
         for (int l = (int)top - 1; l >= 0; l--) {
             const uint32_t s = a.c.level_off[l], e = a.c.level_off[l + 1];
-            for (uint32_t g = s + threadIdx.x; g < e; g += blockDim.x) {
-                if (!((nzb[g >> 5] >> (g & 31)) & 1u)) continue;
-                uint32_t smask = 0;
-#pragma unroll
-                for (int k = 0; k < kCoverSlots; k++)
-                    if ((uint32_t)k < ns && ((a.M[(size_t)g * a.ld + pw[k]] >> pb[k]) & 1u)) smask |= 1u << k;
-                if (!smask) continue;
-                const GateRec r = load_rec(a.c.rec + g);
-                const uint32_t fx = a.first_x[g], fy = a.first_y[g];
-                pdf_u128 H[kCoverSlots], Cc[kCoverSlots];
-#pragma unroll
-                for (int k = 0; k < kCoverSlots; k++) {
-                    H[k] = rec_po(r) ? 1 : 0;
-                    Cc[k] = 0;
-                }
-                const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
-                for (uint32_t q = 0; q < nfo; q++) {
-                    const uint32_t fo = __ldg(a.c.edges + eb + q);
-                    uint32_t sl = hash_slot(fo, cmask);
-                    for (uint32_t probe = 0; probe < cap; probe++) {
-                        const uint32_t key = keys[sl];
-                        if (key == fo) {
-                            bool hovf = false;
-#pragma unroll
-                            for (int k = 0; k < kCoverSlots; k++) {
-                                Cc[k] = add_sat(Cc[k], cv[(size_t)sl * kCoverSlots + k], ovf);
-                                H[k] = add_sat(H[k], hv[(size_t)sl * kCoverSlots + k], hovf);
+            if (e > s) {
+                const uint32_t q0 = s >> 5, q1 = (e - 1) >> 5;
+                for (uint32_t q = q0 + threadIdx.x; q <= q1; q += blockDim.x) {
+                    uint32_t bits = nzb[q];
+                    if (q == q0) bits &= 0xFFFFFFFFu << (s & 31);
+                    if (q == q1) bits &= 0xFFFFFFFFu >> (31 - ((e - 1) & 31));
+                    while (bits) {
+                        const uint32_t g = q * 32 + (__ffs(bits) - 1);
+                        bits &= bits - 1;
+                        if (!((a.M[(size_t)g * a.ld + wp] >> bit) & 1u)) continue;
+                        const GateRec r = load_rec(a.c.rec + g);
+                        pdf_u128 H = rec_po(r) ? 1 : 0, C = 0;
+                        const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
+                        for (uint32_t k = 0; k < nfo; k++) {
+                            const uint32_t fo = __ldg(a.c.edges + eb + k);
+                            uint32_t sl = hash_slot(fo, cmask);
+                            for (uint32_t probe = 0; probe < cap; probe++) {
+                                const uint32_t key = keys[sl];
+                                if (key == fo) {
+                                    bool dummy = false;
+                                    C = add_sat(C, cv[sl], ovf);
+                                    H = add_sat(H, hv[sl], dummy);
+                                    break;
+                                }
+                                if (key == kEmpty) break;
+                                sl = (sl + 1) & cmask;
                             }
-                            break;
                         }
-                        if (key == kEmpty) break;
-                        sl = (sl + 1) & cmask;
-                    }
-                }
-                pdf_u128 hs[kCoverSlots], cs[kCoverSlots];
-#pragma unroll
-                for (int k = 0; k < kCoverSlots; k++) {
-                    hs[k] = 0;
-                    cs[k] = 0;
-                    if (!((smask >> k) & 1u)) continue;
-                    const bool first = fx == pid[k] || fy == pid[k];
-                    cs[k] = first ? add_sat(Cc[k], H[k], ovf) : Cc[k];
-                    hs[k] = first ? 0 : H[k];
-                    if (cs[k] == ~(pdf_u128)0) ovf = true;
-                    if (rec_type(r) == PDF_INPT) {
-                        hs[k] = 0;
-                        if (l == 0) total = add_sat(total, cs[k], ovf);
-                    }
-                }
-                if (l > 0) {  // level-0 values are never read
-                    uint32_t sl = hash_slot(g, cmask);
-                    uint32_t probe = 0;
-                    for (; probe < cap; probe++) {
-                        if (atomicCAS(keys + sl, kEmpty, g) == kEmpty) break;
-                        sl = (sl + 1) & cmask;
-                    }
-                    if (probe == cap) {
-                        atomicOr(&a.acc->err, kErrHashFull);
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < kCoverSlots; k++) {
-                            hv[(size_t)sl * kCoverSlots + k] = hs[k];
-                            cv[(size_t)sl * kCoverSlots + k] = cs[k];
+                        const bool first = a.first_x[g] == pid || a.first_y[g] == pid;
+                        pdf_u128 c = C, h = H;
+                        if (first) {
+                            c = add_sat(C, H, ovf);
+                            h = 0;
+                        }
+                        if (c == ~(pdf_u128)0) ovf = true;
+                        if (rec_type(r) == PDF_INPT) {
+                            h = 0;
+                            if (l == 0) total = add_sat(total, c, ovf);
+                        }
+                        if (l > 0) {  // level-0 values are never read
+                            uint32_t sl = hash_slot(g, cmask);
+                            uint32_t probe = 0;
+                            for (; probe < cap; probe++) {
+                                if (atomicCAS(keys + sl, kEmpty, g) == kEmpty) break;
+                                sl = (sl + 1) & cmask;
+                            }
+                            if (probe == cap) {
+                                atomicOr(&a.acc->err, kErrHashFull);  // table full
+                            } else {
+                                hv[sl] = h;
+                                cv[sl] = c;
+                            }
                         }
                     }
                 }
             }
             __syncthreads();
         }
-    }
-    // Block sum of the counts.
-    for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
-    if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        pdf_u128 t = threadIdx.x < (blockDim.x + 31) / 32 ? s_red[threadIdx.x] : 0;
-        bool o2 = false;
-        for (int d = 16; d > 0; d >>= 1) t = add_sat(t, shfl_down_u128(t, d), o2);
-        if (threadIdx.x == 0) {
-            if (o2 || s_flags) atomicOr(&a.acc->batch_flags, PDF_FLAG_OVERFLOW);
-            if (t) atomic_add_u128(&a.acc->batch_lo, &a.acc->batch_hi, &a.acc->batch_flags, t);
+        // Block sum of the pair's count.
+        for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
+        if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
+        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            pdf_u128 t = threadIdx.x < (blockDim.x + 31) / 32 ? s_red[threadIdx.x] : 0;
+            bool o2 = false;
+            for (int d = 16; d > 0; d >>= 1) t = add_sat(t, shfl_down_u128(t, d), o2);
+            if (threadIdx.x == 0) {
+                if (o2 || s_flags) atomicOr(&a.acc->batch_flags, PDF_FLAG_OVERFLOW);
+                if (t) atomic_add_u128(&a.acc->batch_lo, &a.acc->batch_hi, &a.acc->batch_flags, t);
+            }
         }
+        __syncthreads();
     }
 }
 
@@ -923,19 +852,18 @@ cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, 
     }
 }
 
-size_t cover_smem_bytes(uint32_t hash_cap) {
-    return (((size_t)hash_cap * 4 + 127) & ~(size_t)127) + (size_t)hash_cap * kCoverSlots * 2 * sizeof(pdf_u128);
-}
+size_t cover_smem_bytes(uint32_t hash_cap) { return (size_t)hash_cap * (4 + 2 * sizeof(pdf_u128)); }
 
-cudaError_t launch_cover(const CoverArgs &a, uint32_t threads, cudaStream_t st) {
+cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st) {
     const uint32_t W = (uint32_t)((a.n_pairs + 31) / 32);
     cudaError_t e = cudaMemsetAsync(a.active, 0, (size_t)W * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     k_active<<<(a.c.n_gates + 255) / 256, 256, 0, st>>>(a);
+    k_active_compact<<<1, 1024, 0, st>>>(a, W);
     const size_t smem = cover_smem_bytes(a.hash_cap);
     e = cudaFuncSetAttribute(k_cover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_cover<<<(W + a.bw - 1) / a.bw, threads, smem, st>>>(a);
+    k_cover<<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

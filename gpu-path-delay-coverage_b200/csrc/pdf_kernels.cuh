@@ -24,10 +24,11 @@ enum FwdMode {
 
 struct FwdArgs {
     DevCircuit c;
-    const Piece *pieces;          // level-ordered runs of gates (the staging unit)
+    const Piece *pieces;          // level-ordered runs of gates (the unit of staging and of sync)
     uint32_t n_pieces;
     uint32_t cap, ecap;           // gates / edge words per staging buffer
-    uint32_t farcap;              // far fan-in slots per prefetch buffer (0: no prefetch)
+    const uint32_t *far_ids;      // per piece, the far fan-ins it reads (Piece::far_off / far_n)
+    uint32_t farcap;              // slots per far buffer (>= every piece's far_n)
     const uint32_t *pi_v, *pi_t;  // [n_pi][pi_ld]
     uint64_t pi_ld;
     uint32_t *V, *T, *M;          // planes [n_gates][ld]
@@ -41,10 +42,13 @@ struct FwdArgs {
     uint64_t n_pairs;
     uint32_t W;                   // ceil(n_pairs / 32)
     uint32_t pair_base;
-    uint32_t ring_gates;          // forward ring slots (power of two, or 0)
+    uint32_t ring_gates;          // forward ring slots R (power of two, >= cap)
     uint32_t ring2_gates;         // reverse ring slots (power of two, or 0)
     // shared-memory byte offsets
-    uint32_t off_ring, off_rec, off_edge, off_slot, off_bm, off_pbits, off_mbar;
+    uint32_t off_ring;            // forward: ring [3][R][BW]; reverse: ring2 [R2][BW]
+    uint32_t off_rec;             // [2][cap] staged gate records
+    uint32_t off_edge;            // reverse: [2][ecap] staged edges; forward: far buffers [2][3][farcap][BW]
+    uint32_t off_bm, off_pbits, off_mbar;
 };
 
 // Device error bits (DevAcc::err and the circuit's error word).
@@ -74,6 +78,8 @@ struct CoverArgs {
     uint64_t n_pairs;
     uint32_t pair_base;
     uint32_t *active;             // [W] bitmap of first-detecting pairs
+    uint32_t *active_list;        // [min(n_pairs, 2 * n_gates)] their indices, ascending
+    uint32_t *active_count;       // [1]
     DevAcc *acc;
     uint32_t hash_cap;            // entries of the per-CTA shared-memory table (power of two)
 };
@@ -81,7 +87,7 @@ struct CoverArgs {
 // Host-side launchers (pdf_kernels.cu).  All return cudaError_t of the launch.
 cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st);
-cudaError_t launch_cover(const CoverArgs &a, uint32_t threads, cudaStream_t st);
+cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st);
 size_t cover_smem_bytes(uint32_t hash_cap);
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M,
                                uint64_t ld, uint64_t n_pairs, uint32_t pair_base,

@@ -270,8 +270,9 @@ pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark,
  * (pdf_circuit_create allocates); this call then allocates and frees nothing.
  * Its scratch is one fixed array of 8 MiB in device memory, held by every GPU
  * that loads the library until the process exits; a chunk needs
- * ceil(ceil(n_pairs/32)/tile_words) * ceil(n_gates/32) * 4 bytes of it plus a
- * few KiB, and larger requests return PDF_ELIMIT.  The caller passes the
+ * 4 * (ceil(ceil(n_pairs/32)/tile_words) * ceil(n_gates/32)
+ *      + ceil(n_pairs/32) + min(n_pairs, 2 * n_gates)) bytes of it plus about
+ * 1 KiB, and larger requests return PDF_ELIMIT.  The caller passes the
  * pruned mark plane (as pdf_cover) and the first-detect ids as device arrays
  * of n_gates uint32 (for example copied out with pdf_state_first_copy); the
  * chunk's count is returned in *chunk_total (the call waits for it).

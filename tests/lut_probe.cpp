@@ -44,5 +44,24 @@ int main() {
             }
         }
     }
+    // One-pass side-input test (sens_step / sens_result) for AND..NOR with
+    // 2..4 fan-ins and every input code combination.
+    for (int robust = 0; robust < 2; robust++)
+        for (uint32_t type = PDF_AND; type <= PDF_NOR; type++)
+            for (uint32_t nfi = 2; nfi <= 4; nfi++)
+                for (uint32_t cmb = 0; cmb < (1u << (2 * nfi)); cmb++) {
+                    const bool or_like = type == PDF_OR || type == PDF_NOR;
+                    SensAcc s;
+                    sens_init(s);
+                    for (uint32_t x = 0; x < nfi; x++) {
+                        const uint32_t c = (cmb >> (2 * x)) & 3;
+                        if (robust)
+                            sens_step<1>(s, or_like, (c & 1) << 9, (c >> 1) << 9);
+                        else
+                            sens_step<0>(s, or_like, (c & 1) << 9, (c >> 1) << 9);
+                    }
+                    const uint32_t r = robust ? sens_result<1>(s) : sens_result<0>(s);
+                    std::printf("sensall %d %u %u %u %u\n", robust, type, nfi, cmb, (r >> 9) & 1);
+                }
     return 0;
 }

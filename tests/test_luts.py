@@ -129,3 +129,17 @@ def test_device_mark_flags_equal_reference(probe):
             assert R.AND <= t <= R.NOR and nfi >= 2
         if R.AND <= t <= R.NOR and nfi >= 2:
             assert sens
+
+
+def test_device_side_input_test_equals_reference(probe):
+    """One-pass OR_i AND_{x != i} sens(on=i, off=x) (markkernel.cuh:253-261)
+    against the reference's tables, every code combination of 2..4 fan-ins."""
+    seen = 0
+    for mode, t, nfi, cmb, got in probe["sensall"]:
+        codes = [(cmb >> (2 * x)) & 3 for x in range(nfi)]
+        tab = R.SENS[mode][t - 2]
+        want = int(any(all((tab >> (codes[i] * 4 + codes[x])) & 1 for x in range(nfi) if x != i)
+                       for i in range(nfi)))
+        assert got == want, (mode, t, nfi, codes)
+        seen += 1
+    assert seen == 2 * 4 * (16 + 64 + 256)
