@@ -405,6 +405,11 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
                         }
                     }
                     recs[g].w[3 + q] = sw;
+                    if (sw & SRC_PLANE || sw & SRC_FAR) recs[f].w[0] |= RF_SPILL;
+                }
+                for (uint32_t q = kInlineFanins; q < nl->nfi[g]; q++) {  // read from edges[] at run time
+                    const uint32_t f = edges[eoff[g] + q];
+                    if (f < lo) recs[f].w[0] |= RF_SPILL;
                 }
             }
             for (uint32_t f : list) seen[f] = 0xFFFFFFFFu;
@@ -700,6 +705,7 @@ FwdArgs base_fwd(pdf_circuit *c, uint64_t n_pairs) {
     a.ecap = c->ecap;
     a.n_pairs = n_pairs;
     a.W = (uint32_t)((n_pairs + 31) / 32);
+    a.store_all = 1;
     a.bm_words = (c->info.n_gates + 31) / 32;
     a.bm_shared = c->bm_shared;
     a.far_ids = c->far.as<uint32_t>();
@@ -803,6 +809,8 @@ pdf_status grade_mark_locked(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr, 
     a.pi_v = pv;
     a.pi_t = pt;
     a.pi_ld = pld;
+    // with no plane asked for, only the rows read back are written
+    a.store_all = out && (out->sim_v || out->sim_t || out->mark) ? 1u : 0u;
     if (direct) {
         a.V = out->sim_v;
         a.T = out->sim_t;

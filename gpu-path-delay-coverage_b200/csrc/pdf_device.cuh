@@ -52,6 +52,7 @@ enum : uint32_t {
     RF_SENS = 1u << 20,    // the mark needs the side-input test (AND..XNOR, nfi >= 2)
     RF_MARKF0 = 1u << 21,  // mark = transition & mark of fan-in 0
     RF_INPT = 1u << 22,    // primary input: mark = transition
+    RF_SPILL = 1u << 23,   // a later gate reads this gate's plane rows from global memory
 };
 
 PDF_HD uint32_t rec_type(const GateRec &r) { return r.w[0] & 0xFu; }

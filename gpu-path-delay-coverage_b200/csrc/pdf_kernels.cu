@@ -533,17 +533,23 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
                     }
                 }
             }
-            const size_t o = (size_t)g * a.ld + w0;
-            if (MODE != FWD_MARK) {
-                vst<BW>(a.V + o, V);
-                vst<BW>(a.T + o, T);
+            const bool marked = MODE != FWD_SIM && vany(M);
+            // plane rows: every row when asked for; else the rows that are
+            // read back (far fan-ins, and the marked gates the prune, merge
+            // and cover visit)
+            if (a.store_all || (h & RF_SPILL) || marked) {
+                const size_t o = (size_t)g * a.ld + w0;
+                if (MODE != FWD_MARK) {
+                    vst<BW>(a.V + o, V);
+                    vst<BW>(a.T + o, T);
+                }
+                if (MODE != FWD_SIM) vst<BW>(a.M + o, M);
             }
-            if (MODE != FWD_SIM) vst<BW>(a.M + o, M);
             const uint32_t slot = (g & Rm) * BW;
             vst<BW>(rV + slot, V);
             vst<BW>(rT + slot, T);
             if (MODE != FWD_SIM) vst<BW>(rM + slot, M);
-            if (MODE != FWD_SIM && vany(M)) {
+            if (marked) {
                 bitmap_set_aggregated(S.bm, g);
                 any = true;
             }

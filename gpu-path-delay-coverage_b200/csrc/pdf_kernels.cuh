@@ -33,6 +33,8 @@ struct FwdArgs {
     uint64_t pi_ld;
     uint32_t *V, *T, *M;          // planes [n_gates][ld]
     uint64_t ld;
+    uint32_t store_all;           // 1: write every plane row; 0: only the rows read back later
+                                  // (RF_SPILL gates, gates with a forward mark)
     uint32_t *nzb;                // [n_blocks][bm_words] gates with a nonzero mark
     uint32_t *blk_maxlvl;         // [n_blocks] highest level holding a mark (+1), 0 = none
     uint32_t bm_words;

@@ -147,6 +147,28 @@ def test_no_outputs_requested():
     np.testing.assert_array_equal(got["fx"], want.first_x)
 
 
+@pytest.mark.parametrize("case", ["wide_levels", "deep_wide_fanin", "c2_default", "c2_robust"])
+def test_rows_read_back_only(case):
+    """With no plane asked for, the forward pass writes only the plane rows
+    that are read back (far fan-ins, marked gates).  On circuits larger than
+    the shared-memory ring the counts, flags and first ids still match."""
+    mode, opts = 0, {}
+    if case == "wide_levels":
+        nl, n, opts = circuits.random_small(99, n_gates=12000, n_pi=1500, n_po=3000, depth=7), 700, {"tile_words": 8}
+    elif case == "deep_wide_fanin":
+        nl, n = circuits.random_small(77, n_gates=20000, n_pi=400, n_po=2000, depth=90, fmin=1, fmax=8), 1000
+    else:
+        w = P.WORKLOADS["c2"]
+        nl, n = P.gen_netlist(w["gen"]), 4096
+        mode = 1 if case == "c2_robust" else 0
+    codes = helpers.rand_codes(np.random.default_rng(len(case)), nl.n_pi, n)
+    want = O.grade(nl, codes, n, mark_mode=mode)
+    got = gpu_grade(nl, codes, n, mode, outputs=False, **opts)
+    np.testing.assert_array_equal(got["fx"], want.first_x)
+    np.testing.assert_array_equal(got["fy"], want.first_y)
+    assert got["total"] == want.total and got["flags"] == want.flags
+
+
 def test_device_buffers():
     import torch
     nl = SUITE[5][1]
