@@ -321,6 +321,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         r.w[0] = make_rec_header(nl->type[g], nl->po[g], nl->nfi[g]);
         r.w[1] = nl->nfo[g];
         r.w[2] = (uint32_t)eoff[g];  // w[3..6]: source words, set with the launch plan below
+        r.w[7] = nl->nfi[g] ? edges[eoff[g]] : 0;
     }
 
     // Launch plan: CTAs of `threads` threads own `bw` words of pairs; two
@@ -434,14 +435,17 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     while (rmin < c->cap) rmin *= 2;
     uint32_t rmax = rmin;
     while ((uint64_t)rmax < 2 * (uint64_t)G && fixed + (size_t)rmax * 2 * c->bw * 12 <= budget) rmax *= 2;
+    // the ring's memory also holds the reverse pass's row staging buffers
+    const size_t rows_bytes = (size_t)2 * c->cap * 2 * c->bw * 4;
+    auto ring_bytes = [&](size_t R) { return std::max(R * c->bw * 12, rows_bytes); };
     uint32_t ring = 0;
     for (uint32_t R = rmax; R >= rmin && !ring; R /= 2)
-        if (fixed + al(std::max(edge_bytes, 64 * far_entry)) + (size_t)R * c->bw * 12 <= budget) ring = R;
+        if (fixed + al(std::max(edge_bytes, 64 * far_entry)) + ring_bytes(R) <= budget) ring = R;
     if (!ring) {
         delete c;
         return PDF_ENOTSUP;
     }
-    const size_t far_room = budget - fixed - (size_t)ring * c->bw * 12;
+    const size_t far_room = budget - fixed - ring_bytes(ring);
     const uint32_t far_limit = (uint32_t)std::min<size_t>(kMaxFar, (far_room & ~(size_t)127) / far_entry) & ~3u;
     const uint32_t farcap = std::max<uint32_t>(4, (far_lists(ring, far_limit) + 3) & ~3u);
     if (far_ids.empty()) far_ids.push_back(0);
@@ -460,12 +464,15 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->off_mbar = (uint32_t)off;
     off += 128;
     c->off_ring = (uint32_t)off;
+    // reverse pass: ring2 and the row staging buffers [2][cap][2][bw] share
+    // the ring's memory
     uint32_t ring2 = 0;
-    for (uint32_t r = 1; (size_t)r * c->bw * 4 <= (size_t)ring * c->bw * 12; r *= 2) ring2 = r;
+    for (uint32_t r = 1; (size_t)r * c->bw * 4 + rows_bytes <= ring_bytes(ring); r *= 2) ring2 = r;
     c->ring2 = ring2;
-    c->fwd_smem = off + (size_t)ring * c->bw * 12;
+    c->fwd_smem = off + ring_bytes(ring);
+    // nets one pair may mark in the cover: as many as its shared memory holds
     c->hash_cap = 4096;
-    while (c->hash_cap > 64 && cover_smem_bytes(c->hash_cap) > prop.sharedMemPerBlockOptin) c->hash_cap /= 2;
+    while (c->hash_cap > 256 && cover_smem_bytes(c->hash_cap) > prop.sharedMemPerBlockOptin) c->hash_cap -= 256;
     c->cover_threads = 256;
     c->cover_grid = (uint32_t)prop.multiProcessorCount;
 
@@ -842,7 +849,9 @@ pdf_status grade_mark_locked(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr, 
         s->pe = &s->prof.back();
         PDF_CUDA(cudaEventRecord(s->pe->ev[0], cs));
     }
-    PDF_CUDA(launch_batch_begin(acc, cs));
+    // the forward kernel also clears the batch count and the cover's active pairs
+    a.acc = acc;
+    a.active = s->ws.active.as<uint32_t>();
     PDF_CUDA(launch_forward(a, FWD_FUSED, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
     if (s->pe) PDF_CUDA(cudaEventRecord(s->pe->ev[1], cs));
     if (out && !direct) {
@@ -869,8 +878,7 @@ pdf_status grade_cover_locked(pdf_circuit *c, pdf_state *s, cudaStream_t cs) {
     CoverArgs ca = base_cover(c, s->ws, s->pend_M, s->pend_ld, s->pend_n, base, s->first_x.as<uint32_t>(),
                               s->first_y.as<uint32_t>(), acc);
     if (s->pe) PDF_CUDA(cudaEventRecord(s->pe->ev[2], cs));  // cover starts (after any exchange)
-    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
-    PDF_CUDA(launch_batch_end(acc, s->pend_n, cs));
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, false, cs));  // closes the batch
     if (s->pe) {
         PDF_CUDA(cudaEventRecord(s->pe->ev[3], cs));
         s->pe = nullptr;
@@ -1050,8 +1058,7 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
                                       s->ws.maxlvl.as<uint32_t>(), (c->info.n_gates + 31) / 32, cs));
     CoverArgs ca = base_cover(c, s->ws, mark, ld, n_pairs, (uint32_t)pair_base, s->first_x.as<uint32_t>(),
                               s->first_y.as<uint32_t>(), acc);
-    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
-    PDF_CUDA(launch_batch_end(acc, n_pairs, cs));
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, true, cs));  // closes the batch
     PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));
     const DevAcc &h = *s->host_acc;
@@ -1118,8 +1125,7 @@ extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, ui
     ca.active_list = active_list;
     ca.acc = acc;
     ca.hash_cap = c->hash_cap;
-    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, cs));
-    PDF_CUDA(launch_batch_end(acc, n_pairs, cs));
+    PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, true, cs));  // closes the batch
     DevAcc h{};
     PDF_CUDA(cudaMemcpyAsync(&h, acc, sizeof h, cudaMemcpyDeviceToHost, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));

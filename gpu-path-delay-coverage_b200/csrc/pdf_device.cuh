@@ -31,7 +31,7 @@ typedef unsigned __int128 pdf_u128;
 //          SRC_PLANE | f   the plane row of gate f in global memory
 //          SRC_FAR | s     slot s of the piece's far buffer (prefetched)
 //          s               slot s of the shared-memory ring of recent gates
-//   w[7] = 0
+//   w[7] = fan-in 0 (its gate id; 0 without fan-ins)
 // Fan-ins past the fourth are read from edges[] (ring or plane row).
 struct __align__(16) GateRec {
     uint32_t w[8];

@@ -10,7 +10,7 @@
 //               dataflow: each gate waits only for its own fan-ins), then,
 //               in the same CTA, the prune (levels descending) and the
 //               first-detect merge over the gates whose marks are nonzero.
-//   k_active / k_active_compact / k_cover
+//   k_active / k_cover
 //               path counting, only for pairs that first-detect some net
 //               (every other pair credits nothing), over only the nets those
 //               pairs mark, in exact 128-bit integers.
@@ -222,27 +222,38 @@ __device__ __forceinline__ bool vany(const Vec<BW> &v) {
 
 // The side-input test of a marked multi-input gate (markkernel.cuh:253-261
 // with robust()/nonrobust(), :43-72) in one pass over its nfi fan-ins
-// (sens_step, pdf_device.cuh).  fetch(q, V, T) reads fan-in q.
+// (sens_step, pdf_device.cuh).  fetch(q, V, T) reads fan-in q; fan-ins 0..3
+// are unrolled.
 template <int BW, int ROBUST, class Fetch>
 __device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, uint32_t nfi, Fetch fetch) {
     const bool or_like = (r.w[0] & RF_IM) != 0;
     SensAcc acc[BW];
 #pragma unroll
     for (int j = 0; j < BW; j++) sens_init(acc[j]);
-    for (uint32_t q = 0; q < nfi; q++) {
+    auto step = [&](uint32_t q) {
         Vec<BW> v, t;
         fetch(q, v, t);
 #pragma unroll
         for (int j = 0; j < BW; j++) sens_step<ROBUST>(acc[j], or_like, v.x[j], t.x[j]);
-    }
+    };
+#pragma unroll
+    for (int q = 0; q < kInlineFanins; q++)
+        if ((uint32_t)q < nfi) step(q);
+    for (uint32_t q = kInlineFanins; q < nfi; q++) step(q);
     Vec<BW> out;
 #pragma unroll
     for (int j = 0; j < BW; j++) out.x[j] = sens_result<ROBUST>(acc[j]);
     return out;
 }
 
-// Reverse pass (prune) and merge of k_forward, after its forward pass.
-// `phase` carries the parity bits of the two record mbarriers.
+// Reverse pass (prune, markkernel.cuh:271-293) and first-detect merge
+// (mergekernel.cuh:116-198) of k_forward, after its forward pass: only
+// pieces that hold a forward mark, descending, only gates whose bitmap bit is
+// set.  While piece i runs, the mark (and value) rows of the next marked
+// piece's marked gates are copied into a staging buffer with cp.async.  A
+// gate's pruned mark is final once its fan-outs are, so it is folded into
+// first_x / first_y right away.  `phase` carries the parity bits of the two
+// record mbarriers.
 template <int BW, int MODE>
 __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem &S, uint32_t blk, uint32_t *gbm,
                                                 uint32_t phase) {
@@ -250,6 +261,7 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
     const uint32_t *edges = a.c.edges;
     const uint32_t R2 = a.ring2_gates, R2m = R2 - 1;
     uint32_t *ring2 = S.ring;
+    uint32_t *mst = S.ring + (size_t)R2 * BW;  // [2][cap][2][BW]: M and V rows
     auto prev_marked = [&](int from) -> int {  // highest marked piece index < from
         for (int q = (from - 1) >> 5; q >= 0 && from > 0; q--) {
             uint32_t bits = S.pbits[q];
@@ -258,24 +270,43 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
         }
         return -1;
     };
+    auto stage_rows = [&](const Piece &Q, int b) {
+        for (uint32_t gi = threadIdx.x; gi < Q.b - Q.a; gi += blockDim.x) {
+            const uint32_t g = Q.a + gi;
+            if (!bit_test(S.bm, g)) continue;
+            uint32_t *d = mst + ((size_t)b * a.cap + gi) * 2 * BW;
+            const size_t o = (size_t)g * a.ld + w0;
+            cp_async_vec<BW>(d, a.M + o);
+            if (MODE == FWD_FUSED) cp_async_vec<BW>(d + BW, a.V + o);
+        }
+    };
     bool failed = false;
     int cur = prev_marked((int)a.n_pieces);
     uint32_t maxlvl = 0;
     int sbuf = 0;
-    if (cur >= 0 && threadIdx.x == 0) stage_piece(a, S, a.pieces[cur], 0, true);
+    if (cur >= 0) {
+        if (threadIdx.x == 0) stage_piece(a, S, a.pieces[cur], 0, true);
+        stage_rows(a.pieces[cur], 0);
+        cp_async_wait_all();
+    }
     while (cur >= 0) {
         const int nxt = prev_marked(cur);
         const Piece P = a.pieces[cur];
-        if (threadIdx.x == 0 && nxt >= 0) stage_piece(a, S, a.pieces[nxt], sbuf ^ 1, true);
+        if (nxt >= 0) {
+            if (threadIdx.x == 0) stage_piece(a, S, a.pieces[nxt], sbuf ^ 1, true);
+            stage_rows(a.pieces[nxt], sbuf ^ 1);
+        }
         const bool ok = mbar_wait(S.mbar + sbuf, (phase >> sbuf) & 1u);
         phase ^= 1u << sbuf;
         if (__syncthreads_or(!ok)) {
             failed = true;
             if (nxt >= 0) (void)mbar_wait(S.mbar + (sbuf ^ 1), (phase >> (sbuf ^ 1)) & 1u);
+            cp_async_wait_all();
             break;
         }
         const GateRec *recs = S.rec + (size_t)sbuf * a.cap;
         const uint32_t *es = S.edge + (size_t)sbuf * a.ecap;
+        const uint32_t *rows = mst + (size_t)sbuf * a.cap * 2 * BW;
         const bool staged = P.ea != 0xFFFFFFFFu;
         const uint32_t win = P.a + R2;  // fan-outs below this are in ring2
         bool any = false;
@@ -283,7 +314,7 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
             const uint32_t g = P.a + gi;
             if (!bit_test(S.bm, g)) continue;
             const GateRec &r = recs[gi];
-            const Vec<BW> mk = vld<BW>(a.M + (size_t)g * a.ld + w0);
+            const Vec<BW> mk = vld<BW>(rows + (size_t)gi * 2 * BW);
             Vec<BW> keep;
 #pragma unroll
             for (int j = 0; j < BW; j++) keep.x[j] = rec_po(r) ? 0xFFFFFFFFu : 0u;
@@ -308,9 +339,23 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
             if (changed) vst<BW>(a.M + (size_t)g * a.ld + w0, nm);
             if (g < win) vst<BW>(ring2 + (g & R2m) * BW, nm);
             const bool nz = vany(nm);
-            if (!nz) atomicAnd(S.bm + (g >> 5), ~(1u << (g & 31)));
+            if (!nz) {
+                atomicAnd(S.bm + (g >> 5), ~(1u << (g & 31)));
+            } else if (MODE == FWD_FUSED) {  // merge: first falling / rising pair
+                const Vec<BW> v = vld<BW>(rows + (size_t)gi * 2 * BW + BW);
+                uint32_t cx = kEmpty, cy = kEmpty;
+#pragma unroll
+                for (int j = BW - 1; j >= 0; j--) {  // lowest word wins
+                    const uint32_t x = nm.x[j] & ~v.x[j], y = nm.x[j] & v.x[j];
+                    if (x) cx = (w0 + j) * 32 + (__ffs(x) - 1);
+                    if (y) cy = (w0 + j) * 32 + (__ffs(y) - 1);
+                }
+                if (cx != kEmpty) atomicMin(a.first_x + g, a.pair_base + cx);
+                if (cy != kEmpty) atomicMin(a.first_y + g, a.pair_base + cy);
+            }
             any |= nz;
         }
+        cp_async_wait_all();  // this thread's rows for the next piece
         if (__syncthreads_or(any) && P.level + 1 > maxlvl) maxlvl = P.level + 1;
         cur = nxt;
         sbuf ^= 1;
@@ -318,25 +363,6 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
     if (failed) {
         if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
         return;
-    }
-
-    // ------------------------------------------------------------- merge
-    const uint32_t gend = a.c.level_off[maxlvl];
-    if (MODE == FWD_FUSED) {
-        for (uint32_t g = threadIdx.x; g < gend; g += blockDim.x) {
-            if (!bit_test(S.bm, g)) continue;
-            const Vec<BW> m = vld<BW>(a.M + (size_t)g * a.ld + w0);
-            const Vec<BW> v = vld<BW>(a.V + (size_t)g * a.ld + w0);
-            uint32_t cx = kEmpty, cy = kEmpty;
-#pragma unroll
-            for (int j = BW - 1; j >= 0; j--) {  // lowest word wins
-                const uint32_t x = m.x[j] & ~v.x[j], y = m.x[j] & v.x[j];
-                if (x) cx = (w0 + j) * 32 + (__ffs(x) - 1);
-                if (y) cy = (w0 + j) * 32 + (__ffs(y) - 1);
-            }
-            if (cx != kEmpty) atomicMin(a.first_x + g, a.pair_base + cx);
-            if (cy != kEmpty) atomicMin(a.first_y + g, a.pair_base + cy);
-        }
     }
     // publish the bitmap of surviving marks for the cover kernels
     if (a.bm_shared && gbm)
@@ -363,15 +389,10 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
 // into a far buffer with cp.async; piece i + 1 reads them from there.  A
 // far fan-in the list could not hold is read from its plane row.
 //
-// Reverse (prune, markkernel.cuh:271-293): only pieces that hold a forward
-// mark, descending, only gates whose bitmap bit is set.  Pruned marks of
-// recent gates sit in a second ring (the same memory, R2 slots of BW words):
-// during piece [a, b) a fan-out fo is read from it iff fo < a + R2 and only
-// gates g < a + R2 write it.
-//
-// Merge (mergekernel.cuh:116-198) needs no level order: one sweep over the
-// surviving marks folds the first falling / rising pair of every net into
-// first_x / first_y with atomicMin.
+// Reverse (prune, markkernel.cuh:271-293) and merge (mergekernel.cuh:116-198):
+// see prune_and_merge.  Pruned marks of recent gates sit in a second ring
+// (the same memory, R2 slots of BW words): during piece [a, b) a fan-out fo
+// is read from it iff fo < a + R2 and only gates g < a + R2 write it.
 //
 // Plane rows are read and written BW words at a time: ld and pi_ld are
 // multiples of BW and every row holds all n_blocks * BW words; words at or
@@ -409,6 +430,17 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
     if (MODE != FWD_SIM)
         for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) S.bm[q] = 0;
     for (uint32_t q = threadIdx.x; q < (a.n_pieces + 31) / 32; q += blockDim.x) S.pbits[q] = 0;
+    if (MODE == FWD_FUSED) {  // the batch's cover state (the cover kernels run after this one)
+        // active words w0 .. w0 + BW - 1 of this block; word W (the count) by the last block
+        if (a.active && threadIdx.x < BW && w0 + threadIdx.x <= a.W) a.active[w0 + threadIdx.x] = 0;
+        if (a.active && blk == 0 && threadIdx.x == 0) a.active[a.W] = 0;
+        if (a.acc && blk == 0 && threadIdx.x == 0) {
+            a.acc->batch_lo = 0;
+            a.acc->batch_hi = 0;
+            a.acc->batch_flags = 0;
+            a.acc->done = 0;
+        }
+    }
     __shared__ uint32_t s_fail;
     if (threadIdx.x == 0) {
         s_fail = 0;
@@ -456,7 +488,8 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
             const uint32_t g = P.a + gi;
             const GateRec r = recs[gi];
             const uint32_t h = r.w[0];
-            // source word of fan-in q (pdf_device.cuh)
+            // source word of fan-in q (pdf_device.cuh); q is a constant for
+            // the inline fan-ins 0..3
             auto srcw = [&](uint32_t q) -> uint32_t {
                 if (q < (uint32_t)kInlineFanins) return r.w[3 + q];
                 const uint32_t f = __ldg(edges + r.w[2] + q);
@@ -496,12 +529,16 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
                     for (int j = 0; j < BW; j++) eval_first(h, fv.x[j], ft.x[j], V.x[j], v1.x[j]);
                 }
                 const uint32_t nfold = hdr_nfold(h);
-                for (uint32_t q = 1; q <= nfold; q++) {
+                auto fold = [&](uint32_t q) {
                     const uint32_t sq = srcw(q);
                     const Vec<BW> fv = load(sq, 0), ft = load(sq, 1);
 #pragma unroll
                     for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
-                }
+                };
+#pragma unroll
+                for (int q = 1; q < kInlineFanins; q++)
+                    if ((uint32_t)q <= nfold) fold(q);
+                for (uint32_t q = kInlineFanins; q <= nfold; q++) fold(q);
 #pragma unroll
                 for (int j = 0; j < BW; j++) eval_finish(h, V.x[j], v1.x[j], T.x[j]);
                 if (tail) {
@@ -517,7 +554,8 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
             if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
                 if (h & RF_INPT) {
                     M = T;
-                } else if ((h & RF_MARKF0) && vany(T)) {
+                } else if ((h & RF_MARKF0) && vany(T) && (!a.bm_shared || bit_test(S.bm, r.w[7]))) {
+                    // fan-in 0 (gate w[7]) holds a mark: its bitmap bit is set
                     const Vec<BW> m0 = load(r.w[3], 2);
 #pragma unroll
                     for (int j = 0; j < BW; j++) M.x[j] = T.x[j] & m0.x[j];
@@ -573,44 +611,36 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
 // Cover.
 // ---------------------------------------------------------------------------
 
-// Pairs that first-detect some net in this batch.
+// Pairs that first-detect some net in this batch: bitmap, and a list (in no
+// order) of each such pair once.
 __global__ void k_active(const CoverArgs a) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= a.c.n_gates) return;
-    const uint32_t fx = a.first_x[g], fy = a.first_y[g];
-    const uint32_t dx = fx - a.pair_base, dy = fy - a.pair_base;
-    if (fx != kEmpty && dx < a.n_pairs) atomicOr(a.active + (dx >> 5), 1u << (dx & 31));
-    if (fy != kEmpty && dy < a.n_pairs) atomicOr(a.active + (dy >> 5), 1u << (dy & 31));
+    const uint32_t f[2] = {a.first_x[g], a.first_y[g]};
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const uint32_t d = f[k] - a.pair_base;
+        if (f[k] == kEmpty || d >= a.n_pairs) continue;
+        const uint32_t bit = 1u << (d & 31);
+        if (!(atomicOr(a.active + (d >> 5), bit) & bit)) a.active_list[atomicAdd(a.active_count, 1u)] = d;
+    }
 }
 
-// Ordered list of the active pairs (one CTA).
-__global__ void __launch_bounds__(1024) k_active_compact(const CoverArgs a, uint32_t W) {
-    __shared__ uint32_t s_cnt[1024];
-    const uint32_t per = (W + blockDim.x - 1) / blockDim.x;
-    const uint32_t q0 = threadIdx.x * per, q1 = min(W, q0 + per);
-    uint32_t cnt = 0;
-    for (uint32_t q = q0; q < q1; q++) cnt += __popc(a.active[q]);
-    s_cnt[threadIdx.x] = cnt;
-    __syncthreads();
-    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {  // inclusive scan
-        const uint32_t v = threadIdx.x >= off ? s_cnt[threadIdx.x - off] : 0u;
-        __syncthreads();
-        s_cnt[threadIdx.x] += v;
-        __syncthreads();
+// Close a batch: total = min(2^128 - 1, total + batch); flags are sticky.
+__device__ void batch_close(DevAcc *acc, uint64_t n_pairs) {
+    pdf_u128 b = ((pdf_u128)acc->batch_hi << 64) | acc->batch_lo;
+    if (acc->batch_flags & PDF_FLAG_OVERFLOW) {
+        b = ~(pdf_u128)0;
+        acc->batch_lo = ~0ull;
+        acc->batch_hi = ~0ull;
     }
-    uint32_t pos = s_cnt[threadIdx.x] - cnt;
-    for (uint32_t q = q0; q < q1; q++) {
-        uint32_t bits = a.active[q];
-        while (bits) {
-            a.active_list[pos++] = q * 32 + (__ffs(bits) - 1);
-            bits &= bits - 1;
-        }
-    }
-    if (threadIdx.x == blockDim.x - 1) *a.active_count = s_cnt[threadIdx.x];
-}
-
-__device__ __forceinline__ uint32_t hash_slot(uint32_t g, uint32_t mask) {
-    return (g * 2654435761u) & mask;
+    pdf_u128 t = ((pdf_u128)acc->total_hi << 64) | acc->total_lo;
+    bool ovf = false;
+    t = add_sat(t, b, ovf);
+    acc->total_lo = (unsigned long long)t;
+    acc->total_hi = (unsigned long long)(t >> 64);
+    acc->flags |= acc->batch_flags | (ovf ? PDF_FLAG_OVERFLOW : 0u);
+    acc->pairs += n_pairs;
 }
 
 __device__ __forceinline__ pdf_u128 shfl_down_u128(pdf_u128 v, int d) {
@@ -637,22 +667,98 @@ __device__ void atomic_add_u128(unsigned long long *lo, unsigned long long *hi, 
     }
 }
 
-// One CTA per active pair (persistent over the list).  Walks the levels that
-// hold marks in the pair's column block, from the top down, over the nets
-// the pair marks (kernCover, coverkernel.cuh:193-229):
+// Exclusive prefix sum of one value per thread over the CTA (blockDim a
+// multiple of 32, <= 1024); *total gets the sum.  Uses s_warp[32].
+__device__ __forceinline__ uint32_t block_scan_excl(uint32_t v, uint32_t *s_warp, uint32_t *total) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= (uint32_t)d) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, d);
+            if (lane >= (uint32_t)d) w += y;
+        }
+        if (lane < nw) s_warp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp ? s_warp[warp - 1] : 0u) + x - v;
+    *total = s_warp[nw - 1];
+    __syncthreads();
+    return before;
+}
+
+// Index of gate g in the ascending list lid[0, n), or kEmpty.
+__device__ __forceinline__ uint32_t find_net(const uint32_t *lid, uint32_t n, uint32_t g) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (lid[mid] < g) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && lid[lo] == g ? lo : kEmpty;
+}
+
+// Level of gate g: the last l with level_off[l] <= g.
+__device__ __forceinline__ uint32_t level_of(const uint32_t *lo_tab, uint32_t n_levels, uint32_t g) {
+    uint32_t lo = 0, hi = n_levels;  // answer in [lo, hi)
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (lo_tab[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Path counting (kernCover, coverkernel.cuh:193-229, and kernSumSingle,
+// :77-105) for the pairs that first-detect some net.  One CTA per such pair
+// (persistent over the list).  All global reads are gathered first, each
+// phase in parallel across the CTA:
+//   A  the nets with a surviving mark in the pair's column block (bitmap
+//      words, in gate order, CAND at a time),
+//   B  of those, the nets the pair itself marks (one mark word each): the
+//      pair's net list, ascending (hence level order),
+//   C  per listed net its record, first-detect ids, level, and its fan-outs
+//      that are listed (as list indices);
+// then the recurrence runs in shared memory, levels descending:
 //   H = [po] + sum h(fo);  C = sum c(fo);  first = pid is first_x or first_y
 //   c = C + (first ? H : 0);  h = first ? 0 : H;  h = 0 on INPT
-// (unmarked nets hold h = c = 0 and are never stored).  (h, c) live in a
-// shared-memory open-addressing table keyed by net id.  Level-0 INPT c values
-// are summed into the batch count (kernSumSingle, coverkernel.cuh:77-105).
-__global__ void __launch_bounds__(512) k_cover(const CoverArgs a) {
+// (a net the pair does not mark has h = c = 0).  Level-0 INPT c values are
+// the pair's count.  A pair marking more than net_cap nets reports
+// kErrHashFull; fan-out lists past the adjacency buffer are read in place.
+constexpr uint32_t kCoverCand = 4096;   // candidates per chunk (128 bitmap words)
+constexpr uint32_t kCoverLevels = 2048; // level table entries kept in shared memory
+constexpr uint32_t kNetPo = 1u << 31, kNetInpt = 1u << 30, kNetFirst = 1u << 29, kNetLevel = (1u << 29) - 1;
+__global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
-    const uint32_t cap = a.hash_cap, cmask = cap - 1;
+    const uint32_t cap = a.hash_cap, acap = 4 * cap;
     pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw);
     pdf_u128 *cv = hv + cap;
-    uint32_t *keys = reinterpret_cast<uint32_t *>(cv + cap);
-    __shared__ pdf_u128 s_red[32];
+    uint32_t *lid = reinterpret_cast<uint32_t *>(cv + cap);  // [cap] listed nets, ascending
+    uint32_t *info = lid + cap;                               // [cap] kNet* flags | level
+    uint32_t *aoff = info + cap;                              // [cap] adjacency offset, kEmpty: read in place
+    uint32_t *acnt = aoff + cap;                              // [cap] adjacency length
+    uint32_t *adj = acnt + cap;                               // [4 cap] listed fan-outs (list indices)
+    uint32_t *cand = adj + acap;                              // [kCoverCand]
+    uint32_t *lvt = cand + kCoverCand;                        // [kCoverLevels] level_off
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_n, s_adj, s_over;
+    __shared__ pdf_u128 s_red[8];
     __shared__ unsigned int s_flags;
+
+    const uint32_t L = a.c.n_levels;
+    const bool lv_shared = L + 1 <= kCoverLevels;
+    if (lv_shared)
+        for (uint32_t i = threadIdx.x; i <= L; i += blockDim.x) lvt[i] = a.c.level_off[i];
+    const uint32_t *lo_tab = lv_shared ? lvt : a.c.level_off;
+    __syncthreads();
 
     const uint32_t n_active = *a.active_count;
     for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) {
@@ -661,72 +767,135 @@ __global__ void __launch_bounds__(512) k_cover(const CoverArgs a) {
         const uint32_t wp = p >> 5, bit = p & 31, blk = wp / a.bw;
         const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
         const uint32_t top = a.blk_maxlvl[blk];
-        for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) keys[i] = kEmpty;
-        if (threadIdx.x == 0) s_flags = 0;
+        const uint32_t gend = lo_tab[top];
+        const uint32_t nwords = (gend + 31) / 32;
+        if (threadIdx.x == 0) {
+            s_n = 0;
+            s_adj = 0;
+            s_over = 0;
+            s_flags = 0;
+        }
         __syncthreads();
+        // ---- A, B: the pair's nets, in gate order
+        for (uint32_t q0 = 0; q0 < nwords; q0 += kCoverCand / 32) {
+            const uint32_t q = q0 + threadIdx.x;
+            uint32_t bits = 0;
+            if (threadIdx.x < kCoverCand / 32 && q < nwords) {
+                bits = nzb[q];
+                if (q == nwords - 1 && (gend & 31)) bits &= (1u << (gend & 31)) - 1u;
+            }
+            uint32_t nc;
+            uint32_t pos = block_scan_excl(__popc(bits), s_warp, &nc);
+            while (bits) {
+                cand[pos++] = q * 32 + (__ffs(bits) - 1);
+                bits &= bits - 1;
+            }
+            __syncthreads();
+            // each thread tests a contiguous run of candidates (order kept)
+            const uint32_t per = (nc + blockDim.x - 1) / blockDim.x;
+            const uint32_t c0 = min(nc, threadIdx.x * per), c1 = min(nc, c0 + per);
+            uint32_t keep = 0, nk = 0;  // per <= kCoverCand / 256 = 16: one bit each
+            uint32_t mw[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) mw[k] = c0 + k < c1 ? a.M[(size_t)cand[c0 + k] * a.ld + wp] : 0u;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const uint32_t m = (mw[k] >> bit) & 1u;
+                keep |= m << k;
+                nk += m;
+            }
+            uint32_t nl;
+            const uint32_t at = block_scan_excl(nk, s_warp, &nl);
+            const uint32_t base = s_n;
+            if (base + nl > cap) {
+                if (threadIdx.x == 0) s_over = 1;
+            } else {
+                uint32_t o = base + at;
+                for (uint32_t i = c0; i < c1; i++)
+                    if ((keep >> (i - c0)) & 1u) lid[o++] = cand[i];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0 && !s_over) s_n = base + nl;
+            __syncthreads();
+            if (s_over) break;
+        }
+        if (s_over) {
+            if (threadIdx.x == 0) atomicOr(&a.acc->err, kErrHashFull);  // more nets than the list holds
+            __syncthreads();
+            continue;
+        }
+        const uint32_t n = s_n;
+        // ---- C: records, first ids, levels, listed fan-outs
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t g = lid[i];
+            const GateRec r = load_rec(a.c.rec + g);
+            const uint32_t fx = a.first_x[g], fy = a.first_y[g];
+            const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
+            uint32_t k = 0;
+            for (uint32_t j = 0; j < nfo; j += 4) {  // four fan-out loads in flight
+                uint32_t fo[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) fo[u] = j + u < nfo ? __ldg(a.c.edges + eb + j + u) : kEmpty;
+#pragma unroll
+                for (int u = 0; u < 4; u++) k += fo[u] != kEmpty && find_net(lid, n, fo[u]) != kEmpty ? 1u : 0u;
+            }
+            info[i] = (rec_po(r) ? kNetPo : 0u) | (rec_type(r) == PDF_INPT ? kNetInpt : 0u) |
+                      (fx == pid || fy == pid ? kNetFirst : 0u) | level_of(lo_tab, L, g);
+            const uint32_t o = k ? atomicAdd(&s_adj, k) : 0u;
+            if (o + k > acap) {
+                aoff[i] = kEmpty;  // fan-outs read in place during the recurrence
+                acnt[i] = nfo;
+            } else {
+                aoff[i] = o;
+                acnt[i] = k;
+                uint32_t w = o;
+                for (uint32_t j = 0; j < nfo && k; j++) {
+                    const uint32_t x = find_net(lid, n, __ldg(a.c.edges + eb + j));
+                    if (x != kEmpty) adj[w++] = x;
+                }
+            }
+        }
+        __syncthreads();
+        // ---- the recurrence, levels descending
         pdf_u128 total = 0;
         bool ovf = false;
-        for (int l = (int)top - 1; l >= 0; l--) {
-            const uint32_t s = a.c.level_off[l], e = a.c.level_off[l + 1];
-            if (e > s) {
-                const uint32_t q0 = s >> 5, q1 = (e - 1) >> 5;
-                for (uint32_t q = q0 + threadIdx.x; q <= q1; q += blockDim.x) {
-                    uint32_t bits = nzb[q];
-                    if (q == q0) bits &= 0xFFFFFFFFu << (s & 31);
-                    if (q == q1) bits &= 0xFFFFFFFFu >> (31 - ((e - 1) & 31));
-                    while (bits) {
-                        const uint32_t g = q * 32 + (__ffs(bits) - 1);
-                        bits &= bits - 1;
-                        if (!((a.M[(size_t)g * a.ld + wp] >> bit) & 1u)) continue;
-                        const GateRec r = load_rec(a.c.rec + g);
-                        pdf_u128 H = rec_po(r) ? 1 : 0, C = 0;
-                        const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
-                        for (uint32_t k = 0; k < nfo; k++) {
-                            const uint32_t fo = __ldg(a.c.edges + eb + k);
-                            uint32_t sl = hash_slot(fo, cmask);
-                            for (uint32_t probe = 0; probe < cap; probe++) {
-                                const uint32_t key = keys[sl];
-                                if (key == fo) {
-                                    bool dummy = false;
-                                    C = add_sat(C, cv[sl], ovf);
-                                    H = add_sat(H, hv[sl], dummy);
-                                    break;
-                                }
-                                if (key == kEmpty) break;
-                                sl = (sl + 1) & cmask;
-                            }
-                        }
-                        const bool first = a.first_x[g] == pid || a.first_y[g] == pid;
-                        pdf_u128 c = C, h = H;
-                        if (first) {
-                            c = add_sat(C, H, ovf);
-                            h = 0;
-                        }
-                        if (c == ~(pdf_u128)0) ovf = true;
-                        if (rec_type(r) == PDF_INPT) {
-                            h = 0;
-                            if (l == 0) total = add_sat(total, c, ovf);
-                        }
-                        if (l > 0) {  // level-0 values are never read
-                            uint32_t sl = hash_slot(g, cmask);
-                            uint32_t probe = 0;
-                            for (; probe < cap; probe++) {
-                                if (atomicCAS(keys + sl, kEmpty, g) == kEmpty) break;
-                                sl = (sl + 1) & cmask;
-                            }
-                            if (probe == cap) {
-                                atomicOr(&a.acc->err, kErrHashFull);  // table full
-                            } else {
-                                hv[sl] = h;
-                                cv[sl] = c;
-                            }
-                        }
+        const uint32_t lv_hi = n ? (info[n - 1] & kNetLevel) : 0;
+        for (int lv = (int)lv_hi; lv >= 0 && n; lv--) {
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint32_t inf = info[i];
+                if ((inf & kNetLevel) != (uint32_t)lv) continue;
+                pdf_u128 H = (inf & kNetPo) ? 1 : 0, C = 0;
+                bool dummy = false;
+                auto add = [&](uint32_t x) {
+                    C = add_sat(C, cv[x], ovf);
+                    H = add_sat(H, hv[x], dummy);
+                };
+                if (aoff[i] != kEmpty) {
+                    for (uint32_t j = 0; j < acnt[i]; j++) add(adj[aoff[i] + j]);
+                } else {
+                    const GateRec r = load_rec(a.c.rec + lid[i]);
+                    const uint32_t eb = r.w[2] + rec_nfi(r);
+                    for (uint32_t j = 0; j < acnt[i]; j++) {
+                        const uint32_t x = find_net(lid, n, __ldg(a.c.edges + eb + j));
+                        if (x != kEmpty) add(x);
                     }
                 }
+                pdf_u128 c = C, h = H;
+                if (inf & kNetFirst) {
+                    c = add_sat(C, H, ovf);
+                    h = 0;
+                }
+                if (c == ~(pdf_u128)0) ovf = true;
+                if (inf & kNetInpt) {
+                    h = 0;
+                    if (lv == 0) total = add_sat(total, c, ovf);
+                }
+                hv[i] = h;
+                cv[i] = c;
             }
             __syncthreads();
         }
-        // Block sum of the pair's count.
+        // ---- the pair's count into the batch count
         for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
         if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
         if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
@@ -741,6 +910,15 @@ __global__ void __launch_bounds__(512) k_cover(const CoverArgs a) {
             }
         }
         __syncthreads();
+    }
+    // the last CTA to finish closes the batch
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&a.acc->done, 1u) == gridDim.x - 1) {
+            __threadfence();
+            batch_close(a.acc, a.n_pairs);
+            a.acc->done = 0;
+        }
     }
 }
 
@@ -797,23 +975,7 @@ __global__ void k_batch_begin(DevAcc *acc) {
     acc->batch_lo = 0;
     acc->batch_hi = 0;
     acc->batch_flags = 0;
-}
-
-// total = min(2^128 - 1, total + batch); flags are sticky.
-__global__ void k_batch_end(DevAcc *acc, uint64_t n_pairs) {
-    pdf_u128 b = ((pdf_u128)acc->batch_hi << 64) | acc->batch_lo;
-    if (acc->batch_flags & PDF_FLAG_OVERFLOW) {
-        b = ~(pdf_u128)0;
-        acc->batch_lo = ~0ull;
-        acc->batch_hi = ~0ull;
-    }
-    pdf_u128 t = ((pdf_u128)acc->total_hi << 64) | acc->total_lo;
-    bool ovf = false;
-    t = add_sat(t, b, ovf);
-    acc->total_lo = (unsigned long long)t;
-    acc->total_hi = (unsigned long long)(t >> 64);
-    acc->flags |= acc->batch_flags | (ovf ? PDF_FLAG_OVERFLOW : 0u);
-    acc->pairs += n_pairs;
+    acc->done = 0;
 }
 
 template <int BW, int ROBUST, int MODE>
@@ -858,16 +1020,19 @@ cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, 
     }
 }
 
-size_t cover_smem_bytes(uint32_t hash_cap) { return (size_t)hash_cap * (4 + 2 * sizeof(pdf_u128)); }
+size_t cover_smem_bytes(uint32_t net_cap) {
+    return (size_t)net_cap * (2 * sizeof(pdf_u128) + 4 * 4 + 4 * 4) + (kCoverCand + kCoverLevels) * 4;
+}
 
-cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st) {
+cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bool zero_active, cudaStream_t st) {
     const uint32_t W = (uint32_t)((a.n_pairs + 31) / 32);
-    cudaError_t e = cudaMemsetAsync(a.active, 0, (size_t)W * sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
+    if (zero_active) {
+        cudaError_t e = cudaMemsetAsync(a.active, 0, (size_t)(W + 1) * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+    }
     k_active<<<(a.c.n_gates + 255) / 256, 256, 0, st>>>(a);
-    k_active_compact<<<1, 1024, 0, st>>>(a, W);
     const size_t smem = cover_smem_bytes(a.hash_cap);
-    e = cudaFuncSetAttribute(k_cover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_cover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_cover<<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
@@ -899,11 +1064,6 @@ cudaError_t launch_bitmap_from_marks(const DevCircuit &c, const uint32_t *M, uin
 
 cudaError_t launch_batch_begin(DevAcc *acc, cudaStream_t st) {
     k_batch_begin<<<1, 1, 0, st>>>(acc);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_batch_end(DevAcc *acc, uint64_t n_pairs, cudaStream_t st) {
-    k_batch_end<<<1, 1, 0, st>>>(acc, n_pairs);
     return cudaGetLastError();
 }
 

@@ -22,6 +22,18 @@ enum FwdMode {
     FWD_MARK = 2     // sim planes given; forward mark + prune (pdf_mark)
 };
 
+// Batch accumulators kept in device memory by a pdf_state.
+struct DevAcc {
+    unsigned long long batch_lo, batch_hi;  // this batch's count
+    unsigned long long total_lo, total_hi;  // running total
+    unsigned long long pairs;
+    unsigned int flags;                     // PDF_FLAG_*
+    unsigned int batch_flags;
+    unsigned int err;                       // device-side error code (0 = none)
+    unsigned int done;                      // cover CTAs finished (the last one closes the batch)
+    unsigned int pad[2];
+};
+
 struct FwdArgs {
     DevCircuit c;
     const Piece *pieces;          // level-ordered runs of gates (the unit of staging and of sync)
@@ -40,6 +52,8 @@ struct FwdArgs {
     uint32_t bm_words;
     uint32_t bm_shared;           // 1: the bitmap lives in shared memory during the kernel
     uint32_t *first_x, *first_y;  // [n_gates] (FWD_FUSED only)
+    DevAcc *acc;                  // FWD_FUSED: the batch count, zeroed by block 0 (may be null)
+    uint32_t *active;             // FWD_FUSED: the cover's active-pair bitmap [W] + count, zeroed (may be null)
     uint32_t *err;                // device error word (PDF_ETIMEOUT on a wait that expired)
     uint64_t n_pairs;
     uint32_t W;                   // ceil(n_pairs / 32)
@@ -57,17 +71,6 @@ struct FwdArgs {
 constexpr unsigned int kErrTimeout = 0x4u;     // a bounded wait expired (PDF_ETIMEOUT)
 constexpr unsigned int kErrHashFull = 0x100u;  // a pair marked more nets than the cover table holds
 
-// Batch accumulators kept in device memory by a pdf_state.
-struct DevAcc {
-    unsigned long long batch_lo, batch_hi;  // this batch's count
-    unsigned long long total_lo, total_hi;  // running total
-    unsigned long long pairs;
-    unsigned int flags;                     // PDF_FLAG_*
-    unsigned int batch_flags;
-    unsigned int err;                       // device-side error code (0 = none)
-    unsigned int pad[3];
-};
-
 struct CoverArgs {
     DevCircuit c;
     const uint32_t *M;            // pruned marks [n_gates][ld]
@@ -80,16 +83,19 @@ struct CoverArgs {
     uint64_t n_pairs;
     uint32_t pair_base;
     uint32_t *active;             // [W] bitmap of first-detecting pairs
-    uint32_t *active_list;        // [min(n_pairs, 2 * n_gates)] their indices, ascending
+    uint32_t *active_list;        // [min(n_pairs, 2 * n_gates)] their indices, in no order
     uint32_t *active_count;       // [1]
     DevAcc *acc;
-    uint32_t hash_cap;            // entries of the per-CTA shared-memory table (power of two)
+    uint32_t hash_cap;            // nets one pair may mark (the cover's shared-memory net list)
 };
 
 // Host-side launchers (pdf_kernels.cu).  All return cudaError_t of the launch.
 cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st);
-cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, cudaStream_t st);
+// Cover of one batch: k_active then k_cover, whose last CTA closes the batch
+// (total += batch, pairs += n_pairs).  The active bitmap [W] and its count
+// must be zero (k_forward clears them; zero_active asks for a memset).
+cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bool zero_active, cudaStream_t st);
 size_t cover_smem_bytes(uint32_t hash_cap);
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M,
                                uint64_t ld, uint64_t n_pairs, uint32_t pair_base,
@@ -102,6 +108,5 @@ constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
 cudaError_t noalloc_scratch(int device, unsigned char **out);
 
 cudaError_t launch_batch_begin(DevAcc *acc, cudaStream_t st);
-cudaError_t launch_batch_end(DevAcc *acc, uint64_t n_pairs, cudaStream_t st);
 
 #endif
