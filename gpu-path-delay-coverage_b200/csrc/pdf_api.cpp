@@ -333,7 +333,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     }
     c->bw = o.tile_words ? o.tile_words : 4;
     const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
-    c->threads = o.threads ? std::min(o.threads, max_threads) : 512;
+    uint32_t threads_default = 512;  // set from the piece size below
     const size_t budget = c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
                                       : std::min<size_t>(prop.sharedMemPerBlockOptin,
                                                          prop.sharedMemPerMultiprocessor / 2 - 2048);
@@ -347,6 +347,10 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     for (uint32_t l = 1; l < L; l++) widest = std::max(widest, nl->level_offsets[l + 1] - nl->level_offsets[l]);
     if (L == 1) widest = inf.max_level_width;
     c->cap = std::min<uint32_t>(512, (widest + 31) & ~31u);
+    // one thread per gate of a piece plus two warps that have none: they
+    // issue the next piece's far-row copies
+    threads_default = std::min<uint32_t>(max_threads, c->cap + 64);
+    c->threads = o.threads ? std::min(o.threads, max_threads) : threads_default;
     c->ecap = 2048;
     std::vector<Piece> pieces;
     auto f4 = [](uint64_t x) { return x & ~(uint64_t)3; };
@@ -778,8 +782,13 @@ pdf_status stage_pairs(pdf_circuit *c, Workspace &ws, const pdf_pairs *pr, const
     PDF_CUDA(ws.pi.ensure(2 * npi * Wp * 4));
     uint32_t *dv = ws.pi.as<uint32_t>(), *dt = dv + npi * Wp;
     const cudaMemcpyKind k = pr->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    PDF_CUDA(cudaMemcpy2DAsync(dv, Wp * 4, pr->v, pr->ld * 4, W * 4, npi, k, st));
-    PDF_CUDA(cudaMemcpy2DAsync(dt, Wp * 4, pr->t, pr->ld * 4, W * 4, npi, k, st));
+    if (pr->ld == Wp) {  // rows already at the device pitch: one contiguous copy per plane
+        PDF_CUDA(cudaMemcpyAsync(dv, pr->v, npi * Wp * 4, k, st));
+        PDF_CUDA(cudaMemcpyAsync(dt, pr->t, npi * Wp * 4, k, st));
+    } else {
+        PDF_CUDA(cudaMemcpy2DAsync(dv, Wp * 4, pr->v, pr->ld * 4, W * 4, npi, k, st));
+        PDF_CUDA(cudaMemcpy2DAsync(dt, Wp * 4, pr->t, pr->ld * 4, W * 4, npi, k, st));
+    }
     *v = dv;
     *t = dt;
     *ld = Wp;
