@@ -168,7 +168,8 @@ def run_reference(args):
     n = w["pairs"]
     v, t = P.gen_pairs(P.pair_seed(w["gen"].seed), nl.n_pi, n)
     threads = os.cpu_count() or 1
-    n_sample = min(n, args.ref_sample)
+    G = nl.n_gates
+    n_sample = min(n, args.ref_sample or (n if G * n <= 2e9 else max(32, int(6.5e8 / G) // 32 * 32)))
     codes = P.codes_from_planes(v[:, :P.words(n_sample)], t[:, :P.words(n_sample)], n_sample)
     for _ in range(args.warmup):
         O.grade(nl, codes, n_sample, mark_mode=P.MARK_ROBUST, threads=threads)
@@ -344,7 +345,8 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         O = oracle()
-        line["cpu_baseline"] = cpu_baseline(P, O, nl, v, t, min(n, args.cpu_sample), os.cpu_count() or 1)
+        sample = args.cpu_sample or (n if G * n <= 2e9 else max(32, int(1.3e9 / G) // 32 * 32))
+        line["cpu_baseline"] = cpu_baseline(P, O, nl, v, t, min(n, sample), os.cpu_count() or 1)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -360,8 +362,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2")
-    ap.add_argument("--cpu-sample", type=int, default=1 << 30)
-    ap.add_argument("--ref-sample", type=int, default=1 << 30)
+    # CPU samples: pairs per timed CPU run (0 = the whole workload up to 2e9
+    # gate-evals, else about 1.3e9 gate-evals for the baseline and 6.5e8 per
+    # reference-arm step: a few seconds on the host cores)
+    ap.add_argument("--cpu-sample", type=int, default=0)
+    ap.add_argument("--ref-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

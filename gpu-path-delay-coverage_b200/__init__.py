@@ -27,6 +27,7 @@ UNKN, INPT, AND, NAND, OR, NOR, XOR, XNOR, BUFF, NOT, FROM, DFF = range(12)
 S0, S1, T0, T1 = range(4)
 MARK_DEFAULT, MARK_ROBUST = 0, 1
 FLAG_OVERFLOW = 1
+BATCH_APPEND = 1
 NONE = 0xFFFFFFFF
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "EOVERFLOW", 4: "ETIMEOUT", 5: "ECUDA",
@@ -69,6 +70,15 @@ class Totals_t(C.Structure):
 class CircuitOpts_t(C.Structure):
     _fields_ = [("device", C.c_int), ("mark_mode", C.c_int), ("max_pairs", C.c_uint32),
                 ("tile_words", C.c_uint32), ("threads", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+
+class BatchJob_t(C.Structure):
+    _fields_ = [("circuit", C.c_void_p), ("state", C.c_void_p), ("pairs", Pairs_t), ("pair_base", C.c_uint64)]
+
+
+class BatchInfo_t(C.Structure):
+    _fields_ = [("n_jobs", C.c_uint32), ("tile_words", C.c_uint32), ("threads", C.c_uint32),
+                ("ctas", C.c_uint32), ("gate_evals", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
 class CircuitInfo_t(C.Structure):
@@ -120,6 +130,14 @@ ABI = [
                             C.POINTER(Totals_t), C.c_void_p]),
     ("pdf_cover_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_void_p, C.POINTER(Totals_t), C.c_void_p]),
+    ("pdf_batch_create", C.c_int, [C.POINTER(BatchJob_t), C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("pdf_batch_destroy", None, [C.c_void_p]),
+    ("pdf_batch_query", C.c_int, [C.c_void_p, C.POINTER(BatchInfo_t)]),
+    ("pdf_batch_run_async", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pdf_batch_run", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pdf_batch_autotune", C.c_int, [C.POINTER(C.POINTER(Netlist_t)), C.POINTER(C.c_uint64), C.c_uint32,
+                                     C.POINTER(CircuitOpts_t), C.c_uint32, C.POINTER(CircuitOpts_t),
+                                     C.POINTER(C.c_float)]),
     ("pdf_gen_netlist", C.c_int, [C.POINTER(GenParams_t), C.POINTER(C.c_void_p)]),
     ("pdf_netbuf_from", C.c_int, [C.POINTER(Netlist_t), C.POINTER(C.c_void_p)]),
     ("pdf_netbuf_view", None, [C.c_void_p, C.POINTER(Netlist_t)]),
@@ -423,6 +441,60 @@ def make_pairs(v, t, n_pairs: int) -> Pairs_t:
 def make_outputs(sim_v=None, sim_t=None, mark=None) -> Outputs_t:
     ref = next(x for x in (sim_v, sim_t, mark) if x is not None)
     return Outputs_t(_addr(sim_v), _addr(sim_t), _addr(mark), ref.shape[1], _on_device(ref))
+
+
+class Batch:
+    """Many (circuit, state, device pairs) jobs graded per pass (pdf_batch_*).
+
+    jobs: (Circuit, State, v, t, n_pairs, pair_base) with v, t device tensors
+    of shape [n_pi, ld]; the tensors must stay alive (and at their address)
+    while the batch exists.  append: each run advances every job's pair_base
+    by its pair count."""
+
+    def __init__(self, jobs, append: bool = False):
+        self.jobs = list(jobs)  # keeps circuits, states and pair tensors alive
+        arr = (BatchJob_t * len(self.jobs))()
+        for k, (c, s, v, t, n, base) in enumerate(self.jobs):
+            arr[k] = BatchJob_t(c.h, s.h, make_pairs(v, t, n), base)
+        h = C.c_void_p()
+        check(lib().pdf_batch_create(arr, len(self.jobs), BATCH_APPEND if append else 0, C.byref(h)),
+              "pdf_batch_create")
+        self.h = h
+
+    def info(self) -> BatchInfo_t:
+        i = BatchInfo_t()
+        check(lib().pdf_batch_query(self.h, C.byref(i)), "pdf_batch_query")
+        return i
+
+    def run_async(self, stream: int = 0):
+        check(lib().pdf_batch_run_async(self.h, C.c_void_p(stream)), "pdf_batch_run_async")
+
+    def run(self, stream: int = 0):
+        check(lib().pdf_batch_run(self.h, C.c_void_p(stream)), "pdf_batch_run")
+
+    def close(self):
+        if self.h:
+            lib().pdf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_autotune(netlists, n_pairs, mark_mode: int = MARK_DEFAULT, reps: int = 3, device: int = 0):
+    """Best tile width for grading these circuits as one batch: (opts, ms per pass)."""
+    views = [nl.view() for nl in netlists]
+    ptrs = (C.POINTER(Netlist_t) * len(views))(*[C.pointer(v) for v in views])
+    npairs = (C.c_uint64 * len(views))(*n_pairs)
+    base = CircuitOpts_t(device, mark_mode, 0, 0, 0)
+    best = CircuitOpts_t()
+    ms = C.c_float()
+    check(lib().pdf_batch_autotune(ptrs, npairs, len(views), C.byref(base), reps, C.byref(best), C.byref(ms)),
+          "pdf_batch_autotune")
+    return best, ms.value
 
 
 def grade(c: Circuit, s: State, v, t, n_pairs: int, pair_base: int = 0, sim_v=None, sim_t=None,

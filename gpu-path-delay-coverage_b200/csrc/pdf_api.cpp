@@ -1145,3 +1145,271 @@ extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, ui
     chunk_total->reserved = 0;
     return err_status(h.err);
 }
+
+// ---------------------------------------------------------------------------
+// Batched grading.
+// ---------------------------------------------------------------------------
+
+struct pdf_batch {
+    int device = 0;
+    std::vector<pdf_circuit *> circuits;
+    std::vector<pdf_state *> states;
+    BatchLaunch L{};
+    DevBuf fargs, cargs, bpref, gpref, items, ctl;
+    uint64_t gate_evals = 0, bytes = 0;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        exec = nullptr;
+        graph = nullptr;
+        cap_stream = nullptr;
+        fargs.release();
+        cargs.release();
+        bpref.release();
+        gpref.release();
+        items.release();
+        ctl.release();
+    }
+};
+
+extern "C" pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out) {
+    if (!out) return PDF_EINVAL;
+    *out = nullptr;
+    if (!jobs || !n_jobs || (flags & ~(uint32_t)PDF_BATCH_APPEND)) return PDF_EINVAL;
+    pdf_circuit *c0 = jobs[0].circuit;
+    if (!c0) return PDF_EINVAL;
+    for (uint32_t i = 0; i < n_jobs; i++) {
+        const pdf_batch_job &j = jobs[i];
+        if (!j.circuit || !j.state || j.state->c != j.circuit || j.circuit->device != c0->device ||
+            j.circuit->bw != c0->bw || j.circuit->mark_mode != c0->mark_mode)
+            return PDF_EINVAL;
+        const uint64_t n = j.pairs.n_pairs, W = (n + 31) / 32;
+        if (n == 0 || !j.pairs.on_device || j.pair_base + n > 0xFFFFFFFFull ||
+            !planes_fit(j.circuit, W, j.pairs.ld, {j.pairs.v, j.pairs.t}))
+            return PDF_EINVAL;
+    }
+    DeviceGuard dg(c0->device);
+    if (!dg.ok) return PDF_ECUDA;
+    pdf_batch *b = new (std::nothrow) pdf_batch();
+    if (!b) return PDF_ENOMEM;
+    b->device = c0->device;
+    auto fail = [&](pdf_status st) {
+        b->release();
+        delete b;
+        (void)cudaGetLastError();
+        return st;
+    };
+    std::vector<FwdArgs> fa(n_jobs);
+    std::vector<CoverArgs> ca(n_jobs);
+    std::vector<uint32_t> bp(n_jobs + 1, 0), gp(n_jobs + 1, 0);
+    uint64_t items = 0;
+    BatchLaunch &L = b->L;
+    L.bw = c0->bw;
+    L.robust = c0->mark_mode == PDF_MARK_ROBUST ? 1u : 0u;
+    L.hash_cap = c0->hash_cap;
+    for (uint32_t i = 0; i < n_jobs; i++) {
+        const pdf_batch_job &j = jobs[i];
+        pdf_circuit *c = j.circuit;
+        pdf_state *s = j.state;
+        const uint64_t n = j.pairs.n_pairs, W = (n + 31) / 32, G = c->info.n_gates;
+        if (ensure_ws(c, s->ws, W, true) != PDF_OK) return fail(PDF_ENOMEM);
+        FwdArgs a = base_fwd(c, n);
+        a.pi_v = j.pairs.v;
+        a.pi_t = j.pairs.t;
+        a.pi_ld = j.pairs.ld;
+        a.store_all = 0;
+        a.ld = s->ws.plane_ld;
+        a.V = s->ws.planes.as<uint32_t>();
+        a.T = a.V + G * a.ld;
+        a.M = a.T + G * a.ld;
+        a.nzb = s->ws.nzb.as<uint32_t>();
+        a.blk_maxlvl = s->ws.maxlvl.as<uint32_t>();
+        a.first_x = s->first_x.as<uint32_t>();
+        a.first_y = s->first_y.as<uint32_t>();
+        a.pair_base = (uint32_t)j.pair_base;
+        DevAcc *acc = s->acc.as<DevAcc>();
+        a.err = &acc->err;
+        a.acc = acc;
+        a.active = s->ws.active.as<uint32_t>();
+        fa[i] = a;
+        ca[i] = base_cover(c, s->ws, a.M, a.ld, n, (uint32_t)j.pair_base, a.first_x, a.first_y, acc);
+        const uint64_t blocks = (W + c->bw - 1) / c->bw;
+        if (bp[i] + blocks > 0x7FFFFFFFull || gp[i] + G > 0xFFFFFFFFull) return fail(PDF_ENOTSUP);
+        bp[i + 1] = bp[i] + (uint32_t)blocks;
+        gp[i + 1] = gp[i] + (uint32_t)G;
+        items += std::min<uint64_t>(W * 32, 2 * G);
+        L.threads = std::max(L.threads, c->threads);
+        L.fwd_smem = std::max(L.fwd_smem, c->fwd_smem);
+        L.cover_grid = std::max(L.cover_grid, c->cover_grid);
+        b->gate_evals += G * n;
+        b->circuits.push_back(c);
+        b->states.push_back(s);
+    }
+    L.n = n_jobs;
+    L.total_blocks = bp[n_jobs];
+    L.total_gates = gp[n_jobs];
+    L.append = (flags & PDF_BATCH_APPEND) ? 1u : 0u;
+    if (b->fargs.ensure(sizeof(FwdArgs) * n_jobs) != cudaSuccess ||
+        b->cargs.ensure(sizeof(CoverArgs) * n_jobs) != cudaSuccess ||
+        b->bpref.ensure(4 * (n_jobs + 1)) != cudaSuccess || b->gpref.ensure(4 * (n_jobs + 1)) != cudaSuccess ||
+        b->items.ensure(sizeof(uint2) * std::max<uint64_t>(items, 1)) != cudaSuccess ||
+        b->ctl.ensure(sizeof(BatchCtl)) != cudaSuccess)
+        return fail(PDF_ENOMEM);
+    if (cudaMemcpy(b->fargs.p, fa.data(), sizeof(FwdArgs) * n_jobs, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->cargs.p, ca.data(), sizeof(CoverArgs) * n_jobs, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->bpref.p, bp.data(), 4 * (n_jobs + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->gpref.p, gp.data(), 4 * (n_jobs + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->ctl.p, 0, sizeof(BatchCtl)) != cudaSuccess)
+        return fail(PDF_ECUDA);
+    L.fargs = b->fargs.as<FwdArgs>();
+    L.cargs = b->cargs.as<CoverArgs>();
+    L.bpref = b->bpref.as<uint32_t>();
+    L.gpref = b->gpref.as<uint32_t>();
+    L.items = b->items.as<uint2>();
+    L.ctl = b->ctl.as<BatchCtl>();
+    b->bytes = b->fargs.bytes + b->cargs.bytes + b->bpref.bytes + b->gpref.bytes + b->items.bytes + b->ctl.bytes;
+    if (prepare_batch(L) != cudaSuccess) return fail(PDF_ECUDA);
+    if (cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PDF_ECUDA);
+    *out = b;
+    return PDF_OK;
+}
+
+extern "C" void pdf_batch_destroy(pdf_batch *b) {
+    if (!b) return;
+    DeviceGuard dg(b->device);
+    b->release();
+    delete b;
+}
+
+extern "C" pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info) {
+    if (!b || !info) return PDF_EINVAL;
+    info->n_jobs = b->L.n;
+    info->tile_words = b->L.bw;
+    info->threads = b->L.threads;
+    info->ctas = b->L.total_blocks;
+    info->gate_evals = b->gate_evals;
+    info->device_bytes = b->bytes;
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_batch_run_async(pdf_batch *b, void *stream) {
+    if (!b) return PDF_EINVAL;
+    DeviceGuard dg(b->device);
+    if (!dg.ok) return PDF_ECUDA;
+    if (!b->exec) {  // capture the three launches once
+        PDF_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t le = launch_batch(b->L, b->cap_stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(b->cap_stream, &g);
+        if (le != cudaSuccess || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            (void)cudaGetLastError();
+            return PDF_ECUDA;
+        }
+        b->graph = g;
+        PDF_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    PDF_CUDA(cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)));
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_batch_run(pdf_batch *b, void *stream) {
+    pdf_status st = pdf_batch_run_async(b, stream);
+    if (st != PDF_OK) return st;
+    DeviceGuard dg(b->device);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    PDF_CUDA(cudaStreamSynchronize(cs));
+    unsigned int err = 0;
+    for (size_t i = 0; i < b->states.size(); i++) {
+        DevAcc h{};
+        unsigned int ce = 0;
+        PDF_CUDA(cudaMemcpy(&h, b->states[i]->acc.p, sizeof h, cudaMemcpyDeviceToHost));
+        PDF_CUDA(cudaMemcpy(&ce, b->circuits[i]->err.p, sizeof ce, cudaMemcpyDeviceToHost));
+        err |= h.err | ce;
+    }
+    return err_status(err);
+}
+
+// Autotuner of the batch tile width: times the whole batch at each candidate.
+extern "C" pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, const uint64_t *n_pairs, uint32_t n,
+                                         const pdf_circuit_opts *base, uint32_t reps, pdf_circuit_opts *best,
+                                         float *best_ms) {
+    if (!netlists || !n_pairs || !n || !best || reps == 0) return PDF_EINVAL;
+    const pdf_circuit_opts b0 = base ? *base : pdf_circuit_opts{};
+    DeviceGuard dg(b0.device);
+    if (!dg.ok) return PDF_ECUDA;
+    float best_t = 0.0f;
+    uint32_t best_w = 0;
+    pdf_status last = PDF_OK;
+    for (uint32_t tw : {2u, 4u, 8u}) {
+        pdf_circuit_opts o = b0;
+        o.tile_words = tw;
+        std::vector<pdf_circuit *> cs(n, nullptr);
+        std::vector<pdf_state *> ss(n, nullptr);
+        std::vector<void *> bufs(n, nullptr);
+        std::vector<pdf_batch_job> jobs(n);
+        pdf_batch *b = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        pdf_status st = PDF_OK;
+        for (uint32_t i = 0; i < n && st == PDF_OK; i++) {
+            st = pdf_circuit_create(netlists[i], &o, &cs[i]);
+            if (st == PDF_OK) st = pdf_state_create(cs[i], &ss[i]);
+            if (st != PDF_OK) break;
+            const uint64_t np = n_pairs[i], W = (np + 31) / 32, ld = (W + tw - 1) / tw * tw;
+            const uint32_t npi = cs[i]->info.n_pi;
+            std::vector<uint32_t> v(npi * ld), t(npi * ld);
+            st = pdf_gen_pairs(0x7A11u + i, npi, np, ld, v.data(), t.data());
+            if (st != PDF_OK) break;
+            if (cudaMalloc(&bufs[i], 2 * npi * ld * 4) != cudaSuccess) {
+                st = PDF_ENOMEM;
+                break;
+            }
+            uint32_t *dv = static_cast<uint32_t *>(bufs[i]), *dt = dv + npi * ld;
+            if (cudaMemcpy(dv, v.data(), npi * ld * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(dt, t.data(), npi * ld * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+                st = PDF_ECUDA;
+                break;
+            }
+            jobs[i] = pdf_batch_job{cs[i], ss[i], pdf_pairs{dv, dt, np, ld, 1}, 0};
+        }
+        if (st == PDF_OK) st = pdf_batch_create(jobs.data(), n, 0, &b);
+        if (st == PDF_OK) st = pdf_batch_run(b, nullptr);  // warm-up (captures the graph)
+        float ms = 0.0f;
+        if (st == PDF_OK) {
+            if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+                cudaEventRecord(e0, nullptr) != cudaSuccess)
+                st = PDF_ECUDA;
+            for (uint32_t r = 0; r < reps && st == PDF_OK; r++) st = pdf_batch_run_async(b, nullptr);
+            if (st == PDF_OK && (cudaEventRecord(e1, nullptr) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                 cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                st = PDF_ECUDA;
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        pdf_batch_destroy(b);
+        for (uint32_t i = 0; i < n; i++) {
+            pdf_state_destroy(ss[i]);
+            pdf_circuit_destroy(cs[i]);
+            if (bufs[i]) cudaFree(bufs[i]);
+        }
+        (void)cudaGetLastError();
+        if (st != PDF_OK) {  // a tile that does not fit is skipped
+            last = st;
+            continue;
+        }
+        ms /= (float)reps;
+        if (!best_w || ms < best_t) {
+            best_t = ms;
+            best_w = tw;
+        }
+    }
+    if (!best_w) return last;
+    *best = b0;
+    best->tile_words = best_w;
+    if (best_ms) *best_ms = best_t;
+    return PDF_OK;
+}

@@ -398,8 +398,9 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
 // multiples of BW and every row holds all n_blocks * BW words; words at or
 // past ceil(n_pairs / 32) are masked to zero.
 // ---------------------------------------------------------------------------
+// One CTA's work: column block `blk` of the circuit in `a`.
 template <int BW, int ROBUST, int MODE>
-__global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
+__device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk) {
     extern __shared__ __align__(128) unsigned char smraw[];
     FwdSmem S;
     S.ring = reinterpret_cast<uint32_t *>(smraw + a.off_ring);
@@ -408,7 +409,6 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
     S.far = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
     S.pbits = reinterpret_cast<uint32_t *>(smraw + a.off_pbits);
     S.mbar = reinterpret_cast<uint64_t *>(smraw + a.off_mbar);
-    const uint32_t blk = blockIdx.x;
     const uint32_t w0 = blk * BW;
     S.bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
     uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
@@ -607,23 +607,34 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
     }
 }
 
+template <int BW, int ROBUST, int MODE>
+__global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
+    forward_cta<BW, ROBUST, MODE>(a, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // Cover.
 // ---------------------------------------------------------------------------
 
 // Pairs that first-detect some net in this batch: bitmap, and a list (in no
 // order) of each such pair once.
-__global__ void k_active(const CoverArgs a) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= a.c.n_gates) return;
+// Gate g: its first-detecting pairs into the bitmap; emit(d) for each pair
+// whose bit it set.
+template <class Emit>
+__device__ __forceinline__ void active_gate(const CoverArgs &a, uint32_t g, Emit emit) {
     const uint32_t f[2] = {a.first_x[g], a.first_y[g]};
 #pragma unroll
     for (int k = 0; k < 2; k++) {
         const uint32_t d = f[k] - a.pair_base;
         if (f[k] == kEmpty || d >= a.n_pairs) continue;
         const uint32_t bit = 1u << (d & 31);
-        if (!(atomicOr(a.active + (d >> 5), bit) & bit)) a.active_list[atomicAdd(a.active_count, 1u)] = d;
+        if (!(atomicOr(a.active + (d >> 5), bit) & bit)) emit(d);
     }
+}
+__global__ void k_active(const CoverArgs a) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.c.n_gates) return;
+    active_gate(a, g, [&](uint32_t d) { a.active_list[atomicAdd(a.active_count, 1u)] = d; });
 }
 
 // Close a batch: total = min(2^128 - 1, total + batch); flags are sticky.
@@ -736,7 +747,16 @@ __device__ __forceinline__ uint32_t level_of(const uint32_t *lo_tab, uint32_t n_
 constexpr uint32_t kCoverCand = 4096;   // candidates per chunk (128 bitmap words)
 constexpr uint32_t kCoverLevels = 2048; // level table entries kept in shared memory
 constexpr uint32_t kNetPo = 1u << 31, kNetInpt = 1u << 30, kNetFirst = 1u << 29, kNetLevel = (1u << 29) - 1;
-__global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
+// Byte offset of the level table in k_cover's shared memory: after h, c
+// (u128), the net list, flags, adjacency offsets and lengths, 4 cap
+// adjacency entries and the candidates.
+__host__ __device__ constexpr size_t cover_smem_lvt(uint32_t cap) {
+    return (size_t)cap * (2 * sizeof(pdf_u128) + 4 * 4 + 4 * 4) + (size_t)kCoverCand * 4;
+}
+
+// The cover of pair p (index within the batch) of the circuit in `a`;
+// lo_tab is its level table (shared or global memory).
+__device__ __forceinline__ void cover_pair(const CoverArgs &a, const uint32_t p, const uint32_t *lo_tab) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const uint32_t cap = a.hash_cap, acap = 4 * cap;
     pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw);
@@ -747,170 +767,172 @@ __global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
     uint32_t *acnt = aoff + cap;                              // [cap] adjacency length
     uint32_t *adj = acnt + cap;                               // [4 cap] listed fan-outs (list indices)
     uint32_t *cand = adj + acap;                              // [kCoverCand]
-    uint32_t *lvt = cand + kCoverCand;                        // [kCoverLevels] level_off
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_n, s_adj, s_over;
     __shared__ pdf_u128 s_red[8];
     __shared__ unsigned int s_flags;
 
     const uint32_t L = a.c.n_levels;
+    const uint32_t pid = a.pair_base + p;
+    const uint32_t wp = p >> 5, bit = p & 31, blk = wp / a.bw;
+    const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
+    const uint32_t top = a.blk_maxlvl[blk];
+    const uint32_t gend = lo_tab[top];
+    const uint32_t nwords = (gend + 31) / 32;
+    if (threadIdx.x == 0) {
+        s_n = 0;
+        s_adj = 0;
+        s_over = 0;
+        s_flags = 0;
+    }
+    __syncthreads();
+    // ---- A, B: the pair's nets, in gate order
+    for (uint32_t q0 = 0; q0 < nwords; q0 += kCoverCand / 32) {
+        const uint32_t q = q0 + threadIdx.x;
+        uint32_t bits = 0;
+        if (threadIdx.x < kCoverCand / 32 && q < nwords) {
+            bits = nzb[q];
+            if (q == nwords - 1 && (gend & 31)) bits &= (1u << (gend & 31)) - 1u;
+        }
+        uint32_t nc;
+        uint32_t pos = block_scan_excl(__popc(bits), s_warp, &nc);
+        while (bits) {
+            cand[pos++] = q * 32 + (__ffs(bits) - 1);
+            bits &= bits - 1;
+        }
+        __syncthreads();
+        // each thread tests a contiguous run of candidates (order kept)
+        const uint32_t per = (nc + blockDim.x - 1) / blockDim.x;
+        const uint32_t c0 = min(nc, threadIdx.x * per), c1 = min(nc, c0 + per);
+        uint32_t keep = 0, nk = 0;  // per <= kCoverCand / 256 = 16: one bit each
+        uint32_t mw[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) mw[k] = c0 + k < c1 ? a.M[(size_t)cand[c0 + k] * a.ld + wp] : 0u;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const uint32_t m = (mw[k] >> bit) & 1u;
+            keep |= m << k;
+            nk += m;
+        }
+        uint32_t nl;
+        const uint32_t at = block_scan_excl(nk, s_warp, &nl);
+        const uint32_t base = s_n;
+        if (base + nl > cap) {
+            if (threadIdx.x == 0) s_over = 1;
+        } else {
+            uint32_t o = base + at;
+            for (uint32_t i = c0; i < c1; i++)
+                if ((keep >> (i - c0)) & 1u) lid[o++] = cand[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && !s_over) s_n = base + nl;
+        __syncthreads();
+        if (s_over) break;
+    }
+    if (s_over) {
+        if (threadIdx.x == 0) atomicOr(&a.acc->err, kErrHashFull);  // more nets than the list holds
+        __syncthreads();
+        return;
+    }
+    const uint32_t n = s_n;
+    // ---- C: records, first ids, levels, listed fan-outs
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t g = lid[i];
+        const GateRec r = load_rec(a.c.rec + g);
+        const uint32_t fx = a.first_x[g], fy = a.first_y[g];
+        const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
+        uint32_t k = 0;
+        for (uint32_t j = 0; j < nfo; j += 4) {  // four fan-out loads in flight
+            uint32_t fo[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) fo[u] = j + u < nfo ? __ldg(a.c.edges + eb + j + u) : kEmpty;
+#pragma unroll
+            for (int u = 0; u < 4; u++) k += fo[u] != kEmpty && find_net(lid, n, fo[u]) != kEmpty ? 1u : 0u;
+        }
+        info[i] = (rec_po(r) ? kNetPo : 0u) | (rec_type(r) == PDF_INPT ? kNetInpt : 0u) |
+                  (fx == pid || fy == pid ? kNetFirst : 0u) | level_of(lo_tab, L, g);
+        const uint32_t o = k ? atomicAdd(&s_adj, k) : 0u;
+        if (o + k > acap) {
+            aoff[i] = kEmpty;  // fan-outs read in place during the recurrence
+            acnt[i] = nfo;
+        } else {
+            aoff[i] = o;
+            acnt[i] = k;
+            uint32_t w = o;
+            for (uint32_t j = 0; j < nfo && k; j++) {
+                const uint32_t x = find_net(lid, n, __ldg(a.c.edges + eb + j));
+                if (x != kEmpty) adj[w++] = x;
+            }
+        }
+    }
+    __syncthreads();
+    // ---- the recurrence, levels descending
+    pdf_u128 total = 0;
+    bool ovf = false;
+    const uint32_t lv_hi = n ? (info[n - 1] & kNetLevel) : 0;
+    for (int lv = (int)lv_hi; lv >= 0 && n; lv--) {
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t inf = info[i];
+            if ((inf & kNetLevel) != (uint32_t)lv) continue;
+            pdf_u128 H = (inf & kNetPo) ? 1 : 0, C = 0;
+            bool dummy = false;
+            auto add = [&](uint32_t x) {
+                C = add_sat(C, cv[x], ovf);
+                H = add_sat(H, hv[x], dummy);
+            };
+            if (aoff[i] != kEmpty) {
+                for (uint32_t j = 0; j < acnt[i]; j++) add(adj[aoff[i] + j]);
+            } else {
+                const GateRec r = load_rec(a.c.rec + lid[i]);
+                const uint32_t eb = r.w[2] + rec_nfi(r);
+                for (uint32_t j = 0; j < acnt[i]; j++) {
+                    const uint32_t x = find_net(lid, n, __ldg(a.c.edges + eb + j));
+                    if (x != kEmpty) add(x);
+                }
+            }
+            pdf_u128 c = C, h = H;
+            if (inf & kNetFirst) {
+                c = add_sat(C, H, ovf);
+                h = 0;
+            }
+            if (c == ~(pdf_u128)0) ovf = true;
+            if (inf & kNetInpt) {
+                h = 0;
+                if (lv == 0) total = add_sat(total, c, ovf);
+            }
+            hv[i] = h;
+            cv[i] = c;
+        }
+        __syncthreads();
+    }
+    // ---- the pair's count into the batch count
+    for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
+    if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        pdf_u128 t = threadIdx.x < (blockDim.x + 31) / 32 ? s_red[threadIdx.x] : 0;
+        bool o2 = false;
+        for (int d = 16; d > 0; d >>= 1) t = add_sat(t, shfl_down_u128(t, d), o2);
+        if (threadIdx.x == 0) {
+            if (o2 || s_flags) atomicOr(&a.acc->batch_flags, PDF_FLAG_OVERFLOW);
+            if (t) atomic_add_u128(&a.acc->batch_lo, &a.acc->batch_hi, &a.acc->batch_flags, t);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint32_t *lvt = reinterpret_cast<uint32_t *>(smraw + cover_smem_lvt(a.hash_cap));  // [kCoverLevels] level_off
+    const uint32_t L = a.c.n_levels;
     const bool lv_shared = L + 1 <= kCoverLevels;
     if (lv_shared)
         for (uint32_t i = threadIdx.x; i <= L; i += blockDim.x) lvt[i] = a.c.level_off[i];
     const uint32_t *lo_tab = lv_shared ? lvt : a.c.level_off;
     __syncthreads();
-
     const uint32_t n_active = *a.active_count;
-    for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) {
-        const uint32_t p = a.active_list[ai];
-        const uint32_t pid = a.pair_base + p;
-        const uint32_t wp = p >> 5, bit = p & 31, blk = wp / a.bw;
-        const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
-        const uint32_t top = a.blk_maxlvl[blk];
-        const uint32_t gend = lo_tab[top];
-        const uint32_t nwords = (gend + 31) / 32;
-        if (threadIdx.x == 0) {
-            s_n = 0;
-            s_adj = 0;
-            s_over = 0;
-            s_flags = 0;
-        }
-        __syncthreads();
-        // ---- A, B: the pair's nets, in gate order
-        for (uint32_t q0 = 0; q0 < nwords; q0 += kCoverCand / 32) {
-            const uint32_t q = q0 + threadIdx.x;
-            uint32_t bits = 0;
-            if (threadIdx.x < kCoverCand / 32 && q < nwords) {
-                bits = nzb[q];
-                if (q == nwords - 1 && (gend & 31)) bits &= (1u << (gend & 31)) - 1u;
-            }
-            uint32_t nc;
-            uint32_t pos = block_scan_excl(__popc(bits), s_warp, &nc);
-            while (bits) {
-                cand[pos++] = q * 32 + (__ffs(bits) - 1);
-                bits &= bits - 1;
-            }
-            __syncthreads();
-            // each thread tests a contiguous run of candidates (order kept)
-            const uint32_t per = (nc + blockDim.x - 1) / blockDim.x;
-            const uint32_t c0 = min(nc, threadIdx.x * per), c1 = min(nc, c0 + per);
-            uint32_t keep = 0, nk = 0;  // per <= kCoverCand / 256 = 16: one bit each
-            uint32_t mw[16];
-#pragma unroll
-            for (int k = 0; k < 16; k++) mw[k] = c0 + k < c1 ? a.M[(size_t)cand[c0 + k] * a.ld + wp] : 0u;
-#pragma unroll
-            for (int k = 0; k < 16; k++) {
-                const uint32_t m = (mw[k] >> bit) & 1u;
-                keep |= m << k;
-                nk += m;
-            }
-            uint32_t nl;
-            const uint32_t at = block_scan_excl(nk, s_warp, &nl);
-            const uint32_t base = s_n;
-            if (base + nl > cap) {
-                if (threadIdx.x == 0) s_over = 1;
-            } else {
-                uint32_t o = base + at;
-                for (uint32_t i = c0; i < c1; i++)
-                    if ((keep >> (i - c0)) & 1u) lid[o++] = cand[i];
-            }
-            __syncthreads();
-            if (threadIdx.x == 0 && !s_over) s_n = base + nl;
-            __syncthreads();
-            if (s_over) break;
-        }
-        if (s_over) {
-            if (threadIdx.x == 0) atomicOr(&a.acc->err, kErrHashFull);  // more nets than the list holds
-            __syncthreads();
-            continue;
-        }
-        const uint32_t n = s_n;
-        // ---- C: records, first ids, levels, listed fan-outs
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const uint32_t g = lid[i];
-            const GateRec r = load_rec(a.c.rec + g);
-            const uint32_t fx = a.first_x[g], fy = a.first_y[g];
-            const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
-            uint32_t k = 0;
-            for (uint32_t j = 0; j < nfo; j += 4) {  // four fan-out loads in flight
-                uint32_t fo[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) fo[u] = j + u < nfo ? __ldg(a.c.edges + eb + j + u) : kEmpty;
-#pragma unroll
-                for (int u = 0; u < 4; u++) k += fo[u] != kEmpty && find_net(lid, n, fo[u]) != kEmpty ? 1u : 0u;
-            }
-            info[i] = (rec_po(r) ? kNetPo : 0u) | (rec_type(r) == PDF_INPT ? kNetInpt : 0u) |
-                      (fx == pid || fy == pid ? kNetFirst : 0u) | level_of(lo_tab, L, g);
-            const uint32_t o = k ? atomicAdd(&s_adj, k) : 0u;
-            if (o + k > acap) {
-                aoff[i] = kEmpty;  // fan-outs read in place during the recurrence
-                acnt[i] = nfo;
-            } else {
-                aoff[i] = o;
-                acnt[i] = k;
-                uint32_t w = o;
-                for (uint32_t j = 0; j < nfo && k; j++) {
-                    const uint32_t x = find_net(lid, n, __ldg(a.c.edges + eb + j));
-                    if (x != kEmpty) adj[w++] = x;
-                }
-            }
-        }
-        __syncthreads();
-        // ---- the recurrence, levels descending
-        pdf_u128 total = 0;
-        bool ovf = false;
-        const uint32_t lv_hi = n ? (info[n - 1] & kNetLevel) : 0;
-        for (int lv = (int)lv_hi; lv >= 0 && n; lv--) {
-            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-                const uint32_t inf = info[i];
-                if ((inf & kNetLevel) != (uint32_t)lv) continue;
-                pdf_u128 H = (inf & kNetPo) ? 1 : 0, C = 0;
-                bool dummy = false;
-                auto add = [&](uint32_t x) {
-                    C = add_sat(C, cv[x], ovf);
-                    H = add_sat(H, hv[x], dummy);
-                };
-                if (aoff[i] != kEmpty) {
-                    for (uint32_t j = 0; j < acnt[i]; j++) add(adj[aoff[i] + j]);
-                } else {
-                    const GateRec r = load_rec(a.c.rec + lid[i]);
-                    const uint32_t eb = r.w[2] + rec_nfi(r);
-                    for (uint32_t j = 0; j < acnt[i]; j++) {
-                        const uint32_t x = find_net(lid, n, __ldg(a.c.edges + eb + j));
-                        if (x != kEmpty) add(x);
-                    }
-                }
-                pdf_u128 c = C, h = H;
-                if (inf & kNetFirst) {
-                    c = add_sat(C, H, ovf);
-                    h = 0;
-                }
-                if (c == ~(pdf_u128)0) ovf = true;
-                if (inf & kNetInpt) {
-                    h = 0;
-                    if (lv == 0) total = add_sat(total, c, ovf);
-                }
-                hv[i] = h;
-                cv[i] = c;
-            }
-            __syncthreads();
-        }
-        // ---- the pair's count into the batch count
-        for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
-        if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
-        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            pdf_u128 t = threadIdx.x < (blockDim.x + 31) / 32 ? s_red[threadIdx.x] : 0;
-            bool o2 = false;
-            for (int d = 16; d > 0; d >>= 1) t = add_sat(t, shfl_down_u128(t, d), o2);
-            if (threadIdx.x == 0) {
-                if (o2 || s_flags) atomicOr(&a.acc->batch_flags, PDF_FLAG_OVERFLOW);
-                if (t) atomic_add_u128(&a.acc->batch_lo, &a.acc->batch_hi, &a.acc->batch_flags, t);
-            }
-        }
-        __syncthreads();
-    }
+    for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) cover_pair(a, a.active_list[ai], lo_tab);
     // the last CTA to finish closes the batch
     if (threadIdx.x == 0) {
         __threadfence();
@@ -920,6 +942,84 @@ __global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
             a.acc->done = 0;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Batched grading: many circuits in one pass of three launches.  Circuit i
+// owns CTAs [bpref[i], bpref[i+1]) of k_batch_forward and gates
+// [gpref[i], gpref[i+1]) of k_batch_active; the first-detecting pairs of all
+// circuits form one item list that k_batch_cover works through.  Each
+// circuit's arguments live in device arrays, so the launches can be captured
+// once in a CUDA graph and replayed; with `append` the last cover CTA also
+// advances every circuit's pair_base by its pair count, so the next replay
+// grades the next vector pairs of each circuit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t prefix_find(const uint32_t *pref, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;  // last i with pref[i] <= x
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(pref + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int BW, int ROBUST>
+__global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
+    k_batch_forward(const FwdArgs *args, const uint32_t *bpref, uint32_t n, BatchCtl *ctl) {
+    __shared__ FwdArgs s_a;
+    __shared__ uint32_t s_blk;
+    if (threadIdx.x == 0) {
+        const uint32_t ci = prefix_find(bpref, n, blockIdx.x);
+        s_a = args[ci];
+        s_blk = blockIdx.x - __ldg(bpref + ci);
+        if (blockIdx.x == 0) {
+            ctl->n_items = 0;
+            ctl->done = 0;
+        }
+    }
+    __syncthreads();
+    forward_cta<BW, ROBUST, FWD_FUSED>(s_a, s_blk);
+}
+
+__global__ void k_batch_active(const CoverArgs *args, const uint32_t *gpref, uint32_t n, uint2 *items,
+                               BatchCtl *ctl) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= __ldg(gpref + n)) return;
+    const uint32_t ci = prefix_find(gpref, n, t);
+    const CoverArgs &a = args[ci];
+    active_gate(a, t - __ldg(gpref + ci),
+                [&](uint32_t d) { items[atomicAdd(&ctl->n_items, 1u)] = make_uint2(ci, d); });
+}
+
+__global__ void __launch_bounds__(256) k_batch_cover(CoverArgs *args, FwdArgs *fargs, uint32_t n, const uint2 *items,
+                                                     BatchCtl *ctl, uint32_t append) {
+    __shared__ CoverArgs s_a;
+    __shared__ uint32_t s_last;
+    const uint32_t n_items = ctl->n_items;
+    for (uint32_t ai = blockIdx.x; ai < n_items; ai += gridDim.x) {
+        const uint2 it = items[ai];
+        if (threadIdx.x == 0) s_a = args[it.x];
+        __syncthreads();
+        cover_pair(s_a, it.y, s_a.c.level_off);  // ends with a barrier
+    }
+    // the last CTA to finish closes every circuit's batch
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ctl->done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint64_t np = args[i].n_pairs;
+        batch_close(args[i].acc, np);
+        if (append) {
+            args[i].pair_base += (uint32_t)np;
+            fargs[i].pair_base += (uint32_t)np;
+        }
+    }
+    if (threadIdx.x == 0) ctl->done = 0;
 }
 
 // Dense first-detect merge over given planes (stage call pdf_merge): one warp
@@ -1020,9 +1120,7 @@ cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, 
     }
 }
 
-size_t cover_smem_bytes(uint32_t net_cap) {
-    return (size_t)net_cap * (2 * sizeof(pdf_u128) + 4 * 4 + 4 * 4) + (kCoverCand + kCoverLevels) * 4;
-}
+size_t cover_smem_bytes(uint32_t net_cap) { return cover_smem_lvt(net_cap) + (size_t)kCoverLevels * 4; }
 
 cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bool zero_active, cudaStream_t st) {
     const uint32_t W = (uint32_t)((a.n_pairs + 31) / 32);
@@ -1036,6 +1134,55 @@ cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bo
     if (e != cudaSuccess) return e;
     k_cover<<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+template <int BW, int ROBUST>
+cudaError_t prepare_batch_t(const BatchLaunch &b) {
+    cudaError_t e = cudaFuncSetAttribute(k_batch_forward<BW, ROBUST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)b.fwd_smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_batch_cover, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)cover_smem_bytes(b.hash_cap));
+}
+
+template <int BW, int ROBUST>
+cudaError_t launch_batch_t(const BatchLaunch &b, cudaStream_t st) {
+    k_batch_forward<BW, ROBUST><<<b.total_blocks, b.threads, b.fwd_smem, st>>>(b.fargs, b.bpref, b.n, b.ctl);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_batch_active<<<(b.total_gates + 255) / 256, 256, 0, st>>>(b.cargs, b.gpref, b.n, b.items, b.ctl);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_batch_cover<<<b.cover_grid, 256, cover_smem_bytes(b.hash_cap), st>>>(b.cargs, b.fargs, b.n, b.items, b.ctl,
+                                                                         b.append);
+    return cudaGetLastError();
+}
+
+cudaError_t prepare_batch(const BatchLaunch &b) {
+    switch (b.bw * 2 + (b.robust ? 1 : 0)) {
+        case 2: return prepare_batch_t<1, 0>(b);
+        case 3: return prepare_batch_t<1, 1>(b);
+        case 4: return prepare_batch_t<2, 0>(b);
+        case 5: return prepare_batch_t<2, 1>(b);
+        case 8: return prepare_batch_t<4, 0>(b);
+        case 9: return prepare_batch_t<4, 1>(b);
+        case 16: return prepare_batch_t<8, 0>(b);
+        case 17: return prepare_batch_t<8, 1>(b);
+        default: return cudaErrorInvalidValue;
+    }
+}
+cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
+    if (!b.n || !b.total_blocks) return cudaErrorInvalidValue;
+    switch (b.bw * 2 + (b.robust ? 1 : 0)) {
+        case 2: return launch_batch_t<1, 0>(b, st);
+        case 3: return launch_batch_t<1, 1>(b, st);
+        case 4: return launch_batch_t<2, 0>(b, st);
+        case 5: return launch_batch_t<2, 1>(b, st);
+        case 8: return launch_batch_t<4, 0>(b, st);
+        case 9: return launch_batch_t<4, 1>(b, st);
+        case 16: return launch_batch_t<8, 0>(b, st);
+        case 17: return launch_batch_t<8, 1>(b, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M, uint64_t ld,

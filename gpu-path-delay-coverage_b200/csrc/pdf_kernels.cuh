@@ -89,6 +89,26 @@ struct CoverArgs {
     uint32_t hash_cap;            // nets one pair may mark (the cover's shared-memory net list)
 };
 
+// Batched grading (k_batch_forward, k_batch_active, k_batch_cover).
+struct BatchCtl {
+    unsigned int n_items;  // first-detecting (circuit, pair) items of this pass
+    unsigned int done;     // cover CTAs finished
+    unsigned int pad[2];
+};
+struct BatchLaunch {
+    FwdArgs *fargs;        // [n] per circuit, device
+    CoverArgs *cargs;      // [n] per circuit, device
+    const uint32_t *bpref; // [n + 1] first forward CTA of each circuit
+    const uint32_t *gpref; // [n + 1] first gate of each circuit
+    uint2 *items;          // [sum of min(n_pairs, 2 n_gates)]
+    BatchCtl *ctl;
+    uint32_t n, total_blocks, total_gates;
+    uint32_t bw, robust, threads, cover_grid, hash_cap, append;
+    size_t fwd_smem;
+};
+cudaError_t prepare_batch(const BatchLaunch &b);  // kernel attributes; call before launching or capturing
+cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st);
+
 // Host-side launchers (pdf_kernels.cu).  All return cudaError_t of the launch.
 cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st);

@@ -284,6 +284,57 @@ pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, uint64_t n_pa
                              uint64_t pair_base, const uint32_t *first_x, const uint32_t *first_y,
                              pdf_totals *chunk_total, void *stream);
 
+/* ---- batched grading: many circuits in one pass ---- */
+
+/*
+ * A batch grades the vector pairs of many (circuit, state) jobs in one pass of
+ * three kernel launches, captured once as a CUDA graph and replayed by each
+ * pdf_batch_run.  Each job's result is the same as pdf_grade of that job alone
+ * (its state's first-detect ids and totals).  No reference counterpart: the
+ * reference grades one circuit per process (main.cu:129-235).
+ *
+ * Jobs borrow their circuit and state (both must outlive the batch, and the
+ * state must not be graded elsewhere meanwhile); all circuits share one
+ * device, mark mode and tile width.  pairs are device planes (on_device = 1,
+ * ld a multiple of the tile width, 16-byte aligned rows) that stay bound to the
+ * batch: rewrite their contents between runs to grade new pairs.  With
+ * PDF_BATCH_APPEND each run also advances every job's pair_base by its pair
+ * count, so consecutive runs grade consecutive batches of each job's pairs
+ * (as consecutive pdf_grade calls would).
+ */
+typedef struct pdf_batch pdf_batch;
+typedef struct pdf_batch_job {
+    pdf_circuit *circuit;
+    pdf_state *state;
+    pdf_pairs pairs;
+    uint64_t pair_base; /* global id of the job's first pair in the first run */
+} pdf_batch_job;
+enum { PDF_BATCH_APPEND = 1 };
+typedef struct pdf_batch_info {
+    uint32_t n_jobs, tile_words, threads, ctas;
+    uint64_t gate_evals; /* per run: sum over jobs of n_gates * n_pairs */
+    uint64_t device_bytes;
+} pdf_batch_info;
+pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out);
+void pdf_batch_destroy(pdf_batch *b);
+pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info);
+/* One pass over every job, stream-ordered (the first call captures the graph). */
+pdf_status pdf_batch_run_async(pdf_batch *b, void *stream);
+/* pdf_batch_run_async, then wait; reports a device-side error of any job. */
+pdf_status pdf_batch_run(pdf_batch *b, void *stream);
+
+/*
+ * Autotuner of the batch's tile shape: for each candidate tile width (words of
+ * 32 pairs per CTA: 2, 4, 8) it builds the circuits, states and pair planes of
+ * the given netlists and pair counts (seeded pairs), times `reps` graph
+ * replays after a warm-up, and returns the fastest options in *best (the
+ * other fields copied from *base) with its milliseconds per run in *best_ms.
+ * All it allocates is freed before it returns.
+ */
+pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, const uint64_t *n_pairs, uint32_t n,
+                              const pdf_circuit_opts *base, uint32_t reps, pdf_circuit_opts *best,
+                              float *best_ms);
+
 /* ---- synthetic inputs (seeded, host-side) ---- */
 
 typedef struct pdf_gen_params {

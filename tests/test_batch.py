@@ -1,0 +1,105 @@
+"""Batched grading (pdf_batch_*): many circuits of uneven size and pair count
+in one pass of three launches replayed from a CUDA graph.  Every job's
+first-detect ids, count and flags must equal grading that job alone."""
+import numpy as np
+import pytest
+
+import circuits
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+P = helpers.pdf()
+O = helpers.oracle()
+
+
+def _jobs(mode, tile=4, seed=0):
+    """Circuits of many shapes and pair counts (including ragged tails)."""
+    import torch
+    shapes = [s[1] for s in circuits.small_suite()[:6]]
+    shapes += [circuits.random_small(500 + seed, n_gates=3000, n_pi=120, n_po=400, depth=25),
+               circuits.random_small(600 + seed, n_gates=12000, n_pi=1500, n_po=3000, depth=7),
+               circuits.random_small(700 + seed, n_gates=8000, n_pi=300, n_po=800, depth=60, fmax=6),
+               circuits.hub(150), circuits.diamond_chain(20)]
+    counts = [33, 1000, 1, 2500, 64, 777, 4096, 700, 3001, 900, 40]
+    rng = np.random.default_rng(11 + seed)
+    jobs, want = [], []
+    for nl, n in zip(shapes, counts):
+        codes = helpers.rand_codes(rng, nl.n_pi, n)
+        ld = (P.words(n) + tile - 1) // tile * tile
+        v, t = P.planes_from_codes(codes, ld)
+        c = P.Circuit(nl, mark_mode=mode, tile_words=tile)
+        s = P.State(c)
+        dv = torch.from_numpy(v.view(np.int32)).cuda()
+        dt = torch.from_numpy(t.view(np.int32)).cuda()
+        jobs.append((c, s, dv, dt, n, 0))
+        want.append((nl, codes, n))
+    return jobs, want
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_equals_each_job_alone(mode):
+    jobs, want = _jobs(mode)
+    b = P.Batch(jobs)
+    b.run()
+    info = b.info()
+    assert info.n_jobs == len(jobs)
+    assert info.gate_evals == sum(nl.n_gates * n for nl, _, n in want)
+    for (c, s, *_), (nl, codes, n) in zip(jobs, want):
+        w = O.grade(nl, codes, n, mark_mode=mode)
+        fx, fy, tot = s.snapshot()
+        np.testing.assert_array_equal(fx, w.first_x)
+        np.testing.assert_array_equal(fy, w.first_y)
+        assert tot.value == w.total and tot.flags == w.flags and tot.pairs == n
+
+
+def test_batch_replay_is_stable():
+    """A second replay over the same pairs adds the same counts again."""
+    jobs, want = _jobs(1, seed=1)
+    b = P.Batch(jobs)
+    b.run()
+    first = [s.snapshot()[2].value for _, s, *_ in jobs]
+    b.run()
+    again = [s.snapshot()[2].value for _, s, *_ in jobs]
+    assert again == [2 * x for x in first]
+    assert sum(first) > 0
+
+
+def test_batch_append_grades_consecutive_pairs():
+    """With append, run k grades pairs [k n, (k+1) n) of each job (the pair
+    planes rewritten between runs); the state equals one grading of all."""
+    import torch
+    jobs, want = _jobs(0, seed=2)
+    rng = np.random.default_rng(99)
+    extra = []
+    b = P.Batch(jobs, append=True)
+    b.run()
+    for (c, s, dv, dt, n, _), (nl, codes, _) in zip(jobs, want):
+        more = helpers.rand_codes(rng, nl.n_pi, n)
+        v, t = P.planes_from_codes(more, dv.shape[1])
+        dv.copy_(torch.from_numpy(v.view(np.int32)))
+        dt.copy_(torch.from_numpy(t.view(np.int32)))
+        extra.append(more)
+    torch.cuda.synchronize()
+    b.run()
+    for (c, s, *_), (nl, codes, n), more in zip(jobs, want, extra):
+        w = O.grade(nl, np.concatenate([codes, more], axis=1), 2 * n, chunk=n)
+        fx, fy, tot = s.snapshot()
+        np.testing.assert_array_equal(fx, w.first_x)
+        np.testing.assert_array_equal(fy, w.first_y)
+        assert tot.value == w.total and tot.pairs == 2 * n
+
+
+def test_batch_rejects_mixed_tiles():
+    jobs, _ = _jobs(0)
+    c, s, dv, dt, n, base = jobs[0]
+    c8 = P.Circuit(c.netlist, tile_words=8)
+    s8 = P.State(c8)
+    with pytest.raises(P.PdfError):
+        P.Batch([jobs[1], (c8, s8, dv, dt, n, base)])
+
+
+def test_autotune_picks_a_tile():
+    nls = [circuits.random_small(800 + k, n_gates=2000 * (k + 1), n_pi=100, n_po=300, depth=20) for k in range(4)]
+    opts, ms = P.batch_autotune(nls, [1024, 3000, 5000, 700], mark_mode=1, reps=2)
+    assert opts.tile_words in (2, 4, 8) and ms > 0
