@@ -577,5 +577,22 @@ WORKLOADS = {
 }
 
 
+def batch_workload(seed: int = SEED_BASE + 4, count: int = 256):
+    """The mixed-size batch: `count` netlists with gate counts log-uniform in
+    500..200,000 (PI and PO about G/13, at least 16), depth uniform in
+    20..150, and pair counts log-uniform in 1,024..65,536.  Returns a list of
+    (GenParams, n_pairs)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        g = int(round(np.exp(rng.uniform(np.log(500), np.log(200000)))))
+        depth = int(rng.integers(20, 151))
+        g = max(g, depth * 4)
+        pio = max(16, g // 13)
+        n = int(round(np.exp(rng.uniform(np.log(1024), np.log(65536)))))
+        out.append((GenParams(seed * 1000 + k, g, pio, pio, depth), n))
+    return out
+
+
 def pair_seed(gen_seed: int) -> int:
     return gen_seed ^ PAIR_SEED_XOR
