@@ -81,6 +81,19 @@ class BatchInfo_t(C.Structure):
                 ("ctas", C.c_uint32), ("gate_evals", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
+class ServerOpts_t(C.Structure):
+    _fields_ = [("device", C.c_int), ("mark_mode", C.c_int), ("tile_words", C.c_uint32),
+                ("batch_pairs", C.c_uint32), ("max_jobs", C.c_uint32), ("reserved", C.c_uint32),
+                ("hbm_budget", C.c_uint64)]
+
+
+class ServerStats_t(C.Structure):
+    _fields_ = [("jobs_done", C.c_uint64), ("jobs_active", C.c_uint64), ("jobs_queued", C.c_uint64),
+                ("batches", C.c_uint64), ("steps", C.c_uint64), ("gate_evals", C.c_uint64),
+                ("busy_s", C.c_double), ("lat_p50_ms", C.c_double), ("lat_p99_ms", C.c_double),
+                ("lat_max_ms", C.c_double), ("bytes_in_use", C.c_uint64)]
+
+
 class CircuitInfo_t(C.Structure):
     _fields_ = [("n_gates", C.c_uint32), ("n_levels", C.c_uint32), ("n_pi", C.c_uint32),
                 ("n_po", C.c_uint32), ("max_level_width", C.c_uint32), ("max_nfi", C.c_uint32),
@@ -138,6 +151,13 @@ ABI = [
     ("pdf_batch_autotune", C.c_int, [C.POINTER(C.POINTER(Netlist_t)), C.POINTER(C.c_uint64), C.c_uint32,
                                      C.POINTER(CircuitOpts_t), C.c_uint32, C.POINTER(CircuitOpts_t),
                                      C.POINTER(C.c_float)]),
+    ("pdf_server_create", C.c_int, [C.POINTER(ServerOpts_t), C.POINTER(C.c_void_p)]),
+    ("pdf_server_destroy", None, [C.c_void_p]),
+    ("pdf_server_submit", C.c_int, [C.c_void_p, C.POINTER(Netlist_t), C.c_void_p, C.c_void_p, C.c_uint64,
+                                    C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("pdf_server_step", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    ("pdf_server_result", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Totals_t), C.c_void_p, C.c_void_p]),
+    ("pdf_server_query", C.c_int, [C.c_void_p, C.POINTER(ServerStats_t)]),
     ("pdf_gen_netlist", C.c_int, [C.POINTER(GenParams_t), C.POINTER(C.c_void_p)]),
     ("pdf_netbuf_from", C.c_int, [C.POINTER(Netlist_t), C.POINTER(C.c_void_p)]),
     ("pdf_netbuf_view", None, [C.c_void_p, C.POINTER(Netlist_t)]),
@@ -475,6 +495,58 @@ class Batch:
     def close(self):
         if self.h:
             lib().pdf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching grader (pdf_server_*).  Keeps every submitted job's
+    netlist and host pair planes alive until its result has been read."""
+
+    def __init__(self, mark_mode: int = MARK_DEFAULT, batch_pairs: int = 4096, tile_words: int = 4,
+                 hbm_budget: int = 0, max_jobs: int = 0, device: int = 0):
+        o = ServerOpts_t(device, mark_mode, tile_words, batch_pairs, max_jobs, 0, hbm_budget)
+        h = C.c_void_p()
+        check(lib().pdf_server_create(C.byref(o), C.byref(h)), "pdf_server_create")
+        self.h = h
+        self.keep = {}
+
+    def submit(self, nl: Netlist, v: np.ndarray, t: np.ndarray, n_pairs: int) -> int:
+        v = np.ascontiguousarray(v, np.uint32)
+        t = np.ascontiguousarray(t, np.uint32)
+        jid = C.c_uint64()
+        check(lib().pdf_server_submit(self.h, C.byref(nl.view()), v.ctypes.data, t.ctypes.data, v.shape[1],
+                                      n_pairs, C.byref(jid)), "pdf_server_submit")
+        self.keep[jid.value] = (nl, v, t)
+        return jid.value
+
+    def step(self) -> int:
+        r = C.c_uint32()
+        check(lib().pdf_server_step(self.h, C.byref(r)), "pdf_server_step")
+        return r.value
+
+    def result(self, jid: int):
+        nl = self.keep[jid][0]
+        fx = np.zeros(nl.n_gates, np.uint32)
+        fy = np.zeros(nl.n_gates, np.uint32)
+        tot = Totals_t()
+        check(lib().pdf_server_result(self.h, jid, C.byref(tot), fx.ctypes.data, fy.ctypes.data),
+              "pdf_server_result")
+        return fx, fy, tot
+
+    def stats(self) -> ServerStats_t:
+        s = ServerStats_t()
+        check(lib().pdf_server_query(self.h, C.byref(s)), "pdf_server_query")
+        return s
+
+    def close(self):
+        if self.h:
+            lib().pdf_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

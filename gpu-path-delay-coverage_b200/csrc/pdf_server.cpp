@@ -1,0 +1,277 @@
+// pdf_server.cpp -- serving loop: continuous batching of grading jobs over
+// the public C ABI (circuits, states and pdf_batch_*).
+//
+// A job owns a device circuit, a coverage state and a pair buffer of one
+// batch while it is active.  Each step admits queued jobs in arrival order
+// while the estimated device footprint fits the budget, copies the next
+// batch of every active job into its buffer, grades all of them in one
+// append-mode batched pass and retires the jobs whose pairs are done.  The
+// batched pass is rebuilt only when the set of active jobs (or a job's batch
+// size, on its last batch) changes; otherwise its captured graph is replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "pdf.h"
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Job {
+    uint64_t id = 0;
+    pdf_netbuf *net = nullptr;  // copy of the netlist until the job retires
+    pdf_netlist view{};
+    const uint32_t *hv = nullptr, *ht = nullptr;  // caller's host planes
+    uint64_t hld = 0, n_pairs = 0, done = 0;
+    uint64_t bytes = 0;  // footprint estimate
+    pdf_circuit *c = nullptr;
+    pdf_state *s = nullptr;
+    uint32_t *dv = nullptr;  // [2][n_pi][ld] one batch of pairs
+    uint64_t ld = 0, cur = 0;  // words per row, pairs of the batch in flight
+    double t_ready = 0.0;
+};
+
+struct Result {
+    pdf_totals total{};
+    std::vector<uint32_t> fx, fy;
+};
+
+}  // namespace
+
+struct pdf_server {
+    pdf_server_opts o{};
+    uint64_t next_id = 1;
+    std::deque<Job *> queue;
+    std::vector<Job *> active;
+    std::map<uint64_t, Result> results;
+    pdf_batch *batch = nullptr;
+    bool dirty = true;
+    uint64_t used = 0;
+    cudaStream_t stream = nullptr;
+    pdf_server_stats st{};
+    std::vector<double> lat_ms;
+};
+
+namespace {
+
+// Device bytes of an active job: netlist, plan, state, workspace and pair
+// buffer (an upper estimate from the netlist and the batch size).
+uint64_t footprint(const pdf_netlist &nl, uint64_t batch_pairs, uint32_t bw) {
+    const uint64_t G = nl.n_gates, W = (batch_pairs + 31) / 32, ld = (W + bw - 1) / bw * bw;
+    const uint64_t npi = nl.level_offsets[1];
+    return 64 * G + 24 * nl.n_edges       // records, edges, fan-out lists, far lists
+           + 8 * G                        // first-detect ids
+           + 12 * G * ld                  // V, T, M planes of one batch
+           + (ld / bw) * ((G + 31) / 32) * 4 + 8 * ld * 32 + 4 * ld  // bitmaps, active pairs
+           + 8 * npi * ld                 // pair buffer
+           + (1u << 20);
+}
+
+void free_job(Job *j) {
+    if (j->dv) cudaFree(j->dv);
+    pdf_state_destroy(j->s);
+    pdf_circuit_destroy(j->c);
+    pdf_netbuf_free(j->net);
+    delete j;
+}
+
+}  // namespace
+
+extern "C" pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server **out) {
+    if (!out) return PDF_EINVAL;
+    *out = nullptr;
+    pdf_server_opts o = opts ? *opts : pdf_server_opts{};
+    if (!o.tile_words) o.tile_words = 4;
+    if (!o.batch_pairs) o.batch_pairs = 4096;
+    if (!o.max_jobs) o.max_jobs = 1024;
+    if (o.batch_pairs % 32 || (o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8) ||
+        (o.mark_mode != PDF_MARK_DEFAULT && o.mark_mode != PDF_MARK_ROBUST))
+        return PDF_EINVAL;
+    if (cudaSetDevice(o.device) != cudaSuccess) return PDF_ENODEV;
+    if (!o.hbm_budget) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return PDF_ECUDA;
+        o.hbm_budget = fr / 2;
+    }
+    pdf_server *srv = new (std::nothrow) pdf_server();
+    if (!srv) return PDF_ENOMEM;
+    srv->o = o;
+    if (cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete srv;
+        return PDF_ECUDA;
+    }
+    *out = srv;
+    return PDF_OK;
+}
+
+extern "C" void pdf_server_destroy(pdf_server *srv) {
+    if (!srv) return;
+    cudaSetDevice(srv->o.device);
+    cudaStreamSynchronize(srv->stream);
+    pdf_batch_destroy(srv->batch);
+    for (Job *j : srv->active) free_job(j);
+    for (Job *j : srv->queue) free_job(j);
+    cudaStreamDestroy(srv->stream);
+    delete srv;
+}
+
+extern "C" pdf_status pdf_server_submit(pdf_server *srv, const pdf_netlist *nl, const uint32_t *v, const uint32_t *t,
+                                        uint64_t ld, uint64_t n_pairs, uint64_t *job_id) {
+    if (!srv || !nl || !v || !t || !n_pairs || ld < (n_pairs + 31) / 32 || n_pairs > 0xFFFFFFFFull)
+        return PDF_EINVAL;
+    pdf_status st = pdf_netlist_check(nl, nullptr, 0);
+    if (st != PDF_OK) return st;
+    Job *j = new (std::nothrow) Job();
+    if (!j) return PDF_ENOMEM;
+    if ((st = pdf_netbuf_from(nl, &j->net)) != PDF_OK) {
+        delete j;
+        return st;
+    }
+    pdf_netbuf_view(j->net, &j->view);
+    j->id = srv->next_id++;
+    j->hv = v;
+    j->ht = t;
+    j->hld = ld;
+    j->n_pairs = n_pairs;
+    j->bytes = footprint(j->view, srv->o.batch_pairs, srv->o.tile_words);
+    j->t_ready = now_s();
+    srv->queue.push_back(j);
+    if (job_id) *job_id = j->id;
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
+    if (!srv) return PDF_EINVAL;
+    if (retired) *retired = 0;
+    if (cudaSetDevice(srv->o.device) != cudaSuccess) return PDF_ECUDA;
+    const double t0 = now_s();
+    pdf_status st = PDF_OK;
+    // admission, in arrival order, by footprint
+    while (!srv->queue.empty() && srv->active.size() < srv->o.max_jobs) {
+        Job *j = srv->queue.front();
+        if (srv->used + j->bytes > srv->o.hbm_budget && !srv->active.empty()) break;
+        pdf_circuit_opts co{};
+        co.device = srv->o.device;
+        co.mark_mode = srv->o.mark_mode;
+        co.tile_words = srv->o.tile_words;
+        co.max_pairs = srv->o.batch_pairs;
+        // on failure the job stays queued with nothing allocated
+        auto undo = [&](pdf_status e) {
+            if (j->dv) cudaFree(j->dv);
+            pdf_state_destroy(j->s);
+            pdf_circuit_destroy(j->c);
+            j->dv = nullptr;
+            j->s = nullptr;
+            j->c = nullptr;
+            (void)cudaGetLastError();
+            return e;
+        };
+        if ((st = pdf_circuit_create(&j->view, &co, &j->c)) != PDF_OK) return undo(st);
+        if ((st = pdf_state_create(j->c, &j->s)) != PDF_OK) return undo(st);
+        const uint64_t W = srv->o.batch_pairs / 32, npi = j->view.level_offsets[1];
+        j->ld = (W + srv->o.tile_words - 1) / srv->o.tile_words * srv->o.tile_words;
+        if (cudaMalloc(&j->dv, 2 * npi * j->ld * 4) != cudaSuccess) return undo(PDF_ENOMEM);
+        if (cudaMemset(j->dv, 0, 2 * npi * j->ld * 4) != cudaSuccess) return undo(PDF_ECUDA);
+        srv->used += j->bytes;
+        srv->queue.pop_front();
+        srv->active.push_back(j);
+        srv->dirty = true;
+    }
+    if (srv->active.empty()) return PDF_OK;
+    // the next batch of every active job
+    for (Job *j : srv->active) {
+        const uint64_t n = std::min<uint64_t>(srv->o.batch_pairs, j->n_pairs - j->done);
+        if (n != j->cur) srv->dirty = true;
+        j->cur = n;
+        const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32, W = (n + 31) / 32;
+        uint32_t *dv = j->dv, *dt = j->dv + npi * j->ld;
+        if (cudaMemcpy2DAsync(dv, j->ld * 4, j->hv + w0, j->hld * 4, W * 4, npi, cudaMemcpyHostToDevice,
+                              srv->stream) != cudaSuccess ||
+            cudaMemcpy2DAsync(dt, j->ld * 4, j->ht + w0, j->hld * 4, W * 4, npi, cudaMemcpyHostToDevice,
+                              srv->stream) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return PDF_ECUDA;
+        }
+    }
+    if (srv->dirty) {
+        pdf_batch_destroy(srv->batch);
+        srv->batch = nullptr;
+        std::vector<pdf_batch_job> jobs;
+        for (Job *j : srv->active) {
+            const uint64_t npi = j->view.level_offsets[1];
+            jobs.push_back(pdf_batch_job{j->c, j->s, pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1},
+                                         j->done});
+        }
+        if ((st = pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), PDF_BATCH_APPEND, &srv->batch)) != PDF_OK)
+            return st;
+        srv->dirty = false;
+    }
+    if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
+    const double t1 = now_s();
+    srv->st.steps++;
+    // account, advance, retire
+    std::vector<Job *> keep;
+    for (Job *j : srv->active) {
+        srv->lat_ms.push_back(1e3 * (t1 - j->t_ready));
+        j->t_ready = t1;
+        srv->st.batches++;
+        srv->st.gate_evals += (uint64_t)j->view.n_gates * j->cur;
+        j->done += j->cur;
+        if (j->done < j->n_pairs) {
+            keep.push_back(j);
+            continue;
+        }
+        Result r;
+        r.fx.resize(j->view.n_gates);
+        r.fy.resize(j->view.n_gates);
+        if ((st = pdf_state_snapshot(j->s, r.fx.data(), r.fy.data(), &r.total)) != PDF_OK) return st;
+        srv->results[j->id] = std::move(r);
+        srv->used -= j->bytes;
+        free_job(j);
+        srv->st.jobs_done++;
+        srv->dirty = true;
+        if (retired) (*retired)++;
+    }
+    srv->active.swap(keep);
+    srv->st.busy_s += now_s() - t0;
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_server_result(pdf_server *srv, uint64_t job_id, pdf_totals *total, uint32_t *first_x,
+                                        uint32_t *first_y) {
+    if (!srv) return PDF_EINVAL;
+    auto it = srv->results.find(job_id);
+    if (it == srv->results.end()) return PDF_EINVAL;
+    if (total) *total = it->second.total;
+    if (first_x) std::memcpy(first_x, it->second.fx.data(), it->second.fx.size() * 4);
+    if (first_y) std::memcpy(first_y, it->second.fy.data(), it->second.fy.size() * 4);
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_server_query(const pdf_server *srv, pdf_server_stats *stats) {
+    if (!srv || !stats) return PDF_EINVAL;
+    *stats = srv->st;
+    stats->jobs_active = srv->active.size();
+    stats->jobs_queued = srv->queue.size();
+    stats->bytes_in_use = srv->used;
+    std::vector<double> l = srv->lat_ms;
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        auto q = [&](double f) { return l[std::min(l.size() - 1, (size_t)(f * (l.size() - 1) + 0.5))]; };
+        stats->lat_p50_ms = q(0.50);
+        stats->lat_p99_ms = q(0.99);
+        stats->lat_max_ms = l.back();
+    }
+    return PDF_OK;
+}

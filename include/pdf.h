@@ -335,6 +335,55 @@ pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, const uint64_t
                               const pdf_circuit_opts *base, uint32_t reps, pdf_circuit_opts *best,
                               float *best_ms);
 
+/* ---- serving: continuous batching of grading jobs ---- */
+
+/*
+ * A server grades jobs that arrive over time.  A job is a netlist plus all
+ * its vector pairs (host planes, kept by the caller until the job is done);
+ * it is graded in batches of `batch_pairs` pairs that append to the job's
+ * device-resident coverage state.  Each pdf_server_step admits queued jobs
+ * in arrival order while their device footprint fits `hbm_budget` (and
+ * fewer than `max_jobs` are active), grades the next batch of every active
+ * job in one batched pass (pdf_batch_*), and retires jobs whose pairs are
+ * all graded (their results stay readable).  Jobs that arrive while a step
+ * runs join at the next step, so work of jobs of different ages overlaps on
+ * the device.  A job's result equals pdf_grade of all its pairs in batches of
+ * batch_pairs.  Per-batch latency is the time from the batch being ready
+ * (submission, or the previous batch's end) to its result.  No reference
+ * counterpart: the reference grades one circuit per process (main.cu).
+ */
+typedef struct pdf_server pdf_server;
+typedef struct pdf_server_opts {
+    int device;
+    int mark_mode;          /* PDF_MARK_* for every job */
+    uint32_t tile_words;    /* 0 = 4 */
+    uint32_t batch_pairs;   /* pairs per batch, a multiple of 32 (0 = 4096) */
+    uint32_t max_jobs;      /* active jobs at most (0 = 1024) */
+    uint32_t reserved;
+    uint64_t hbm_budget;    /* bytes of device memory for active jobs (0 = half the free memory) */
+} pdf_server_opts;
+typedef struct pdf_server_stats {
+    uint64_t jobs_done, jobs_active, jobs_queued;
+    uint64_t batches;       /* job batches graded */
+    uint64_t steps;         /* batched passes run */
+    uint64_t gate_evals;    /* graded so far */
+    double busy_s;          /* time inside pdf_server_step */
+    double lat_p50_ms, lat_p99_ms, lat_max_ms; /* per-batch latency */
+    uint64_t bytes_in_use;
+} pdf_server_stats;
+pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server **out);
+void pdf_server_destroy(pdf_server *srv);
+/* Queue a job: v, t are host planes [n_pi][ld] of n_pairs pairs. */
+pdf_status pdf_server_submit(pdf_server *srv, const pdf_netlist *nl, const uint32_t *v, const uint32_t *t,
+                             uint64_t ld, uint64_t n_pairs, uint64_t *job_id);
+/* One step; *retired gets the number of jobs that finished in it. */
+pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired);
+/* Result of a finished job: its total (and first-detect ids, if non-null, n_gates each).
+ * PDF_EINVAL while the job is still queued or active. */
+pdf_status pdf_server_result(pdf_server *srv, uint64_t job_id, pdf_totals *total, uint32_t *first_x,
+                             uint32_t *first_y);
+pdf_status pdf_server_query(const pdf_server *srv, pdf_server_stats *stats);
+
 /* ---- synthetic inputs (seeded, host-side) ---- */
 
 typedef struct pdf_gen_params {
