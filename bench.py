@@ -163,7 +163,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     P, O = pkg(), oracle()
-    if args.workload == "c4":  # the batch's circuit nearest 20,000 gates stands for it
+    if args.workload in ("c4", "c5"):  # the batch's circuit nearest 20,000 gates stands for it
         spec = P.batch_workload()
         g, n = min(spec, key=lambda x: abs(x[0].n_gates - 20000))
         w = {"gen": g, "pairs": n}
@@ -190,7 +190,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded)",
-        "config": workload_config(P, args.workload if args.workload != "c4" else "c4-member", nl, n_sample),
+        "config": workload_config(P, args.workload if args.workload not in ("c4", "c5") else args.workload + "-member", nl, n_sample),
         "cpu_baseline": {"value": val, "unit": "gate-evals/s", "cores": threads, "kind": "port",
                          "sample": f"first {n_sample} of {n} pairs per step"},
         "e2e": {"value": val, "unit": "gate-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -500,6 +500,84 @@ def run_batched(args):
     return 0
 
 
+def run_served(args):
+    """--workload c5: jobs drawn from the mixed-size distribution arrive as a
+    Poisson stream (200 jobs/s); each appends 4,096-pair batches until its
+    65,536 pairs are graded.  Reports throughput and per-batch latency; every
+    served result is checked against grading the job offline."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    P = pkg()
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n_jobs, per_job, batch, rate = args.jobs, 65536, 4096, 200.0
+    spec = P.batch_workload()[:n_jobs]
+    rng = np.random.default_rng(0x5EED0005)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_jobs))
+    jobs = []
+    for g, _ in spec:
+        nl = P.gen_netlist(g)
+        v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, per_job)
+        jobs.append((nl, v, t))
+    units = sum(nl.n_gates * per_job for nl, _, _ in jobs)
+    srv = P.Server(mark_mode=P.MARK_ROBUST, batch_pairs=batch, hbm_budget=int(args.hbm_gb * (1 << 30)))
+    ids = [None] * n_jobs
+    sampler = ClockSampler(gpu_id_for_smi(torch, int(os.environ.get("LOCAL_RANK", "0"))))
+    sampler.start()
+    time.sleep(0.3)
+    t0 = time.perf_counter()
+    k = 0
+    while k < n_jobs or srv.stats().jobs_done < n_jobs:
+        now = time.perf_counter() - t0
+        while k < n_jobs and arrivals[k] <= now:
+            nl, v, t = jobs[k]
+            ids[k] = srv.submit(nl, v, t, per_job)
+            k += 1
+        if srv.stats().jobs_active + srv.stats().jobs_queued == 0:
+            time.sleep(max(0.0, min(0.001, arrivals[k] - now)) if k < n_jobs else 0.0)
+            continue
+        srv.step()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    st = srv.stats()
+    # every served result against the job graded offline in one call
+    same = True
+    for (nl, v, t), jid in zip(jobs, ids):
+        fx, fy, tot = srv.result(jid)
+        c = P.Circuit(nl, mark_mode=P.MARK_ROBUST, max_pairs=per_job)
+        s2 = P.State(c)
+        want = P.grade(c, s2, v, t, per_job)
+        wfx, wfy, _ = s2.snapshot()
+        same &= want.value == tot.value and np.array_equal(wfx, fx) and np.array_equal(wfy, fy)
+        s2.close()
+        c.close()
+    line = {
+        "metric": "gate-evals/s", "value": units / wall, "unit": "gate-evals/s", "n_gpus": 1, "steps": int(st.steps),
+        "warmup": 0, "ms_per_step": 1e3 * st.busy_s / max(1, st.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+        "config": {"workload": f"c5: {n_jobs} jobs from the c4 size distribution, Poisson arrivals at "
+                               f"{rate:.0f} jobs/s, {batch}-pair appends up to {per_job} pairs per job",
+                   "mark_mode": "robust (LUT_R)", "hbm_budget_gib": args.hbm_gb,
+                   "outputs": "path count and first-detect ids per job"},
+        "latency_ms": {"p50": st.lat_p50_ms, "p99": st.lat_p99_ms, "max": st.lat_max_ms,
+                       "per": "job batch, from ready (submission or previous batch) to result"},
+        "wall_s": wall, "busy_s": st.busy_s, "batches": int(st.batches),
+        "e2e": {"value": units / wall, "unit": "gate-evals/s",
+                "h2d_bytes_per_step": int(sum(2 * nl.n_pi * (per_job // 32) * 4 for nl, _, _ in jobs) / max(1, st.steps)),
+                "d2h_bytes_per_step": 64},
+        "gpu_launches": 3 * int(st.steps),
+        "clocks": clocks,
+        "result_stable": bool(same),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    srv.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -513,11 +591,15 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--ref-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--jobs", type=int, default=64, help="c5: jobs in the arrival stream")
+    ap.add_argument("--hbm-gb", type=float, default=64.0, help="c5: device memory for active jobs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "c4":
         return run_batched(args)
+    if args.workload == "c5":
+        return run_served(args)
     return run_ours(args)
 
 

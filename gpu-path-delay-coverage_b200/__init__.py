@@ -27,7 +27,7 @@ UNKN, INPT, AND, NAND, OR, NOR, XOR, XNOR, BUFF, NOT, FROM, DFF = range(12)
 S0, S1, T0, T1 = range(4)
 MARK_DEFAULT, MARK_ROBUST = 0, 1
 FLAG_OVERFLOW = 1
-BATCH_APPEND = 1
+BATCH_APPEND, BATCH_NO_GRAPH = 1, 2
 NONE = 0xFFFFFFFF
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "EOVERFLOW", 4: "ETIMEOUT", 5: "ECUDA",
@@ -83,7 +83,7 @@ class BatchInfo_t(C.Structure):
 
 class ServerOpts_t(C.Structure):
     _fields_ = [("device", C.c_int), ("mark_mode", C.c_int), ("tile_words", C.c_uint32),
-                ("batch_pairs", C.c_uint32), ("max_jobs", C.c_uint32), ("reserved", C.c_uint32),
+                ("batch_pairs", C.c_uint32), ("max_jobs", C.c_uint32), ("workers", C.c_uint32),
                 ("hbm_budget", C.c_uint64)]
 
 
@@ -122,6 +122,7 @@ ABI = [
     ("pdf_state_destroy", None, [C.c_void_p]),
     ("pdf_state_reset", C.c_int, [C.c_void_p]),
     ("pdf_state_reset_async", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pdf_state_reserve", C.c_int, [C.c_void_p, C.c_uint64]),
     ("pdf_state_profile", C.c_int, [C.c_void_p, C.c_int]),
     ("pdf_state_profile_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     ("pdf_state_snapshot", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Totals_t)]),
@@ -145,6 +146,7 @@ ABI = [
                                     C.c_void_p, C.POINTER(Totals_t), C.c_void_p]),
     ("pdf_batch_create", C.c_int, [C.POINTER(BatchJob_t), C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("pdf_batch_destroy", None, [C.c_void_p]),
+    ("pdf_batch_rebind", C.c_int, [C.c_void_p, C.POINTER(BatchJob_t), C.c_uint32, C.c_uint32]),
     ("pdf_batch_query", C.c_int, [C.c_void_p, C.POINTER(BatchInfo_t)]),
     ("pdf_batch_run_async", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pdf_batch_run", C.c_int, [C.c_void_p, C.c_void_p]),
@@ -472,14 +474,27 @@ class Batch:
     by its pair count."""
 
     def __init__(self, jobs, append: bool = False):
+        self.h = None
         self.jobs = list(jobs)  # keeps circuits, states and pair tensors alive
-        arr = (BatchJob_t * len(self.jobs))()
-        for k, (c, s, v, t, n, base) in enumerate(self.jobs):
-            arr[k] = BatchJob_t(c.h, s.h, make_pairs(v, t, n), base)
         h = C.c_void_p()
-        check(lib().pdf_batch_create(arr, len(self.jobs), BATCH_APPEND if append else 0, C.byref(h)),
-              "pdf_batch_create")
+        check(lib().pdf_batch_create(self._arr(self.jobs), len(self.jobs), BATCH_APPEND if append else 0,
+                                     C.byref(h)), "pdf_batch_create")
         self.h = h
+
+    @staticmethod
+    def _arr(jobs):
+        arr = (BatchJob_t * len(jobs))()
+        for k, (c, s, v, t, n, base) in enumerate(jobs):
+            arr[k] = BatchJob_t(c.h, s.h, make_pairs(v, t, n), base)
+        return arr
+
+    def rebind(self, jobs, append: bool = False):
+        """Point this batch at another job list (pdf_batch_rebind); no run of
+        it may be in flight."""
+        jobs = list(jobs)
+        check(lib().pdf_batch_rebind(self.h, self._arr(jobs), len(jobs), BATCH_APPEND if append else 0),
+              "pdf_batch_rebind")
+        self.jobs = jobs
 
     def info(self) -> BatchInfo_t:
         i = BatchInfo_t()

@@ -114,7 +114,7 @@ struct ProfEvents {
 struct pdf_state {
     pdf_circuit *c = nullptr;
     DevBuf first_x, first_y, acc;
-    DevAcc *host_acc = nullptr;  // pinned
+    DevAcc *host_acc = nullptr;  // host copy of the accumulators (read after a stream sync)
     Workspace ws;
     std::mutex mu;
     bool profiling = false;
@@ -235,21 +235,25 @@ extern "C" pdf_status pdf_netlist_check(const pdf_netlist *nl, char *msg, size_t
                     nl->nfo[g]);
             return PDF_EINVAL;
         }
-    // Multiset comparison: count (source, consumer) occurrences both ways.
+    // Multiset comparison: the consumers of each gate (transposed from the
+    // fan-in lists by a counting sort, hence ascending) against its fan-out
+    // list, sorted.  Linear in the edges apart from sorting each list.
     {
-        std::vector<std::pair<uint32_t, uint32_t>> in, out;
-        in.reserve(nl->n_edges / 2 + 1);
-        out.reserve(nl->n_edges / 2 + 1);
+        std::vector<uint64_t> start(G + 1, 0);
+        for (uint32_t g = 0; g < G; g++) start[g + 1] = start[g] + cnt[g];
+        std::vector<uint32_t> cons(start[G]);
+        std::vector<uint64_t> fill(start.begin(), start.end() - 1);
+        for (uint32_t g = 0; g < G; g++)
+            for (uint32_t j = 0; j < nl->nfi[g]; j++) cons[fill[nl->edges[nl->edge_offset[g] + j]]++] = g;
+        std::vector<uint32_t> fo;
         for (uint32_t g = 0; g < G; g++) {
-            for (uint32_t j = 0; j < nl->nfi[g]; j++) in.emplace_back(nl->edges[nl->edge_offset[g] + j], g);
-            for (uint32_t k = 0; k < nl->nfo[g]; k++)
-                out.emplace_back(g, nl->edges[nl->edge_offset[g] + nl->nfi[g] + k]);
-        }
-        std::sort(in.begin(), in.end());
-        std::sort(out.begin(), out.end());
-        if (in != out) {
-            set_msg(msg, len, "fan-out lists are not the transpose of the fan-in lists");
-            return PDF_EINVAL;
+            const uint32_t *e = nl->edges + nl->edge_offset[g] + nl->nfi[g];
+            fo.assign(e, e + nl->nfo[g]);
+            std::sort(fo.begin(), fo.end());
+            if (!std::equal(fo.begin(), fo.end(), cons.begin() + start[g])) {
+                set_msg(msg, len, "fan-out lists are not the transpose of the fan-in lists (gate %llu)", g);
+                return PDF_EINVAL;
+            }
         }
     }
     set_msg(msg, len, "ok");
@@ -326,8 +330,14 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
 
     // Launch plan: CTAs of `threads` threads own `bw` words of pairs; two
     // CTAs per SM share its shared memory.
-    cudaDeviceProp prop{};
-    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess) {
+    struct {
+        int sharedMemPerBlockOptin = 0, sharedMemPerMultiprocessor = 0, multiProcessorCount = 0;
+    } prop;
+    if (cudaDeviceGetAttribute(&prop.sharedMemPerBlockOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, o.device) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&prop.sharedMemPerMultiprocessor, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                               o.device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&prop.multiProcessorCount, cudaDevAttrMultiProcessorCount, o.device) != cudaSuccess) {
         delete c;
         return PDF_ECUDA;
     }
@@ -335,8 +345,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
     uint32_t threads_default = 512;  // set from the piece size below
     const size_t budget = c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
-                                      : std::min<size_t>(prop.sharedMemPerBlockOptin,
-                                                         prop.sharedMemPerMultiprocessor / 2 - 2048);
+                                      : std::min<size_t>((size_t)prop.sharedMemPerBlockOptin,
+                                                         (size_t)prop.sharedMemPerMultiprocessor / 2 - 2048);
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
     // Pieces (the kernels' unit of staging and of synchronisation), sized
@@ -476,7 +486,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->fwd_smem = off + ring_bytes(ring);
     // nets one pair may mark in the cover: as many as its shared memory holds
     c->hash_cap = 4096;
-    while (c->hash_cap > 256 && cover_smem_bytes(c->hash_cap) > prop.sharedMemPerBlockOptin) c->hash_cap -= 256;
+    while (c->hash_cap > 256 && cover_smem_bytes(c->hash_cap) > (size_t)prop.sharedMemPerBlockOptin) c->hash_cap -= 256;
     c->cover_threads = 256;
     c->cover_grid = (uint32_t)prop.multiProcessorCount;
 
@@ -557,7 +567,7 @@ extern "C" pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out) {
     const size_t G = c->info.n_gates;
     if (s->first_x.ensure(4 * G) != cudaSuccess || s->first_y.ensure(4 * G) != cudaSuccess ||
         s->acc.ensure(sizeof(DevAcc)) != cudaSuccess ||
-        cudaMallocHost(&s->host_acc, sizeof(DevAcc)) != cudaSuccess) {
+        !(s->host_acc = new (std::nothrow) DevAcc())) {
         (void)cudaGetLastError();
         pdf_state_destroy(s);
         return PDF_ENOMEM;
@@ -580,7 +590,7 @@ extern "C" void pdf_state_destroy(pdf_state *s) {
     s->first_x.release();
     s->first_y.release();
     s->acc.release();
-    if (s->host_acc) cudaFreeHost(s->host_acc);
+    delete s->host_acc;
     delete s;
 }
 
@@ -1155,11 +1165,12 @@ struct pdf_batch {
     std::vector<pdf_circuit *> circuits;
     std::vector<pdf_state *> states;
     BatchLaunch L{};
-    DevBuf fargs, cargs, bpref, gpref, items, ctl;
+    DevBuf ctl;  // control word, arguments, prefixes and items in one block
     uint64_t gate_evals = 0, bytes = 0;
     cudaStream_t cap_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    bool use_graph = true;
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -1167,19 +1178,16 @@ struct pdf_batch {
         exec = nullptr;
         graph = nullptr;
         cap_stream = nullptr;
-        fargs.release();
-        cargs.release();
-        bpref.release();
-        gpref.release();
-        items.release();
         ctl.release();
     }
 };
 
-extern "C" pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out) {
-    if (!out) return PDF_EINVAL;
-    *out = nullptr;
-    if (!jobs || !n_jobs || (flags & ~(uint32_t)PDF_BATCH_APPEND)) return PDF_EINVAL;
+namespace {
+
+// (Re)build batch b for these jobs: per-circuit arguments and prefixes in
+// one device block, which is reused when it is large enough.
+pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags) {
+    if (!jobs || !n_jobs || (flags & ~(uint32_t)(PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH))) return PDF_EINVAL;
     pdf_circuit *c0 = jobs[0].circuit;
     if (!c0) return PDF_EINVAL;
     for (uint32_t i = 0; i < n_jobs; i++) {
@@ -1192,22 +1200,20 @@ extern "C" pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_job
             !planes_fit(j.circuit, W, j.pairs.ld, {j.pairs.v, j.pairs.t}))
             return PDF_EINVAL;
     }
-    DeviceGuard dg(c0->device);
-    if (!dg.ok) return PDF_ECUDA;
-    pdf_batch *b = new (std::nothrow) pdf_batch();
-    if (!b) return PDF_ENOMEM;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
     b->device = c0->device;
-    auto fail = [&](pdf_status st) {
-        b->release();
-        delete b;
-        (void)cudaGetLastError();
-        return st;
-    };
+    b->circuits.clear();
+    b->states.clear();
+    b->gate_evals = 0;
     std::vector<FwdArgs> fa(n_jobs);
     std::vector<CoverArgs> ca(n_jobs);
     std::vector<uint32_t> bp(n_jobs + 1, 0), gp(n_jobs + 1, 0);
     uint64_t items = 0;
     BatchLaunch &L = b->L;
+    L = BatchLaunch{};
     L.bw = c0->bw;
     L.robust = c0->mark_mode == PDF_MARK_ROBUST ? 1u : 0u;
     L.hash_cap = c0->hash_cap;
@@ -1216,7 +1222,7 @@ extern "C" pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_job
         pdf_circuit *c = j.circuit;
         pdf_state *s = j.state;
         const uint64_t n = j.pairs.n_pairs, W = (n + 31) / 32, G = c->info.n_gates;
-        if (ensure_ws(c, s->ws, W, true) != PDF_OK) return fail(PDF_ENOMEM);
+        if (ensure_ws(c, s->ws, W, true) != PDF_OK) return PDF_ENOMEM;
         FwdArgs a = base_fwd(c, n);
         a.pi_v = j.pairs.v;
         a.pi_t = j.pairs.t;
@@ -1238,7 +1244,7 @@ extern "C" pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_job
         fa[i] = a;
         ca[i] = base_cover(c, s->ws, a.M, a.ld, n, (uint32_t)j.pair_base, a.first_x, a.first_y, acc);
         const uint64_t blocks = (W + c->bw - 1) / c->bw;
-        if (bp[i] + blocks > 0x7FFFFFFFull || gp[i] + G > 0xFFFFFFFFull) return fail(PDF_ENOTSUP);
+        if (bp[i] + blocks > 0x7FFFFFFFull || gp[i] + G > 0xFFFFFFFFull) return PDF_ENOTSUP;
         bp[i + 1] = bp[i] + (uint32_t)blocks;
         gp[i + 1] = gp[i] + (uint32_t)G;
         items += std::min<uint64_t>(W * 32, 2 * G);
@@ -1253,29 +1259,62 @@ extern "C" pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_job
     L.total_blocks = bp[n_jobs];
     L.total_gates = gp[n_jobs];
     L.append = (flags & PDF_BATCH_APPEND) ? 1u : 0u;
-    if (b->fargs.ensure(sizeof(FwdArgs) * n_jobs) != cudaSuccess ||
-        b->cargs.ensure(sizeof(CoverArgs) * n_jobs) != cudaSuccess ||
-        b->bpref.ensure(4 * (n_jobs + 1)) != cudaSuccess || b->gpref.ensure(4 * (n_jobs + 1)) != cudaSuccess ||
-        b->items.ensure(sizeof(uint2) * std::max<uint64_t>(items, 1)) != cudaSuccess ||
-        b->ctl.ensure(sizeof(BatchCtl)) != cudaSuccess)
-        return fail(PDF_ENOMEM);
-    if (cudaMemcpy(b->fargs.p, fa.data(), sizeof(FwdArgs) * n_jobs, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(b->cargs.p, ca.data(), sizeof(CoverArgs) * n_jobs, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(b->bpref.p, bp.data(), 4 * (n_jobs + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(b->gpref.p, gp.data(), 4 * (n_jobs + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(b->ctl.p, 0, sizeof(BatchCtl)) != cudaSuccess)
-        return fail(PDF_ECUDA);
-    L.fargs = b->fargs.as<FwdArgs>();
-    L.cargs = b->cargs.as<CoverArgs>();
-    L.bpref = b->bpref.as<uint32_t>();
-    L.gpref = b->gpref.as<uint32_t>();
-    L.items = b->items.as<uint2>();
-    L.ctl = b->ctl.as<BatchCtl>();
-    b->bytes = b->fargs.bytes + b->cargs.bytes + b->bpref.bytes + b->gpref.bytes + b->items.bytes + b->ctl.bytes;
-    if (prepare_batch(L) != cudaSuccess) return fail(PDF_ECUDA);
-    if (cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PDF_ECUDA);
+    b->use_graph = !(flags & PDF_BATCH_NO_GRAPH);
+    // one device block: control word, circuit arguments, prefixes, then items
+    auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_f = a256(sizeof(BatchCtl)), o_c = o_f + a256(sizeof(FwdArgs) * n_jobs),
+                 o_b = o_c + a256(sizeof(CoverArgs) * n_jobs), o_g = o_b + a256(4 * (n_jobs + 1)),
+                 o_i = o_g + a256(4 * (n_jobs + 1)), total = o_i + sizeof(uint2) * std::max<uint64_t>(items, 1);
+    std::vector<unsigned char> hbuf(o_i, 0);
+    std::memcpy(hbuf.data() + o_f, fa.data(), sizeof(FwdArgs) * n_jobs);
+    std::memcpy(hbuf.data() + o_c, ca.data(), sizeof(CoverArgs) * n_jobs);
+    std::memcpy(hbuf.data() + o_b, bp.data(), 4 * (n_jobs + 1));
+    std::memcpy(hbuf.data() + o_g, gp.data(), 4 * (n_jobs + 1));
+    if (b->ctl.ensure(total) != cudaSuccess) return PDF_ENOMEM;
+    if (cudaMemcpy(b->ctl.p, hbuf.data(), o_i, cudaMemcpyHostToDevice) != cudaSuccess) return PDF_ECUDA;
+    unsigned char *base = b->ctl.as<unsigned char>();
+    L.ctl = reinterpret_cast<BatchCtl *>(base);
+    L.fargs = reinterpret_cast<FwdArgs *>(base + o_f);
+    L.cargs = reinterpret_cast<CoverArgs *>(base + o_c);
+    L.bpref = reinterpret_cast<const uint32_t *>(base + o_b);
+    L.gpref = reinterpret_cast<const uint32_t *>(base + o_g);
+    L.items = reinterpret_cast<uint2 *>(base + o_i);
+    b->bytes = b->ctl.bytes;
+    if (prepare_batch(L) != cudaSuccess) return PDF_ECUDA;
+    if (b->use_graph && !b->cap_stream &&
+        cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return PDF_ECUDA;
+    return PDF_OK;
+}
+
+}  // namespace
+
+extern "C" pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out) {
+    if (!out) return PDF_EINVAL;
+    *out = nullptr;
+    if (!jobs || !n_jobs || !jobs[0].circuit) return PDF_EINVAL;
+    DeviceGuard dg(jobs[0].circuit->device);
+    if (!dg.ok) return PDF_ECUDA;
+    pdf_batch *b = new (std::nothrow) pdf_batch();
+    if (!b) return PDF_ENOMEM;
+    const pdf_status st = batch_build(b, jobs, n_jobs, flags);
+    if (st != PDF_OK) {
+        b->release();
+        delete b;
+        (void)cudaGetLastError();
+        return st;
+    }
     *out = b;
     return PDF_OK;
+}
+
+extern "C" pdf_status pdf_batch_rebind(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags) {
+    if (!b || !jobs || !n_jobs || !jobs[0].circuit || jobs[0].circuit->device != b->device) return PDF_EINVAL;
+    DeviceGuard dg(b->device);
+    if (!dg.ok) return PDF_ECUDA;
+    const pdf_status st = batch_build(b, jobs, n_jobs, flags);
+    if (st != PDF_OK) (void)cudaGetLastError();
+    return st;
 }
 
 extern "C" void pdf_batch_destroy(pdf_batch *b) {
@@ -1300,6 +1339,10 @@ extern "C" pdf_status pdf_batch_run_async(pdf_batch *b, void *stream) {
     if (!b) return PDF_EINVAL;
     DeviceGuard dg(b->device);
     if (!dg.ok) return PDF_ECUDA;
+    if (!b->use_graph) {
+        PDF_CUDA(launch_batch(b->L, static_cast<cudaStream_t>(stream)));
+        return PDF_OK;
+    }
     if (!b->exec) {  // capture the three launches once
         PDF_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
         const cudaError_t le = launch_batch(b->L, b->cap_stream);
@@ -1322,16 +1365,10 @@ extern "C" pdf_status pdf_batch_run(pdf_batch *b, void *stream) {
     if (st != PDF_OK) return st;
     DeviceGuard dg(b->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    BatchCtl h{};
+    PDF_CUDA(cudaMemcpyAsync(&h, b->ctl.p, sizeof h, cudaMemcpyDeviceToHost, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));
-    unsigned int err = 0;
-    for (size_t i = 0; i < b->states.size(); i++) {
-        DevAcc h{};
-        unsigned int ce = 0;
-        PDF_CUDA(cudaMemcpy(&h, b->states[i]->acc.p, sizeof h, cudaMemcpyDeviceToHost));
-        PDF_CUDA(cudaMemcpy(&ce, b->circuits[i]->err.p, sizeof ce, cudaMemcpyDeviceToHost));
-        err |= h.err | ce;
-    }
-    return err_status(err);
+    return err_status(h.err);
 }
 
 // Autotuner of the batch tile width: times the whole batch at each candidate.
@@ -1412,4 +1449,12 @@ extern "C" pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, con
     best->tile_words = best_w;
     if (best_ms) *best_ms = best_t;
     return PDF_OK;
+}
+
+extern "C" pdf_status pdf_state_reserve(pdf_state *s, uint64_t n_pairs) {
+    if (!s || !n_pairs) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    std::lock_guard<std::mutex> lk(s->mu);
+    return ensure_ws(s->c, s->ws, (n_pairs + 31) / 32, true);
 }

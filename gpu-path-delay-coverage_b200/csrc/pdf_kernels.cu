@@ -976,6 +976,7 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
         if (blockIdx.x == 0) {
             ctl->n_items = 0;
             ctl->done = 0;
+            ctl->err = 0;
         }
     }
     __syncthreads();
@@ -1011,14 +1012,18 @@ __global__ void __launch_bounds__(256) k_batch_cover(CoverArgs *args, FwdArgs *f
     __syncthreads();
     if (!s_last) return;
     __threadfence();
+    unsigned int err = 0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint64_t np = args[i].n_pairs;
+        err |= args[i].acc->err;
         batch_close(args[i].acc, np);
         if (append) {
             args[i].pair_base += (uint32_t)np;
             fargs[i].pair_base += (uint32_t)np;
         }
     }
+    err = __reduce_or_sync(0xFFFFFFFFu, err);
+    if ((threadIdx.x & 31) == 0 && err) atomicOr(&ctl->err, err);
     if (threadIdx.x == 0) ctl->done = 0;
 }
 

@@ -93,7 +93,8 @@ struct CoverArgs {
 struct BatchCtl {
     unsigned int n_items;  // first-detecting (circuit, pair) items of this pass
     unsigned int done;     // cover CTAs finished
-    unsigned int pad[2];
+    unsigned int err;      // OR of every circuit's device error word after the pass
+    unsigned int pad;
 };
 struct BatchLaunch {
     FwdArgs *fargs;        // [n] per circuit, device

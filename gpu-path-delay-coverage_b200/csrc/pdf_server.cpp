@@ -1,22 +1,28 @@
 // pdf_server.cpp -- serving loop: continuous batching of grading jobs over
 // the public C ABI (circuits, states and pdf_batch_*).
 //
-// A job owns a device circuit, a coverage state and a pair buffer of one
-// batch while it is active.  Each step admits queued jobs in arrival order
-// while the estimated device footprint fits the budget, copies the next
-// batch of every active job into its buffer, grades all of them in one
-// append-mode batched pass and retires the jobs whose pairs are done.  The
-// batched pass is rebuilt only when the set of active jobs (or a job's batch
-// size, on its last batch) changes; otherwise its captured graph is replayed.
+// A job owns a device circuit, a coverage state with its workspace, its
+// vector pairs (uploaded once) and a pair buffer of one batch while it is
+// active.  A worker thread prepares queued jobs in arrival order while the
+// estimated device footprint fits the budget (host plan, device upload) on
+// worker threads, so that work overlaps the grading.  Each step admits the prepared jobs, copies
+// the next batch of every active job into its buffer (device to device),
+// grades all of them in one append-mode batched pass and retires the jobs
+// whose pairs are done.  The batched pass is rebuilt only when the set of
+// active jobs (or a job's batch size, on its last batch) changes; it launches
+// its kernels directly (no graph capture while workers call into CUDA).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "pdf.h"
@@ -39,12 +45,15 @@ struct Job {
     pdf_state *s = nullptr;
     uint32_t *dv = nullptr;  // [2][n_pi][ld] one batch of pairs
     uint64_t ld = 0, cur = 0;  // words per row, pairs of the batch in flight
+    uint32_t *dall = nullptr;  // [2][n_pi][hld] all the job's pairs, on the device while active
+    pdf_status prep = PDF_OK;  // outcome of the preparation
     double t_ready = 0.0;
 };
 
 struct Result {
     pdf_totals total{};
     std::vector<uint32_t> fx, fy;
+    pdf_status status = PDF_OK;
 };
 
 }  // namespace
@@ -52,15 +61,23 @@ struct Result {
 struct pdf_server {
     pdf_server_opts o{};
     uint64_t next_id = 1;
-    std::deque<Job *> queue;
     std::vector<Job *> active;
     std::map<uint64_t, Result> results;
     pdf_batch *batch = nullptr;
     bool dirty = true;
-    uint64_t used = 0;
     cudaStream_t stream = nullptr;
     pdf_server_stats st{};
     std::vector<double> lat_ms;
+    // shared with the worker (under mu)
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Job *> queue;     // submitted, not yet prepared
+    std::deque<Job *> ready;     // prepared, not yet active
+    std::deque<Job *> retired;   // results taken, device memory still to free (by a worker)
+    uint64_t used = 0;           // footprint of prepared + active jobs
+    uint64_t n_active = 0;       // jobs prepared or active
+    bool stop = false;
+    std::vector<std::thread> workers;
 };
 
 namespace {
@@ -78,12 +95,96 @@ uint64_t footprint(const pdf_netlist &nl, uint64_t batch_pairs, uint32_t bw) {
            + (1u << 20);
 }
 
+// The job's pairs, uploaded once at admission.
+uint64_t pairs_bytes(const pdf_netlist &nl, uint64_t hld) { return 8 * (uint64_t)nl.level_offsets[1] * hld; }
+
 void free_job(Job *j) {
     if (j->dv) cudaFree(j->dv);
+    if (j->dall) cudaFree(j->dall);
     pdf_state_destroy(j->s);
     pdf_circuit_destroy(j->c);
     pdf_netbuf_free(j->net);
     delete j;
+}
+
+}  // namespace
+
+namespace {
+
+// Circuit, state with its workspace, pair buffers and the job's pairs on the
+// device.  On failure nothing stays allocated and j->prep holds the status.
+void prepare(const pdf_server_opts &o, Job *j, cudaStream_t up) {
+    pdf_circuit_opts co{};
+    co.device = o.device;
+    co.mark_mode = o.mark_mode;
+    co.tile_words = o.tile_words;
+    co.max_pairs = o.batch_pairs;
+    const uint64_t W = o.batch_pairs / 32, npi = j->view.level_offsets[1];
+    j->ld = (W + o.tile_words - 1) / o.tile_words * o.tile_words;
+    const size_t hb = (size_t)npi * j->hld * 4;
+    pdf_status st = pdf_circuit_create(&j->view, &co, &j->c);
+    if (st == PDF_OK) st = pdf_state_create(j->c, &j->s);
+    if (st == PDF_OK) st = pdf_state_reserve(j->s, o.batch_pairs);
+    if (st == PDF_OK && (cudaMalloc(&j->dv, 2 * npi * j->ld * 4) != cudaSuccess ||
+                         cudaMalloc(&j->dall, pairs_bytes(j->view, j->hld)) != cudaSuccess))
+        st = PDF_ENOMEM;
+    if (st == PDF_OK && (cudaMemsetAsync(j->dv, 0, 2 * npi * j->ld * 4, up) != cudaSuccess ||
+                         cudaMemcpyAsync(j->dall, j->hv, hb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
+                         cudaMemcpyAsync(j->dall + npi * j->hld, j->ht, hb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
+                         cudaStreamSynchronize(up) != cudaSuccess))
+        st = PDF_ECUDA;
+    if (st != PDF_OK) {
+        if (j->dv) cudaFree(j->dv);
+        if (j->dall) cudaFree(j->dall);
+        pdf_state_destroy(j->s);
+        pdf_circuit_destroy(j->c);
+        j->dv = nullptr;
+        j->dall = nullptr;
+        j->s = nullptr;
+        j->c = nullptr;
+        (void)cudaGetLastError();
+    }
+    j->prep = st;
+}
+
+// Worker (several run): takes queued jobs in arrival order while they fit the
+// budget and prepares them.
+void work(pdf_server *srv) {
+    cudaSetDevice(srv->o.device);
+    cudaStream_t up = nullptr;
+    cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+    std::unique_lock<std::mutex> lk(srv->mu);
+    for (;;) {
+        srv->cv.wait(lk, [&] {
+            if (srv->stop || !srv->retired.empty()) return true;
+            if (srv->queue.empty() || srv->n_active >= srv->o.max_jobs) return false;
+            return srv->n_active == 0 || srv->used + srv->queue.front()->bytes <= srv->o.hbm_budget;
+        });
+        if (srv->stop) break;
+        if (!srv->retired.empty()) {  // freeing synchronises the device: keep it off the step
+            Job *r = srv->retired.front();
+            srv->retired.pop_front();
+            const uint64_t bytes = r->bytes;
+            lk.unlock();
+            free_job(r);
+            lk.lock();
+            srv->used -= bytes;
+            srv->n_active--;
+            srv->cv.notify_all();
+            continue;
+        }
+        Job *j = srv->queue.front();
+        srv->queue.pop_front();
+        srv->used += j->bytes;
+        srv->n_active++;
+        lk.unlock();
+        prepare(srv->o, j, up);
+        lk.lock();
+        srv->ready.push_back(j);
+        srv->cv.notify_all();
+    }
+    lk.unlock();
+    if (up) cudaStreamDestroy(up);
 }
 
 }  // namespace
@@ -111,16 +212,25 @@ extern "C" pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server 
         delete srv;
         return PDF_ECUDA;
     }
+    for (uint32_t k = 0; k < (o.workers ? o.workers : 4); k++) srv->workers.emplace_back(work, srv);
     *out = srv;
     return PDF_OK;
 }
 
 extern "C" void pdf_server_destroy(pdf_server *srv) {
     if (!srv) return;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stop = true;
+    }
+    srv->cv.notify_all();
+    for (std::thread &w : srv->workers) w.join();
     cudaSetDevice(srv->o.device);
     cudaStreamSynchronize(srv->stream);
     pdf_batch_destroy(srv->batch);
     for (Job *j : srv->active) free_job(j);
+    for (Job *j : srv->ready) free_job(j);
+    for (Job *j : srv->retired) free_job(j);
     for (Job *j : srv->queue) free_job(j);
     cudaStreamDestroy(srv->stream);
     delete srv;
@@ -130,8 +240,10 @@ extern "C" pdf_status pdf_server_submit(pdf_server *srv, const pdf_netlist *nl, 
                                         uint64_t ld, uint64_t n_pairs, uint64_t *job_id) {
     if (!srv || !nl || !v || !t || !n_pairs || ld < (n_pairs + 31) / 32 || n_pairs > 0xFFFFFFFFull)
         return PDF_EINVAL;
-    pdf_status st = pdf_netlist_check(nl, nullptr, 0);
-    if (st != PDF_OK) return st;
+    // the netlist is checked where the job is prepared (pdf_circuit_create);
+    // a job that fails there reports the status from pdf_server_result
+    if (!nl->n_gates || !nl->n_levels || !nl->level_offsets) return PDF_EINVAL;
+    pdf_status st = PDF_OK;
     Job *j = new (std::nothrow) Job();
     if (!j) return PDF_ENOMEM;
     if ((st = pdf_netbuf_from(nl, &j->net)) != PDF_OK) {
@@ -144,9 +256,13 @@ extern "C" pdf_status pdf_server_submit(pdf_server *srv, const pdf_netlist *nl, 
     j->ht = t;
     j->hld = ld;
     j->n_pairs = n_pairs;
-    j->bytes = footprint(j->view, srv->o.batch_pairs, srv->o.tile_words);
+    j->bytes = footprint(j->view, srv->o.batch_pairs, srv->o.tile_words) + pairs_bytes(j->view, ld);
     j->t_ready = now_s();
-    srv->queue.push_back(j);
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->queue.push_back(j);
+    }
+    srv->cv.notify_one();
     if (job_id) *job_id = j->id;
     return PDF_OK;
 }
@@ -157,36 +273,29 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     if (cudaSetDevice(srv->o.device) != cudaSuccess) return PDF_ECUDA;
     const double t0 = now_s();
     pdf_status st = PDF_OK;
-    // admission, in arrival order, by footprint
-    while (!srv->queue.empty() && srv->active.size() < srv->o.max_jobs) {
-        Job *j = srv->queue.front();
-        if (srv->used + j->bytes > srv->o.hbm_budget && !srv->active.empty()) break;
-        pdf_circuit_opts co{};
-        co.device = srv->o.device;
-        co.mark_mode = srv->o.mark_mode;
-        co.tile_words = srv->o.tile_words;
-        co.max_pairs = srv->o.batch_pairs;
-        // on failure the job stays queued with nothing allocated
-        auto undo = [&](pdf_status e) {
-            if (j->dv) cudaFree(j->dv);
-            pdf_state_destroy(j->s);
-            pdf_circuit_destroy(j->c);
-            j->dv = nullptr;
-            j->s = nullptr;
-            j->c = nullptr;
-            (void)cudaGetLastError();
-            return e;
-        };
-        if ((st = pdf_circuit_create(&j->view, &co, &j->c)) != PDF_OK) return undo(st);
-        if ((st = pdf_state_create(j->c, &j->s)) != PDF_OK) return undo(st);
-        const uint64_t W = srv->o.batch_pairs / 32, npi = j->view.level_offsets[1];
-        j->ld = (W + srv->o.tile_words - 1) / srv->o.tile_words * srv->o.tile_words;
-        if (cudaMalloc(&j->dv, 2 * npi * j->ld * 4) != cudaSuccess) return undo(PDF_ENOMEM);
-        if (cudaMemset(j->dv, 0, 2 * npi * j->ld * 4) != cudaSuccess) return undo(PDF_ECUDA);
-        srv->used += j->bytes;
-        srv->queue.pop_front();
-        srv->active.push_back(j);
-        srv->dirty = true;
+    // admission: the jobs the worker has prepared (in arrival order); with
+    // none active, wait (up to a second) for the first one in preparation
+    {
+        std::unique_lock<std::mutex> lk(srv->mu);
+        if (srv->active.empty() && srv->ready.empty() && srv->n_active > 0)
+            srv->cv.wait_for(lk, std::chrono::seconds(1), [&] { return !srv->ready.empty(); });
+        while (!srv->ready.empty()) {
+            Job *j = srv->ready.front();
+            srv->ready.pop_front();
+            if (j->prep != PDF_OK) {  // could not be prepared: its result reports why
+                Result r;
+                r.total.flags = 0;
+                r.status = j->prep;
+                srv->results[j->id] = std::move(r);
+                srv->used -= j->bytes;
+                srv->n_active--;
+                free_job(j);
+                srv->st.jobs_done++;
+                continue;
+            }
+            srv->active.push_back(j);
+            srv->dirty = true;
+        }
     }
     if (srv->active.empty()) return PDF_OK;
     // the next batch of every active job
@@ -196,25 +305,26 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         j->cur = n;
         const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32, W = (n + 31) / 32;
         uint32_t *dv = j->dv, *dt = j->dv + npi * j->ld;
-        if (cudaMemcpy2DAsync(dv, j->ld * 4, j->hv + w0, j->hld * 4, W * 4, npi, cudaMemcpyHostToDevice,
-                              srv->stream) != cudaSuccess ||
-            cudaMemcpy2DAsync(dt, j->ld * 4, j->ht + w0, j->hld * 4, W * 4, npi, cudaMemcpyHostToDevice,
-                              srv->stream) != cudaSuccess) {
+        const uint32_t *sv = j->dall + w0, *stp = j->dall + npi * j->hld + w0;
+        if (cudaMemcpy2DAsync(dv, j->ld * 4, sv, j->hld * 4, W * 4, npi, cudaMemcpyDeviceToDevice, srv->stream) !=
+                cudaSuccess ||
+            cudaMemcpy2DAsync(dt, j->ld * 4, stp, j->hld * 4, W * 4, npi, cudaMemcpyDeviceToDevice, srv->stream) !=
+                cudaSuccess) {
             (void)cudaGetLastError();
             return PDF_ECUDA;
         }
     }
     if (srv->dirty) {
-        pdf_batch_destroy(srv->batch);
-        srv->batch = nullptr;
         std::vector<pdf_batch_job> jobs;
         for (Job *j : srv->active) {
             const uint64_t npi = j->view.level_offsets[1];
             jobs.push_back(pdf_batch_job{j->c, j->s, pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1},
                                          j->done});
         }
-        if ((st = pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), PDF_BATCH_APPEND, &srv->batch)) != PDF_OK)
-            return st;
+        const uint32_t fl = PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH;
+        st = srv->batch ? pdf_batch_rebind(srv->batch, jobs.data(), (uint32_t)jobs.size(), fl)
+                        : pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), fl, &srv->batch);
+        if (st != PDF_OK) return st;
         srv->dirty = false;
     }
     if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
@@ -237,8 +347,11 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         r.fy.resize(j->view.n_gates);
         if ((st = pdf_state_snapshot(j->s, r.fx.data(), r.fy.data(), &r.total)) != PDF_OK) return st;
         srv->results[j->id] = std::move(r);
-        srv->used -= j->bytes;
-        free_job(j);
+        {
+            std::lock_guard<std::mutex> lk(srv->mu);
+            srv->retired.push_back(j);
+        }
+        srv->cv.notify_all();
         srv->st.jobs_done++;
         srv->dirty = true;
         if (retired) (*retired)++;
@@ -253,6 +366,7 @@ extern "C" pdf_status pdf_server_result(pdf_server *srv, uint64_t job_id, pdf_to
     if (!srv) return PDF_EINVAL;
     auto it = srv->results.find(job_id);
     if (it == srv->results.end()) return PDF_EINVAL;
+    if (it->second.status != PDF_OK) return it->second.status;
     if (total) *total = it->second.total;
     if (first_x) std::memcpy(first_x, it->second.fx.data(), it->second.fx.size() * 4);
     if (first_y) std::memcpy(first_y, it->second.fy.data(), it->second.fy.size() * 4);
@@ -262,9 +376,13 @@ extern "C" pdf_status pdf_server_result(pdf_server *srv, uint64_t job_id, pdf_to
 extern "C" pdf_status pdf_server_query(const pdf_server *srv, pdf_server_stats *stats) {
     if (!srv || !stats) return PDF_EINVAL;
     *stats = srv->st;
-    stats->jobs_active = srv->active.size();
-    stats->jobs_queued = srv->queue.size();
-    stats->bytes_in_use = srv->used;
+    pdf_server *m = const_cast<pdf_server *>(srv);
+    {
+        std::lock_guard<std::mutex> lk(m->mu);
+        stats->jobs_active = srv->active.size() + srv->ready.size();
+        stats->jobs_queued = srv->queue.size();
+        stats->bytes_in_use = srv->used;
+    }
     std::vector<double> l = srv->lat_ms;
     if (!l.empty()) {
         std::sort(l.begin(), l.end());

@@ -192,6 +192,9 @@ pdf_status pdf_state_restore(pdf_state *s, const uint32_t *first_x,
 
 /* Stream-ordered reset: clears the state on `stream` without waiting. */
 pdf_status pdf_state_reset_async(pdf_state *s, void *stream);
+/* Allocate now the device workspace that grading batches of up to n_pairs
+ * pairs needs (otherwise allocated by the first such call). */
+pdf_status pdf_state_reserve(pdf_state *s, uint64_t n_pairs);
 
 /* Device timing of grading calls with CUDA events on the grading stream.
  * enable = 1 clears and starts recording, 0 stops.  pdf_state_profile_read
@@ -309,7 +312,12 @@ typedef struct pdf_batch_job {
     pdf_pairs pairs;
     uint64_t pair_base; /* global id of the job's first pair in the first run */
 } pdf_batch_job;
-enum { PDF_BATCH_APPEND = 1 };
+enum {
+    PDF_BATCH_APPEND = 1,   /* each run advances every job's pair_base by its pair count */
+    PDF_BATCH_NO_GRAPH = 2  /* launch the kernels directly instead of replaying a captured graph
+                               (for batches rebuilt often, or when other host threads make
+                               device-synchronising CUDA calls while a run might capture) */
+};
 typedef struct pdf_batch_info {
     uint32_t n_jobs, tile_words, threads, ctas;
     uint64_t gate_evals; /* per run: sum over jobs of n_gates * n_pairs */
@@ -317,6 +325,12 @@ typedef struct pdf_batch_info {
 } pdf_batch_info;
 pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out);
 void pdf_batch_destroy(pdf_batch *b);
+/* Point an existing batch at another set of jobs (same rules as
+ * pdf_batch_create; same device).  Its device memory is reused when large
+ * enough, so a loop whose job set changes often allocates and frees little.
+ * No run of the batch may be in flight.  On failure the batch must not be
+ * run until a rebind succeeds. */
+pdf_status pdf_batch_rebind(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags);
 pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info);
 /* One pass over every job, stream-ordered (the first call captures the graph). */
 pdf_status pdf_batch_run_async(pdf_batch *b, void *stream);
@@ -359,7 +373,7 @@ typedef struct pdf_server_opts {
     uint32_t tile_words;    /* 0 = 4 */
     uint32_t batch_pairs;   /* pairs per batch, a multiple of 32 (0 = 4096) */
     uint32_t max_jobs;      /* active jobs at most (0 = 1024) */
-    uint32_t reserved;
+    uint32_t workers;       /* host threads preparing admitted jobs (0 = 4) */
     uint64_t hbm_budget;    /* bytes of device memory for active jobs (0 = half the free memory) */
 } pdf_server_opts;
 typedef struct pdf_server_stats {

@@ -90,6 +90,25 @@ def test_batch_append_grades_consecutive_pairs():
         assert tot.value == w.total and tot.pairs == 2 * n
 
 
+def test_batch_rebind_to_other_jobs():
+    """A batch rebound to a different (smaller, then larger) job list grades
+    exactly that list; jobs left out are not touched."""
+    jobs, want = _jobs(1, seed=3)
+    b = P.Batch(jobs[:3])
+    b.run()
+    b.rebind(jobs[3:])
+    b.run()
+    b.rebind(jobs[:2])
+    b.run()
+    assert b.info().n_jobs == 2
+    for k, ((c, s, *_), (nl, codes, n)) in enumerate(zip(jobs, want)):
+        w = O.grade(nl, codes, n, mark_mode=1)
+        fx, fy, tot = s.snapshot()
+        runs = 2 if k < 2 else 1
+        assert tot.value == runs * w.total and tot.pairs == runs * n
+        np.testing.assert_array_equal(fx, w.first_x)
+
+
 def test_batch_rejects_mixed_tiles():
     jobs, _ = _jobs(0)
     c, s, dv, dt, n, base = jobs[0]

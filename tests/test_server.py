@@ -42,7 +42,7 @@ def _serve(jobs, budget=0, mode=1, arrive_every=2):
             ids.append(srv.submit(nl, v, t, n))
         srv.step()
         steps += 1
-        assert steps < 10000
+        assert steps < 100000
     res = [srv.result(i) for i in ids]
     return res, srv.stats()
 
