@@ -28,6 +28,7 @@ S0, S1, T0, T1 = range(4)
 MARK_DEFAULT, MARK_ROBUST = 0, 1
 FLAG_OVERFLOW = 1
 BATCH_APPEND, BATCH_NO_GRAPH = 1, 2
+BENCH_BRANCHES = 1
 NONE = 0xFFFFFFFF
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "EOVERFLOW", 4: "ETIMEOUT", 5: "ECUDA",
@@ -167,6 +168,19 @@ ABI = [
     ("pdf_gen_pairs", C.c_int, [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("pdf_pairs_from_vectors", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
                                          C.c_void_p]),
+    ("pdf_mark_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
+                                   C.c_void_p]),
+    ("pdf_read_bench", C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    ("pdf_write_bench", C.c_int, [C.POINTER(Netlist_t), C.c_char_p]),
+    ("pdf_read_level", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    ("pdf_write_level", C.c_int, [C.POINTER(Netlist_t), C.c_char_p]),
+    ("pdf_vectors_dim", C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    ("pdf_vectors_read", C.c_int, [C.c_char_p, C.c_uint32, C.c_uint64, C.c_void_p]),
+    ("pdf_dump_sim", C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64,
+                               C.c_uint64, C.c_int]),
+    ("pdf_dump_mark", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64,
+                                C.c_int]),
+    ("pdf_dump_merge", C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint32]),
 ]
 
 
@@ -288,11 +302,16 @@ class GenParams:
 
 def gen_netlist(p: GenParams) -> Netlist:
     """Seeded synthetic netlist (pdf_gen_netlist)."""
-    L = lib()
     gp = GenParams_t(p.seed, p.n_gates, p.n_pi, p.n_po, p.depth, p.fanin_min, p.fanin_max,
                      p.fanout_dist, p.zipf_s, p.fanout_max, p.type_mask)
     h = C.c_void_p()
-    check(L.pdf_gen_netlist(C.byref(gp), C.byref(h)), "pdf_gen_netlist")
+    check(lib().pdf_gen_netlist(C.byref(gp), C.byref(h)), "pdf_gen_netlist")
+    return _take_netbuf(h)
+
+
+def _take_netbuf(h) -> Netlist:
+    """Copy a library-owned netlist into a Netlist and free it."""
+    L = lib()
     try:
         v = Netlist_t()
         L.pdf_netbuf_view(h, C.byref(v))
@@ -307,6 +326,65 @@ def gen_netlist(p: GenParams) -> Netlist:
                        arr(v.edges, E, np.uint32) if E else np.zeros(0, np.uint32))
     finally:
         L.pdf_netbuf_free(h)
+
+
+def _read_netlist(call, *args) -> Netlist:
+    h = C.c_void_p()
+    msg = C.create_string_buffer(512)
+    st = call(*args, C.byref(h), msg, len(msg))
+    if st != 0:
+        raise PdfError(st, msg.value.decode(errors="replace"))
+    return _take_netbuf(h)
+
+
+def read_bench(path: str, branches: bool = False) -> Netlist:
+    """ISCAS .bench netlist, levelized, flip-flops cut for full scan (pdf_read_bench)."""
+    return _read_netlist(lib().pdf_read_bench, os.fsencode(path), BENCH_BRANCHES if branches else 0)
+
+
+def read_level(path: str) -> Netlist:
+    """Levelized text netlist (pdf_read_level)."""
+    return _read_netlist(lib().pdf_read_level, os.fsencode(path))
+
+
+def write_bench(nl: Netlist, path: str) -> None:
+    check(lib().pdf_write_bench(C.byref(nl.view()), os.fsencode(path)), "pdf_write_bench")
+
+
+def write_level(nl: Netlist, path: str) -> None:
+    check(lib().pdf_write_level(C.byref(nl.view()), os.fsencode(path)), "pdf_write_level")
+
+
+def read_vectors(path: str) -> np.ndarray:
+    """A vector file as vec[n_pi][n_vec] of 0/1 bytes (pdf_vectors_dim + pdf_vectors_read)."""
+    n, w = C.c_uint64(), C.c_uint32()
+    check(lib().pdf_vectors_dim(os.fsencode(path), C.byref(n), C.byref(w)), "pdf_vectors_dim")
+    vec = np.zeros((w.value, n.value), np.uint8)
+    check(lib().pdf_vectors_read(os.fsencode(path), w.value, n.value, vec.ctypes.data), "pdf_vectors_read")
+    return vec
+
+
+def dump_sim(path: str, sim_v: np.ndarray, sim_t: np.ndarray, n_pairs: int, pair_base: int = 0,
+             append: bool = False) -> None:
+    """gpusim-p2.log layout from host planes [n_gates][ld] (pdf_dump_sim)."""
+    sim_v = np.ascontiguousarray(sim_v, np.uint32)
+    sim_t = np.ascontiguousarray(sim_t, np.uint32)
+    check(lib().pdf_dump_sim(os.fsencode(path), sim_v.ctypes.data, sim_t.ctypes.data, sim_v.shape[0], n_pairs,
+                             sim_v.shape[1], pair_base, int(append)), "pdf_dump_sim")
+
+
+def dump_mark(path: str, mark: np.ndarray, n_pairs: int, pair_base: int = 0, append: bool = False) -> None:
+    """gpumark.log layout from a host plane [n_gates][ld] (pdf_dump_mark)."""
+    mark = np.ascontiguousarray(mark, np.uint32)
+    check(lib().pdf_dump_mark(os.fsencode(path), mark.ctypes.data, mark.shape[0], n_pairs, mark.shape[1],
+                              pair_base, int(append)), "pdf_dump_mark")
+
+
+def dump_merge(path: str, first_x: np.ndarray, first_y: np.ndarray) -> None:
+    """gpumerge.log layout (pdf_dump_merge)."""
+    fx = np.ascontiguousarray(first_x, np.uint32)
+    fy = np.ascontiguousarray(first_y, np.uint32)
+    check(lib().pdf_dump_merge(os.fsencode(path), fx.ctypes.data, fy.ctypes.data, len(fx)), "pdf_dump_merge")
 
 
 def words(n_pairs: int) -> int:
@@ -625,6 +703,12 @@ def stage_sim(c: Circuit, v, t, n_pairs, sim_v, sim_t, stream: int = 0):
 def stage_mark(c: Circuit, sim_v, sim_t, mark, n_pairs, stream: int = 0):
     check(lib().pdf_mark(c.h, _addr(sim_v), _addr(sim_t), _addr(mark), n_pairs, mark.shape[1],
                          C.c_void_p(stream)), "pdf_mark")
+
+
+def stage_mark_forward(c: Circuit, sim_v, sim_t, mark, n_pairs, stream: int = 0):
+    """Forward marks before the removal pass (pdf_mark_forward)."""
+    check(lib().pdf_mark_forward(c.h, _addr(sim_v), _addr(sim_t), _addr(mark), n_pairs, mark.shape[1],
+                                 C.c_void_p(stream)), "pdf_mark_forward")
 
 
 def stage_merge(c: Circuit, s: State, sim_v, mark, n_pairs, pair_base, stream: int = 0):

@@ -1016,8 +1016,10 @@ extern "C" pdf_status pdf_sim(pdf_circuit *c, const pdf_pairs *pr, uint32_t *sim
     return PDF_OK;
 }
 
-extern "C" pdf_status pdf_mark(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t,
-                               uint32_t *mark, uint64_t n_pairs, uint64_t ld, void *stream) {
+namespace {
+
+pdf_status mark_planes(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t, uint32_t *mark,
+                       uint64_t n_pairs, uint64_t ld, void *stream, bool prune) {
     if (!c || !sim_v || !sim_t || !mark || n_pairs == 0 || ld < (n_pairs + 31) / 32) return PDF_EINVAL;
     DeviceGuard dg(c->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
@@ -1042,11 +1044,24 @@ extern "C" pdf_status pdf_mark(pdf_circuit *c, const uint32_t *sim_v, const uint
     }
     a.nzb = c->stage.nzb.as<uint32_t>();
     a.blk_maxlvl = c->stage.maxlvl.as<uint32_t>();
+    a.no_prune = prune ? 0u : 1u;
     PDF_CUDA(launch_forward(a, FWD_MARK, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
     if (!direct)
         PDF_CUDA(cudaMemcpy2DAsync(mark, ld * 4, a.M, a.ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));
     return PDF_OK;
+}
+
+}  // namespace
+
+extern "C" pdf_status pdf_mark(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t,
+                               uint32_t *mark, uint64_t n_pairs, uint64_t ld, void *stream) {
+    return mark_planes(c, sim_v, sim_t, mark, n_pairs, ld, stream, true);
+}
+
+extern "C" pdf_status pdf_mark_forward(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t,
+                                       uint32_t *mark, uint64_t n_pairs, uint64_t ld, void *stream) {
+    return mark_planes(c, sim_v, sim_t, mark, n_pairs, ld, stream, false);
 }
 
 extern "C" pdf_status pdf_merge(pdf_circuit *c, pdf_state *s, const uint32_t *sim_v, const uint32_t *mark,

@@ -602,6 +602,7 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
         }
     }
     if constexpr (MODE != FWD_SIM) {
+        if (MODE == FWD_MARK && a.no_prune) return;
         __syncthreads();
         prune_and_merge<BW, MODE>(a, S, blk, gbm, phase);
     }

@@ -47,6 +47,7 @@ struct FwdArgs {
     uint64_t ld;
     uint32_t store_all;           // 1: write every plane row; 0: only the rows read back later
                                   // (RF_SPILL gates, gates with a forward mark)
+    uint32_t no_prune;            // FWD_MARK: stop after the forward marks (no removal pass)
     uint32_t *nzb;                // [n_blocks][bm_words] gates with a nonzero mark
     uint32_t *blk_maxlvl;         // [n_blocks] highest level holding a mark (+1), 0 = none
     uint32_t bm_words;

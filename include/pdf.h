@@ -250,6 +250,10 @@ pdf_status pdf_sim(pdf_circuit *c, const pdf_pairs *pairs, uint32_t *sim_v,
  * marks that reach no primary output. */
 pdf_status pdf_mark(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t,
                     uint32_t *mark, uint64_t n_pairs, uint64_t ld, void *stream);
+/* The forward marks alone, before the removal pass: the first level loop of
+ * gpuMarkPaths (markkernel.cuh:297-322), dumped as gpumark-full.log (:323-324). */
+pdf_status pdf_mark_forward(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *sim_t,
+                            uint32_t *mark, uint64_t n_pairs, uint64_t ld, void *stream);
 /* gpuMergeSegments<1> (mergekernel.cuh:200-267): fold the first marking pair
  * of every net (split by transition direction) into the state. */
 pdf_status pdf_merge(pdf_circuit *c, pdf_state *s, const uint32_t *sim_v,
@@ -433,6 +437,53 @@ pdf_status pdf_gen_pairs(uint64_t seed, uint32_t n_pi, uint64_t n_pairs, uint64_
  * to vector 0.  vec is n_pi rows of n_vec bytes (0/1).  Produces n_vec pairs. */
 pdf_status pdf_pairs_from_vectors(const uint8_t *vec, uint32_t n_pi, uint64_t n_vec,
                                   uint64_t ld, uint32_t *v, uint32_t *t);
+
+/* ---- netlist and vector files, debug dumps (the fcount command line) ---- */
+
+/*
+ * The reference reads circuits and vectors through its util/ submodule
+ * (Circuit::read_bench, Circuit::load, get_vector_dim, read_vectors;
+ * main.cu:128-156), which the reference snapshot does not contain; these
+ * formats are this library's own.
+ *
+ * ISCAS .bench: INPUT(n), OUTPUT(n), n = TYPE(a, b, ...) with TYPE one of
+ * AND NAND OR NOR XOR XNOR NOT BUF BUFF FROM DFF, '#' comments.  Flip-flops are
+ * cut for full scan: the output of q = DFF(d) becomes a primary input (after
+ * the declared inputs) and d a primary output.  Gates are levelized (level =
+ * longest distance from an input) and numbered by level, then file order.
+ * PDF_BENCH_BRANCHES inserts a FROM gate on every fan-out branch of a net
+ * read more than once.  On error, msg (if given) names the file and line.
+ */
+#define PDF_BENCH_BRANCHES 0x1u
+pdf_status pdf_read_bench(const char *path, uint32_t flags, pdf_netbuf **out, char *msg, size_t msg_len);
+/* Writes gates as g<id>; reading it back gives the same netlist when its
+ * levels are longest-path levels, it has no DFF gates and fan-outs are listed
+ * in consumer order. */
+pdf_status pdf_write_bench(const pdf_netlist *nl, const char *path);
+/* Levelized text: a line "pdf-level 1", a line "n_gates n_levels", then one
+ * line per gate in id order: "id level TYPE po nfi fan-ins... nfo fan-outs...".
+ * Round-trips every field of a pdf_netlist. */
+pdf_status pdf_read_level(const char *path, pdf_netbuf **out, char *msg, size_t msg_len);
+pdf_status pdf_write_level(const pdf_netlist *nl, const char *path);
+/* Vector files: one vector per line, one '0'/'1' per primary input
+ * (whitespace ignored, '#' comments).  pdf_vectors_dim returns the vector
+ * count and width (get_vector_dim); pdf_vectors_read fills vec[n_pi][n_vec]
+ * (the layout pdf_pairs_from_vectors takes) and fails unless the file holds
+ * exactly n_vec vectors of n_pi bits. */
+pdf_status pdf_vectors_dim(const char *path, uint64_t *n_vec, uint32_t *width);
+pdf_status pdf_vectors_read(const char *path, uint32_t n_pi, uint64_t n_vec, uint8_t *vec);
+/* Text dumps of host planes in the reference's debug-log layouts: a header of
+ * gate ids then one line per pair, "Vector <pair_base + p>:" and a code per
+ * gate (S0/S1/T0/T1; debugSimulationOutput, simkernel.cuh:250-295) or a mark
+ * (Y/N; debugMarkOutput, markkernel.cuh:357-394).  append != 0 adds lines to
+ * an existing file without the header (later chunks).  pdf_dump_merge writes
+ * "Gate <g>: x,y" per net with ids as signed 32-bit, -1 = none
+ * (debugMergeOutput, mergekernel.cuh:269-284). */
+pdf_status pdf_dump_sim(const char *path, const uint32_t *sim_v, const uint32_t *sim_t, uint32_t n_gates,
+                        uint64_t n_pairs, uint64_t ld, uint64_t pair_base, int append);
+pdf_status pdf_dump_mark(const char *path, const uint32_t *mark, uint32_t n_gates, uint64_t n_pairs,
+                         uint64_t ld, uint64_t pair_base, int append);
+pdf_status pdf_dump_merge(const char *path, const uint32_t *first_x, const uint32_t *first_y, uint32_t n_gates);
 
 #ifdef __cplusplus
 }
