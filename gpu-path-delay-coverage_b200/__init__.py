@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(_HERE, "libpdf_b200.so")
 # gate codes (pdf.h)
 UNKN, INPT, AND, NAND, OR, NOR, XOR, XNOR, BUFF, NOT, FROM, DFF = range(12)
 S0, S1, T0, T1 = range(4)
-MARK_DEFAULT, MARK_ROBUST = 0, 1
+MARK_DEFAULT, MARK_ROBUST, MARK_FIXED_ROBUST, MARK_FIXED_NONROBUST = 0, 1, 2, 3
 FLAG_OVERFLOW = 1
 BATCH_APPEND, BATCH_NO_GRAPH = 1, 2
 BENCH_BRANCHES = 1

@@ -1,7 +1,7 @@
 // fcount.cpp -- command line with the reference's flags and output line
 // (main.cu:24-235), on the C ABI of libpdf_b200.
 //
-//   fcount --bench CIRCUIT [--robust] [--segs 1] [--num_patterns N]
+//   fcount --bench CIRCUIT [--robust] [--fixed] [--segs 1] [--num_patterns N]
 //          [--verbose [--sim] [--mark] [--merge]] [--branches] [--device D]
 //          VECTORS...
 //
@@ -35,7 +35,7 @@
 namespace {
 
 int verbose_flag = 0, sim_flag = 0, mark_flag = 0, merge_flag = 0, cover_flag = 0, robust_flag = 0,
-    branches_flag = 0;
+    branches_flag = 0, fixed_flag = 0;
 
 [[noreturn]] void die(const std::string &what) {
     std::cerr << "fcount: " << what << std::endl;
@@ -71,6 +71,8 @@ void usage(const char *argv0) {
     std::printf("\t--verbose with --sim / --mark / --merge : write gpusim-p2.log / gpumark-full.log and\n"
                 "\t                       gpumark.log / gpumerge.log\n");
     std::printf("\t--branches : .bench only, a FROM gate on every fan-out branch\n");
+    std::printf("\t--fixed : true n-input gates and textbook side conditions (non-robust; robust\n"
+                "\t          with --robust) instead of the reference's semantics\n");
     std::printf("\t--device N : CUDA device\n");
 }
 
@@ -96,6 +98,7 @@ int main(int argc, char *argv[]) {
                                            {"robust", no_argument, &robust_flag, 1},
                                            {"brief", no_argument, &verbose_flag, 0},
                                            {"branches", no_argument, &branches_flag, 1},
+                                           {"fixed", no_argument, &fixed_flag, 1},
                                            {"help", no_argument, nullptr, 'h'},
                                            {"bench", required_argument, nullptr, 'b'},
                                            {"num_patterns", required_argument, nullptr, 'o'},
@@ -151,7 +154,8 @@ int main(int argc, char *argv[]) {
 
     pdf_circuit_opts co{};
     co.device = device;
-    co.mark_mode = robust_flag ? PDF_MARK_ROBUST : PDF_MARK_DEFAULT;
+    co.mark_mode = fixed_flag ? (robust_flag ? PDF_MARK_FIXED_ROBUST : PDF_MARK_FIXED_NONROBUST)
+                              : (robust_flag ? PDF_MARK_ROBUST : PDF_MARK_DEFAULT);
     pdf_circuit *ckt = nullptr;
     check(pdf_circuit_create(&nl, &co, &ckt), "pdf_circuit_create");
     const bool dumps = verbose_flag && (sim_flag || mark_flag || merge_flag);

@@ -270,7 +270,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     if (st != PDF_OK) return st;
     pdf_circuit_opts o{};
     if (opts) o = *opts;
-    if (o.mark_mode != PDF_MARK_DEFAULT && o.mark_mode != PDF_MARK_ROBUST) return PDF_EINVAL;
+    if (o.mark_mode < PDF_MARK_DEFAULT || o.mark_mode > PDF_MARK_FIXED_NONROBUST) return PDF_EINVAL;
     if (o.tile_words && o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8)
         return PDF_EINVAL;
     if (o.threads && (o.threads < 64 || o.threads > 1024 || o.threads % 32)) return PDF_EINVAL;
@@ -322,7 +322,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     for (uint32_t g = 0; g < G; g++) {
         GateRec &r = recs[g];
         std::memset(&r, 0, sizeof r);
-        r.w[0] = make_rec_header(nl->type[g], nl->po[g], nl->nfi[g]);
+        r.w[0] = make_rec_header(nl->type[g], nl->po[g], nl->nfi[g], o.mark_mode >= PDF_MARK_FIXED_ROBUST);
         r.w[1] = nl->nfo[g];
         r.w[2] = (uint32_t)eoff[g];  // w[3..6]: source words, set with the launch plan below
         r.w[7] = nl->nfi[g] ? edges[eoff[g]] : 0;
@@ -1230,7 +1230,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     BatchLaunch &L = b->L;
     L = BatchLaunch{};
     L.bw = c0->bw;
-    L.robust = c0->mark_mode == PDF_MARK_ROBUST ? 1u : 0u;
+    L.sem = (uint32_t)c0->mark_mode;
     L.hash_cap = c0->hash_cap;
     for (uint32_t i = 0; i < n_jobs; i++) {
         const pdf_batch_job &j = jobs[i];

@@ -24,7 +24,7 @@
 typedef unsigned __int128 pdf_u128;
 
 // Gate record, 32 bytes, one per gate, built at circuit upload.
-//   w[0] = type | po << 4 | nfi << 8 | RF_* flags (bits 16..22) | nfold << 24
+//   w[0] = type | po << 4 | RF_* flags (bits 5..7, 16..23) | nfi << 8 | nfold << 24
 //   w[1] = nfo
 //   w[2] = edge offset: fan-ins at edges[w2 + j], fan-outs at edges[w2 + nfi + k]
 //   w[3..6] = where the forward kernel reads fan-ins 0..3 (source words):
@@ -53,6 +53,10 @@ enum : uint32_t {
     RF_MARKF0 = 1u << 21,  // mark = transition & mark of fan-in 0
     RF_INPT = 1u << 22,    // primary input: mark = transition
     RF_SPILL = 1u << 23,   // a later gate reads this gate's plane rows from global memory
+    // true n-input semantics (PDF_MARK_FIXED_*)
+    RF_XOR = 1u << 5,      // fold steps are XOR (XOR, XNOR)
+    RF_OINV = 1u << 6,     // the folded value is inverted under both vectors (NAND, NOR, XNOR)
+    RF_MANY = 1u << 7,     // mark = transition & OR over fan-ins i of (mark(i) & side test for i)
 };
 
 PDF_HD uint32_t rec_type(const GateRec &r) { return r.w[0] & 0xFu; }
@@ -60,12 +64,19 @@ PDF_HD uint32_t rec_po(const GateRec &r) { return (r.w[0] >> 4) & 1u; }
 PDF_HD uint32_t rec_nfi(const GateRec &r) { return (r.w[0] >> 8) & 0xFFu; }
 PDF_HD uint32_t hdr_nfold(uint32_t h) { return h >> 24; }
 
-// Header word of a gate (w[0]).
-PDF_HD uint32_t make_rec_header(uint32_t type, uint32_t po, uint32_t nfi) {
+// Header word of a gate (w[0]); `fixed` selects the true n-input semantics
+// for AND..XNOR (every other type is evaluated as in the reference).
+PDF_HD uint32_t make_rec_header(uint32_t type, uint32_t po, uint32_t nfi, bool fixed = false) {
     uint32_t f = 0, nfold = 0;
     const bool two_input = type >= PDF_AND && type <= PDF_XNOR;
     const bool copy = type == PDF_BUFF || type == PDF_FROM || type == PDF_DFF;
-    if (type == PDF_INPT) {
+    if (fixed && two_input) {
+        if (type == PDF_OR || type == PDF_NOR) f |= RF_IM;
+        if (type == PDF_XOR || type == PDF_XNOR) f |= RF_XOR;
+        if (type == PDF_NAND || type == PDF_NOR || type == PDF_XNOR) f |= RF_OINV;
+        f |= nfi >= 2 ? (RF_SENS | RF_MANY) : RF_MARKF0;
+        nfold = nfi - 1;
+    } else if (type == PDF_INPT) {
         f |= RF_INPT;
     } else if (copy) {
         f |= RF_MARKF0;  // :126-130 copy fan-in 0; mark follows fan-in 0 (:242-246)
@@ -95,15 +106,26 @@ PDF_HD void eval_first(uint32_t h, uint32_t fV, uint32_t fT, uint32_t &V, uint32
     V = fV ^ n;
     v1 = fV ^ fT ^ n;
 }
+// FIX: the true n-input semantics, where a fold step may also be XOR and the
+// result is inverted once at the end (RF_OINV) instead of per step.
+template <bool FIX = false>
 PDF_HD void eval_fold(uint32_t h, uint32_t &V, uint32_t &v1, uint32_t rV, uint32_t rT) {
     const uint32_t im = flagmask(h, RF_IM), x = im ^ flagmask(h, RF_OM);
-    V = ((V ^ im) & (rV ^ im)) ^ x;
-    v1 = ((v1 ^ im) & (rV ^ rT ^ im)) ^ x;
+    if (FIX) {
+        const uint32_t xm = flagmask(h, RF_XOR);
+        V = (xm & (V ^ rV)) | (~xm & (((V ^ im) & (rV ^ im)) ^ x));
+        v1 = (xm & (v1 ^ rV ^ rT)) | (~xm & (((v1 ^ im) & (rV ^ rT ^ im)) ^ x));
+    } else {
+        V = ((V ^ im) & (rV ^ im)) ^ x;
+        v1 = ((v1 ^ im) & (rV ^ rT ^ im)) ^ x;
+    }
 }
+template <bool FIX = false>
 PDF_HD void eval_finish(uint32_t h, uint32_t &V, uint32_t v1, uint32_t &T) {
     const uint32_t keep = ~flagmask(h, RF_KILL);
     T = (V ^ v1) & keep;
     V &= keep;
+    if (FIX) V ^= flagmask(h, RF_OINV);  // inverting both vectors keeps the transition flag
 }
 
 // Two-input fold step val = OP2(val, r) on bit-planes (simkernel.cuh:146 via
@@ -210,6 +232,24 @@ PDF_HD uint32_t sens_result(const SensAcc &s) {
     uint32_t r = (s.z0[0] & s.a[0]) | (s.z1[0] & s.an[0]);
     if (!ROBUST) r |= (s.z0[1] & s.a[1]) | (s.z1[1] & s.an[1]);
     return r;
+}
+
+// The FIXED tables factor the same way, per gate class (and: AND/NAND, or:
+// OR/NOR, xor: XOR/XNOR; masks all-ones for the gate's class, else zero):
+//   robust     A1 = T & ~V (~V dropped for xor),  B1 = and: V,  or: ~V & ~T,  xor: ~T
+//              A2 = T & V (none for xor),         B2 = and: V & ~T,  or: ~V
+//   nonrobust  A1 = T,  B1 = and: V,  or: ~V,  xor: all
+// and the candidate must carry a mark itself: Ak is ANDed with the fan-in's
+// mark M, which makes the result OR_i (M(i) & AND_{x != i} sens(i, x)).
+template <int NONROBUST>
+PDF_HD void sens_step_fixed(SensAcc &s, uint32_t mand, uint32_t mor, uint32_t mxor, uint32_t V, uint32_t T,
+                            uint32_t M) {
+    if (NONROBUST) {
+        sens_term(s, 0, T & M, (V & mand) | (~V & mor) | mxor);
+    } else {
+        sens_term(s, 0, T & M & (mxor | ~V), (V & mand) | (~V & ~T & mor) | (~T & mxor));
+        sens_term(s, 1, T & V & M & ~mxor, (V & ~T & mand) | (~V & mor) | mxor);
+    }
 }
 
 // A run of gates of one level, the unit of staging and of synchronisation.

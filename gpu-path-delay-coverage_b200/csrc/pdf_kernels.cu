@@ -246,6 +246,30 @@ __device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, uint32_t nfi, Fetc
     return out;
 }
 
+// The FIXED modes' test (sens_step_fixed): OR over fan-ins i carrying a mark
+// of AND over the other fan-ins of the side table; fetch also gives marks.
+template <int BW, int NONROBUST, class Fetch3>
+__device__ __forceinline__ Vec<BW> sens_any_fixed(const GateRec &r, uint32_t nfi, Fetch3 fetch) {
+    const uint32_t mor = flagmask(r.w[0], RF_IM), mxor = flagmask(r.w[0], RF_XOR), mand = ~(mor | mxor);
+    SensAcc acc[BW];
+#pragma unroll
+    for (int j = 0; j < BW; j++) sens_init(acc[j]);
+    auto step = [&](uint32_t q) {
+        Vec<BW> v, t, m;
+        fetch(q, v, t, m);
+#pragma unroll
+        for (int j = 0; j < BW; j++) sens_step_fixed<NONROBUST>(acc[j], mand, mor, mxor, v.x[j], t.x[j], m.x[j]);
+    };
+#pragma unroll
+    for (int q = 0; q < kInlineFanins; q++)
+        if ((uint32_t)q < nfi) step(q);
+    for (uint32_t q = kInlineFanins; q < nfi; q++) step(q);
+    Vec<BW> out;
+#pragma unroll
+    for (int j = 0; j < BW; j++) out.x[j] = sens_result<NONROBUST>(acc[j]);
+    return out;
+}
+
 // Reverse pass (prune, markkernel.cuh:271-293) and first-detect merge
 // (mergekernel.cuh:116-198) of k_forward, after its forward pass: only
 // pieces that hold a forward mark, descending, only gates whose bitmap bit is
@@ -399,8 +423,11 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
 // past ceil(n_pairs / 32) are masked to zero.
 // ---------------------------------------------------------------------------
 // One CTA's work: column block `blk` of the circuit in `a`.
-template <int BW, int ROBUST, int MODE>
+// SEM: the circuit's PDF_MARK_* mode (0, 1: the reference's tables; 2, 3:
+// true n-input gates with the FIXED tables).
+template <int BW, int SEM, int MODE>
 __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk) {
+    constexpr bool FIX = SEM >= 2;
     extern __shared__ __align__(128) unsigned char smraw[];
     FwdSmem S;
     S.ring = reinterpret_cast<uint32_t *>(smraw + a.off_ring);
@@ -533,14 +560,14 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
                     const uint32_t sq = srcw(q);
                     const Vec<BW> fv = load(sq, 0), ft = load(sq, 1);
 #pragma unroll
-                    for (int j = 0; j < BW; j++) eval_fold(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
+                    for (int j = 0; j < BW; j++) eval_fold<FIX>(h, V.x[j], v1.x[j], fv.x[j], ft.x[j]);
                 };
 #pragma unroll
                 for (int q = 1; q < kInlineFanins; q++)
                     if ((uint32_t)q <= nfold) fold(q);
                 for (uint32_t q = kInlineFanins; q <= nfold; q++) fold(q);
 #pragma unroll
-                for (int j = 0; j < BW; j++) eval_finish(h, V.x[j], v1.x[j], T.x[j]);
+                for (int j = 0; j < BW; j++) eval_finish<FIX>(h, V.x[j], v1.x[j], T.x[j]);
                 if (tail) {
 #pragma unroll
                     for (int j = 0; j < BW; j++) {
@@ -565,10 +592,21 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
                             fv = load(sq, 0);
                             ft = load(sq, 1);
                         };
-                        const Vec<BW> sv = sens_any<BW, ROBUST>(r, rec_nfi(r), fetch);
+                        const Vec<BW> sv = sens_any<BW, SEM & 1>(r, rec_nfi(r), fetch);
 #pragma unroll
                         for (int j = 0; j < BW; j++) M.x[j] &= sv.x[j];
                     }
+                } else if (FIX && (h & RF_MANY) && vany(T)) {
+                    // any fan-in may carry the path: its own mark enters the side test
+                    auto fetch3 = [&](uint32_t q, Vec<BW> &fv, Vec<BW> &ft, Vec<BW> &fm) {
+                        const uint32_t sq = srcw(q);
+                        fv = load(sq, 0);
+                        ft = load(sq, 1);
+                        fm = load(sq, 2);
+                    };
+                    const Vec<BW> sv = sens_any_fixed<BW, SEM == PDF_MARK_FIXED_NONROBUST>(r, rec_nfi(r), fetch3);
+#pragma unroll
+                    for (int j = 0; j < BW; j++) M.x[j] = T.x[j] & sv.x[j];
                 }
             }
             const bool marked = MODE != FWD_SIM && vany(M);
@@ -608,9 +646,9 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
     }
 }
 
-template <int BW, int ROBUST, int MODE>
+template <int BW, int SEM, int MODE>
 __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs a) {
-    forward_cta<BW, ROBUST, MODE>(a, blockIdx.x);
+    forward_cta<BW, SEM, MODE>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -965,7 +1003,7 @@ __device__ __forceinline__ uint32_t prefix_find(const uint32_t *pref, uint32_t n
     return lo;
 }
 
-template <int BW, int ROBUST>
+template <int BW, int SEM>
 __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
     k_batch_forward(const FwdArgs *args, const uint32_t *bpref, uint32_t n, BatchCtl *ctl) {
     __shared__ FwdArgs s_a;
@@ -981,7 +1019,7 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
         }
     }
     __syncthreads();
-    forward_cta<BW, ROBUST, FWD_FUSED>(s_a, s_blk);
+    forward_cta<BW, SEM, FWD_FUSED>(s_a, s_blk);
 }
 
 __global__ void k_batch_active(const CoverArgs *args, const uint32_t *gpref, uint32_t n, uint2 *items,
@@ -1084,9 +1122,9 @@ __global__ void k_batch_begin(DevAcc *acc) {
     acc->done = 0;
 }
 
-template <int BW, int ROBUST, int MODE>
+template <int BW, int SEM, int MODE>
 cudaError_t launch_fwd_t(const FwdArgs &a, uint32_t threads, size_t smem, cudaStream_t st) {
-    auto kern = k_forward<BW, ROBUST, MODE>;
+    auto kern = k_forward<BW, SEM, MODE>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const uint32_t blocks = (a.W + BW - 1) / BW;
@@ -1095,33 +1133,36 @@ cudaError_t launch_fwd_t(const FwdArgs &a, uint32_t threads, size_t smem, cudaSt
     return cudaGetLastError();
 }
 
-template <int BW>
-cudaError_t launch_fwd_bw(const FwdArgs &a, int mode, int robust, uint32_t threads, size_t smem,
-                          cudaStream_t st) {
-    if (robust) {
-        switch (mode) {
-            case FWD_FUSED: return launch_fwd_t<BW, 1, FWD_FUSED>(a, threads, smem, st);
-            case FWD_SIM: return launch_fwd_t<BW, 1, FWD_SIM>(a, threads, smem, st);
-            default: return launch_fwd_t<BW, 1, FWD_MARK>(a, threads, smem, st);
-        }
-    }
+template <int BW, int SEM>
+cudaError_t launch_fwd_sem(const FwdArgs &a, int mode, uint32_t threads, size_t smem, cudaStream_t st) {
     switch (mode) {
-        case FWD_FUSED: return launch_fwd_t<BW, 0, FWD_FUSED>(a, threads, smem, st);
-        case FWD_SIM: return launch_fwd_t<BW, 0, FWD_SIM>(a, threads, smem, st);
-        default: return launch_fwd_t<BW, 0, FWD_MARK>(a, threads, smem, st);
+        case FWD_FUSED: return launch_fwd_t<BW, SEM, FWD_FUSED>(a, threads, smem, st);
+        case FWD_SIM: return launch_fwd_t<BW, SEM, FWD_SIM>(a, threads, smem, st);
+        default: return launch_fwd_t<BW, SEM, FWD_MARK>(a, threads, smem, st);
+    }
+}
+
+template <int BW>
+cudaError_t launch_fwd_bw(const FwdArgs &a, int mode, int sem, uint32_t threads, size_t smem, cudaStream_t st) {
+    switch (sem) {
+        case 0: return launch_fwd_sem<BW, 0>(a, mode, threads, smem, st);
+        case 1: return launch_fwd_sem<BW, 1>(a, mode, threads, smem, st);
+        case 2: return launch_fwd_sem<BW, 2>(a, mode, threads, smem, st);
+        case 3: return launch_fwd_sem<BW, 3>(a, mode, threads, smem, st);
+        default: return cudaErrorInvalidValue;
     }
 }
 
 }  // namespace
 
 
-cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
+cudaError_t launch_forward(const FwdArgs &a, int mode, int sem, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st) {
     switch (bw) {
-        case 1: return launch_fwd_bw<1>(a, mode, robust, threads, smem, st);
-        case 2: return launch_fwd_bw<2>(a, mode, robust, threads, smem, st);
-        case 4: return launch_fwd_bw<4>(a, mode, robust, threads, smem, st);
-        case 8: return launch_fwd_bw<8>(a, mode, robust, threads, smem, st);
+        case 1: return launch_fwd_bw<1>(a, mode, sem, threads, smem, st);
+        case 2: return launch_fwd_bw<2>(a, mode, sem, threads, smem, st);
+        case 4: return launch_fwd_bw<4>(a, mode, sem, threads, smem, st);
+        case 8: return launch_fwd_bw<8>(a, mode, sem, threads, smem, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1142,18 +1183,18 @@ cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bo
     return cudaGetLastError();
 }
 
-template <int BW, int ROBUST>
+template <int BW, int SEM>
 cudaError_t prepare_batch_t(const BatchLaunch &b) {
-    cudaError_t e = cudaFuncSetAttribute(k_batch_forward<BW, ROBUST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_batch_forward<BW, SEM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)b.fwd_smem);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_batch_cover, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)cover_smem_bytes(b.hash_cap));
 }
 
-template <int BW, int ROBUST>
+template <int BW, int SEM>
 cudaError_t launch_batch_t(const BatchLaunch &b, cudaStream_t st) {
-    k_batch_forward<BW, ROBUST><<<b.total_blocks, b.threads, b.fwd_smem, st>>>(b.fargs, b.bpref, b.n, b.ctl);
+    k_batch_forward<BW, SEM><<<b.total_blocks, b.threads, b.fwd_smem, st>>>(b.fargs, b.bpref, b.n, b.ctl);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_batch_active<<<(b.total_gates + 255) / 256, 256, 0, st>>>(b.cargs, b.gpref, b.n, b.items, b.ctl);
@@ -1163,32 +1204,31 @@ cudaError_t launch_batch_t(const BatchLaunch &b, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t prepare_batch(const BatchLaunch &b) {
-    switch (b.bw * 2 + (b.robust ? 1 : 0)) {
-        case 2: return prepare_batch_t<1, 0>(b);
-        case 3: return prepare_batch_t<1, 1>(b);
-        case 4: return prepare_batch_t<2, 0>(b);
-        case 5: return prepare_batch_t<2, 1>(b);
-        case 8: return prepare_batch_t<4, 0>(b);
-        case 9: return prepare_batch_t<4, 1>(b);
-        case 16: return prepare_batch_t<8, 0>(b);
-        case 17: return prepare_batch_t<8, 1>(b);
+// (tile words, semantics) -> the instantiation; `prep` selects prepare or launch
+template <int BW>
+cudaError_t batch_bw(const BatchLaunch &b, cudaStream_t st, bool prep) {
+    switch (b.sem) {
+        case 0: return prep ? prepare_batch_t<BW, 0>(b) : launch_batch_t<BW, 0>(b, st);
+        case 1: return prep ? prepare_batch_t<BW, 1>(b) : launch_batch_t<BW, 1>(b, st);
+        case 2: return prep ? prepare_batch_t<BW, 2>(b) : launch_batch_t<BW, 2>(b, st);
+        case 3: return prep ? prepare_batch_t<BW, 3>(b) : launch_batch_t<BW, 3>(b, st);
         default: return cudaErrorInvalidValue;
     }
 }
-cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
-    if (!b.n || !b.total_blocks) return cudaErrorInvalidValue;
-    switch (b.bw * 2 + (b.robust ? 1 : 0)) {
-        case 2: return launch_batch_t<1, 0>(b, st);
-        case 3: return launch_batch_t<1, 1>(b, st);
-        case 4: return launch_batch_t<2, 0>(b, st);
-        case 5: return launch_batch_t<2, 1>(b, st);
-        case 8: return launch_batch_t<4, 0>(b, st);
-        case 9: return launch_batch_t<4, 1>(b, st);
-        case 16: return launch_batch_t<8, 0>(b, st);
-        case 17: return launch_batch_t<8, 1>(b, st);
+cudaError_t batch_dispatch(const BatchLaunch &b, cudaStream_t st, bool prep) {
+    switch (b.bw) {
+        case 1: return batch_bw<1>(b, st, prep);
+        case 2: return batch_bw<2>(b, st, prep);
+        case 4: return batch_bw<4>(b, st, prep);
+        case 8: return batch_bw<8>(b, st, prep);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t prepare_batch(const BatchLaunch &b) { return batch_dispatch(b, nullptr, true); }
+cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
+    if (!b.n || !b.total_blocks) return cudaErrorInvalidValue;
+    return batch_dispatch(b, st, false);
 }
 
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M, uint64_t ld,

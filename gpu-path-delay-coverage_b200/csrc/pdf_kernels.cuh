@@ -105,14 +105,14 @@ struct BatchLaunch {
     uint2 *items;          // [sum of min(n_pairs, 2 n_gates)]
     BatchCtl *ctl;
     uint32_t n, total_blocks, total_gates;
-    uint32_t bw, robust, threads, cover_grid, hash_cap, append;
+    uint32_t bw, sem, threads, cover_grid, hash_cap, append;  // sem: PDF_MARK_*
     size_t fwd_smem;
 };
 cudaError_t prepare_batch(const BatchLaunch &b);  // kernel attributes; call before launching or capturing
 cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st);
 
 // Host-side launchers (pdf_kernels.cu).  All return cudaError_t of the launch.
-cudaError_t launch_forward(const FwdArgs &a, int mode, int robust, uint32_t bw, uint32_t threads,
+cudaError_t launch_forward(const FwdArgs &a, int mode, int sem, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st);
 // Cover of one batch: k_active then k_cover, whose last CTA closes the batch
 // (total += batch, pairs += n_pairs).  The active bitmap [W] and its count

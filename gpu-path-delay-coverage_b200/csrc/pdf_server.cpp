@@ -197,7 +197,7 @@ extern "C" pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server 
     if (!o.batch_pairs) o.batch_pairs = 4096;
     if (!o.max_jobs) o.max_jobs = 1024;
     if (o.batch_pairs % 32 || (o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8) ||
-        (o.mark_mode != PDF_MARK_DEFAULT && o.mark_mode != PDF_MARK_ROBUST))
+        o.mark_mode < PDF_MARK_DEFAULT || o.mark_mode > PDF_MARK_FIXED_NONROBUST)
         return PDF_EINVAL;
     if (cudaSetDevice(o.device) != cudaSuccess) return PDF_ENODEV;
     if (!o.hbm_budget) {

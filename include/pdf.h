@@ -137,16 +137,33 @@ typedef struct pdf_totals {
 typedef struct pdf_circuit pdf_circuit;
 typedef struct pdf_state pdf_state;
 
-/* Robust mode.  The reference reads one of two sensitisation tables
- * (markkernel.cuh:36-37, selected at :255-259 by --robust, main.cu:53). */
+/* Semantics and sensitisation table.  The reference reads one of two tables
+ * (markkernel.cuh:36-37, selected at :255-259 by --robust, main.cu:53); the
+ * first two modes reproduce it exactly, quirks included (multi-input gates
+ * as a left fold of the 2-input table, XOR/XNOR with several fan-ins S0, the
+ * mark of fan-in 0 required for every on-path candidate).
+ *
+ * The FIXED modes have no reference counterpart: AND..XNOR are true n-input
+ * functions (XOR/XNOR evaluated, NAND(a) = NOT a), and a gate is marked when
+ * its output transitions and some fan-in i carries a mark and a transition
+ * with every other fan-in passing the side-input table for (i, other):
+ *   FIXED_ROBUST     AND/NAND: on T0 -> side S1 or T1, on T1 -> side S1
+ *                    OR/NOR:   on T0 -> side S0, on T1 -> side S0 or T0
+ *                    XOR/XNOR: side S0 or S1          {0x2A00,0x2A00,0x5100,0x5100,0x3300,0x3300}
+ *   FIXED_NONROBUST  side final value non-controlling (S1/T1 for AND/NAND,
+ *                    S0/T0 for OR/NOR), any side for XOR/XNOR
+ *                                                     {0xAA00,0xAA00,0x5500,0x5500,0xFF00,0xFF00}
+ * Pruning, merge and cover are the same in every mode. */
 enum {
-    PDF_MARK_DEFAULT = 0,  /* LUT_NR: {0x2A00,0x2A00,0x5100,0x5100,0,0} (no --robust) */
-    PDF_MARK_ROBUST = 1    /* LUT_R:  {0x2200,0x2200,0x1100,0x1100,0,0} (--robust)    */
+    PDF_MARK_DEFAULT = 0,          /* LUT_NR: {0x2A00,0x2A00,0x5100,0x5100,0,0} (no --robust) */
+    PDF_MARK_ROBUST = 1,           /* LUT_R:  {0x2200,0x2200,0x1100,0x1100,0,0} (--robust)    */
+    PDF_MARK_FIXED_ROBUST = 2,     /* textbook robust, true n-input gates */
+    PDF_MARK_FIXED_NONROBUST = 3   /* textbook non-robust, true n-input gates */
 };
 
 typedef struct pdf_circuit_opts {
     int device;          /* CUDA device ordinal */
-    int mark_mode;       /* PDF_MARK_DEFAULT or PDF_MARK_ROBUST */
+    int mark_mode;       /* PDF_MARK_* */
     uint32_t max_pairs;  /* largest batch this circuit will grade (sizes scratch); 0 = 65536 */
     uint32_t tile_words; /* 0 = autotune; else words (32 pairs) per CTA column block: 1,2,4,8 */
     uint32_t threads;    /* 0 = autotune; else threads per CTA: 128..1024 */

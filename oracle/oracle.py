@@ -36,13 +36,14 @@ def lib() -> C.CDLL:
         L.pdfo_sens.restype = C.c_int
         L.pdfo_sens.argtypes = [C.c_int, C.c_int, C.c_uint8, C.c_uint8]
         L.pdfo_sim.argtypes = [P, P, C.c_uint64, P, C.c_int]
+        L.pdfo_sim_mode.argtypes = [P, P, C.c_uint64, P, C.c_int, C.c_int]
         L.pdfo_sim_vectors.argtypes = [P, P, C.c_uint64, P, C.c_int]
         L.pdfo_mark.argtypes = [P, P, C.c_uint64, C.c_int, P, C.c_int, C.c_int]
         L.pdfo_merge.argtypes = [P, P, P, C.c_uint64, C.c_uint64, P, P, C.c_int]
         L.pdfo_cover.argtypes = [P, P, C.c_uint64, C.c_uint64, P, P, P, P, P, C.c_int]
         L.pdfo_grade.argtypes = [P, P, C.c_uint64, C.c_uint64, C.c_int, C.c_uint64, P, P, P, P, P, P, P,
                                  P, C.c_int]
-        for f in ("pdfo_sim", "pdfo_sim_vectors", "pdfo_mark", "pdfo_merge", "pdfo_cover", "pdfo_grade"):
+        for f in ("pdfo_sim", "pdfo_sim_mode", "pdfo_sim_vectors", "pdfo_mark", "pdfo_merge", "pdfo_cover", "pdfo_grade"):
             getattr(L, f).restype = C.c_int
         _lib = L
     return _lib
@@ -90,10 +91,11 @@ def grade(nl, pi_codes: np.ndarray, n_pairs: int, pair_base: int = 0, mark_mode:
     return Result(fx, fy, (hi.value << 64) | lo.value, fl.value, sim, mark, chunk_totals)
 
 
-def sim(nl, pi_codes: np.ndarray, n_pairs: int, threads: int = 0) -> np.ndarray:
+def sim(nl, pi_codes: np.ndarray, n_pairs: int, threads: int = 0, mark_mode: int = 0) -> np.ndarray:
+    """Transition codes [n_gates][n_pairs]; mark_mode 2, 3 use the FIXED gate semantics."""
     out = np.zeros((nl.n_gates, n_pairs), np.uint8)
     pi = np.ascontiguousarray(pi_codes, dtype=np.uint8)
-    lib().pdfo_sim(_nl(nl), pi.ctypes.data, n_pairs, out.ctypes.data, threads)
+    lib().pdfo_sim_mode(_nl(nl), pi.ctypes.data, n_pairs, out.ctypes.data, mark_mode, threads)
     return out
 
 

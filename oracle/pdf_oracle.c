@@ -38,6 +38,11 @@ static const uint8_t LUT_NOT[4] = {1, 0, 3, 2};
 /* Sensitisation tables (markkernel.cuh:36-37), indexed by type - 2. */
 static const uint16_t SENS_NR[6] = {0x2A00, 0x2A00, 0x5100, 0x5100, 0x0000, 0x0000};
 static const uint16_t SENS_R[6] = {0x2200, 0x2200, 0x1100, 0x1100, 0x0000, 0x0000};
+/* FIXED modes (no reference counterpart), same LUT_16 layout, bit on*4+off:
+ * textbook robust (on c->nc: side steady nc; on nc->c: side final nc; XOR:
+ * side steady) and non-robust (side final nc; XOR: any side). */
+static const uint16_t SENS_FIXED_R[6] = {0x2A00, 0x2A00, 0x5100, 0x5100, 0x3300, 0x3300};
+static const uint16_t SENS_FIXED_NR[6] = {0xAA00, 0xAA00, 0x5500, 0x5500, 0xFF00, 0xFF00};
 
 /* tex2D(lut, val, r) on a 4x4 array = lut[r * 4 + val] (simkernel.cuh:51-56). */
 uint8_t pdfo_lut2(int type, uint8_t val, uint8_t r) {
@@ -62,7 +67,11 @@ uint8_t pdfo_not(uint8_t v) { return LUT_NOT[v & 3]; }
 /* LUT_16(LUT[type - 2], on, off) (markkernel.cuh:39-41,49). */
 int pdfo_sens(int mark_mode, int type, uint8_t on, uint8_t off) {
     if (type < PDF_AND || type > PDF_XNOR) return 0;
-    const uint16_t t = (mark_mode == PDF_MARK_ROBUST ? SENS_R : SENS_NR)[type - 2];
+    const uint16_t *tab = mark_mode == PDF_MARK_ROBUST          ? SENS_R
+                          : mark_mode == PDF_MARK_FIXED_ROBUST    ? SENS_FIXED_R
+                          : mark_mode == PDF_MARK_FIXED_NONROBUST ? SENS_FIXED_NR
+                                                                  : SENS_NR;
+    const uint16_t t = tab[type - 2];
     return (t >> (((on & 3) << 2) + (off & 3))) & 1;
 }
 
@@ -111,9 +120,37 @@ static void part_range(uint64_t n, int parts, int i, uint64_t *lo, uint64_t *hi)
  * INPT rows come from `pi` (already-formed pair codes).
  */
 static void sim_gate(const pdf_netlist *nl, uint32_t g, const uint8_t *pi, uint64_t n_pairs,
-                     uint8_t *sim, uint64_t p0, uint64_t p1) {
+                     uint8_t *sim, uint64_t p0, uint64_t p1, int fixed) {
     uint8_t *row = sim + (uint64_t)g * n_pairs;
     const int type = nl->type[g];
+    if (fixed && type >= PDF_AND && type <= PDF_XNOR) {
+        /* FIXED: the gate's n-input function under each vector separately */
+        const int inv = type == PDF_NAND || type == PDF_NOR || type == PDF_XNOR;
+        for (uint64_t p = p0; p < p1; p++) {
+            uint8_t v1 = 0, v2 = 0;
+            for (uint32_t j = 0; j < nl->nfi[g]; j++) {
+                const uint8_t c = sim[(uint64_t)fanin(nl, g, j) * n_pairs + p];
+                const uint8_t b2 = c & 1, b1 = (uint8_t)(b2 ^ (c >> 1));
+                if (j == 0) {
+                    v1 = b1;
+                    v2 = b2;
+                } else if (type == PDF_AND || type == PDF_NAND) {
+                    v1 &= b1;
+                    v2 &= b2;
+                } else if (type == PDF_OR || type == PDF_NOR) {
+                    v1 |= b1;
+                    v2 |= b2;
+                } else {
+                    v1 ^= b1;
+                    v2 ^= b2;
+                }
+            }
+            v1 ^= (uint8_t)inv;
+            v2 ^= (uint8_t)inv;
+            row[p] = pdfo_stable(v1, v2);
+        }
+        return;
+    }
     switch (type) {
         case PDF_INPT: /* :112-125 */
             memcpy(row + p0, pi + (uint64_t)g * n_pairs + p0, p1 - p0);
@@ -143,6 +180,12 @@ static void sim_gate(const pdf_netlist *nl, uint32_t g, const uint8_t *pi, uint6
 
 int pdfo_sim(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs, uint8_t *sim,
              int threads) {
+    return pdfo_sim_mode(nl, pi_codes, n_pairs, sim, PDF_MARK_DEFAULT, threads);
+}
+
+int pdfo_sim_mode(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs, uint8_t *sim,
+                  int mark_mode, int threads) {
+    const int fixed = mark_mode >= PDF_MARK_FIXED_ROBUST;
     const int nt = nthreads(threads);
 #pragma omp parallel num_threads(nt)
     {
@@ -154,7 +197,7 @@ int pdfo_sim(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs, u
         uint64_t p0, p1;
         part_range(n_pairs, cnt, tid, &p0, &p1);
         if (p0 < p1)
-            for (uint32_t g = 0; g < nl->n_gates; g++) sim_gate(nl, g, pi_codes, n_pairs, sim, p0, p1);
+            for (uint32_t g = 0; g < nl->n_gates; g++) sim_gate(nl, g, pi_codes, n_pairs, sim, p0, p1, fixed);
     }
     return 0;
 }
@@ -209,8 +252,10 @@ static void mark_forward_gate(const pdf_netlist *nl, uint32_t g, const uint8_t *
             case PDF_NAND:
             case PDF_AND: /* :253-261 with robust()/nonrobust() (:43-72) */
                 for (uint32_t f1 = 0; f1 < nfi; f1++) {
-                    /* oldmark is fan-in 0's mark for every candidate (:254) */
-                    const uint8_t oldmark = mark[(uint64_t)fanin(nl, g, 0) * n_pairs + p];
+                    /* oldmark is fan-in 0's mark for every candidate (:254); the
+                     * FIXED modes take the candidate's own mark */
+                    const uint32_t from = mark_mode >= PDF_MARK_FIXED_ROBUST ? f1 : 0;
+                    const uint8_t oldmark = mark[(uint64_t)fanin(nl, g, from) * n_pairs + p];
                     const uint8_t on = sim[(uint64_t)fanin(nl, g, f1) * n_pairs + p];
                     uint8_t tmp = 0xFF;
                     for (uint32_t f2 = 0; f2 < nfi; f2++) {
@@ -406,7 +451,7 @@ int pdfo_grade(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs,
         const uint64_t K = n_pairs - start < chunk ? n_pairs - start : chunk;
         for (uint32_t i = 0; i < n_pi; i++)
             memcpy(pi + (uint64_t)i * K, pi_codes + (uint64_t)i * n_pairs + start, K);
-        pdfo_sim(nl, pi, K, sim, threads);                                 /* main.cu:175 */
+        pdfo_sim_mode(nl, pi, K, sim, mark_mode, threads);                 /* main.cu:175 */
         pdfo_mark(nl, sim, K, mark_mode, mark, 1, threads);                /* main.cu:182 */
         pdfo_merge(nl, sim, mark, K, pair_base + start, first_x, first_y, threads); /* :185 */
         uint64_t clo = 0, chi = 0;

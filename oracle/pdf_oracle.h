@@ -34,6 +34,10 @@ int pdfo_sens(int mark_mode, int type, uint8_t on, uint8_t off);
 /* Stage functions over byte arrays [n_gates][n_pairs]. */
 int pdfo_sim(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs,
              uint8_t *sim, int threads);
+/* pdfo_sim with the gate semantics of mark_mode (PDF_MARK_FIXED_* evaluate
+ * AND..XNOR as true n-input functions; pdfo_sim is PDF_MARK_DEFAULT). */
+int pdfo_sim_mode(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs,
+                  uint8_t *sim, int mark_mode, int threads);
 int pdfo_sim_vectors(const pdf_netlist *nl, const uint8_t *vec, uint64_t n_vec,
                      uint8_t *sim, int threads);
 int pdfo_mark(const pdf_netlist *nl, const uint8_t *sim, uint64_t n_pairs, int mark_mode,

@@ -63,5 +63,40 @@ int main() {
                     const uint32_t r = robust ? sens_result<1>(s) : sens_result<0>(s);
                     std::printf("sensall %d %u %u %u %u\n", robust, type, nfi, cmb, (r >> 9) & 1);
                 }
+    // FIXED semantics: header-driven evaluation with true n-input gates, and
+    // the one-pass side test with per-fan-in marks, for AND..XNOR with 1..4
+    // fan-ins, every code combination and every mark pattern.
+    for (uint32_t type = PDF_AND; type <= PDF_XNOR; type++)
+        for (uint32_t nfi = 1; nfi <= 4; nfi++) {
+            const uint32_t h = make_rec_header(type, 0, nfi, true);
+            std::printf("fflags %u %u %u %u %u\n", type, nfi, (h & RF_MARKF0) ? 1 : 0, (h & RF_MANY) ? 1 : 0,
+                        (h & RF_SENS) ? 1 : 0);
+            for (uint32_t cmb = 0; cmb < (1u << (2 * nfi)); cmb++) {
+                uint32_t V, v1, T;
+                eval_first(h, (cmb & 1) << 3, ((cmb >> 1) & 1) << 3, V, v1);
+                for (uint32_t j = 1; j <= hdr_nfold(h); j++) {
+                    const uint32_t c = (cmb >> (2 * j)) & 3;
+                    eval_fold<true>(h, V, v1, (c & 1) << 3, (c >> 1) << 3);
+                }
+                eval_finish<true>(h, V, v1, T);
+                std::printf("fgate %u %u %u %u\n", type, nfi, cmb, ((V >> 3) & 1) | (((T >> 3) & 1) << 1));
+                if (nfi < 2) continue;
+                const uint32_t mor = flagmask(h, RF_IM), mxor = flagmask(h, RF_XOR), mand = ~(mor | mxor);
+                for (int nonrobust = 0; nonrobust < 2; nonrobust++)
+                    for (uint32_t marks = 0; marks < (1u << nfi); marks++) {
+                        SensAcc s;
+                        sens_init(s);
+                        for (uint32_t x = 0; x < nfi; x++) {
+                            const uint32_t c = (cmb >> (2 * x)) & 3, m = ((marks >> x) & 1) << 11;
+                            if (nonrobust)
+                                sens_step_fixed<1>(s, mand, mor, mxor, (c & 1) << 11, (c >> 1) << 11, m);
+                            else
+                                sens_step_fixed<0>(s, mand, mor, mxor, (c & 1) << 11, (c >> 1) << 11, m);
+                        }
+                        const uint32_t r = nonrobust ? sens_result<1>(s) : sens_result<0>(s);
+                        std::printf("fsens %d %u %u %u %u %u\n", nonrobust, type, nfi, cmb, marks, (r >> 11) & 1);
+                    }
+            }
+        }
     return 0;
 }

@@ -25,6 +25,26 @@ SENS = {  # mark_mode -> table indexed by type - 2
     0: [0x2A00, 0x2A00, 0x5100, 0x5100, 0, 0],
     1: [0x2200, 0x2200, 0x1100, 0x1100, 0, 0],
 }
+FIXED_MODES = (2, 3)  # true n-input gates; no reference counterpart
+
+
+def fixed_side_ok(mode: int, t: int, on: int, off: int) -> bool:
+    """FIXED side-input conditions stated from their definitions (not as tables):
+    robust: on c->nc needs side steady nc, on nc->c side final nc, XOR steady;
+    non-robust: side final value nc, XOR any.  on must transition."""
+    if on < 2:
+        return False
+    xor = t in (XOR, XNOR)
+    nc = 1 if t in (AND, NAND) else 0           # non-controlling value
+    off_final, off_steady = off & 1, off < 2
+    if mode == 3:
+        return True if xor else off_final == nc
+    if xor:
+        return off_steady
+    on_final = on & 1
+    if on_final == nc:                          # c -> nc
+        return off_steady and off_final == nc
+    return off_final == nc                      # nc -> c
 
 
 def per_vector(op, a: int, b: int) -> int:
@@ -35,13 +55,26 @@ def per_vector(op, a: int, b: int) -> int:
     return v2 | ((v1 ^ v2) << 1)
 
 
-def sim_pair(nl, pi_codes, p):
+def sim_pair(nl, pi_codes, p, mode: int = 0):
     G = nl.n_gates
     val = [0] * G
     for g in range(G):
         t = int(nl.type[g])
         fi = [int(x) for x in nl.fanins(g)]
-        if t == INPT:
+        if mode in FIXED_MODES and AND <= t <= XNOR:
+            bits = [[(val[f] & 1) ^ (val[f] >> 1) for f in fi], [val[f] & 1 for f in fi]]
+            out = []
+            for vs in bits:  # vector 1, vector 2
+                if t in (AND, NAND):
+                    o = int(all(vs))
+                elif t in (OR, NOR):
+                    o = int(any(vs))
+                else:
+                    o = sum(vs) & 1
+                out.append(o ^ (1 if t in (NAND, NOR, XNOR) else 0))
+            v1, v2 = out
+            val[g] = v2 | ((v1 ^ v2) << 1)
+        elif t == INPT:
             val[g] = int(pi_codes[g][p])
         elif t in (BUFF, FROM, DFF):
             val[g] = val[fi[0]]
@@ -67,6 +100,11 @@ def mark_pair(nl, val, mode: int, prune: bool = True):
             r = trans
         elif t in (FROM, BUFF, DFF, NOT):
             r = m[fi[0]]
+        elif AND <= t <= XNOR and mode in FIXED_MODES:
+            r = 0
+            for i in range(len(fi)):
+                ok = all(fixed_side_ok(mode, t, val[fi[i]], val[fi[j]]) for j in range(len(fi)) if j != i)
+                r |= int(ok) & m[fi[i]]
         elif AND <= t <= XNOR:
             r = 0
             for i in range(len(fi)):
@@ -93,7 +131,7 @@ def grade(nl, pi_codes, n_pairs: int, mode: int = 0, pair_base: int = 0, first_x
     fy = [0xFFFFFFFF] * G if first_y is None else list(first_y)
     vals, marks = [], []
     for p in range(n_pairs):
-        v = sim_pair(nl, pi_codes, p)
+        v = sim_pair(nl, pi_codes, p, mode)
         m = mark_pair(nl, v, mode)
         vals.append(v)
         marks.append(m)

@@ -37,7 +37,7 @@ def _jobs(mode, tile=4, seed=0):
     return jobs, want
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_batch_equals_each_job_alone(mode):
     jobs, want = _jobs(mode)
     b = P.Batch(jobs)

@@ -239,6 +239,18 @@ def test_cli_total_equals_oracle(tmp_path, robust):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("flags, mode", [(["--fixed"], 3), (["--fixed", "--robust"], 2)])
+def test_cli_fixed_modes(tmp_path, flags, mode):
+    nl = circuits.random_small(79, n_gates=1500, n_pi=50, n_po=100, depth=20)
+    level = str(tmp_path / "c.level")
+    P.write_level(nl, level)
+    vec, vpath = _vectors(tmp_path, nl.n_pi, 500, 4)
+    (m,) = _run(flags + ["--bench", level, vpath])
+    v, t = P.pairs_from_vectors(vec)
+    assert int(m.group(10)) == O.grade(nl, P.codes_from_planes(v, t, 500), 500, mark_mode=mode).total
+
+
+@pytest.mark.gpu
 def test_cli_logs_equal_oracle_planes(tmp_path):
     nl = circuits.random_small(78, n_gates=300, n_pi=16, n_po=40, depth=12)
     bench = str(tmp_path / "c.bench")

@@ -60,7 +60,7 @@ def assert_same(nl, codes, n, mode=0, chunk=0, **kw):
 SUITE = circuits.small_suite()
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 @pytest.mark.parametrize("idx", range(len(SUITE)))
 def test_suite(idx, mode):
     name, nl = SUITE[idx]
@@ -83,6 +83,16 @@ def test_launch_shapes(tile_words, threads):
     nl = circuits.random_small(4242, n_gates=400, n_pi=30, n_po=120, depth=10)
     rng = np.random.default_rng(7)
     assert_same(nl, helpers.rand_codes(rng, nl.n_pi, 2000), 2000, tile_words=tile_words, threads=threads)
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("tile_words", [1, 2, 4, 8])
+def test_fixed_modes_every_tile(tile_words, mode):
+    """True n-input gates (XOR evaluated, several fan-ins carrying marks),
+    wide fan-in and fan-ins past the ring, against the oracle's FIXED mode."""
+    nl = circuits.random_small(4343, n_gates=3000, n_pi=200, n_po=500, depth=9, fmax=6)
+    rng = np.random.default_rng(9)
+    assert_same(nl, helpers.rand_codes(rng, nl.n_pi, 1500), 1500, mode, tile_words=tile_words)
 
 
 def test_levels_wider_than_the_ring():

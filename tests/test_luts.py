@@ -143,3 +143,60 @@ def test_device_side_input_test_equals_reference(probe):
         assert got == want, (mode, t, nfi, codes)
         seen += 1
     assert seen == 2 * 4 * (16 + 64 + 256)
+
+
+# ---- FIXED semantics (no reference counterpart; stated from the definitions)
+
+
+def _fixed_gate(t, codes):
+    """True n-input function of AND..XNOR under each vector (refmodel.sim_pair)."""
+    out = []
+    for vec in (1, 2):
+        vs = [(c & 1) if vec == 2 else ((c & 1) ^ (c >> 1)) for c in codes]
+        if t in (R.AND, R.NAND):
+            o = int(all(vs))
+        elif t in (R.OR, R.NOR):
+            o = int(any(vs))
+        else:
+            o = sum(vs) & 1
+        out.append(o ^ int(t in (R.NAND, R.NOR, R.XNOR)))
+    v1, v2 = out
+    return v2 | ((v1 ^ v2) << 1)
+
+
+def test_device_fixed_gate_evaluation(probe):
+    seen = 0
+    for t, nfi, cmb, code in probe["fgate"]:
+        codes = [(cmb >> (2 * x)) & 3 for x in range(nfi)]
+        assert code == _fixed_gate(t, codes), (t, nfi, codes)
+        seen += 1
+    assert seen == 6 * (4 + 16 + 64 + 256)
+
+
+def test_device_fixed_flags(probe):
+    for t, nfi, markf0, many, sens in probe["fflags"]:
+        assert (markf0, many, sens) == ((1, 0, 0) if nfi == 1 else (0, 1, 1)), (t, nfi)
+
+
+def test_device_fixed_side_test(probe):
+    """OR over marked candidates i of AND over x != i of the FIXED side
+    condition, every code and mark combination of 2..4 fan-ins."""
+    seen = 0
+    for nonrobust, t, nfi, cmb, marks, got in probe["fsens"]:
+        mode = 3 if nonrobust else 2
+        codes = [(cmb >> (2 * x)) & 3 for x in range(nfi)]
+        want = int(any((marks >> i) & 1 and all(R.fixed_side_ok(mode, t, codes[i], codes[x])
+                                                   for x in range(nfi) if x != i)
+                       for i in range(nfi)))
+        assert got == want, (mode, t, nfi, codes, marks)
+        seen += 1
+    assert seen == 2 * 6 * (16 * 4 + 64 * 8 + 256 * 16)
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+def test_oracle_fixed_tables_equal_definitions(mode):
+    for t in range(R.AND, R.XNOR + 1):
+        for on in range(4):
+            for off in range(4):
+                assert helpers.oracle().lib().pdfo_sens(mode, t, on, off) == int(R.fixed_side_ok(mode, t, on, off)), \
+                    (mode, t, on, off)

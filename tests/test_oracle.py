@@ -28,7 +28,7 @@ def _check(nl, mode, n_pairs, seed):
     return total
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_oracle_equals_python_model(mode):
     totals = [_check(nl, mode, 40, 17 + i) for i, (_, nl) in enumerate(SUITE)]
     assert sum(totals) > 0, "suite must exercise nonzero path counts"
@@ -105,3 +105,28 @@ def test_vector_stream_pairs():
     v1 = np.roll(vec, 0, axis=1)
     v2 = np.roll(vec, -1, axis=1)
     np.testing.assert_array_equal(codes, (v2 | ((v1 ^ v2) << 1)).astype(np.uint8))
+
+
+def test_fixed_modes_evaluate_true_gates():
+    # a 3-input NAND: the reference folds NAND(NAND(a, b), c); FIXED is NOT(a & b & c)
+    nl = P.Netlist([0, 3, 4], [P.INPT] * 3 + [P.NAND], [0, 0, 0, 1], [0, 0, 0, 3], [1, 1, 1, 0],
+                   [0, 1, 2, 3], [3, 3, 3, 0, 1, 2])
+    codes = np.array([[R.S1], [R.S1], [R.S1]], np.uint8)
+    assert O.sim(nl, codes, 1, mark_mode=0)[3, 0] == R.S1  # NAND(NAND(1,1),1) = NAND(0,1) = 1
+    assert O.sim(nl, codes, 1, mark_mode=2)[3, 0] == R.S0
+    # XOR with two inputs: S0 in the reference, evaluated in FIXED
+    nl = P.Netlist([0, 2, 3], [P.INPT] * 2 + [P.XOR], [0, 0, 1], [0, 0, 2], [1, 1, 0], [0, 1, 2], [2, 2, 0, 1])
+    codes = np.array([[R.T1], [R.S0]], np.uint8)
+    assert O.sim(nl, codes, 1, mark_mode=0)[2, 0] == R.S0
+    assert O.sim(nl, codes, 1, mark_mode=3)[2, 0] == R.T1
+    assert O.grade(nl, codes, 1, mark_mode=0).total == 0
+    assert O.grade(nl, codes, 1, mark_mode=2).total == 1  # the path from input 0, side steady
+
+
+def test_fixed_marks_follow_any_fanin():
+    # AND(a, b) with a steady and b rising: the reference needs fan-in 0's
+    # mark (a has no transition, so no mark); FIXED takes the path through b
+    nl = P.Netlist([0, 2, 3], [P.INPT] * 2 + [P.AND], [0, 0, 1], [0, 0, 2], [1, 1, 0], [0, 1, 2], [2, 2, 0, 1])
+    codes = np.array([[R.S1], [R.T1]], np.uint8)
+    assert O.grade(nl, codes, 1, mark_mode=0).total == 0
+    assert O.grade(nl, codes, 1, mark_mode=2).total == 1

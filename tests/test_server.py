@@ -47,7 +47,7 @@ def _serve(jobs, budget=0, mode=1, arrive_every=2):
     return res, srv.stats()
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 3])
 def test_served_results_equal_offline_grading(mode):
     jobs = _jobs()
     res, st = _serve(jobs, mode=mode)
