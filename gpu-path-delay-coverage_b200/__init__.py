@@ -70,7 +70,8 @@ class Totals_t(C.Structure):
 
 class CircuitOpts_t(C.Structure):
     _fields_ = [("device", C.c_int), ("mark_mode", C.c_int), ("max_pairs", C.c_uint32),
-                ("tile_words", C.c_uint32), ("threads", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("tile_words", C.c_uint32), ("threads", C.c_uint32), ("seg_len", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class BatchJob_t(C.Structure):
@@ -99,7 +100,8 @@ class CircuitInfo_t(C.Structure):
     _fields_ = [("n_gates", C.c_uint32), ("n_levels", C.c_uint32), ("n_pi", C.c_uint32),
                 ("n_po", C.c_uint32), ("max_level_width", C.c_uint32), ("max_nfi", C.c_uint32),
                 ("max_nfo", C.c_uint32), ("tile_words", C.c_uint32), ("threads", C.c_uint32),
-                ("n_edges", C.c_uint64), ("device_bytes", C.c_uint64), ("max_pairs", C.c_uint64)]
+                ("n_edges", C.c_uint64), ("device_bytes", C.c_uint64), ("max_pairs", C.c_uint64),
+                ("seg_len", C.c_uint32), ("reserved", C.c_uint32), ("n_segments", C.c_uint64)]
 
 
 class GenParams_t(C.Structure):
@@ -181,6 +183,8 @@ ABI = [
     ("pdf_dump_mark", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64,
                                 C.c_int]),
     ("pdf_dump_merge", C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    ("pdf_dump_segments", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p]),
+    ("pdf_circuit_segments", C.c_int, [C.c_void_p, C.c_void_p]),
 ]
 
 
@@ -387,6 +391,15 @@ def dump_merge(path: str, first_x: np.ndarray, first_y: np.ndarray) -> None:
     check(lib().pdf_dump_merge(os.fsencode(path), fx.ctypes.data, fy.ctypes.data, len(fx)), "pdf_dump_merge")
 
 
+def dump_segments(path: str, segs: np.ndarray, first_x: np.ndarray, first_y: np.ndarray) -> None:
+    """gpumerge.log layout of segments (pdf_dump_segments)."""
+    sg = np.ascontiguousarray(segs, np.uint32)
+    fx = np.ascontiguousarray(first_x, np.uint32)
+    fy = np.ascontiguousarray(first_y, np.uint32)
+    check(lib().pdf_dump_segments(os.fsencode(path), sg.ctypes.data, sg.shape[1], sg.shape[0], fx.ctypes.data,
+                                  fy.ctypes.data), "pdf_dump_segments")
+
+
 def words(n_pairs: int) -> int:
     return (n_pairs + 31) // 32
 
@@ -444,18 +457,27 @@ class Circuit:
     """A netlist uploaded to one device (pdf_circuit_create)."""
 
     def __init__(self, nl: Netlist, device: int = 0, mark_mode: int = MARK_DEFAULT,
-                 max_pairs: int = 0, tile_words: int = 0, threads: int = 0):
+                 max_pairs: int = 0, tile_words: int = 0, threads: int = 0, seg_len: int = 1):
+        self.h = None
         self.netlist = nl
         self.mark_mode = mark_mode
-        o = CircuitOpts_t(device, mark_mode, max_pairs, tile_words, threads)
+        o = CircuitOpts_t(device, mark_mode, max_pairs, tile_words, threads, seg_len)
         h = C.c_void_p()
         check(lib().pdf_circuit_create(C.byref(nl.view()), C.byref(o), C.byref(h)), "pdf_circuit_create")
         self.h = h
+        self.n_first = self.info().n_segments  # entries of a state's first-detect arrays
 
     def info(self) -> CircuitInfo_t:
         i = CircuitInfo_t()
         check(lib().pdf_circuit_query(self.h, C.byref(i)), "pdf_circuit_query")
         return i
+
+    def segments(self) -> np.ndarray:
+        """The segment list [n_segments][seg_len] (pdf_circuit_segments)."""
+        i = self.info()
+        out = np.zeros((i.n_segments, max(1, i.seg_len)), np.uint32)
+        check(lib().pdf_circuit_segments(self.h, out.ctypes.data), "pdf_circuit_segments")
+        return out
 
     def close(self):
         if self.h:
@@ -494,7 +516,7 @@ class State:
         return list(ms), n.value
 
     def snapshot(self):
-        G = self.circuit.netlist.n_gates
+        G = self.circuit.n_first
         fx = np.zeros(G, np.uint32)
         fy = np.zeros(G, np.uint32)
         tot = Totals_t()

@@ -17,7 +17,7 @@
 // each timed on its own from the host (call to device idle), and
 // the stage's planes are written to the reference's log files in the current
 // directory: gpusim-p2.log (--sim), gpumark-full.log and gpumark.log
-// (--mark), gpumerge.log (--merge).
+// (--mark), gpumerge.log (--merge; per segment with --segs N > 1).
 #include <cuda_runtime.h>
 #include <getopt.h>
 
@@ -65,7 +65,7 @@ void usage(const char *argv0) {
     std::printf("Usage: %s --bench CIRCUIT [options] VECTORS...\n", argv0);
     std::printf("\t--bench /path/to/ckt : the circuit; a name containing \"bench\" is read as ISCAS .bench,\n"
                 "\t                       anything else as pdf-level text\n");
-    std::printf("\t--segs N : segment length; this build grades segments of length 1\n");
+    std::printf("\t--segs N : Run fault grading over segments of length N, where 1 <= N <= 8\n");
     std::printf("\t--robust : robust sensitisation table (LUT_R) instead of the default (LUT_NR)\n");
     std::printf("\t--num_patterns N : vector pairs per pass (rounded up to a multiple of 32)\n");
     std::printf("\t--verbose with --sim / --mark / --merge : write gpusim-p2.log / gpumark-full.log and\n"
@@ -121,8 +121,7 @@ int main(int argc, char *argv[]) {
                 break;
             case 's':
                 segs = std::atoi(optarg);
-                if (segs < 1 || segs > 8) die("segment lengths outside 1..8 are not supported");
-                if (segs > 1) die("this build grades segments of length 1 only (--segs 1)");
+                if (segs < 1 || segs > 8) die("Segment lengths over 8 are not supported!");
                 break;
             case 'd':
                 device = std::atoi(optarg);
@@ -154,10 +153,20 @@ int main(int argc, char *argv[]) {
 
     pdf_circuit_opts co{};
     co.device = device;
+    co.seg_len = (uint32_t)segs;
     co.mark_mode = fixed_flag ? (robust_flag ? PDF_MARK_FIXED_ROBUST : PDF_MARK_FIXED_NONROBUST)
                               : (robust_flag ? PDF_MARK_ROBUST : PDF_MARK_DEFAULT);
     pdf_circuit *ckt = nullptr;
     check(pdf_circuit_create(&nl, &co, &ckt), "pdf_circuit_create");
+    pdf_circuit_info ci{};
+    check(pdf_circuit_query(ckt, &ci), "pdf_circuit_query");
+    const uint64_t n_first = ci.n_segments;  // first-detect entries: nets, or segments
+    std::vector<uint32_t> seg_list;
+    if (segs > 1) {
+        std::clog << "Segments of " << segs << " nets: " << n_first << std::endl;
+        seg_list.resize(n_first * segs);
+        check(pdf_circuit_segments(ckt, seg_list.data()), "pdf_circuit_segments");
+    }
     const bool dumps = verbose_flag && (sim_flag || mark_flag || merge_flag);
     if (verbose_flag && cover_flag) std::clog << "gpucover.log is not written by this build" << std::endl;
 
@@ -211,7 +220,7 @@ int main(int argc, char *argv[]) {
             check_cuda(cudaMalloc(&dm.p, (size_t)G * cw * 4), "cudaMalloc");
             check_cuda(cudaMalloc(&dmf.p, (size_t)G * cw * 4), "cudaMalloc");
             std::vector<uint32_t> hp((size_t)G * cw), hq((size_t)G * cw);
-            std::vector<uint32_t> fx(G), fy(G);
+            std::vector<uint32_t> fx(n_first), fy(n_first);
             auto timed = [](auto fn) {
                 const auto t0 = std::chrono::steady_clock::now();
                 fn();
@@ -255,7 +264,11 @@ int main(int argc, char *argv[]) {
                     check(pdf_dump_mark("gpumark.log", hq.data(), G, n, cw, p0, app), "pdf_dump_mark");
                 }
                 check(pdf_state_snapshot(st, fx.data(), fy.data(), &total), "pdf_state_snapshot");
-                if (merge_flag) check(pdf_dump_merge("gpumerge.log", fx.data(), fy.data(), G), "pdf_dump_merge");
+                if (merge_flag && segs > 1)
+                    check(pdf_dump_segments("gpumerge.log", seg_list.data(), segs, n_first, fx.data(), fy.data()),
+                          "pdf_dump_segments");
+                else if (merge_flag)
+                    check(pdf_dump_merge("gpumerge.log", fx.data(), fy.data(), G), "pdf_dump_merge");
                 std::cerr << "GPU Coverage: " << u128_string(batch.hi, batch.lo)
                           << ", total: " << u128_string(total.hi, total.lo) << std::endl;
             }

@@ -79,6 +79,8 @@ struct DeviceGuard {
 // stage calls).
 struct Workspace {
     DevBuf nzb, maxlvl, active, active_list;
+    DevBuf seg_first;  // (net, pair) hash set of the cover with segments
+    uint64_t seg_first_mask = 0;
     DevBuf planes;   // internal V, T, M planes when the caller gives none
     DevBuf pi;       // staged host pairs
     uint64_t plane_ld = 0, plane_words = 0;
@@ -87,6 +89,8 @@ struct Workspace {
         maxlvl.release();
         active.release();
         active_list.release();
+        seg_first.release();
+        seg_first_mask = 0;
         planes.release();
         pi.release();
     }
@@ -105,6 +109,22 @@ struct pdf_circuit {
     uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
     Workspace stage;  // scratch of the stage calls
     std::mutex mu;    // serialises the stage scratch
+    // segments longer than one net
+    uint32_t seg_len = 1;
+    uint64_t n_segs = 0;
+    DevBuf segs, seg_off;
+    // entries of a state's first-detect arrays: one per segment
+    uint64_t n_first() const { return seg_len > 1 ? n_segs : info.n_gates; }
+    SegArgs seg_args() const {
+        SegArgs a{};
+        if (seg_len > 1) {
+            a.segs = segs.as<uint32_t>();
+            a.seg_off = seg_off.as<uint32_t>();
+            a.N = seg_len;
+            a.S = (uint32_t)n_segs;
+        }
+        return a;
+    }
 };
 
 struct ProfEvents {
@@ -262,6 +282,74 @@ extern "C" pdf_status pdf_netlist_check(const pdf_netlist *nl, char *msg, size_t
 
 // ---------------------------------------------------------------------------
 
+namespace {
+
+// Segments of N nets (2..8): every directed subpath of N nets, listed by
+// first net ascending, then depth first along fan-outs in edge order (the
+// reference's generateSegmentList lives in its missing util/segment.cuh).
+// Counted first (paths of k nets from g = sum over fan-outs of paths of k - 1
+// nets), then written as [S][N] with a CSR offset per first net.
+constexpr uint64_t kMaxSegWords = 1ull << 28;  // S * N gate ids at most (1 GiB)
+
+pdf_status build_segments(pdf_circuit *c, const pdf_netlist *nl, uint32_t N) {
+    const uint32_t G = nl->n_gates;
+    auto fo = [&](uint32_t g, uint32_t k) { return nl->edges[nl->edge_offset[g] + nl->nfi[g] + k]; };
+    std::vector<uint64_t> cnt(G, 1), nxt(G);
+    for (uint32_t k = 1; k < N; k++) {
+        for (uint32_t g = 0; g < G; g++) {
+            uint64_t t = 0;
+            for (uint32_t j = 0; j < nl->nfo[g]; j++) t = std::min(t + cnt[fo(g, j)], kMaxSegWords + 1);
+            nxt[g] = t;
+        }
+        cnt.swap(nxt);
+    }
+    std::vector<uint32_t> off(G + 1, 0);
+    uint64_t S = 0;
+    for (uint32_t g = 0; g < G; g++) {
+        S += cnt[g];
+        if (S * N > kMaxSegWords) return PDF_ENOTSUP;
+        off[g + 1] = (uint32_t)S;
+    }
+    std::vector<uint32_t> segs;
+    try {
+        segs.resize(S * N);
+    } catch (const std::bad_alloc &) {
+        return PDF_ENOMEM;
+    }
+    uint32_t path[8], idx[8];
+    uint64_t w = 0;
+    for (uint32_t g0 = 0; g0 < G; g0++) {
+        int d = 0;
+        path[0] = g0;
+        idx[0] = 0;
+        while (d >= 0) {
+            if ((uint32_t)d == N - 1) {
+                std::memcpy(segs.data() + w, path, N * 4);
+                w += N;
+                d--;
+            } else if (idx[d] < nl->nfo[path[d]]) {
+                path[d + 1] = fo(path[d], idx[d]++);
+                idx[d + 1] = 0;
+                d++;
+            } else {
+                d--;
+            }
+        }
+    }
+    if (w != S * N) return PDF_EINVAL;
+    if (c->segs.ensure(std::max<uint64_t>(S * N * 4, 16)) != cudaSuccess ||
+        c->seg_off.ensure((uint64_t)(G + 1) * 4) != cudaSuccess)
+        return PDF_ENOMEM;
+    if ((S && cudaMemcpy(c->segs.p, segs.data(), S * N * 4, cudaMemcpyHostToDevice) != cudaSuccess) ||
+        cudaMemcpy(c->seg_off.p, off.data(), (uint64_t)(G + 1) * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        return PDF_ECUDA;
+    c->seg_len = N;
+    c->n_segs = S;
+    return PDF_OK;
+}
+
+}  // namespace
+
 extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circuit_opts *opts,
                                          pdf_circuit **out) {
     if (!out) return PDF_EINVAL;
@@ -271,6 +359,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     pdf_circuit_opts o{};
     if (opts) o = *opts;
     if (o.mark_mode < PDF_MARK_DEFAULT || o.mark_mode > PDF_MARK_FIXED_NONROBUST) return PDF_EINVAL;
+    if (o.seg_len > 8) return PDF_EINVAL;
     if (o.tile_words && o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8)
         return PDF_EINVAL;
     if (o.threads && (o.threads < 64 || o.threads > 1024 || o.threads % 32)) return PDF_EINVAL;
@@ -491,6 +580,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->cover_grid = (uint32_t)prop.multiProcessorCount;
 
     auto fail = [&](pdf_status st2) {
+        c->segs.release();
+        c->seg_off.release();
         c->rec.release();
         c->edges.release();
         c->level_off.release();
@@ -530,8 +621,29 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     inf.tile_words = c->bw;
     inf.threads = c->threads;
     inf.max_pairs = o.max_pairs ? o.max_pairs : 65536;
-    inf.device_bytes = c->rec.bytes + c->edges.bytes + c->level_off.bytes + c->pieces.bytes + c->far.bytes;
+    if (o.seg_len > 1) {
+        const pdf_status sst = build_segments(c, nl, o.seg_len);
+        if (sst != PDF_OK) {
+            (void)cudaGetLastError();
+            return fail(sst);
+        }
+    }
+    inf.seg_len = c->seg_len;
+    inf.n_segments = c->n_first();
+    inf.device_bytes = c->rec.bytes + c->edges.bytes + c->level_off.bytes + c->pieces.bytes + c->far.bytes +
+                       c->segs.bytes + c->seg_off.bytes;
     *out = c;
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_circuit_segments(const pdf_circuit *c, uint32_t *gates) {
+    if (!c || !gates) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    if (c->seg_len <= 1) {
+        for (uint32_t g = 0; g < c->info.n_gates; g++) gates[g] = g;
+        return PDF_OK;
+    }
+    PDF_CUDA(cudaMemcpy(gates, c->segs.p, (size_t)c->n_segs * c->seg_len * 4, cudaMemcpyDeviceToHost));
     return PDF_OK;
 }
 
@@ -545,6 +657,8 @@ extern "C" void pdf_circuit_destroy(pdf_circuit *c) {
     c->pieces.release();
     c->far.release();
     c->err.release();
+    c->segs.release();
+    c->seg_off.release();
     delete c;
 }
 
@@ -564,7 +678,7 @@ extern "C" pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out) {
     pdf_state *s = new (std::nothrow) pdf_state();
     if (!s) return PDF_ENOMEM;
     s->c = c;
-    const size_t G = c->info.n_gates;
+    const size_t G = c->n_first();  // first-detect entries: nets, or segments
     if (s->first_x.ensure(4 * G) != cudaSuccess || s->first_y.ensure(4 * G) != cudaSuccess ||
         s->acc.ensure(sizeof(DevAcc)) != cudaSuccess ||
         !(s->host_acc = new (std::nothrow) DevAcc())) {
@@ -597,7 +711,7 @@ extern "C" void pdf_state_destroy(pdf_state *s) {
 extern "C" pdf_status pdf_state_reset(pdf_state *s) {
     if (!s) return PDF_EINVAL;
     DeviceGuard dg(s->c->device);
-    const size_t G = s->c->info.n_gates;
+    const size_t G = s->c->n_first();
     PDF_CUDA(cudaDeviceSynchronize());
     PDF_CUDA(cudaMemset(s->first_x.p, 0xFF, 4 * G));
     PDF_CUDA(cudaMemset(s->first_y.p, 0xFF, 4 * G));
@@ -610,7 +724,7 @@ extern "C" pdf_status pdf_state_reset_async(pdf_state *s, void *stream) {
     if (!s) return PDF_EINVAL;
     DeviceGuard dg(s->c->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    const size_t G = s->c->info.n_gates;
+    const size_t G = s->c->n_first();
     PDF_CUDA(cudaMemsetAsync(s->first_x.p, 0xFF, 4 * G, cs));
     PDF_CUDA(cudaMemsetAsync(s->first_y.p, 0xFF, 4 * G, cs));
     PDF_CUDA(cudaMemsetAsync(s->acc.p, 0, sizeof(DevAcc), cs));
@@ -651,7 +765,7 @@ extern "C" pdf_status pdf_state_snapshot(pdf_state *s, uint32_t *first_x, uint32
                                          pdf_totals *tot) {
     if (!s) return PDF_EINVAL;
     DeviceGuard dg(s->c->device);
-    const size_t G = s->c->info.n_gates;
+    const size_t G = s->c->n_first();
     PDF_CUDA(cudaDeviceSynchronize());
     if (first_x) PDF_CUDA(cudaMemcpy(first_x, s->first_x.p, 4 * G, cudaMemcpyDeviceToHost));
     if (first_y) PDF_CUDA(cudaMemcpy(first_y, s->first_y.p, 4 * G, cudaMemcpyDeviceToHost));
@@ -671,7 +785,7 @@ extern "C" pdf_status pdf_state_restore(pdf_state *s, const uint32_t *first_x,
                                         const uint32_t *first_y, const pdf_totals *tot) {
     if (!s || !first_x || !first_y || !tot) return PDF_EINVAL;
     DeviceGuard dg(s->c->device);
-    const size_t G = s->c->info.n_gates;
+    const size_t G = s->c->n_first();
     PDF_CUDA(cudaDeviceSynchronize());
     PDF_CUDA(cudaMemcpy(s->first_x.p, first_x, 4 * G, cudaMemcpyHostToDevice));
     PDF_CUDA(cudaMemcpy(s->first_y.p, first_y, 4 * G, cudaMemcpyHostToDevice));
@@ -706,7 +820,18 @@ pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes
     PDF_CUDA(ws.maxlvl.ensure(n_blocks * 4));
     // active bitmap [W], then the count; the list holds <= 2 pairs per gate
     PDF_CUDA(ws.active.ensure(W * 4 + 16));
-    PDF_CUDA(ws.active_list.ensure(std::min<uint64_t>(W * 32, 2 * (uint64_t)c->info.n_gates) * 4));
+    PDF_CUDA(ws.active_list.ensure(std::min<uint64_t>(W * 32, 2 * std::max<uint64_t>(c->n_first(), c->info.n_gates)) * 4));
+    if (c->seg_len > 1) {
+        // (net, pair) entries: at most N per first pair of a segment, two per
+        // segment, and one per (net, pair); a table at least twice that
+        const uint64_t most = std::min<uint64_t>(2 * c->n_segs * c->seg_len, (uint64_t)c->info.n_gates * W * 32);
+        uint64_t cap = 1024;
+        while (cap < 2 * most && cap < (1ull << 27)) cap <<= 1;
+        if (ws.seg_first_mask + 1 < cap) {
+            PDF_CUDA(ws.seg_first.ensure(cap * 8));
+            ws.seg_first_mask = cap - 1;
+        }
+    }
     if (need_planes) {
         const uint64_t ld = n_blocks * c->bw;
         if (ws.plane_ld < ld || !ws.planes.p) {
@@ -762,6 +887,11 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
     a.active_list = ws.active_list.as<uint32_t>();
     a.acc = acc;
     a.hash_cap = c->hash_cap;
+    a.seg = c->seg_args();
+    if (c->seg_len > 1) {
+        a.seg_first = ws.seg_first.as<unsigned long long>();
+        a.seg_first_mask = ws.seg_first_mask;
+    }
     return a;
 }
 
@@ -850,8 +980,9 @@ pdf_status grade_mark_locked(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr, 
     }
     a.nzb = s->ws.nzb.as<uint32_t>();
     a.blk_maxlvl = s->ws.maxlvl.as<uint32_t>();
-    a.first_x = s->first_x.as<uint32_t>();
-    a.first_y = s->first_y.as<uint32_t>();
+    // with segments the state holds per-segment ids, merged after the kernel
+    a.first_x = c->seg_len > 1 ? nullptr : s->first_x.as<uint32_t>();
+    a.first_y = c->seg_len > 1 ? nullptr : s->first_y.as<uint32_t>();
     a.pair_base = (uint32_t)pair_base;
     DevAcc *acc = s->acc.as<DevAcc>();
     a.err = &acc->err;
@@ -872,6 +1003,21 @@ pdf_status grade_mark_locked(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr, 
     a.acc = acc;
     a.active = s->ws.active.as<uint32_t>();
     PDF_CUDA(launch_forward(a, FWD_FUSED, c->mark_mode, c->bw, c->threads, c->fwd_smem, cs));
+    if (c->seg_len > 1) {
+        SegMergeArgs sm{};
+        sm.seg = c->seg_args();
+        sm.V = a.V;
+        sm.M = a.M;
+        sm.ld = a.ld;
+        sm.nzb = a.nzb;
+        sm.bm_words = a.bm_words;
+        sm.bw = c->bw;
+        sm.W = (uint32_t)W;
+        sm.pair_base = (uint32_t)pair_base;
+        sm.first_x = s->first_x.as<uint32_t>();
+        sm.first_y = s->first_y.as<uint32_t>();
+        PDF_CUDA(launch_seg_merge(sm, (uint32_t)((W + c->bw - 1) / c->bw), cs));
+    }
     if (s->pe) PDF_CUDA(cudaEventRecord(s->pe->ev[1], cs));
     if (out && !direct) {
         st = copy_plane_out(out->sim_v, out->ld, out->on_device, a.V, a.ld, W, G, cs);
@@ -945,7 +1091,7 @@ extern "C" pdf_status pdf_state_first_copy(pdf_state *s, uint32_t *first_x, uint
     if (!s || !first_x || !first_y) return PDF_EINVAL;
     DeviceGuard dg(s->c->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    const size_t bytes = 4 * (size_t)s->c->info.n_gates;
+    const size_t bytes = 4 * (size_t)s->c->n_first();
     if (to_state) {
         PDF_CUDA(cudaMemcpyAsync(s->first_x.p, first_x, bytes, cudaMemcpyDeviceToDevice, cs));
         PDF_CUDA(cudaMemcpyAsync(s->first_y.p, first_y, bytes, cudaMemcpyDeviceToDevice, cs));
@@ -1071,8 +1217,12 @@ extern "C" pdf_status pdf_merge(pdf_circuit *c, pdf_state *s, const uint32_t *si
     if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
     DeviceGuard dg(c->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    PDF_CUDA(launch_merge_dense(c->dc, sim_v, mark, ld, n_pairs, (uint32_t)pair_base,
-                                s->first_x.as<uint32_t>(), s->first_y.as<uint32_t>(), cs));
+    if (c->seg_len > 1)
+        PDF_CUDA(launch_seg_merge_dense(c->seg_args(), sim_v, mark, ld, n_pairs, (uint32_t)pair_base,
+                                        s->first_x.as<uint32_t>(), s->first_y.as<uint32_t>(), cs));
+    else
+        PDF_CUDA(launch_merge_dense(c->dc, sim_v, mark, ld, n_pairs, (uint32_t)pair_base,
+                                    s->first_x.as<uint32_t>(), s->first_y.as<uint32_t>(), cs));
     return PDF_OK;
 }
 
@@ -1118,6 +1268,7 @@ extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, ui
                                         pdf_totals *chunk_total, void *stream) {
     if (!c || !mark || !first_x || !first_y || !chunk_total || n_pairs == 0 || ld < (n_pairs + 31) / 32)
         return PDF_EINVAL;
+    if (c->seg_len > 1) return PDF_ENOTSUP;  // its fixed scratch holds no (net, pair) set
     if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
     const uint64_t W = (n_pairs + 31) / 32, n_blocks = (W + c->bw - 1) / c->bw;
     const uint64_t bm_words = (c->info.n_gates + 31) / 32;
@@ -1210,6 +1361,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         if (!j.circuit || !j.state || j.state->c != j.circuit || j.circuit->device != c0->device ||
             j.circuit->bw != c0->bw || j.circuit->mark_mode != c0->mark_mode)
             return PDF_EINVAL;
+        if (j.circuit->seg_len > 1) return PDF_ENOTSUP;  // batches grade segments of one net
         const uint64_t n = j.pairs.n_pairs, W = (n + 31) / 32;
         if (n == 0 || !j.pairs.on_device || j.pair_base + n > 0xFFFFFFFFull ||
             !planes_fit(j.circuit, W, j.pairs.ld, {j.pairs.v, j.pairs.t}))

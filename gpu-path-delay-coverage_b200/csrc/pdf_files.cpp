@@ -587,3 +587,16 @@ extern "C" pdf_status pdf_dump_merge(const char *path, const uint32_t *first_x, 
           << "\n";
     return o.good() ? PDF_OK : PDF_EINVAL;
 }
+
+extern "C" pdf_status pdf_dump_segments(const char *path, const uint32_t *gates, uint32_t seg_len,
+                                        uint64_t n_segments, const uint32_t *first_x, const uint32_t *first_y) {
+    if (!path || !gates || !first_x || !first_y || seg_len == 0) return PDF_EINVAL;
+    std::ofstream o(path);
+    if (!o) return PDF_EINVAL;
+    for (uint64_t s = 0; s < n_segments; s++) {
+        o << "Segment " << s << "(";
+        for (uint32_t j = 0; j < seg_len; j++) o << gates[s * seg_len + j] << (j + 1 < seg_len ? "," : "");
+        o << "): " << (int32_t)first_x[s] << "," << (int32_t)first_y[s] << " " << "\n";
+    }
+    return o.good() ? PDF_OK : PDF_EINVAL;
+}

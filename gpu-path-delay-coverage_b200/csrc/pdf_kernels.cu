@@ -16,6 +16,7 @@
 //               pairs mark, in exact 128-bit integers.
 #include "pdf_kernels.cuh"
 
+#include <algorithm>
 #include <mutex>
 
 namespace {
@@ -365,7 +366,7 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
             const bool nz = vany(nm);
             if (!nz) {
                 atomicAnd(S.bm + (g >> 5), ~(1u << (g & 31)));
-            } else if (MODE == FWD_FUSED) {  // merge: first falling / rising pair
+            } else if (MODE == FWD_FUSED && a.first_x) {  // merge: first falling / rising pair
                 const Vec<BW> v = vld<BW>(rows + (size_t)gi * 2 * BW + BW);
                 uint32_t cx = kEmpty, cy = kEmpty;
 #pragma unroll
@@ -676,6 +677,128 @@ __global__ void k_active(const CoverArgs a) {
     active_gate(a, g, [&](uint32_t d) { a.active_list[atomicAdd(a.active_count, 1u)] = d; });
 }
 
+// ---- segments longer than one net ----------------------------------------
+
+constexpr unsigned long long kEmpty64 = ~0ull;
+__device__ __forceinline__ uint64_t key_slot(unsigned long long k, uint64_t mask) {
+    k ^= k >> 33;  // 64-bit finaliser (murmur3 fmix64)
+    k *= 0xFF51AFD7ED558CCDull;
+    k ^= k >> 33;
+    k *= 0xC4CEB9FE1A85EC53ull;
+    k ^= k >> 33;
+    return k & mask;
+}
+// Open addressing, linear probing, at most one pass over the table.
+__device__ __forceinline__ bool first_set_insert(unsigned long long *t, uint64_t mask, unsigned long long key) {
+    uint64_t h = key_slot(key, mask);
+    for (uint64_t i = 0; i <= mask; i++) {
+        const unsigned long long old = atomicCAS(t + h, kEmpty64, key);
+        if (old == kEmpty64 || old == key) return true;
+        h = (h + 1) & mask;
+    }
+    return false;
+}
+__device__ __forceinline__ bool first_set_find(const unsigned long long *t, uint64_t mask, unsigned long long key) {
+    uint64_t h = key_slot(key, mask);
+    for (uint64_t i = 0; i <= mask; i++) {
+        const unsigned long long v = t[h];
+        if (v == key) return true;
+        if (v == kEmpty64) return false;
+        h = (h + 1) & mask;
+    }
+    return false;
+}
+
+// Per segment: its first pairs that fall in this batch mark every net of the
+// segment as first for that pair (findActiveThreads, coverkernel.cuh:130-154),
+// and list the pair as active.
+__global__ void k_seg_first(const CoverArgs a) {
+    const uint32_t N = a.seg.N;
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.seg.S;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t f[2] = {a.first_x[s], a.first_y[s]};
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const uint32_t d = f[k] - a.pair_base;
+            if (f[k] == kEmpty || d >= a.n_pairs) continue;
+            const uint32_t *sg = a.seg.segs + s * N;
+            for (uint32_t i = 0; i < N; i++)
+                if (!first_set_insert(a.seg_first, a.seg_first_mask, ((unsigned long long)sg[i] << 32) | d))
+                    atomicOr(&a.acc->err, kErrHashFull);
+            const uint32_t bit = 1u << (d & 31);
+            if (!(atomicOr(a.active + (d >> 5), bit) & bit)) a.active_list[atomicAdd(a.active_count, 1u)] = d;
+        }
+    }
+}
+
+// After the forward kernel: for each column block, each marked net g0 and
+// each segment starting at g0 whose nets are all marked in the block, the
+// first falling / rising pair marking all of them (kernSegmentReduce2<N>,
+// mergekernel.cuh:116-198; direction by the first net's value, :140-143).
+// One CTA per column block; a warp per bitmap word, lanes over segments.
+__global__ void k_seg_merge(const SegMergeArgs a) {
+    const uint32_t blk = blockIdx.x, w0 = blk * a.bw, wend = min(a.W, w0 + a.bw), N = a.seg.N;
+    const uint32_t *bm = a.nzb + (size_t)blk * a.bm_words;
+    const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (uint32_t q = threadIdx.x >> 5; q < a.bm_words; q += nw) {
+        uint32_t bits = bm[q];
+        while (bits) {
+            const uint32_t g0 = q * 32 + (__ffs(bits) - 1);
+            bits &= bits - 1;
+            const uint32_t s1 = a.seg.seg_off[g0 + 1];
+            for (uint32_t s = a.seg.seg_off[g0] + lane; s < s1; s += 32) {
+                const uint32_t *sg = a.seg.segs + (size_t)s * N;
+                bool ok = true;
+                for (uint32_t i = 1; i < N && ok; i++) ok = bit_test(bm, sg[i]);
+                if (!ok) continue;
+                uint32_t cx = kEmpty, cy = kEmpty;
+                for (uint32_t w = w0; w < wend && (cx == kEmpty || cy == kEmpty); w++) {
+                    uint32_t m = a.M[(size_t)g0 * a.ld + w];
+                    for (uint32_t i = 1; i < N && m; i++) m &= a.M[(size_t)sg[i] * a.ld + w];
+                    if (!m) continue;
+                    const uint32_t v = a.V[(size_t)g0 * a.ld + w];
+                    const uint32_t x = m & ~v, y = m & v;
+                    if (x && cx == kEmpty) cx = w * 32 + (__ffs(x) - 1);
+                    if (y && cy == kEmpty) cy = w * 32 + (__ffs(y) - 1);
+                }
+                if (cx != kEmpty) atomicMin(a.first_x + s, a.pair_base + cx);
+                if (cy != kEmpty) atomicMin(a.first_y + s, a.pair_base + cy);
+            }
+        }
+    }
+}
+
+// Dense variant over given planes (stage call pdf_merge): a warp per
+// (segment, 32-word chunk), warp minimum, one atomicMin per warp.
+__global__ void k_seg_merge_dense(const SegArgs seg, const uint32_t *V, const uint32_t *M, uint64_t ld,
+                                  uint64_t n_pairs, uint32_t W, uint32_t pair_base, uint32_t *first_x,
+                                  uint32_t *first_y) {
+    const uint32_t chunks = (W + 31) / 32;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    if (warp >= (uint64_t)seg.S * chunks) return;
+    const uint32_t s = (uint32_t)(warp / chunks), w = (uint32_t)(warp % chunks) * 32 + lane;
+    const uint32_t *sg = seg.segs + (size_t)s * seg.N;
+    uint32_t cx = kEmpty, cy = kEmpty;
+    if (w < W) {
+        uint32_t m = M[(size_t)sg[0] * ld + w];
+        for (uint32_t i = 1; i < seg.N && m; i++) m &= M[(size_t)sg[i] * ld + w];
+        if (w == W - 1 && (n_pairs & 31)) m &= (1u << (n_pairs & 31)) - 1u;
+        if (m) {
+            const uint32_t v = V[(size_t)sg[0] * ld + w];
+            const uint32_t x = m & ~v, y = m & v;
+            if (x) cx = w * 32 + (__ffs(x) - 1);
+            if (y) cy = w * 32 + (__ffs(y) - 1);
+        }
+    }
+    cx = __reduce_min_sync(0xFFFFFFFFu, cx);
+    cy = __reduce_min_sync(0xFFFFFFFFu, cy);
+    if (lane == 0) {
+        if (cx != kEmpty) atomicMin(first_x + s, pair_base + cx);
+        if (cy != kEmpty) atomicMin(first_y + s, pair_base + cy);
+    }
+}
+
 // Close a batch: total = min(2^128 - 1, total + batch); flags are sticky.
 __device__ void batch_close(DevAcc *acc, uint64_t n_pairs) {
     pdf_u128 b = ((pdf_u128)acc->batch_hi << 64) | acc->batch_lo;
@@ -878,7 +1001,13 @@ __device__ __forceinline__ void cover_pair(const CoverArgs &a, const uint32_t p,
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint32_t g = lid[i];
         const GateRec r = load_rec(a.c.rec + g);
-        const uint32_t fx = a.first_x[g], fy = a.first_y[g];
+        bool first;
+        if (a.seg.N > 1) {
+            first = first_set_find(a.seg_first, a.seg_first_mask, ((unsigned long long)g << 32) | p);
+        } else {
+            const uint32_t fx = a.first_x[g], fy = a.first_y[g];
+            first = fx == pid || fy == pid;
+        }
         const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
         uint32_t k = 0;
         for (uint32_t j = 0; j < nfo; j += 4) {  // four fan-out loads in flight
@@ -889,7 +1018,7 @@ __device__ __forceinline__ void cover_pair(const CoverArgs &a, const uint32_t p,
             for (int u = 0; u < 4; u++) k += fo[u] != kEmpty && find_net(lid, n, fo[u]) != kEmpty ? 1u : 0u;
         }
         info[i] = (rec_po(r) ? kNetPo : 0u) | (rec_type(r) == PDF_INPT ? kNetInpt : 0u) |
-                  (fx == pid || fy == pid ? kNetFirst : 0u) | level_of(lo_tab, L, g);
+                  (first ? kNetFirst : 0u) | level_of(lo_tab, L, g);
         const uint32_t o = k ? atomicAdd(&s_adj, k) : 0u;
         if (o + k > acap) {
             aoff[i] = kEmpty;  // fan-outs read in place during the recurrence
@@ -1175,7 +1304,14 @@ cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bo
         cudaError_t e = cudaMemsetAsync(a.active, 0, (size_t)(W + 1) * sizeof(uint32_t), st);
         if (e != cudaSuccess) return e;
     }
-    k_active<<<(a.c.n_gates + 255) / 256, 256, 0, st>>>(a);
+    if (a.seg.N > 1) {
+        cudaError_t e = cudaMemsetAsync(a.seg_first, 0xFF, (a.seg_first_mask + 1) * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+        const uint32_t blocks = (uint32_t)std::min<uint64_t>(((uint64_t)a.seg.S + 255) / 256, 148u * 16u);
+        k_seg_first<<<std::max(1u, blocks), 256, 0, st>>>(a);
+    } else {
+        k_active<<<(a.c.n_gates + 255) / 256, 256, 0, st>>>(a);
+    }
     const size_t smem = cover_smem_bytes(a.hash_cap);
     cudaError_t e = cudaFuncSetAttribute(k_cover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -1229,6 +1365,24 @@ cudaError_t prepare_batch(const BatchLaunch &b) { return batch_dispatch(b, nullp
 cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
     if (!b.n || !b.total_blocks) return cudaErrorInvalidValue;
     return batch_dispatch(b, st, false);
+}
+
+cudaError_t launch_seg_merge(const SegMergeArgs &a, uint32_t n_blocks, cudaStream_t st) {
+    if (n_blocks == 0) return cudaSuccess;
+    k_seg_merge<<<n_blocks, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_seg_merge_dense(const SegArgs &seg, const uint32_t *V, const uint32_t *M, uint64_t ld,
+                                   uint64_t n_pairs, uint32_t pair_base, uint32_t *first_x, uint32_t *first_y,
+                                   cudaStream_t st) {
+    const uint32_t W = (uint32_t)((n_pairs + 31) / 32);
+    const uint64_t warps = (uint64_t)seg.S * ((W + 31) / 32);
+    const uint64_t blocks = (warps * 32 + 255) / 256;
+    if (blocks == 0) return cudaSuccess;
+    if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    k_seg_merge_dense<<<(unsigned)blocks, 256, 0, st>>>(seg, V, M, ld, n_pairs, W, pair_base, first_x, first_y);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M, uint64_t ld,

@@ -72,6 +72,15 @@ struct FwdArgs {
 constexpr unsigned int kErrTimeout = 0x4u;     // a bounded wait expired (PDF_ETIMEOUT)
 constexpr unsigned int kErrHashFull = 0x100u;  // a pair marked more nets than the cover table holds
 
+// Segments longer than one net (seg_len N = 2..8): directed subpaths of N
+// nets, listed by first net (CSR over it).
+struct SegArgs {
+    const uint32_t *segs;     // [S][N] gate ids
+    const uint32_t *seg_off;  // [n_gates + 1]: segments starting at net g are [seg_off[g], seg_off[g + 1])
+    uint32_t N;               // 0 or 1: per-net first ids (no segment list)
+    uint32_t S;
+};
+
 struct CoverArgs {
     DevCircuit c;
     const uint32_t *M;            // pruned marks [n_gates][ld]
@@ -88,6 +97,22 @@ struct CoverArgs {
     uint32_t *active_count;       // [1]
     DevAcc *acc;
     uint32_t hash_cap;            // nets one pair may mark (the cover's shared-memory net list)
+    // segments longer than one net: first_x / first_y are per segment, and
+    // the (net, pair) pairs where a pair is first are a hash set built by
+    // k_seg_first (keys net << 32 | pair index, ~0 = empty)
+    SegArgs seg;
+    unsigned long long *seg_first;
+    uint64_t seg_first_mask;
+};
+
+// Per-segment first-detect merge after the forward kernel (sparse planes).
+struct SegMergeArgs {
+    SegArgs seg;
+    const uint32_t *V, *M;
+    uint64_t ld;
+    const uint32_t *nzb;          // per column block bitmaps of marked nets (after the prune)
+    uint32_t bm_words, bw, W, pair_base;
+    uint32_t *first_x, *first_y;  // [S]
 };
 
 // Batched grading (k_batch_forward, k_batch_active, k_batch_cover).
@@ -122,6 +147,10 @@ size_t cover_smem_bytes(uint32_t hash_cap);
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M,
                                uint64_t ld, uint64_t n_pairs, uint32_t pair_base,
                                uint32_t *first_x, uint32_t *first_y, cudaStream_t st);
+cudaError_t launch_seg_merge(const SegMergeArgs &a, uint32_t n_blocks, cudaStream_t st);
+cudaError_t launch_seg_merge_dense(const SegArgs &seg, const uint32_t *V, const uint32_t *M, uint64_t ld,
+                                   uint64_t n_pairs, uint32_t pair_base, uint32_t *first_x, uint32_t *first_y,
+                                   cudaStream_t st);
 cudaError_t launch_bitmap_from_marks(const DevCircuit &c, const uint32_t *M, uint64_t ld,
                                      uint64_t n_pairs, uint32_t bw, uint32_t *nzb,
                                      uint32_t *blk_maxlvl, uint32_t bm_words, cudaStream_t st);

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define PDF_ABI_VERSION 1
+#define PDF_ABI_VERSION 2
 
 typedef enum pdf_status {
     PDF_OK = 0,
@@ -167,7 +167,9 @@ typedef struct pdf_circuit_opts {
     uint32_t max_pairs;  /* largest batch this circuit will grade (sizes scratch); 0 = 65536 */
     uint32_t tile_words; /* 0 = autotune; else words (32 pairs) per CTA column block: 1,2,4,8 */
     uint32_t threads;    /* 0 = autotune; else threads per CTA: 128..1024 */
-    uint32_t reserved[3];
+    uint32_t seg_len;    /* path segments of this many nets, 0 or 1 = single nets; up to 8
+                            (fcount --segs N, main.cu:76-81,185-223) */
+    uint32_t reserved[2];
 } pdf_circuit_opts;
 
 typedef struct pdf_circuit_info {
@@ -178,6 +180,9 @@ typedef struct pdf_circuit_info {
     uint64_t n_edges;
     uint64_t device_bytes;   /* netlist + plan + scratch */
     uint64_t max_pairs;
+    uint32_t seg_len;        /* 1, or the segment length */
+    uint32_t reserved;
+    uint64_t n_segments;     /* entries of a state's first-detect arrays: n_gates, or the segments */
 } pdf_circuit_info;
 
 const char *pdf_status_string(int status);
@@ -193,11 +198,29 @@ pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circuit_opts *opt
 void pdf_circuit_destroy(pdf_circuit *c);
 pdf_status pdf_circuit_query(const pdf_circuit *c, pdf_circuit_info *info);
 
+/*
+ * Segments (seg_len N = 2..8; the reference's --segs, with its segment list
+ * from the util/segment.cuh that its snapshot lacks): every directed subpath
+ * of exactly N nets (g_0, ..., g_{N-1}), g_{i+1} a fan-out of g_i, listed by
+ * g_0 ascending, then depth first along fan-outs in edge order.  A segment's
+ * first pair is the first pair marking all its nets, falling (x) or rising
+ * (y) by the value of g_0 (mergekernel.cuh:99-198); in the cover a pair is
+ * first at a net when it is the first pair of a segment through that net
+ * (coverkernel.cuh:115-170).  With N = 1 the segments are the nets.  State
+ * first-detect arrays then hold info.n_segments entries, one per segment.
+ * Segment lists beyond 2^28 gate ids return PDF_ENOTSUP; batches, the server
+ * and pdf_cover_noalloc grade single nets only (PDF_ENOTSUP).
+ * pdf_circuit_segments writes the list as gates[s * N + i] (n_segments * N
+ * entries; for N = 1 the identity).
+ */
+pdf_status pdf_circuit_segments(const pdf_circuit *c, uint32_t *gates);
+
 /* Per-circuit first-detect state and running total: the reference keeps the
  * per-segment first pair ids in dc_seglist across chunks and the total in
  * *totals (main.cu:141,169,224; mergekernel.cuh:205-222).  first_x = first
  * pair marking the net with a falling (T0) transition, first_y = rising (T1);
- * 0xFFFFFFFF = none yet. */
+ * 0xFFFFFFFF = none yet.  The arrays hold info.n_segments entries: one per
+ * net (n_gates), or one per segment when seg_len > 1. */
 pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out);
 void pdf_state_destroy(pdf_state *s);
 pdf_status pdf_state_reset(pdf_state *s);
@@ -251,7 +274,8 @@ pdf_status pdf_grade_mark_async(pdf_circuit *c, pdf_state *s, const pdf_pairs *p
                                 uint64_t pair_base, const pdf_outputs *out, void *stream);
 pdf_status pdf_grade_cover_async(pdf_circuit *c, pdf_state *s, void *stream);
 /* Stream-ordered copy of the state's first-detect ids to (to_state = 0) or
- * from (to_state = 1) device buffers of n_gates uint32 each. */
+ * from (to_state = 1) device buffers of info.n_segments uint32 each (n_gates
+ * for single nets). */
 pdf_status pdf_state_first_copy(pdf_state *s, uint32_t *first_x, uint32_t *first_y, int to_state,
                                 void *stream);
 
@@ -501,6 +525,10 @@ pdf_status pdf_dump_sim(const char *path, const uint32_t *sim_v, const uint32_t 
 pdf_status pdf_dump_mark(const char *path, const uint32_t *mark, uint32_t n_gates, uint64_t n_pairs,
                          uint64_t ld, uint64_t pair_base, int append);
 pdf_status pdf_dump_merge(const char *path, const uint32_t *first_x, const uint32_t *first_y, uint32_t n_gates);
+/* Segments longer than one net: "Segment <s>(g_0,...,g_{N-1}): x,y" per
+ * segment, ids signed (debugSegmentList, mergekernel.cuh:25-46). */
+pdf_status pdf_dump_segments(const char *path, const uint32_t *gates, uint32_t seg_len, uint64_t n_segments,
+                             const uint32_t *first_x, const uint32_t *first_y);
 
 #ifdef __cplusplus
 }

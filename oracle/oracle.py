@@ -43,6 +43,11 @@ def lib() -> C.CDLL:
         L.pdfo_cover.argtypes = [P, P, C.c_uint64, C.c_uint64, P, P, P, P, P, C.c_int]
         L.pdfo_grade.argtypes = [P, P, C.c_uint64, C.c_uint64, C.c_int, C.c_uint64, P, P, P, P, P, P, P,
                                  P, C.c_int]
+        L.pdfo_segments.restype = C.c_uint64
+        L.pdfo_segments.argtypes = [P, C.c_uint32, P, C.c_uint64]
+        L.pdfo_grade_seg.argtypes = [P, P, C.c_uint64, C.c_uint64, C.c_int, C.c_uint64, C.c_uint32, P,
+                                     C.c_uint64, P, P, P, P, P, C.c_int]
+        L.pdfo_grade_seg.restype = C.c_int
         for f in ("pdfo_sim", "pdfo_sim_mode", "pdfo_sim_vectors", "pdfo_mark", "pdfo_merge", "pdfo_cover", "pdfo_grade"):
             getattr(L, f).restype = C.c_int
         _lib = L
@@ -89,6 +94,34 @@ def grade(nl, pi_codes: np.ndarray, n_pairs: int, pair_base: int = 0, mark_mode:
         raise MemoryError("oracle allocation failed")
     chunk_totals = [int(ct[2 * i]) | (int(ct[2 * i + 1]) << 64) for i in range(nchunks)]
     return Result(fx, fy, (hi.value << 64) | lo.value, fl.value, sim, mark, chunk_totals)
+
+
+def segments(nl, seg_len: int) -> np.ndarray:
+    """Segments of seg_len nets as [S][seg_len] gate ids (pdfo_segments order)."""
+    n = int(lib().pdfo_segments(_nl(nl), seg_len, None, 0))
+    out = np.zeros((n, seg_len), np.uint32)
+    if n:
+        lib().pdfo_segments(_nl(nl), seg_len, out.ctypes.data, n)
+    return out
+
+
+def grade_seg(nl, pi_codes: np.ndarray, n_pairs: int, seg_len: int, pair_base: int = 0, mark_mode: int = 0,
+              chunk: int = 0, first_x=None, first_y=None, threads: int = 0) -> Result:
+    """The chunk loop with segments of seg_len nets; first_x / first_y are per segment."""
+    segs = segments(nl, seg_len)
+    S = len(segs)
+    pi = np.ascontiguousarray(pi_codes, dtype=np.uint8)
+    fx = np.full(S, 0xFFFFFFFF, np.uint32) if first_x is None else np.array(first_x, np.uint32)
+    fy = np.full(S, 0xFFFFFFFF, np.uint32) if first_y is None else np.array(first_y, np.uint32)
+    lo, hi, fl = C.c_uint64(0), C.c_uint64(0), C.c_uint32(0)
+    rc = lib().pdfo_grade_seg(_nl(nl), pi.ctypes.data, n_pairs, pair_base, mark_mode, chunk, seg_len,
+                              segs.ctypes.data, S, fx.ctypes.data, fy.ctypes.data, C.addressof(lo),
+                              C.addressof(hi), C.addressof(fl), threads)
+    if rc:
+        raise MemoryError("oracle allocation failed")
+    r = Result(fx, fy, (hi.value << 64) | lo.value, fl.value)
+    r.segs = segs
+    return r
 
 
 def sim(nl, pi_codes: np.ndarray, n_pairs: int, threads: int = 0, mark_mode: int = 0) -> np.ndarray:

@@ -356,9 +356,22 @@ static inline u128 sat_add(u128 a, u128 b, int *ovf) {
  * (marks need fan-in 0's mark), so a saturated c means the true total is at
  * least 2^128; an h that saturates but is never credited changes nothing.
  */
+static int cover_impl(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
+                      const uint32_t *first_x, const uint32_t *first_y, const uint8_t *first_plane,
+                      uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads);
+
 int pdfo_cover(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
                const uint32_t *first_x, const uint32_t *first_y, uint64_t *lo, uint64_t *hi,
                uint32_t *flags, int threads) {
+    return cover_impl(nl, mark, n_pairs, pair_base, first_x, first_y, NULL, lo, hi, flags, threads);
+}
+
+/* first_plane (segments longer than one net): byte [g][p] = 1 when pair p of
+ * the chunk first-detects a segment through g; replaces the first_x/first_y
+ * test (coverkernel.cuh:115-170 finds those pairs per gate). */
+static int cover_impl(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
+                      const uint32_t *first_x, const uint32_t *first_y, const uint8_t *first_plane,
+                      uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads) {
     const uint32_t G = nl->n_gates;
     const uint32_t lvl0 = nl->level_offsets[1];
     const int nt = nthreads(threads);
@@ -394,7 +407,8 @@ int pdfo_cover(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uin
                         C = sat_add(C, c[fo], &ovf);
                         H = sat_add(H, h[fo], &hovf); /* an uncredited overflow is harmless */
                     }
-                    const int first = (first_x[g] == pid) || (first_y[g] == pid); /* :216 */
+                    const int first = first_plane ? first_plane[(uint64_t)g * n_pairs + p] != 0
+                                                  : (first_x[g] == pid) || (first_y[g] == pid); /* :216 */
                     if (first) {
                         c[g] = sat_add(C, H, &ovf); /* :217 */
                         h[g] = 0;                    /* :219 */
@@ -476,6 +490,154 @@ int pdfo_grade(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs,
                 if (mark_out)
                     memcpy(mark_out + (uint64_t)g * n_pairs + start, mark + (uint64_t)g * K, K);
             }
+    }
+    free(pi);
+    free(sim);
+    free(mark);
+    return rc;
+}
+
+/* ---- path segments longer than one net (main.cu:185-223, segs = N > 1) ----
+ *
+ * The reference builds its segment list in util/segment.cuh
+ * (generateSegmentList, mergekernel.cuh:210), which its snapshot does not
+ * contain.  Restated definition: a segment of length N is a directed subpath
+ * of exactly N nets (g_0, ..., g_{N-1}), g_{i+1} a fan-out of g_i; listed by
+ * g_0 ascending, then depth first along fan-outs in edge order.  For N = 1
+ * the segments are the nets, which is the N = 1 path above. */
+
+/* Number of segments of length N (saturates at UINT64_MAX); when out is not
+ * NULL and cap >= the count, writes them as out[s * N + i]. */
+uint64_t pdfo_segments(const pdf_netlist *nl, uint32_t N, uint32_t *out, uint64_t cap) {
+    const uint32_t G = nl->n_gates;
+    if (N == 0 || N > 8) return 0;
+    uint64_t *cnt = (uint64_t *)malloc(sizeof(uint64_t) * G), *nxt = (uint64_t *)malloc(sizeof(uint64_t) * G);
+    if (!cnt || !nxt) {
+        free(cnt);
+        free(nxt);
+        return UINT64_MAX;
+    }
+    for (uint32_t g = 0; g < G; g++) cnt[g] = 1;
+    for (uint32_t k = 1; k < N; k++) {
+        for (uint32_t g = 0; g < G; g++) {
+            uint64_t t = 0;
+            for (uint32_t j = 0; j < nl->nfo[g]; j++) {
+                const uint64_t add = cnt[fanout(nl, g, j)];
+                t = t + add < t ? UINT64_MAX : t + add;
+            }
+            nxt[g] = t;
+        }
+        uint64_t *tmp = cnt;
+        cnt = nxt;
+        nxt = tmp;
+    }
+    uint64_t S = 0;
+    for (uint32_t g = 0; g < G; g++) S = S + cnt[g] < S ? UINT64_MAX : S + cnt[g];
+    free(cnt);
+    free(nxt);
+    if (!out || cap < S || S == UINT64_MAX) return S;
+    uint32_t path[8], idx[8];
+    uint64_t s = 0;
+    for (uint32_t g0 = 0; g0 < G; g0++) {
+        int d = 0;
+        path[0] = g0;
+        idx[0] = 0;
+        while (d >= 0) {
+            if ((uint32_t)d == N - 1) {
+                memcpy(out + s * N, path, N * sizeof(uint32_t));
+                s++;
+                d--;
+                continue;
+            }
+            const uint32_t g = path[d];
+            if (idx[d] < nl->nfo[g]) {
+                path[d + 1] = fanout(nl, g, idx[d]++);
+                idx[d + 1] = 0;
+                d++;
+            } else {
+                d--;
+            }
+        }
+    }
+    return S;
+}
+
+/* kernSegmentReduce2<N> (mergekernel.cuh:116-198): the first pair marking every
+ * net of the segment (has_marked_segment, :99-108), falling (x) or rising (y)
+ * by the value of the segment's first net (:140-143), folded with min. */
+int pdfo_merge_seg(const pdf_netlist *nl, const uint8_t *sim, const uint8_t *mark, uint64_t n_pairs,
+                   uint64_t pair_base, uint32_t N, const uint32_t *segs, uint64_t S, uint32_t *seg_fx,
+                   uint32_t *seg_fy) {
+    (void)nl;
+    for (uint64_t s = 0; s < S; s++) {
+        const uint32_t *sg = segs + s * N;
+        uint32_t fx = 0xFFFFFFFFu, fy = 0xFFFFFFFFu;
+        for (uint64_t p = 0; p < n_pairs && (fx == 0xFFFFFFFFu || fy == 0xFFFFFFFFu); p++) {
+            int all = 1;
+            for (uint32_t i = 0; i < N && all; i++) all = mark[(uint64_t)sg[i] * n_pairs + p] != 0;
+            if (!all) continue;
+            const uint32_t pid = (uint32_t)(pair_base + p);
+            if (sim[(uint64_t)sg[0] * n_pairs + p] & 1) {
+                if (fy == 0xFFFFFFFFu) fy = pid;
+            } else if (fx == 0xFFFFFFFFu) {
+                fx = pid;
+            }
+        }
+        if (fx < seg_fx[s]) seg_fx[s] = fx;
+        if (fy < seg_fy[s]) seg_fy[s] = fy;
+    }
+    return 0;
+}
+
+/* kernCover<N> (coverkernel.cuh:171-230): a pair is first at net g when it is
+ * the first pair of some segment through g (findActiveThreads, :130-154). */
+int pdfo_cover_seg(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
+                   uint32_t N, const uint32_t *segs, uint64_t S, const uint32_t *seg_fx, const uint32_t *seg_fy,
+                   uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads) {
+    uint8_t *fp = (uint8_t *)calloc((size_t)nl->n_gates * n_pairs + 1, 1);
+    if (!fp) return -1;
+    for (uint64_t s = 0; s < S; s++) {
+        const uint32_t f[2] = {seg_fx[s], seg_fy[s]};
+        for (int k = 0; k < 2; k++) {
+            if (f[k] == 0xFFFFFFFFu || f[k] < pair_base || f[k] - pair_base >= n_pairs) continue;
+            for (uint32_t i = 0; i < N; i++) fp[(uint64_t)segs[s * N + i] * n_pairs + (f[k] - pair_base)] = 1;
+        }
+    }
+    const int rc = cover_impl(nl, mark, n_pairs, pair_base, NULL, NULL, fp, lo, hi, flags, threads);
+    free(fp);
+    return rc;
+}
+
+/* The chunk loop of main.cu:171-231 with segments of length N: sim, mark,
+ * gpuMergeSegments<N>, gpuCountPaths<N> per chunk; seg_fx / seg_fy hold S
+ * entries (segments as listed by pdfo_segments). */
+int pdfo_grade_seg(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs, uint64_t pair_base,
+                   int mark_mode, uint64_t chunk, uint32_t N, const uint32_t *segs, uint64_t S, uint32_t *seg_fx,
+                   uint32_t *seg_fy, uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads) {
+    const uint32_t G = nl->n_gates;
+    const uint32_t n_pi = nl->level_offsets[1];
+    if (chunk == 0 || chunk > n_pairs) chunk = n_pairs ? n_pairs : 1;
+    uint8_t *pi = (uint8_t *)malloc((size_t)n_pi * chunk + 1);
+    uint8_t *sim = (uint8_t *)malloc((size_t)G * chunk + 1);
+    uint8_t *mark = (uint8_t *)malloc((size_t)G * chunk + 1);
+    int rc = (!pi || !sim || !mark) ? -1 : 0;
+    for (uint64_t start = 0; rc == 0 && start < n_pairs; start += chunk) {
+        const uint64_t K = n_pairs - start < chunk ? n_pairs - start : chunk;
+        for (uint32_t i = 0; i < n_pi; i++)
+            memcpy(pi + (uint64_t)i * K, pi_codes + (uint64_t)i * n_pairs + start, K);
+        pdfo_sim_mode(nl, pi, K, sim, mark_mode, threads);
+        pdfo_mark(nl, sim, K, mark_mode, mark, 1, threads);
+        pdfo_merge_seg(nl, sim, mark, K, pair_base + start, N, segs, S, seg_fx, seg_fy);
+        uint64_t clo = 0, chi = 0;
+        uint32_t cfl = 0;
+        rc = pdfo_cover_seg(nl, mark, K, pair_base + start, N, segs, S, seg_fx, seg_fy, &clo, &chi, &cfl, threads);
+        if (rc) break;
+        u128 cur = ((u128)*hi << 64) | *lo;
+        int o = 0;
+        cur = sat_add(cur, ((u128)chi << 64) | clo, &o);
+        if (o || (cfl & PDF_FLAG_OVERFLOW)) *flags |= PDF_FLAG_OVERFLOW;
+        *lo = (uint64_t)cur;
+        *hi = (uint64_t)(cur >> 64);
     }
     free(pi);
     free(sim);

@@ -63,6 +63,20 @@ int pdfo_grade(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs,
                uint64_t *lo, uint64_t *hi, uint32_t *flags, uint64_t *chunk_totals,
                int threads);
 
+/* Segments longer than one net (segs = N, 2..8): the list (count returned;
+ * out[s * N + i] written when cap >= count), the merge into per-segment first
+ * ids, the cover, and the chunk loop. */
+uint64_t pdfo_segments(const pdf_netlist *nl, uint32_t N, uint32_t *out, uint64_t cap);
+int pdfo_merge_seg(const pdf_netlist *nl, const uint8_t *sim, const uint8_t *mark, uint64_t n_pairs,
+                   uint64_t pair_base, uint32_t N, const uint32_t *segs, uint64_t S, uint32_t *seg_fx,
+                   uint32_t *seg_fy);
+int pdfo_cover_seg(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
+                   uint32_t N, const uint32_t *segs, uint64_t S, const uint32_t *seg_fx, const uint32_t *seg_fy,
+                   uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads);
+int pdfo_grade_seg(const pdf_netlist *nl, const uint8_t *pi_codes, uint64_t n_pairs, uint64_t pair_base,
+                   int mark_mode, uint64_t chunk, uint32_t N, const uint32_t *segs, uint64_t S, uint32_t *seg_fx,
+                   uint32_t *seg_fy, uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -161,3 +161,64 @@ def grade(nl, pi_codes, n_pairs: int, mode: int = 0, pair_base: int = 0, first_x
             if nl.type[g] == INPT:
                 total += paths(g, False)
     return vals, marks, fx, fy, total
+
+
+def segments(nl, N: int):
+    """Directed subpaths of exactly N nets, by first net ascending, then depth
+    first along fan-outs in edge order."""
+    out = []
+
+    def walk(path):
+        if len(path) == N:
+            out.append(tuple(path))
+            return
+        for fo in nl.fanouts(path[-1]):
+            walk(path + [int(fo)])
+
+    for g in range(nl.n_gates):
+        walk([g])
+    return out
+
+
+def grade_seg(nl, pi_codes, n_pairs: int, N: int, mode: int = 0, pair_base: int = 0):
+    """Segments of N nets: a segment's first pair marks all its nets (x/y by
+    the first net's value); a pair is credited at a net when it first-detects
+    a segment through the net; paths enumerated per pair."""
+    segs = segments(nl, N)
+    fx = [0xFFFFFFFF] * len(segs)
+    fy = [0xFFFFFFFF] * len(segs)
+    vals, marks = [], []
+    for p in range(n_pairs):
+        v = sim_pair(nl, pi_codes, p, mode)
+        m = mark_pair(nl, v, mode)
+        vals.append(v)
+        marks.append(m)
+        for k, sg in enumerate(segs):
+            if all(m[g] for g in sg):
+                if v[sg[0]] & 1:
+                    fy[k] = min(fy[k], pair_base + p)
+                else:
+                    fx[k] = min(fx[k], pair_base + p)
+    total = 0
+    lvl0 = int(nl.level_offsets[1])
+    for p in range(n_pairs):
+        pid = pair_base + p
+        m = marks[p]
+        firsts = set()
+        for k, sg in enumerate(segs):
+            if fx[k] == pid or fy[k] == pid:
+                firsts.update(sg)
+
+        def paths(g, credited):
+            if not m[g]:
+                return 0
+            cr = credited or g in firsts
+            n = 1 if (nl.po[g] == 1 and cr) else 0
+            for fo in nl.fanouts(g):
+                n += paths(int(fo), cr)
+            return n
+
+        for g in range(lvl0):
+            if nl.type[g] == INPT:
+                total += paths(g, False)
+    return segs, fx, fy, total

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_function():
 
 def test_abi_version_and_strings():
     L = P.lib()
-    assert L.pdf_abi_version() == 1
+    assert L.pdf_abi_version() == 2
     assert L.pdf_status_string(0) == b"ok"
     assert L.pdf_status_string(3) == b"path count overflow"
 

@@ -130,3 +130,41 @@ def test_fixed_marks_follow_any_fanin():
     codes = np.array([[R.S1], [R.T1]], np.uint8)
     assert O.grade(nl, codes, 1, mark_mode=0).total == 0
     assert O.grade(nl, codes, 1, mark_mode=2).total == 1
+
+
+@pytest.mark.parametrize("N", [2, 3, 5])
+@pytest.mark.parametrize("mode", [0, 2])
+def test_oracle_segments_equal_python_model(N, mode):
+    tot = 0
+    for i, (_, nl) in enumerate(SUITE[:8]):
+        rng = np.random.default_rng(31 + i)
+        codes = helpers.rand_codes(rng, nl.n_pi, 24)
+        segs, fx, fy, total = R.grade_seg(nl, codes, 24, N, mode)
+        got = O.grade_seg(nl, codes, 24, N, mark_mode=mode)
+        assert [tuple(int(x) for x in s) for s in got.segs] == segs
+        np.testing.assert_array_equal(got.first_x, np.array(fx, np.uint32))
+        np.testing.assert_array_equal(got.first_y, np.array(fy, np.uint32))
+        assert got.total == total
+        tot += total
+    assert tot > 0
+
+
+def test_segments_of_one_net_are_the_nets():
+    nl = SUITE[0][1]
+    rng = np.random.default_rng(3)
+    codes = helpers.rand_codes(rng, nl.n_pi, 50)
+    one = O.grade_seg(nl, codes, 50, 1)
+    ref = O.grade(nl, codes, 50)
+    assert one.total == ref.total
+    np.testing.assert_array_equal(one.first_x, ref.first_x)
+
+
+@pytest.mark.parametrize("chunk", [1, 7, 0])
+def test_segment_chunk_invariance(chunk):
+    nl = SUITE[1][1]
+    rng = np.random.default_rng(4)
+    codes = helpers.rand_codes(rng, nl.n_pi, 60)
+    whole = O.grade_seg(nl, codes, 60, 3)
+    part = O.grade_seg(nl, codes, 60, 3, chunk=chunk)
+    assert part.total == whole.total
+    np.testing.assert_array_equal(part.first_x, whole.first_x)
