@@ -145,12 +145,23 @@ def traffic_summary(workload: str):
 
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(P, O, nl, v, t, n_sample: int, threads: int) -> dict:
+MARK_MODES = {"default": (0, "default (LUT_NR)"), "robust": (1, "robust (LUT_R)"),
+              "fixed-robust": (2, "FIXED robust (true n-input gates)"),
+              "fixed-nonrobust": (3, "FIXED non-robust (true n-input gates)")}
+
+
+def oracle_grade(O, nl, codes, n, mode: int, segs: int, threads: int):
+    if segs > 1:
+        return O.grade_seg(nl, codes, n, segs, mark_mode=mode, threads=threads)
+    return O.grade(nl, codes, n, mark_mode=mode, threads=threads)
+
+
+def cpu_baseline(P, O, nl, v, t, n_sample: int, threads: int, mode: int = 1, segs: int = 1) -> dict:
     """The oracle (a restatement of the reference algorithm; the reference has
     no CPU implementation) on a prefix of the workload's pairs."""
     codes = P.codes_from_planes(v[:, :P.words(n_sample)], t[:, :P.words(n_sample)], n_sample)
     t0 = time.perf_counter()
-    r = O.grade(nl, codes, n_sample, mark_mode=P.MARK_ROBUST, threads=threads)
+    r = oracle_grade(O, nl, codes, n_sample, mode, segs, threads)
     dt = time.perf_counter() - t0
     return {"value": nl.n_gates * n_sample / dt, "unit": "gate-evals/s", "cores": threads, "kind": "port",
             "sample": f"first {n_sample} of the workload's pairs, {nl.n_gates} gates, "
@@ -176,12 +187,13 @@ def run_reference(args):
     G = nl.n_gates
     n_sample = min(n, args.ref_sample or (n if G * n <= 2e9 else max(32, int(6.5e8 / G) // 32 * 32)))
     codes = P.codes_from_planes(v[:, :P.words(n_sample)], t[:, :P.words(n_sample)], n_sample)
+    mode = MARK_MODES[args.mark_mode][0]
     for _ in range(args.warmup):
-        O.grade(nl, codes, n_sample, mark_mode=P.MARK_ROBUST, threads=threads)
+        oracle_grade(O, nl, codes, n_sample, mode, args.segs, threads)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.grade(nl, codes, n_sample, mark_mode=P.MARK_ROBUST, threads=threads)
+        oracle_grade(O, nl, codes, n_sample, mode, args.segs, threads)
         times.append(time.perf_counter() - t0)
     ms = 1e3 * sum(times) / len(times)
     val = nl.n_gates * n_sample / (ms / 1e3)
@@ -190,7 +202,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded)",
-        "config": workload_config(P, args.workload if args.workload not in ("c4", "c5") else args.workload + "-member", nl, n_sample),
+        "config": workload_config(P, args.workload if args.workload not in ("c4", "c5") else args.workload + "-member",
+                                  nl, n_sample, args),
         "cpu_baseline": {"value": val, "unit": "gate-evals/s", "cores": threads, "kind": "port",
                          "sample": f"first {n_sample} of {n} pairs per step"},
         "e2e": {"value": val, "unit": "gate-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -199,12 +212,18 @@ def run_reference(args):
     return 0
 
 
-def workload_config(P, name, nl, n_pairs) -> dict:
-    return {"workload": f"{name}: {nl.n_gates} gates, {nl.n_pi} PI, {int(nl.po.sum())} PO, "
-                        f"depth {nl.n_levels - 1}, {n_pairs} pairs/rank",
-            "gates": nl.n_gates, "pairs_per_rank": n_pairs, "mark_mode": "robust (LUT_R)",
-            "outputs": "path count and first-detect ids (sim/mark planes not requested)",
-            "l2": "flushed between timed steps (256 MiB write)"}
+def workload_config(P, name, nl, n_pairs, args=None) -> dict:
+    cfg = {"workload": f"{name}: {nl.n_gates} gates, {nl.n_pi} PI, {int(nl.po.sum())} PO, "
+                       f"depth {nl.n_levels - 1}, {n_pairs} pairs/rank",
+           "gates": nl.n_gates, "pairs_per_rank": n_pairs,
+           "mark_mode": MARK_MODES[args.mark_mode][1] if args else "robust (LUT_R)",
+           "outputs": "path count and first-detect ids (sim/mark planes not requested)",
+           "l2": "flushed between timed steps (256 MiB write)"}
+    if args and args.segs > 1:
+        cfg["segments"] = args.segs
+    if args and args.tile_words:
+        cfg["tile_words"] = args.tile_words
+    return cfg
 
 
 def run_ours(args):
@@ -230,7 +249,8 @@ def run_ours(args):
     v, t = P.gen_pairs(P.pair_seed(w["gen"].seed) + rank, nl.n_pi, n)
     base = rank * n
 
-    c = P.Circuit(nl, device=local, mark_mode=P.MARK_ROBUST, max_pairs=n)
+    mode = MARK_MODES[args.mark_mode][0]
+    c = P.Circuit(nl, device=local, mark_mode=mode, max_pairs=n, tile_words=args.tile_words, seg_len=args.segs)
     s = P.State(c)
     stream = torch.cuda.current_stream().cuda_stream
     dv = torch.from_numpy(v.view(np.int32)).cuda()
@@ -239,8 +259,8 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     D = _load("pdf_b200_dist", os.path.join(ROOT, "gpu-path-delay-coverage_b200", "dist.py")) if dist else None
-    fx_t = torch.empty(G, dtype=torch.int32, device="cuda")
-    fy_t = torch.empty(G, dtype=torch.int32, device="cuda")
+    fx_t = torch.empty(c.n_first, dtype=torch.int32, device="cuda")  # one id per net, or per segment
+    fy_t = torch.empty(c.n_first, dtype=torch.int32, device="cuda")
 
     # The graded quantities are the path count and the first-detect ids (what
     # fcount reports); the sim and mark planes stay inside the call.
@@ -335,7 +355,7 @@ def run_ours(args):
         "metric": "gate-evals/s", "value": value, "unit": "gate-evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
-        "config": workload_config(P, args.workload, nl, n),
+        "config": workload_config(P, args.workload, nl, n, args),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "kernel": "k_forward",
                      "kernel_ms": fwd_ms, "cover_ms": prof_ms[1] / max(1, prof_calls),
@@ -343,7 +363,8 @@ def run_ours(args):
                      "traffic": tr.get("dram_bytes_per_launch") if tr else None},
         "e2e": {"value": units / (e2e_ms_mean / 1e3), "unit": "gate-evals/s",
                 "h2d_bytes_per_step": int(2 * nl.n_pi * W * 4), "d2h_bytes_per_step": 64},
-        "gpu_launches": 3 * args.steps,  # k_forward, k_active, k_cover
+        # k_forward, k_active, k_cover; with segments k_forward, k_seg_merge, k_seg_first, k_cover
+        "gpu_launches": (4 if args.segs > 1 else 3) * args.steps,
         "clocks": clocks,
         "result_stable": bool(totals_ok),
         "batch_count": job_total,
@@ -351,7 +372,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         O = oracle()
         sample = args.cpu_sample or (n if G * n <= 2e9 else max(32, int(1.3e9 / G) // 32 * 32))
-        line["cpu_baseline"] = cpu_baseline(P, O, nl, v, t, min(n, sample), os.cpu_count() or 1)
+        line["cpu_baseline"] = cpu_baseline(P, O, nl, v, t, min(n, sample), os.cpu_count() or 1, mode, args.segs)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -585,6 +606,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2")
+    ap.add_argument("--mark-mode", choices=sorted(MARK_MODES), default="robust",
+                    help="c1-c3: sensitisation table and gate semantics")
+    ap.add_argument("--segs", type=int, default=1, help="c1-c3: path segments of this many nets (1-8)")
+    ap.add_argument("--tile-words", type=int, default=0, help="c1-c3: words per CTA column block (0 = default)")
     # CPU samples: pairs per timed CPU run (0 = the whole workload up to 2e9
     # gate-evals, else about 1.3e9 gate-evals for the baseline and 6.5e8 per
     # reference-arm step: a few seconds on the host cores)

@@ -430,7 +430,13 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         delete c;
         return PDF_ECUDA;
     }
-    c->bw = o.tile_words ? o.tile_words : 4;
+    // Default tile: 4 words (128 pairs) per CTA; 8 when the circuit's largest
+    // batch still gives at least two 8-word CTAs per SM, which halves the
+    // per-gate work of record decode and staging per pair (1M gates at
+    // 262,144 pairs: 137 ms per batch at 8 words against 165 ms at 4).
+    const uint64_t max_words = ((o.max_pairs ? o.max_pairs : 65536ull) + 31) / 32;
+    c->bw = o.tile_words ? o.tile_words
+                         : (max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u);
     const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
     uint32_t threads_default = 512;  // set from the piece size below
     const size_t budget = c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
