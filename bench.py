@@ -244,7 +244,7 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     w = P.WORKLOADS[args.workload]
     nl = P.gen_netlist(w["gen"])
-    n = w["pairs"]
+    n = args.pairs or w["pairs"]
     G, W = nl.n_gates, P.words(n)
     v, t = P.gen_pairs(P.pair_seed(w["gen"].seed) + rank, nl.n_pi, n)
     base = rank * n
@@ -610,6 +610,8 @@ def main():
                     help="c1-c3: sensitisation table and gate semantics")
     ap.add_argument("--segs", type=int, default=1, help="c1-c3: path segments of this many nets (1-8)")
     ap.add_argument("--tile-words", type=int, default=0, help="c1-c3: words per CTA column block (0 = default)")
+    ap.add_argument("--pairs", type=int, default=0,
+                    help="c1-c3: pairs per rank instead of the workload's (small cases for profiling)")
     # CPU samples: pairs per timed CPU run (0 = the whole workload up to 2e9
     # gate-evals, else about 1.3e9 gate-evals for the baseline and 6.5e8 per
     # reference-arm step: a few seconds on the host cores)

@@ -117,6 +117,7 @@ _lib = None
 ABI = [
     ("pdf_status_string", C.c_char_p, [C.c_int]),
     ("pdf_abi_version", C.c_int, []),
+    ("pdf_last_error", C.c_char_p, []),
     ("pdf_netlist_check", C.c_int, [C.POINTER(Netlist_t), C.c_char_p, C.c_size_t]),
     ("pdf_circuit_create", C.c_int, [C.POINTER(Netlist_t), C.POINTER(CircuitOpts_t), C.POINTER(C.c_void_p)]),
     ("pdf_circuit_destroy", None, [C.c_void_p]),
@@ -205,6 +206,8 @@ def lib() -> C.CDLL:
 
 def check(status: int, what: str) -> None:
     if status != 0:
+        if status in (2, 5):  # ENOMEM, ECUDA: name the CUDA call behind it
+            what = f"{what} [{lib().pdf_last_error().decode(errors='replace')}]"
         raise PdfError(status, what)
 
 

@@ -20,10 +20,18 @@
 namespace {
 
 
+// The last failing CUDA call of this thread, for pdf_last_error().
+thread_local char g_last_error[256];
+static void note_cuda_error(cudaError_t e, const char *call, int line) {
+    std::snprintf(g_last_error, sizeof g_last_error, "%s (%d) at pdf_api.cpp:%d: %.160s", cudaGetErrorName(e),
+                  (int)e, line, call);
+}
+
 #define PDF_CUDA(call)                                  \
     do {                                                \
         cudaError_t e_ = (call);                        \
         if (e_ != cudaSuccess) {                        \
+            note_cuda_error(e_, #call, __LINE__);       \
             (void)cudaGetLastError();                   \
             return e_ == cudaErrorMemoryAllocation ? PDF_ENOMEM : PDF_ECUDA; \
         }                                               \
@@ -156,6 +164,8 @@ void prof_release(std::vector<ProfEvents> &v) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+
+extern "C" const char *pdf_last_error(void) { return g_last_error; }
 
 extern "C" const char *pdf_status_string(int s) {
     switch (s) {
@@ -439,9 +449,12 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
                          : (max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u);
     const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
     uint32_t threads_default = 512;  // set from the piece size below
-    const size_t budget = c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
-                                      : std::min<size_t>((size_t)prop.sharedMemPerBlockOptin,
-                                                         (size_t)prop.sharedMemPerMultiprocessor / 2 - 2048);
+    // dynamic shared memory of the forward kernels; 1 KiB stays for their
+    // static shared variables (the batched kernel keeps its arguments there)
+    const size_t budget = (c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
+                                       : std::min<size_t>((size_t)prop.sharedMemPerBlockOptin,
+                                                          (size_t)prop.sharedMemPerMultiprocessor / 2 - 2048)) -
+                          1024;
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
     // Pieces (the kernels' unit of staging and of synchronisation), sized
@@ -547,6 +560,9 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     // the ring's memory also holds the reverse pass's row staging buffers
     const size_t rows_bytes = (size_t)2 * c->cap * 2 * c->bw * 4;
     auto ring_bytes = [&](size_t R) { return std::max(R * c->bw * 12, rows_bytes); };
+    // The largest ring that fits wins: a smaller ring with longer far lists
+    // was measured slower (1M gates, 5,000-gate levels: 116.8 against 109.9
+    // ms) although it leaves fewer fan-ins to plane-row reads.
     uint32_t ring = 0;
     for (uint32_t R = rmax; R >= rmin && !ring; R /= 2)
         if (fixed + al(std::max(edge_bytes, 64 * far_entry)) + ring_bytes(R) <= budget) ring = R;

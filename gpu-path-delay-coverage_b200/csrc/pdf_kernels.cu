@@ -488,7 +488,9 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
             uint32_t *d = S.far + (size_t)fb * 3 * fplane + (size_t)e * BW;
             cp_async_vec<BW>(d, a.V + o);
             cp_async_vec<BW>(d + fplane, a.T + o);
-            if (MODE != FWD_SIM) cp_async_vec<BW>(d + 2 * fplane, a.M + o);
+            // the reference modes read a fan-in's mark only when its bitmap
+            // bit is set, and unmarked rows are not written (below)
+            if (MODE != FWD_SIM && (FIX || a.store_all || bit_test(S.bm, f))) cp_async_vec<BW>(d + 2 * fplane, a.M + o);
         }
     };
 
@@ -582,7 +584,7 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
             if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
                 if (h & RF_INPT) {
                     M = T;
-                } else if ((h & RF_MARKF0) && vany(T) && (!a.bm_shared || bit_test(S.bm, r.w[7]))) {
+                } else if ((h & RF_MARKF0) && vany(T) && bit_test(S.bm, r.w[7])) {
                     // fan-in 0 (gate w[7]) holds a mark: its bitmap bit is set
                     const Vec<BW> m0 = load(r.w[3], 2);
 #pragma unroll
@@ -620,7 +622,9 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
                     vst<BW>(a.V + o, V);
                     vst<BW>(a.T + o, T);
                 }
-                if (MODE != FWD_SIM) vst<BW>(a.M + o, M);
+                // an unmarked row stays unwritten: its readers (fan-outs in the
+                // reference modes, prune, merge, cover) test the bitmap first
+                if (MODE != FWD_SIM && (FIX || a.store_all || marked)) vst<BW>(a.M + o, M);
             }
             const uint32_t slot = (g & Rm) * BW;
             vst<BW>(rV + slot, V);

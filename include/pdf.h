@@ -187,6 +187,9 @@ typedef struct pdf_circuit_info {
 } pdf_circuit_info;
 
 const char *pdf_status_string(int status);
+/* The last CUDA failure behind a PDF_ECUDA / PDF_ENOMEM of this thread: the
+ * CUDA error name and number and the failing call ("" if none yet). */
+const char *pdf_last_error(void);
 int pdf_abi_version(void);
 
 /* Host-side structural check of a netlist (no device needed).  On failure a
