@@ -225,25 +225,32 @@ __device__ __forceinline__ bool vany(const Vec<BW> &v) {
 // with robust()/nonrobust(), :43-72) in one pass over its nfi fan-ins
 // (sens_step, pdf_device.cuh).  fetch(q, V, T) reads fan-in q; fan-ins 0..3
 // are unrolled.
+// The two-term table (LUT_NR) keeps 8 accumulator words per pair word, so
+// wide tiles take the fan-ins in passes of two words (fan-ins re-read from
+// shared memory) to stay within the launch bound's registers.
 template <int BW, int ROBUST, class Fetch>
 __device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, uint32_t nfi, Fetch fetch) {
     const bool or_like = (r.w[0] & RF_IM) != 0;
-    SensAcc acc[BW];
-#pragma unroll
-    for (int j = 0; j < BW; j++) sens_init(acc[j]);
-    auto step = [&](uint32_t q) {
-        Vec<BW> v, t;
-        fetch(q, v, t);
-#pragma unroll
-        for (int j = 0; j < BW; j++) sens_step<ROBUST>(acc[j], or_like, v.x[j], t.x[j]);
-    };
-#pragma unroll
-    for (int q = 0; q < kInlineFanins; q++)
-        if ((uint32_t)q < nfi) step(q);
-    for (uint32_t q = kInlineFanins; q < nfi; q++) step(q);
+    constexpr int SUB = (ROBUST || BW <= 2) ? BW : 2;
     Vec<BW> out;
 #pragma unroll
-    for (int j = 0; j < BW; j++) out.x[j] = sens_result<ROBUST>(acc[j]);
+    for (int j0 = 0; j0 < BW; j0 += SUB) {
+        SensAcc acc[SUB];
+#pragma unroll
+        for (int j = 0; j < SUB; j++) sens_init(acc[j]);
+        auto step = [&](uint32_t q) {
+            Vec<BW> v, t;
+            fetch(q, v, t);
+#pragma unroll
+            for (int j = 0; j < SUB; j++) sens_step<ROBUST>(acc[j], or_like, v.x[j0 + j], t.x[j0 + j]);
+        };
+#pragma unroll
+        for (int q = 0; q < kInlineFanins; q++)
+            if ((uint32_t)q < nfi) step(q);
+        for (uint32_t q = kInlineFanins; q < nfi; q++) step(q);
+#pragma unroll
+        for (int j = 0; j < SUB; j++) out.x[j0 + j] = sens_result<ROBUST>(acc[j]);
+    }
     return out;
 }
 
@@ -252,22 +259,27 @@ __device__ __forceinline__ Vec<BW> sens_any(const GateRec &r, uint32_t nfi, Fetc
 template <int BW, int NONROBUST, class Fetch3>
 __device__ __forceinline__ Vec<BW> sens_any_fixed(const GateRec &r, uint32_t nfi, Fetch3 fetch) {
     const uint32_t mor = flagmask(r.w[0], RF_IM), mxor = flagmask(r.w[0], RF_XOR), mand = ~(mor | mxor);
-    SensAcc acc[BW];
-#pragma unroll
-    for (int j = 0; j < BW; j++) sens_init(acc[j]);
-    auto step = [&](uint32_t q) {
-        Vec<BW> v, t, m;
-        fetch(q, v, t, m);
-#pragma unroll
-        for (int j = 0; j < BW; j++) sens_step_fixed<NONROBUST>(acc[j], mand, mor, mxor, v.x[j], t.x[j], m.x[j]);
-    };
-#pragma unroll
-    for (int q = 0; q < kInlineFanins; q++)
-        if ((uint32_t)q < nfi) step(q);
-    for (uint32_t q = kInlineFanins; q < nfi; q++) step(q);
+    constexpr int SUB = (NONROBUST || BW <= 2) ? BW : 2;  // passes of two words, as sens_any
     Vec<BW> out;
 #pragma unroll
-    for (int j = 0; j < BW; j++) out.x[j] = sens_result<NONROBUST>(acc[j]);
+    for (int j0 = 0; j0 < BW; j0 += SUB) {
+        SensAcc acc[SUB];
+#pragma unroll
+        for (int j = 0; j < SUB; j++) sens_init(acc[j]);
+        auto step = [&](uint32_t q) {
+            Vec<BW> v, t, m;
+            fetch(q, v, t, m);
+#pragma unroll
+            for (int j = 0; j < SUB; j++)
+                sens_step_fixed<NONROBUST>(acc[j], mand, mor, mxor, v.x[j0 + j], t.x[j0 + j], m.x[j0 + j]);
+        };
+#pragma unroll
+        for (int q = 0; q < kInlineFanins; q++)
+            if ((uint32_t)q < nfi) step(q);
+        for (uint32_t q = kInlineFanins; q < nfi; q++) step(q);
+#pragma unroll
+        for (int j = 0; j < SUB; j++) out.x[j0 + j] = sens_result<NONROBUST>(acc[j]);
+    }
     return out;
 }
 
