@@ -180,6 +180,14 @@ def test_dump_layouts(tmp_path):
                                         "Gate 3:\t   7,3 \n")
 
 
+def test_segment_dump_layout(tmp_path):
+    """debugSegmentList (mergekernel.cuh:25-46): Segment s(g0,...): x,y"""
+    path = str(tmp_path / "seg.log")
+    segs = np.array([[0, 3, 7], [1, 3, 7]], np.uint32)
+    P.dump_segments(path, segs, np.array([5, P.NONE], np.uint32), np.array([P.NONE, 2], np.uint32))
+    assert open(path).read() == "Segment 0(0,3,7): 5,-1 \nSegment 1(1,3,7): -1,2 \n"
+
+
 def test_cli_usage_and_errors(tmp_path):
     if not os.path.exists(FCOUNT):
         pytest.skip("fcount not built")
