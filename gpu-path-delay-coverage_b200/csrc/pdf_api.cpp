@@ -115,6 +115,7 @@ struct pdf_circuit {
     uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
     size_t fwd_smem = 0;
     uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
+    uint32_t occ = 1;  // forward CTAs per SM its registers and shared memory are sized for
     Workspace stage;  // scratch of the stage calls
     std::mutex mu;    // serialises the stage scratch
     // segments longer than one net
@@ -449,12 +450,6 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
                          : (max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u);
     const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
     uint32_t threads_default = 512;  // set from the piece size below
-    // dynamic shared memory of the forward kernels; 1 KiB stays for their
-    // static shared variables (the batched kernel keeps its arguments there)
-    const size_t budget = (c->bw >= 8 ? (size_t)prop.sharedMemPerBlockOptin
-                                       : std::min<size_t>((size_t)prop.sharedMemPerBlockOptin,
-                                                          (size_t)prop.sharedMemPerMultiprocessor / 2 - 2048)) -
-                          1024;
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
     // Pieces (the kernels' unit of staging and of synchronisation), sized
@@ -469,6 +464,24 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     // issue the next piece's far-row copies
     threads_default = std::min<uint32_t>(max_threads, c->cap + 64);
     c->threads = o.threads ? std::min(o.threads, max_threads) : threads_default;
+    // CTAs per SM that the registers allow for this block size (at most 4);
+    // the dynamic shared memory of the forward kernels is then an equal share
+    // of the SM, less 1 KiB per CTA the system keeps and 1 KiB for the
+    // kernels' static variables (the batched kernel keeps its arguments there).
+    {
+        const int regs = forward_kernel_regs(c->bw, c->mark_mode);
+        if (regs <= 0) {
+            delete c;
+            return PDF_ECUDA;
+        }
+        const uint32_t warps = (c->threads + 31) / 32;
+        const uint32_t warp_regs = ((uint32_t)regs * 32 + 255) & ~255u;
+        uint32_t occ = std::min<uint32_t>(65536 / (warps * warp_regs), 2048 / (warps * 32));
+        c->occ = std::max<uint32_t>(1, std::min<uint32_t>(occ, 4));
+    }
+    const size_t budget = std::min<size_t>((size_t)prop.sharedMemPerBlockOptin,
+                                           (size_t)prop.sharedMemPerMultiprocessor / c->occ - 1024) -
+                          1024;
     c->ecap = 2048;
     std::vector<Piece> pieces;
     auto f4 = [](uint64_t x) { return x & ~(uint64_t)3; };
@@ -1406,8 +1419,20 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     L.bw = c0->bw;
     L.sem = (uint32_t)c0->mark_mode;
     L.hash_cap = c0->hash_cap;
-    for (uint32_t i = 0; i < n_jobs; i++) {
-        const pdf_batch_job &j = jobs[i];
+    // Jobs in classes of equal CTAs per SM (1, 2, 4), each class one forward
+    // launch sized for its members, so the CTAs of narrow circuits share SMs
+    // instead of holding the shared memory of the widest member; within a
+    // class the longest level chains go first.
+    std::vector<uint32_t> order(n_jobs);
+    for (uint32_t i = 0; i < n_jobs; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        const pdf_circuit *cx = jobs[x].circuit, *cy = jobs[y].circuit;
+        if (cx->occ != cy->occ) return cx->occ < cy->occ;
+        return cx->n_pieces > cy->n_pieces;
+    });
+    for (uint32_t k = 0; k < n_jobs; k++) {
+        const pdf_batch_job &j = jobs[order[k]];
+        const uint32_t i = k;
         pdf_circuit *c = j.circuit;
         pdf_state *s = j.state;
         const uint64_t n = j.pairs.n_pairs, W = (n + 31) / 32, G = c->info.n_gates;
@@ -1440,12 +1465,22 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         L.threads = std::max(L.threads, c->threads);
         L.fwd_smem = std::max(L.fwd_smem, c->fwd_smem);
         L.cover_grid = std::max(L.cover_grid, c->cover_grid);
+        if (!L.n_class || L.cls[L.n_class - 1].occ != c->occ) {
+            BatchClass &k2 = L.cls[L.n_class++];
+            k2.occ = c->occ;
+            k2.blk0 = bp[i];
+        }
+        BatchClass &cl = L.cls[L.n_class - 1];
+        cl.threads = std::max(cl.threads, c->threads);
+        cl.smem = std::max(cl.smem, c->fwd_smem);
         b->gate_evals += G * n;
         b->circuits.push_back(c);
         b->states.push_back(s);
     }
     L.n = n_jobs;
     L.total_blocks = bp[n_jobs];
+    for (uint32_t k = 0; k < L.n_class; k++)
+        L.cls[k].blocks = (k + 1 < L.n_class ? L.cls[k + 1].blk0 : L.total_blocks) - L.cls[k].blk0;
     L.total_gates = gp[n_jobs];
     L.append = (flags & PDF_BATCH_APPEND) ? 1u : 0u;
     b->use_graph = !(flags & PDF_BATCH_NO_GRAPH);

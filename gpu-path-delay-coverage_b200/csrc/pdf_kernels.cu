@@ -1148,16 +1148,19 @@ __device__ __forceinline__ uint32_t prefix_find(const uint32_t *pref, uint32_t n
     return lo;
 }
 
+// One launch per class of circuits (equal CTAs per SM): this launch's CTAs
+// are the batch's CTAs blk0 .. blk0 + gridDim.x - 1.
 template <int BW, int SEM>
 __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
-    k_batch_forward(const FwdArgs *args, const uint32_t *bpref, uint32_t n, BatchCtl *ctl) {
+    k_batch_forward(const FwdArgs *args, const uint32_t *bpref, uint32_t n, BatchCtl *ctl, uint32_t blk0) {
     __shared__ FwdArgs s_a;
     __shared__ uint32_t s_blk;
     if (threadIdx.x == 0) {
-        const uint32_t ci = prefix_find(bpref, n, blockIdx.x);
+        const uint32_t gb = blk0 + blockIdx.x;
+        const uint32_t ci = prefix_find(bpref, n, gb);
         s_a = args[ci];
-        s_blk = blockIdx.x - __ldg(bpref + ci);
-        if (blockIdx.x == 0) {
+        s_blk = gb - __ldg(bpref + ci);
+        if (gb == 0) {
             ctl->n_items = 0;
             ctl->done = 0;
             ctl->err = 0;
@@ -1301,6 +1304,39 @@ cudaError_t launch_fwd_bw(const FwdArgs &a, int mode, int sem, uint32_t threads,
 }  // namespace
 
 
+namespace {
+template <int BW, int SEM>
+int regs_t() {
+    cudaFuncAttributes fa{}, fb{};
+    if (cudaFuncGetAttributes(&fa, k_forward<BW, SEM, FWD_FUSED>) != cudaSuccess ||
+        cudaFuncGetAttributes(&fb, k_batch_forward<BW, SEM>) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return -1;
+    }
+    return std::max(fa.numRegs, fb.numRegs);
+}
+template <int BW>
+int regs_bw(int sem) {
+    switch (sem) {
+        case 0: return regs_t<BW, 0>();
+        case 1: return regs_t<BW, 1>();
+        case 2: return regs_t<BW, 2>();
+        case 3: return regs_t<BW, 3>();
+        default: return -1;
+    }
+}
+}  // namespace
+
+int forward_kernel_regs(int bw, int sem) {
+    switch (bw) {
+        case 1: return regs_bw<1>(sem);
+        case 2: return regs_bw<2>(sem);
+        case 4: return regs_bw<4>(sem);
+        case 8: return regs_bw<8>(sem);
+        default: return -1;
+    }
+}
+
 cudaError_t launch_forward(const FwdArgs &a, int mode, int sem, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st) {
     switch (bw) {
@@ -1337,8 +1373,10 @@ cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bo
 
 template <int BW, int SEM>
 cudaError_t prepare_batch_t(const BatchLaunch &b) {
+    size_t smem = 0;
+    for (uint32_t k = 0; k < b.n_class; k++) smem = std::max(smem, b.cls[k].smem);
     cudaError_t e = cudaFuncSetAttribute(k_batch_forward<BW, SEM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)b.fwd_smem);
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_batch_cover, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)cover_smem_bytes(b.hash_cap));
@@ -1346,9 +1384,13 @@ cudaError_t prepare_batch_t(const BatchLaunch &b) {
 
 template <int BW, int SEM>
 cudaError_t launch_batch_t(const BatchLaunch &b, cudaStream_t st) {
-    k_batch_forward<BW, SEM><<<b.total_blocks, b.threads, b.fwd_smem, st>>>(b.fargs, b.bpref, b.n, b.ctl);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    cudaError_t e = cudaSuccess;
+    for (uint32_t k = 0; k < b.n_class; k++) {
+        const BatchClass &c = b.cls[k];
+        if (!c.blocks) continue;
+        k_batch_forward<BW, SEM><<<c.blocks, c.threads, c.smem, st>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     k_batch_active<<<(b.total_gates + 255) / 256, 256, 0, st>>>(b.cargs, b.gpref, b.n, b.items, b.ctl);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_batch_cover<<<b.cover_grid, 256, cover_smem_bytes(b.hash_cap), st>>>(b.cargs, b.fargs, b.n, b.items, b.ctl,

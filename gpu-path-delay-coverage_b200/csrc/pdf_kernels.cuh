@@ -122,6 +122,11 @@ struct BatchCtl {
     unsigned int err;      // OR of every circuit's device error word after the pass
     unsigned int pad;
 };
+// One forward launch of a batch: jobs of equal CTAs per SM.
+struct BatchClass {
+    uint32_t occ, blk0, blocks, threads;
+    size_t smem;
+};
 struct BatchLaunch {
     FwdArgs *fargs;        // [n] per circuit, device
     CoverArgs *cargs;      // [n] per circuit, device
@@ -132,7 +137,11 @@ struct BatchLaunch {
     uint32_t n, total_blocks, total_gates;
     uint32_t bw, sem, threads, cover_grid, hash_cap, append;  // sem: PDF_MARK_*
     size_t fwd_smem;
+    uint32_t n_class;      // forward launches: classes of jobs (at most 3: 1, 2, 4 CTAs per SM)
+    BatchClass cls[4];
 };
+// Registers per thread of the fused forward kernel for (tile words, mode); <= 0 on error.
+int forward_kernel_regs(int bw, int sem);
 cudaError_t prepare_batch(const BatchLaunch &b);  // kernel attributes; call before launching or capturing
 cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st);
 
