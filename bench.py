@@ -504,7 +504,7 @@ def run_batched(args):
                      "peak_source": peaks["source"] + " (hbm_gbs)", "traffic": None},
         "e2e": {"value": units / (e2e_ms / 1e3), "unit": "gate-evals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": 64 * len(jobs)},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": int(info.launches) * args.steps,  # forward per occupancy class, active, cover
         "clocks": clocks,
         "result_stable": bool(same),
     }
@@ -586,10 +586,12 @@ def run_served(args):
         "latency_ms": {"p50": st.lat_p50_ms, "p99": st.lat_p99_ms, "max": st.lat_max_ms,
                        "per": "job batch, from ready (submission or previous batch) to result"},
         "wall_s": wall, "busy_s": st.busy_s, "batches": int(st.batches),
+        # the arrival stream caps throughput: all the work over the span of the arrivals
+        "offered_load": units / float(arrivals[-1]),
         "e2e": {"value": units / wall, "unit": "gate-evals/s",
                 "h2d_bytes_per_step": int(sum(2 * nl.n_pi * (per_job // 32) * 4 for nl, _, _ in jobs) / max(1, st.steps)),
                 "d2h_bytes_per_step": 64},
-        "gpu_launches": 3 * int(st.steps),
+        "gpu_launches": int(st.launches),
         "clocks": clocks,
         "result_stable": bool(same),
     }

@@ -80,7 +80,8 @@ class BatchJob_t(C.Structure):
 
 class BatchInfo_t(C.Structure):
     _fields_ = [("n_jobs", C.c_uint32), ("tile_words", C.c_uint32), ("threads", C.c_uint32),
-                ("ctas", C.c_uint32), ("gate_evals", C.c_uint64), ("device_bytes", C.c_uint64)]
+                ("ctas", C.c_uint32), ("gate_evals", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("launches", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class ServerOpts_t(C.Structure):
@@ -93,7 +94,7 @@ class ServerStats_t(C.Structure):
     _fields_ = [("jobs_done", C.c_uint64), ("jobs_active", C.c_uint64), ("jobs_queued", C.c_uint64),
                 ("batches", C.c_uint64), ("steps", C.c_uint64), ("gate_evals", C.c_uint64),
                 ("busy_s", C.c_double), ("lat_p50_ms", C.c_double), ("lat_p99_ms", C.c_double),
-                ("lat_max_ms", C.c_double), ("bytes_in_use", C.c_uint64)]
+                ("lat_max_ms", C.c_double), ("bytes_in_use", C.c_uint64), ("launches", C.c_uint64)]
 
 
 class CircuitInfo_t(C.Structure):

@@ -328,6 +328,8 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         srv->dirty = false;
     }
     if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
+    pdf_batch_info bi{};
+    if (pdf_batch_query(srv->batch, &bi) == PDF_OK) srv->st.launches += bi.launches;
     const double t1 = now_s();
     srv->st.steps++;
     // account, advance, retire

@@ -371,6 +371,8 @@ typedef struct pdf_batch_info {
     uint32_t n_jobs, tile_words, threads, ctas;
     uint64_t gate_evals; /* per run: sum over jobs of n_gates * n_pairs */
     uint64_t device_bytes;
+    uint32_t launches;   /* kernel launches per run: one forward launch per occupancy class, then two */
+    uint32_t reserved;
 } pdf_batch_info;
 pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out);
 void pdf_batch_destroy(pdf_batch *b);
@@ -433,6 +435,7 @@ typedef struct pdf_server_stats {
     double busy_s;          /* time inside pdf_server_step */
     double lat_p50_ms, lat_p99_ms, lat_max_ms; /* per-batch latency */
     uint64_t bytes_in_use;
+    uint64_t launches;      /* kernel launches of the batched passes */
 } pdf_server_stats;
 pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server **out);
 void pdf_server_destroy(pdf_server *srv);
