@@ -112,7 +112,7 @@ struct pdf_circuit {
     DevCircuit dc{};
     uint32_t bw = 4, threads = 512, ring = 0, ring2 = 0, farcap = 0;
     uint32_t cap = 512, ecap = 2048, n_pieces = 0, bm_shared = 0;
-    uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
+    uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_fid = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
     size_t fwd_smem = 0;
     uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
     uint32_t occ = 1;  // forward CTAs per SM its registers and shared memory are sized for
@@ -464,6 +464,9 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     // issue the next piece's far-row copies
     threads_default = std::min<uint32_t>(max_threads, c->cap + 64);
     c->threads = o.threads ? std::min(o.threads, max_threads) : threads_default;
+    // a block size given by the caller also bounds the pieces: threads - 64
+    // gates, so two warps stay free for the far-row copies
+    if (o.threads && c->threads >= 128) c->cap = std::min(c->cap, (c->threads - 64) & ~31u);
     // CTAs per SM that the registers allow for this block size (at most 4);
     // the dynamic shared memory of the forward kernels is then an equal share
     // of the SM, less 1 KiB per CTA the system keeps and 1 KiB for the
@@ -553,7 +556,11 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
             p.far_off = (uint32_t)far_ids.size();
             p.far_n = (uint32_t)list.size();
             far_ids.insert(far_ids.end(), list.begin(), list.end());
+            // lists start on 16-byte boundaries: the kernel stages the next
+            // piece's list by a bulk copy located from this piece's fields
+            while (far_ids.size() & 3) far_ids.push_back(0);
         }
+        for (size_t i = 0; i < pieces.size(); i++) pieces[i].nfar_n = i + 1 < pieces.size() ? pieces[i + 1].far_n : 0;
         return worst;
     };
     // Shared memory of k_forward: 2 record buffers; one region holding the
@@ -576,17 +583,21 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     // The largest ring that fits wins: a smaller ring with longer far lists
     // was measured slower (1M gates, 5,000-gate levels: 116.8 against 109.9
     // ms) although it leaves fewer fan-ins to plane-row reads.
+    // far region (far rows of two pieces, or the reverse pass's edges) and
+    // the two staged far-id lists, for lists of n entries
+    auto far_bytes = [&](size_t n) { return al(std::max(edge_bytes, n * far_entry)) + al(2 * n * 4); };
     uint32_t ring = 0;
     for (uint32_t R = rmax; R >= rmin && !ring; R /= 2)
-        if (fixed + al(std::max(edge_bytes, 64 * far_entry)) + ring_bytes(R) <= budget) ring = R;
+        if (fixed + far_bytes(64) + ring_bytes(R) <= budget) ring = R;
     if (!ring) {
         delete c;
         return PDF_ENOTSUP;
     }
     const size_t far_room = budget - fixed - ring_bytes(ring);
-    const uint32_t far_limit = (uint32_t)std::min<size_t>(kMaxFar, (far_room & ~(size_t)127) / far_entry) & ~3u;
+    uint32_t far_limit = (uint32_t)std::min<size_t>(kMaxFar, far_room / (far_entry + 8)) & ~3u;
+    while (far_limit > 64 && far_bytes(far_limit) > far_room) far_limit -= 4;
     const uint32_t farcap = std::max<uint32_t>(4, (far_lists(ring, far_limit) + 3) & ~3u);
-    if (far_ids.empty()) far_ids.push_back(0);
+    while (far_ids.size() < 4) far_ids.push_back(0);
     c->ring = ring;
     c->farcap = farcap;
     size_t off = 0;
@@ -594,6 +605,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     off += rec_bytes;
     c->off_edge = (uint32_t)off;
     off += al(std::max(edge_bytes, farcap * far_entry));
+    c->off_fid = (uint32_t)off;
+    off += al(2 * (size_t)farcap * 4);
     c->bm_shared = bm_bytes ? 1u : 0u;
     c->off_bm = (uint32_t)off;
     off += bm_bytes;
@@ -896,6 +909,7 @@ FwdArgs base_fwd(pdf_circuit *c, uint64_t n_pairs) {
     a.off_ring = c->off_ring;
     a.off_rec = c->off_rec;
     a.off_edge = c->off_edge;
+    a.off_fid = c->off_fid;
     a.off_bm = c->off_bm;
     a.off_pbits = c->off_pbits;
     a.off_mbar = c->off_mbar;

@@ -259,7 +259,7 @@ struct __align__(16) Piece {
     uint32_t level;
     uint32_t far_off;  // its far fan-ins: far_ids[far_off .. far_off + far_n)
     uint32_t far_n;    // <= kMaxFar
-    uint32_t pad;
+    uint32_t nfar_n;   // far_n of the next piece, whose list starts at far_off + far_n rounded up to 4
 };
 
 // Saturating 128-bit add; sets *ovf on overflow.

@@ -117,22 +117,28 @@ struct FwdSmem {
     GateRec *rec;     // [2][cap] staged gate records of a piece
     uint32_t *edge;   // reverse: [2][ecap] staged edge slices
     uint32_t *far;    // forward: [2][3][farcap][BW] far fan-in V, T, M (same memory as edge)
+    uint32_t *fid;    // forward: [2][farcap] far-id lists staged with the records
     uint32_t *bm;     // nonzero-mark bitmap (shared or global)
     uint32_t *pbits;  // pieces that hold a forward mark
     uint64_t *mbar;   // [2]
 };
 
 // Stage piece `p` into buffer `buf`: its gate records and, for the reverse
-// pass, its edge slice.  Called by one thread.
+// pass, its edge slice; for the forward pass, the far-id list of the piece
+// after it (lists are stored in piece order, each padded to 4 entries, so it
+// starts at p.far_off + 4 * ceil(p.far_n / 4)).  Called by one thread.
 __device__ __forceinline__ void stage_piece(const FwdArgs &a, const FwdSmem &S, const Piece &p, int buf,
                                             bool edges) {
     const uint32_t rb = (p.b - p.a) * (uint32_t)sizeof(GateRec);
     const bool e = edges && p.ea != 0xFFFFFFFFu;
     const uint32_t eb = e ? (p.eb - p.ea) * 4u : 0u;
+    const uint32_t fb = edges ? 0u : ((p.nfar_n + 3u) & ~3u) * 4u;
     fence_proxy_async();
-    mbar_expect_tx(S.mbar + buf, rb + eb);
+    mbar_expect_tx(S.mbar + buf, rb + eb + fb);
     bulk_g2s(S.rec + (size_t)buf * a.cap, a.c.rec + p.a, rb, S.mbar + buf);
     if (e) bulk_g2s(S.edge + (size_t)buf * a.ecap, a.c.edges + p.ea, eb, S.mbar + buf);
+    if (fb)
+        bulk_g2s(S.fid + (size_t)buf * a.farcap, a.far_ids + p.far_off + ((p.far_n + 3u) & ~3u), fb, S.mbar + buf);
 }
 
 // BW consecutive words of one plane row, moved with 16-byte (or 8-byte)
@@ -321,18 +327,26 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
     int cur = prev_marked((int)a.n_pieces);
     uint32_t maxlvl = 0;
     int sbuf = 0;
+    // descriptors of the current and the next marked piece; the one after
+    // is loaded a piece ahead, so its latency hides behind a piece's work
+    Piece Pc{}, Pn{};
     if (cur >= 0) {
-        if (threadIdx.x == 0) stage_piece(a, S, a.pieces[cur], 0, true);
-        stage_rows(a.pieces[cur], 0);
+        Pc = a.pieces[cur];
+        if (threadIdx.x == 0) stage_piece(a, S, Pc, 0, true);
+        stage_rows(Pc, 0);
         cp_async_wait_all();
     }
+    int nxt = cur >= 0 ? prev_marked(cur) : -1;
+    if (nxt >= 0) Pn = a.pieces[nxt];
     while (cur >= 0) {
-        const int nxt = prev_marked(cur);
-        const Piece P = a.pieces[cur];
+        const Piece P = Pc;
         if (nxt >= 0) {
-            if (threadIdx.x == 0) stage_piece(a, S, a.pieces[nxt], sbuf ^ 1, true);
-            stage_rows(a.pieces[nxt], sbuf ^ 1);
+            if (threadIdx.x == 0) stage_piece(a, S, Pn, sbuf ^ 1, true);
+            stage_rows(Pn, sbuf ^ 1);
         }
+        const int nxt2 = nxt >= 0 ? prev_marked(nxt) : -1;
+        Piece Pn2{};
+        if (nxt2 >= 0) Pn2 = a.pieces[nxt2];
         const bool ok = mbar_wait(S.mbar + sbuf, (phase >> sbuf) & 1u);
         phase ^= 1u << sbuf;
         if (__syncthreads_or(!ok)) {
@@ -395,6 +409,9 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
         cp_async_wait_all();  // this thread's rows for the next piece
         if (__syncthreads_or(any) && P.level + 1 > maxlvl) maxlvl = P.level + 1;
         cur = nxt;
+        nxt = nxt2;
+        Pc = Pn;
+        Pn = Pn2;
         sbuf ^= 1;
     }
     if (failed) {
@@ -447,6 +464,7 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
     S.rec = reinterpret_cast<GateRec *>(smraw + a.off_rec);
     S.edge = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
     S.far = reinterpret_cast<uint32_t *>(smraw + a.off_edge);
+    S.fid = reinterpret_cast<uint32_t *>(smraw + a.off_fid);
     S.pbits = reinterpret_cast<uint32_t *>(smraw + a.off_pbits);
     S.mbar = reinterpret_cast<uint64_t *>(smraw + a.off_mbar);
     const uint32_t w0 = blk * BW;
@@ -490,12 +508,12 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
     }
     __syncthreads();
 
-    // Copy the far fan-ins of piece Q into far buffer fb; entry e goes to
-    // thread blockDim - 1 - e, a thread without a gate when the piece
-    // running now is smaller than the CTA.
-    auto prefetch = [&](const Piece &Q, uint32_t fb) {
-        for (uint32_t e = blockDim.x - 1 - threadIdx.x; e < Q.far_n; e += blockDim.x) {
-            const uint32_t f = __ldg(a.far_ids + Q.far_off + e);
+    // Copy the n far fan-ins listed at ids (shared memory) into far buffer
+    // fb; entry e goes to thread blockDim - 1 - e, a thread without a gate
+    // when the piece running now is smaller than the CTA.
+    auto prefetch = [&](uint32_t n, uint32_t fb, const uint32_t *ids) {
+        for (uint32_t e = blockDim.x - 1 - threadIdx.x; e < n; e += blockDim.x) {
+            const uint32_t f = ids[e];
             const size_t o = (size_t)f * a.ld + w0;
             uint32_t *d = S.far + (size_t)fb * 3 * fplane + (size_t)e * BW;
             cp_async_vec<BW>(d, a.V + o);
@@ -508,20 +526,25 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
 
     uint32_t phase = 0;  // bit b: parity of the next wait on mbar[b]
     // ------------------------------------------------------------- forward
-    if (threadIdx.x == 0) stage_piece(a, S, a.pieces[0], 0, false);
+    // Piece i's copy (buffer i & 1) brings its records and piece i + 1's
+    // far-id list, so no global load stands between a piece's start and the
+    // far-row copies of the next piece.  The last thread issues it: it holds
+    // a gate only when the piece fills the CTA.
+    const uint32_t stager = blockDim.x - 1;
+    if (threadIdx.x == stager) stage_piece(a, S, a.pieces[0], 0, false);
     Piece P1 = a.n_pieces > 1 ? a.pieces[1] : a.pieces[0];
     for (uint32_t i = 0; i < a.n_pieces; i++) {
         const Piece P = i == 0 ? a.pieces[0] : P1;
         const int buf = i & 1;
         const bool has_next = i + 1 < a.n_pieces;
         if (has_next) P1 = a.pieces[i + 1];
-        if (threadIdx.x == 0 && has_next) stage_piece(a, S, P1, buf ^ 1, false);
-        if (has_next) prefetch(P1, buf ^ 1);
+        if (threadIdx.x == stager && has_next) stage_piece(a, S, P1, buf ^ 1, false);
         // every thread waits for the records itself; the piece's only
         // barrier is at its end
         const bool ok = mbar_wait(S.mbar + buf, (phase >> buf) & 1u);
         phase ^= 1u << buf;
         if (!ok) s_fail = 1;
+        if (has_next && ok) prefetch(P.nfar_n, buf ^ 1, S.fid + (size_t)buf * a.farcap);
         const GateRec *recs = S.rec + (size_t)buf * a.cap;
         const uint32_t far_sa = smem_u32(S.far) + (uint32_t)buf * 3u * fplane_b;
         const uint32_t ring_lo = P.b - R;  // (wraps below 0: every fan-in is in the ring then)

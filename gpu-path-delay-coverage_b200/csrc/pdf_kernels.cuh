@@ -39,7 +39,8 @@ struct FwdArgs {
     const Piece *pieces;          // level-ordered runs of gates (the unit of staging and of sync)
     uint32_t n_pieces;
     uint32_t cap, ecap;           // gates / edge words per staging buffer
-    const uint32_t *far_ids;      // per piece, the far fan-ins it reads (Piece::far_off / far_n)
+    const uint32_t *far_ids;      // per piece, the far fan-ins it reads (Piece::far_off / far_n),
+                                  // each list padded to a multiple of 4 entries
     uint32_t farcap;              // slots per far buffer (>= every piece's far_n)
     const uint32_t *pi_v, *pi_t;  // [n_pi][pi_ld]
     uint64_t pi_ld;
@@ -65,6 +66,7 @@ struct FwdArgs {
     uint32_t off_ring;            // forward: ring [3][R][BW]; reverse: ring2 [R2][BW]
     uint32_t off_rec;             // [2][cap] staged gate records
     uint32_t off_edge;            // reverse: [2][ecap] staged edges; forward: far buffers [2][3][farcap][BW]
+    uint32_t off_fid;             // forward: [2][farcap] staged far ids of the piece after the staged one
     uint32_t off_bm, off_pbits, off_mbar;
 };
 
