@@ -255,3 +255,27 @@ def test_benchmark_workloads(wl):
     v, t = P.gen_pairs(P.pair_seed(w["gen"].seed), nl.n_pi, n)
     codes = P.codes_from_planes(v, t, n)
     assert_same(nl, codes, n, mode=1)
+
+
+@pytest.mark.parametrize("case", ["uniform_robust", "uniform_default", "zipf_robust"])
+def test_bitmap_in_global_memory(case):
+    """Circuits above 131,072 gates keep each column block's mark bitmap in
+    global memory instead of shared memory (it no longer fits in 16 KB);
+    levels of several thousand gates also overflow the ring, so fan-ins come
+    from far slots and plane rows.  Marks read from each of those places
+    must still match the oracle, with and without plane outputs."""
+    if case.startswith("zipf"):
+        g = P.GenParams(0x5EED0300, 150_000, 2048, 2048, 50, fanout_dist=1, zipf_s=1.5, fanout_max=256)
+    else:
+        g = P.GenParams(0x5EED0301, 140_000, 3000, 3000, 40)
+    nl = P.gen_netlist(g)
+    mode = 0 if case.endswith("default") else 1
+    n = 300
+    codes = helpers.rand_codes(np.random.default_rng(len(case) + 5), nl.n_pi, n)
+    assert_same(nl, codes, n, mode)
+    want = O.grade(nl, codes, n, mark_mode=mode)
+    for tw in (4, 8):
+        got = gpu_grade(nl, codes, n, mode, outputs=False, tile_words=tw)
+        np.testing.assert_array_equal(got["fx"], want.first_x)
+        np.testing.assert_array_equal(got["fy"], want.first_y)
+        assert got["total"] == want.total and got["flags"] == want.flags
