@@ -167,8 +167,8 @@ typedef struct pdf_circuit_opts {
     uint32_t max_pairs;  /* largest batch this circuit will grade (sizes scratch); 0 = 65536 */
     uint32_t tile_words; /* 0 = by batch size (8 when max_pairs gives >= 2 such CTAs per SM,
                             else 4); else words (32 pairs) per CTA column block: 1,2,4,8 */
-    uint32_t threads;    /* 0 = piece capacity + 64; else threads per CTA: 128..1024, and pieces
-                            of at most threads - 64 gates */
+    uint32_t threads;    /* 0 = piece capacity + 64; else threads per CTA: 64..1024, a multiple
+                            of 32; from 128 up, pieces then hold at most threads - 64 gates */
     uint32_t seg_len;    /* path segments of this many nets, 0 or 1 = single nets; up to 8
                             (fcount --segs N, main.cu:76-81,185-223) */
     uint32_t reserved[2];
