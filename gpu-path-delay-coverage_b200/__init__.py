@@ -131,6 +131,7 @@ ABI = [
     ("pdf_state_profile", C.c_int, [C.c_void_p, C.c_int]),
     ("pdf_state_profile_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     ("pdf_state_snapshot", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Totals_t)]),
+    ("pdf_state_snapshot_on", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Totals_t), C.c_void_p]),
     ("pdf_state_restore", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Totals_t)]),
     ("pdf_grade_async", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Pairs_t), C.c_uint64,
                                   C.POINTER(Outputs_t), C.c_void_p]),
@@ -519,13 +520,19 @@ class State:
         check(lib().pdf_state_profile_read(self.h, ms, C.byref(n)), "pdf_state_profile_read")
         return list(ms), n.value
 
-    def snapshot(self):
+    def snapshot(self, stream: int | None = None):
+        """First-detect ids and totals; with a stream, ordered on that stream
+        only (pdf_state_snapshot_on) instead of after a device-wide sync."""
         G = self.circuit.n_first
         fx = np.zeros(G, np.uint32)
         fy = np.zeros(G, np.uint32)
         tot = Totals_t()
-        check(lib().pdf_state_snapshot(self.h, fx.ctypes.data, fy.ctypes.data, C.byref(tot)),
-              "pdf_state_snapshot")
+        if stream is None:
+            check(lib().pdf_state_snapshot(self.h, fx.ctypes.data, fy.ctypes.data, C.byref(tot)),
+                  "pdf_state_snapshot")
+        else:
+            check(lib().pdf_state_snapshot_on(self.h, fx.ctypes.data, fy.ctypes.data, C.byref(tot),
+                                              C.c_void_p(stream)), "pdf_state_snapshot_on")
         return fx, fy, tot
 
     def restore(self, fx, fy, tot: Totals_t):

@@ -52,7 +52,7 @@ struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
     void release() {
-        if (p) cudaFree(p);
+        if (p && cudaFree(p) != cudaSuccess) (void)cudaGetLastError();
         p = nullptr;
         bytes = 0;
     }
@@ -72,12 +72,18 @@ struct DevBuf {
 struct DeviceGuard {
     int prev = -1;
     bool ok = false;
+    // a failure is reported through `ok` and not left pending for the
+    // caller's next cudaGetLastError
     explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            prev = -1;
+            (void)cudaGetLastError();
+        }
         ok = cudaSetDevice(dev) == cudaSuccess;
+        if (!ok) (void)cudaGetLastError();
     }
     ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
+        if (prev >= 0 && cudaSetDevice(prev) != cudaSuccess) (void)cudaGetLastError();
     }
 };
 
@@ -142,6 +148,7 @@ struct ProfEvents {
 
 struct pdf_state {
     pdf_circuit *c = nullptr;
+    int device = 0;  // the circuit's device (destroy does not need the circuit)
     DevBuf first_x, first_y, acc;
     DevAcc *host_acc = nullptr;  // host copy of the accumulators (read after a stream sync)
     Workspace ws;
@@ -726,6 +733,7 @@ extern "C" pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out) {
     pdf_state *s = new (std::nothrow) pdf_state();
     if (!s) return PDF_ENOMEM;
     s->c = c;
+    s->device = c->device;
     const size_t G = c->n_first();  // first-detect entries: nets, or segments
     if (s->first_x.ensure(4 * G) != cudaSuccess || s->first_y.ensure(4 * G) != cudaSuccess ||
         s->acc.ensure(sizeof(DevAcc)) != cudaSuccess ||
@@ -734,10 +742,20 @@ extern "C" pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out) {
         pdf_state_destroy(s);
         return PDF_ENOMEM;
     }
-    pdf_status st = pdf_state_reset(s);
-    if (st != PDF_OK) {
+    // cleared on a stream of its own: a device-wide sync here would wait for
+    // every other circuit's work in flight (a server creates states while it
+    // grades)
+    cudaStream_t cs = nullptr;
+    const bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
+                    cudaMemsetAsync(s->first_x.p, 0xFF, 4 * G, cs) == cudaSuccess &&
+                    cudaMemsetAsync(s->first_y.p, 0xFF, 4 * G, cs) == cudaSuccess &&
+                    cudaMemsetAsync(s->acc.p, 0, sizeof(DevAcc), cs) == cudaSuccess &&
+                    cudaStreamSynchronize(cs) == cudaSuccess;
+    if (cs) cudaStreamDestroy(cs);
+    if (!ok) {
+        note_cuda_error(cudaGetLastError(), "pdf_state_create: clearing the state", __LINE__);
         pdf_state_destroy(s);
-        return st;
+        return PDF_ECUDA;
     }
     *out = s;
     return PDF_OK;
@@ -745,7 +763,7 @@ extern "C" pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out) {
 
 extern "C" void pdf_state_destroy(pdf_state *s) {
     if (!s) return;
-    DeviceGuard dg(s->c ? s->c->device : 0);
+    DeviceGuard dg(s->device);
     prof_release(s->prof);
     prof_release(s->pool);
     s->ws.release();
@@ -819,6 +837,27 @@ extern "C" pdf_status pdf_state_snapshot(pdf_state *s, uint32_t *first_x, uint32
     if (first_y) PDF_CUDA(cudaMemcpy(first_y, s->first_y.p, 4 * G, cudaMemcpyDeviceToHost));
     DevAcc h{};
     PDF_CUDA(cudaMemcpy(&h, s->acc.p, sizeof h, cudaMemcpyDeviceToHost));
+    if (tot) {
+        tot->lo = h.total_lo;
+        tot->hi = h.total_hi;
+        tot->pairs = h.pairs;
+        tot->flags = h.flags;
+        tot->reserved = 0;
+    }
+    return err_status(h.err);
+}
+
+extern "C" pdf_status pdf_state_snapshot_on(pdf_state *s, uint32_t *first_x, uint32_t *first_y, pdf_totals *tot,
+                                            void *stream) {
+    if (!s) return PDF_EINVAL;
+    DeviceGuard dg(s->c->device);
+    const size_t G = s->c->n_first();
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    if (first_x) PDF_CUDA(cudaMemcpyAsync(first_x, s->first_x.p, 4 * G, cudaMemcpyDeviceToHost, cs));
+    if (first_y) PDF_CUDA(cudaMemcpyAsync(first_y, s->first_y.p, 4 * G, cudaMemcpyDeviceToHost, cs));
+    PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
+    PDF_CUDA(cudaStreamSynchronize(cs));
+    const DevAcc &h = *s->host_acc;
     if (tot) {
         tot->lo = h.total_lo;
         tot->hi = h.total_hi;
@@ -1386,13 +1425,32 @@ struct pdf_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool use_graph = true;
+    // side streams and fork/join events of the forward launches per class
+    cudaStream_t side[3] = {};
+    cudaEvent_t fork = nullptr, join[3] = {};
+    cudaStream_t up = nullptr;  // uploads of the control block
+    unsigned char *host_ctl = nullptr;  // mapped pinned staging of the control block
+    size_t host_bytes = 0;
     void release() {
+        if (host_ctl) cudaFreeHost(host_ctl);
+        host_ctl = nullptr;
+        host_bytes = 0;
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (up) cudaStreamDestroy(up);
+        up = nullptr;
+        for (auto &x : side)
+            if (x) cudaStreamDestroy(x);
+        for (auto &x : join)
+            if (x) cudaEventDestroy(x);
+        if (fork) cudaEventDestroy(fork);
         exec = nullptr;
         graph = nullptr;
         cap_stream = nullptr;
+        for (auto &x : side) x = nullptr;
+        for (auto &x : join) x = nullptr;
+        fork = nullptr;
         ctl.release();
     }
 };
@@ -1491,6 +1549,17 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         b->circuits.push_back(c);
         b->states.push_back(s);
     }
+    // one side stream and join event per class after the first
+    if (!b->fork) PDF_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (uint32_t k = 1; k < L.n_class; k++) {
+        if (!b->side[k - 1]) PDF_CUDA(cudaStreamCreateWithFlags(&b->side[k - 1], cudaStreamNonBlocking));
+        if (!b->join[k - 1]) PDF_CUDA(cudaEventCreateWithFlags(&b->join[k - 1], cudaEventDisableTiming));
+    }
+    for (uint32_t k = 0; k < 3; k++) {
+        L.side[k] = b->side[k];
+        L.join[k] = b->join[k];
+    }
+    L.fork = b->fork;
     L.n = n_jobs;
     L.total_blocks = bp[n_jobs];
     for (uint32_t k = 0; k < L.n_class; k++)
@@ -1503,13 +1572,35 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     const size_t o_f = a256(sizeof(BatchCtl)), o_c = o_f + a256(sizeof(FwdArgs) * n_jobs),
                  o_b = o_c + a256(sizeof(CoverArgs) * n_jobs), o_g = o_b + a256(4 * (n_jobs + 1)),
                  o_i = o_g + a256(4 * (n_jobs + 1)), total = o_i + sizeof(uint2) * std::max<uint64_t>(items, 1);
-    std::vector<unsigned char> hbuf(o_i, 0);
-    std::memcpy(hbuf.data() + o_f, fa.data(), sizeof(FwdArgs) * n_jobs);
-    std::memcpy(hbuf.data() + o_c, ca.data(), sizeof(CoverArgs) * n_jobs);
-    std::memcpy(hbuf.data() + o_b, bp.data(), 4 * (n_jobs + 1));
-    std::memcpy(hbuf.data() + o_g, gp.data(), 4 * (n_jobs + 1));
+    // The block is written into mapped pinned host memory and pulled to the
+    // device by a small kernel on the batch's own stream: a copy-engine
+    // transfer would queue behind other host threads' bulk uploads (a
+    // server's arriving jobs), which held passes up for hundreds of ms.
+    if (b->host_bytes < o_i) {
+        const size_t want = std::max<size_t>(o_i, 2 * b->host_bytes);
+        if (b->host_ctl) cudaFreeHost(b->host_ctl);
+        b->host_ctl = nullptr;
+        b->host_bytes = 0;
+        if (cudaHostAlloc(reinterpret_cast<void **>(&b->host_ctl), want, cudaHostAllocMapped) != cudaSuccess)
+            return PDF_ENOMEM;
+        b->host_bytes = want;
+    }
+    unsigned char *hbuf = b->host_ctl;
+    std::memset(hbuf, 0, o_i);
+    std::memcpy(hbuf + o_f, fa.data(), sizeof(FwdArgs) * n_jobs);
+    std::memcpy(hbuf + o_c, ca.data(), sizeof(CoverArgs) * n_jobs);
+    std::memcpy(hbuf + o_b, bp.data(), 4 * (n_jobs + 1));
+    std::memcpy(hbuf + o_g, gp.data(), 4 * (n_jobs + 1));
     if (b->ctl.ensure(total) != cudaSuccess) return PDF_ENOMEM;
-    if (cudaMemcpy(b->ctl.p, hbuf.data(), o_i, cudaMemcpyHostToDevice) != cudaSuccess) return PDF_ECUDA;
+    void *src = nullptr;
+    if (!b->up) PDF_CUDA(cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking));
+    PDF_CUDA(cudaHostGetDevicePointer(&src, hbuf, 0));
+    // the launch below is checked with cudaGetLastError, which would also
+    // report an unchecked failure left on this thread by an earlier call
+    // (this library's or the caller's); start from a clean slate
+    (void)cudaGetLastError();
+    PDF_CUDA(launch_copy_from_host(b->ctl.p, src, o_i / 16, b->up));
+    PDF_CUDA(cudaStreamSynchronize(b->up));
     unsigned char *base = b->ctl.as<unsigned char>();
     L.ctl = reinterpret_cast<BatchCtl *>(base);
     L.fargs = reinterpret_cast<FwdArgs *>(base + o_f);
@@ -1518,7 +1609,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     L.gpref = reinterpret_cast<const uint32_t *>(base + o_g);
     L.items = reinterpret_cast<uint2 *>(base + o_i);
     b->bytes = b->ctl.bytes;
-    if (prepare_batch(L) != cudaSuccess) return PDF_ECUDA;
+    PDF_CUDA(prepare_batch(L));
     if (b->use_graph && !b->cap_stream &&
         cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
         return PDF_ECUDA;
@@ -1580,6 +1671,7 @@ extern "C" pdf_status pdf_batch_run_async(pdf_batch *b, void *stream) {
     if (!b) return PDF_EINVAL;
     DeviceGuard dg(b->device);
     if (!dg.ok) return PDF_ECUDA;
+    (void)cudaGetLastError();  // an unchecked failure of an earlier call is not this run's
     if (!b->use_graph) {
         PDF_CUDA(launch_batch(b->L, static_cast<cudaStream_t>(stream)));
         return PDF_OK;

@@ -1405,14 +1405,31 @@ cudaError_t prepare_batch_t(const BatchLaunch &b) {
                                 (int)cover_smem_bytes(b.hash_cap));
 }
 
+// The classes' forward launches are independent (different circuits), so
+// they run side by side: the first on `st`, the others on side streams that
+// wait for `st` and that `st` waits for before the cover.  Run one after
+// another, a class's last CTAs held the GPU alone (its longest level chain)
+// before the next class could start.
 template <int BW, int SEM>
 cudaError_t launch_batch_t(const BatchLaunch &b, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
+    bool fork = false;  // recorded before the first class's launch, which it must not wait for
+    for (uint32_t k = 1; k < b.n_class; k++) fork |= b.cls[k].blocks && b.side[k - 1];
+    if (fork && (e = cudaEventRecord(b.fork, st)) != cudaSuccess) return e;
     for (uint32_t k = 0; k < b.n_class; k++) {
         const BatchClass &c = b.cls[k];
         if (!c.blocks) continue;
-        k_batch_forward<BW, SEM><<<c.blocks, c.threads, c.smem, st>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
+        cudaStream_t s = st;
+        if (k > 0 && b.side[k - 1]) {
+            s = b.side[k - 1];
+            if ((e = cudaStreamWaitEvent(s, b.fork, 0)) != cudaSuccess) return e;
+        }
+        k_batch_forward<BW, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (s != st) {
+            if ((e = cudaEventRecord(b.join[k - 1], s)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(st, b.join[k - 1], 0)) != cudaSuccess) return e;
+        }
     }
     k_batch_active<<<(b.total_gates + 255) / 256, 256, 0, st>>>(b.cargs, b.gpref, b.n, b.items, b.ctl);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1487,6 +1504,19 @@ cudaError_t launch_bitmap_from_marks(const DevCircuit &c, const uint32_t *M, uin
     const uint64_t n = std::max<uint64_t>((uint64_t)c.n_gates * n_blocks, n_blocks);
     k_bitmap_from_marks<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c, M, ld, n_pairs, W, bw, n_blocks,
                                                                      nzb, blk_maxlvl, bm_words);
+    return cudaGetLastError();
+}
+
+__global__ void k_copy_from_host(uint4 *dst, const uint4 *src, size_t n16) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+cudaError_t launch_copy_from_host(void *dst, const void *src_mapped, size_t n16, cudaStream_t st) {
+    if (n16 == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)std::min<size_t>((n16 + 255) / 256, 64);
+    k_copy_from_host<<<blocks, 256, 0, st>>>(static_cast<uint4 *>(dst), static_cast<const uint4 *>(src_mapped),
+                                             n16);
     return cudaGetLastError();
 }
 

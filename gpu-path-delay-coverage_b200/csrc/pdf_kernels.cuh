@@ -141,6 +141,10 @@ struct BatchLaunch {
     size_t fwd_smem;
     uint32_t n_class;      // forward launches: classes of jobs (at most 3: 1, 2, 4 CTAs per SM)
     BatchClass cls[4];
+    // classes after the first run on side streams, forked from and joined
+    // back to the launching stream (parallel branches when captured)
+    cudaStream_t side[3];
+    cudaEvent_t fork, join[3];
 };
 // Registers per thread of the fused forward kernel for (tile words, mode); <= 0 on error.
 int forward_kernel_regs(int bw, int sem);
@@ -170,5 +174,9 @@ constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
 cudaError_t noalloc_scratch(int device, unsigned char **out);
 
 cudaError_t launch_batch_begin(DevAcc *acc, cudaStream_t st);
+// Copies n16 16-byte words from mapped pinned host memory to device memory
+// with SM loads, so the copy does not queue behind other host threads'
+// transfers on the copy engines.  src and dst 16-byte aligned.
+cudaError_t launch_copy_from_host(void *dst, const void *src_mapped, size_t n16, cudaStream_t st);
 
 #endif

@@ -1,16 +1,18 @@
 // pdf_server.cpp -- serving loop: continuous batching of grading jobs over
 // the public C ABI (circuits, states and pdf_batch_*).
 //
-// A job owns a device circuit, a coverage state with its workspace, its
-// vector pairs (uploaded once) and a pair buffer of one batch while it is
-// active.  A worker thread prepares queued jobs in arrival order while the
-// estimated device footprint fits the budget (host plan, device upload) on
-// worker threads, so that work overlaps the grading.  Each step admits the prepared jobs, copies
-// the next batch of every active job into its buffer (device to device),
-// grades all of them in one append-mode batched pass and retires the jobs
-// whose pairs are done.  The batched pass is rebuilt only when the set of
-// active jobs (or a job's batch size, on its last batch) changes; it launches
-// its kernels directly (no graph capture while workers call into CUDA).
+// A job owns a device circuit, a coverage state with its workspace and its
+// vector pairs (uploaded once).  Worker threads prepare queued jobs in
+// arrival order while the estimated device footprint fits the budget (host
+// plan, device upload), so that work overlaps the grading; a retired job's
+// memory is freed when the next admission needs it or when the server runs
+// out of work (cudaFree waits for the whole device).  Each step admits the
+// prepared jobs, points every active job at its next batch of pairs (a view
+// of the uploaded pairs, or a device-to-device copy into a batch buffer when
+// their pitch does not allow a view), grades all of them in one append-mode
+// batched pass and retires the jobs whose pairs are done.  The pass is
+// rebuilt when its job list or a view changes; it launches its kernels
+// directly (no graph capture while workers call into CUDA).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,6 +47,7 @@ struct Job {
     pdf_state *s = nullptr;
     uint32_t *dv = nullptr;  // [2][n_pi][ld] one batch of pairs
     uint64_t ld = 0, cur = 0;  // words per row, pairs of the batch in flight
+    bool in_place = false;     // the batch in flight is read from dall directly
     uint32_t *dall = nullptr;  // [2][n_pi][hld] all the job's pairs, on the device while active
     pdf_status prep = PDF_OK;  // outcome of the preparation
     double t_ready = 0.0;
@@ -75,7 +78,8 @@ struct pdf_server {
     std::deque<Job *> ready;     // prepared, not yet active
     std::deque<Job *> retired;   // results taken, device memory still to free (by a worker)
     uint64_t used = 0;           // footprint of prepared + active jobs
-    uint64_t n_active = 0;       // jobs prepared or active
+    uint64_t n_active = 0;       // jobs prepared or active (retired ones until freed)
+    uint64_t preparing = 0;      // jobs a worker is preparing now
     bool stop = false;
     std::vector<std::thread> workers;
 };
@@ -154,14 +158,23 @@ void work(pdf_server *srv) {
     cudaStream_t up = nullptr;
     cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
     std::unique_lock<std::mutex> lk(srv->mu);
+    // cudaFree waits for the whole device, the passes in flight included, so
+    // retired jobs are freed only when their memory is needed to admit the
+    // next queued job, or when nothing else is left (every job that is
+    // prepared or active has retired)
+    auto need_free = [&] {
+        if (srv->retired.empty()) return false;
+        if (srv->queue.empty()) return srv->n_active == srv->retired.size();
+        return srv->n_active >= srv->o.max_jobs || srv->used + srv->queue.front()->bytes > srv->o.hbm_budget;
+    };
     for (;;) {
         srv->cv.wait(lk, [&] {
-            if (srv->stop || !srv->retired.empty()) return true;
+            if (srv->stop || need_free()) return true;
             if (srv->queue.empty() || srv->n_active >= srv->o.max_jobs) return false;
             return srv->n_active == 0 || srv->used + srv->queue.front()->bytes <= srv->o.hbm_budget;
         });
         if (srv->stop) break;
-        if (!srv->retired.empty()) {  // freeing synchronises the device: keep it off the step
+        if (need_free()) {  // freeing synchronises the device: keep it off the step
             Job *r = srv->retired.front();
             srv->retired.pop_front();
             const uint64_t bytes = r->bytes;
@@ -177,9 +190,11 @@ void work(pdf_server *srv) {
         srv->queue.pop_front();
         srv->used += j->bytes;
         srv->n_active++;
+        srv->preparing++;
         lk.unlock();
         prepare(srv->o, j, up);
         lk.lock();
+        srv->preparing--;
         srv->ready.push_back(j);
         srv->cv.notify_all();
     }
@@ -274,11 +289,14 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     const double t0 = now_s();
     pdf_status st = PDF_OK;
     // admission: the jobs the worker has prepared (in arrival order); with
-    // none active, wait (up to a second) for the first one in preparation
+    // none active, wait (up to a second) for the first one queued or in
+    // preparation
     {
         std::unique_lock<std::mutex> lk(srv->mu);
-        if (srv->active.empty() && srv->ready.empty() && srv->n_active > 0)
-            srv->cv.wait_for(lk, std::chrono::seconds(1), [&] { return !srv->ready.empty(); });
+        if (srv->active.empty() && srv->ready.empty() && (srv->preparing > 0 || !srv->queue.empty()))
+            srv->cv.wait_for(lk, std::chrono::seconds(1), [&] {
+                return !srv->ready.empty() || (srv->preparing == 0 && srv->queue.empty());
+            });
         while (!srv->ready.empty()) {
             Job *j = srv->ready.front();
             srv->ready.pop_front();
@@ -298,12 +316,22 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         }
     }
     if (srv->active.empty()) return PDF_OK;
-    // the next batch of every active job
+    // the next batch of every active job: read in place from the job's
+    // pairs (rows of words done/32 .. on) when their pitch keeps the kernels'
+    // alignment, which moves the job's view every batch; else copied into the
+    // job's batch buffer (device to device)
+    const uint64_t tw = srv->o.tile_words;
     for (Job *j : srv->active) {
         const uint64_t n = std::min<uint64_t>(srv->o.batch_pairs, j->n_pairs - j->done);
         if (n != j->cur) srv->dirty = true;
         j->cur = n;
         const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32, W = (n + 31) / 32;
+        j->in_place = j->hld % tw == 0 && (npi * j->hld) % 4 == 0 && w0 % 4 == 0 && w0 % tw == 0 &&
+                      w0 + (W + tw - 1) / tw * tw <= j->hld;
+        if (j->in_place) {
+            srv->dirty = true;
+            continue;
+        }
         uint32_t *dv = j->dv, *dt = j->dv + npi * j->ld;
         const uint32_t *sv = j->dall + w0, *stp = j->dall + npi * j->hld + w0;
         if (cudaMemcpy2DAsync(dv, j->ld * 4, sv, j->hld * 4, W * 4, npi, cudaMemcpyDeviceToDevice, srv->stream) !=
@@ -317,9 +345,11 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     if (srv->dirty) {
         std::vector<pdf_batch_job> jobs;
         for (Job *j : srv->active) {
-            const uint64_t npi = j->view.level_offsets[1];
-            jobs.push_back(pdf_batch_job{j->c, j->s, pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1},
-                                         j->done});
+            const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32;
+            const pdf_pairs p = j->in_place
+                                    ? pdf_pairs{j->dall + w0, j->dall + npi * j->hld + w0, j->cur, j->hld, 1}
+                                    : pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1};
+            jobs.push_back(pdf_batch_job{j->c, j->s, p, j->done});
         }
         const uint32_t fl = PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH;
         st = srv->batch ? pdf_batch_rebind(srv->batch, jobs.data(), (uint32_t)jobs.size(), fl)
@@ -347,7 +377,9 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         Result r;
         r.fx.resize(j->view.n_gates);
         r.fy.resize(j->view.n_gates);
-        if ((st = pdf_state_snapshot(j->s, r.fx.data(), r.fy.data(), &r.total)) != PDF_OK) return st;
+        // ordered on the server's stream: a device-wide sync would also wait
+        // for the workers' uploads of arriving jobs
+        if ((st = pdf_state_snapshot_on(j->s, r.fx.data(), r.fy.data(), &r.total, srv->stream)) != PDF_OK) return st;
         srv->results[j->id] = std::move(r);
         {
             std::lock_guard<std::mutex> lk(srv->mu);

@@ -227,6 +227,7 @@ pdf_status pdf_circuit_segments(const pdf_circuit *c, uint32_t *gates);
  * 0xFFFFFFFF = none yet.  The arrays hold info.n_segments entries: one per
  * net (n_gates), or one per segment when seg_len > 1. */
 pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out);
+/* A state may be destroyed before or after its circuit. */
 void pdf_state_destroy(pdf_state *s);
 pdf_status pdf_state_reset(pdf_state *s);
 /* Synchronises with the state's last grading call. Any pointer may be NULL. */
@@ -234,6 +235,14 @@ pdf_status pdf_state_snapshot(pdf_state *s, uint32_t *first_x, uint32_t *first_y
                               pdf_totals *totals);
 pdf_status pdf_state_restore(pdf_state *s, const uint32_t *first_x,
                              const uint32_t *first_y, const pdf_totals *totals);
+/* pdf_state_snapshot ordered on `stream` (the stream of the state's last
+ * grading call): copies after the work queued there and waits for that
+ * stream only, not for the whole device, so copies and kernels of other
+ * streams (another circuit's uploads, say) do not hold it up.  (No reference
+ * counterpart: the reference reads *totals after a device-wide sync,
+ * main.cu:224.) */
+pdf_status pdf_state_snapshot_on(pdf_state *s, uint32_t *first_x, uint32_t *first_y,
+                                 pdf_totals *totals, void *stream);
 
 /* Stream-ordered reset: clears the state on `stream` without waiting. */
 pdf_status pdf_state_reset_async(pdf_state *s, void *stream);

@@ -279,3 +279,30 @@ def test_bitmap_in_global_memory(case):
         np.testing.assert_array_equal(got["fx"], want.first_x)
         np.testing.assert_array_equal(got["fy"], want.first_y)
         assert got["total"] == want.total and got["flags"] == want.flags
+
+
+def test_snapshot_ordered_on_a_stream():
+    """pdf_state_snapshot_on reads a state after the grading queued on one
+    stream (and waits for that stream only): the same ids and totals as the
+    device-wide snapshot and as the oracle."""
+    import torch
+    nl = SUITE[5][1]
+    n = 3000
+    codes = helpers.rand_codes(np.random.default_rng(21), nl.n_pi, n)
+    want = O.grade(nl, codes, n, mark_mode=1)
+    v, t = P.planes_from_codes(codes)
+    c = P.Circuit(nl, mark_mode=1)
+    s = P.State(c)
+    dv, dt = torch.from_numpy(v.view(np.int32)).cuda(), torch.from_numpy(t.view(np.int32)).cuda()
+    side = torch.cuda.Stream()
+    P.grade_async(c, s, P.make_pairs(dv, dt, n), 0, None, side.cuda_stream)
+    fx, fy, tot = s.snapshot(side.cuda_stream)
+    np.testing.assert_array_equal(fx, want.first_x)
+    np.testing.assert_array_equal(fy, want.first_y)
+    assert tot.value == want.total and tot.pairs == n
+    fx2, fy2, tot2 = s.snapshot()
+    np.testing.assert_array_equal(fx, fx2)
+    np.testing.assert_array_equal(fy, fy2)
+    assert tot2.value == tot.value and tot2.flags == tot.flags
+    s.close()
+    c.close()
