@@ -72,9 +72,14 @@ struct DevBuf {
 struct DeviceGuard {
     int prev = -1;
     bool ok = false;
-    // a failure is reported through `ok` and not left pending for the
-    // caller's next cudaGetLastError
+    // Every entry point that touches the device starts here.  Its launches
+    // are checked with cudaGetLastError, which would also report a failure
+    // that an earlier call on this thread left unchecked (the caller's own,
+    // say), so that slot is cleared first; errors that poison the context
+    // come back from every later call anyway.  A failure here is reported
+    // through `ok` and not left pending for the caller's next check.
     explicit DeviceGuard(int dev) {
+        (void)cudaGetLastError();
         if (cudaGetDevice(&prev) != cudaSuccess) {
             prev = -1;
             (void)cudaGetLastError();

@@ -306,3 +306,20 @@ def test_snapshot_ordered_on_a_stream():
     assert tot2.value == tot.value and tot2.flags == tot.flags
     s.close()
     c.close()
+
+
+def test_pending_cuda_error_of_the_caller_is_not_reported():
+    """A failure the caller left unchecked on this thread (here a
+    cudaSetDevice to a device that does not exist) is not reported as this
+    library's error, and the library leaves no error of its own pending."""
+    import ctypes
+    rt = ctypes.CDLL("libcudart.so.12")
+    nl = SUITE[2][1]
+    n = 200
+    codes = helpers.rand_codes(np.random.default_rng(23), nl.n_pi, n)
+    want = O.grade(nl, codes, n)
+    assert rt.cudaSetDevice(9999) != 0  # left pending on purpose
+    got = gpu_grade(nl, codes, n, outputs=False)
+    assert got["total"] == want.total
+    np.testing.assert_array_equal(got["fx"], want.first_x)
+    assert rt.cudaGetLastError() == 0
