@@ -396,7 +396,7 @@ def run_batched(args):
     P = pkg()
     rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    spec = P.batch_workload()
+    spec = P.batch_workload()[:args.circuits]
     nls = [P.gen_netlist(g) for g, _ in spec]
     counts = [n for _, n in spec]
     t0 = time.perf_counter()
@@ -646,6 +646,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--jobs", type=int, default=64, help="c5: jobs in the arrival stream")
+    ap.add_argument("--circuits", type=int, default=256,
+                    help="c4: the first N netlists of the batch (smaller cases for profiling)")
     ap.add_argument("--hbm-gb", type=float, default=64.0, help="c5: device memory for active jobs")
     args = ap.parse_args()
     if args.impl == "reference":
