@@ -400,11 +400,13 @@ def run_batched(args):
     nls = [P.gen_netlist(g) for g, _ in spec]
     counts = [n for _, n in spec]
     t0 = time.perf_counter()
+    threads = args.threads
     if args.tile_words:
         tw, tune_ms = args.tile_words, None
     else:
-        best, tune_ms = P.batch_autotune(nls, counts, mark_mode=P.MARK_ROBUST, reps=2)
+        best, tune_ms = P.batch_autotune(nls, counts, mark_mode=P.MARK_ROBUST, reps=2, threads=args.threads)
         tw = best.tile_words
+        threads = best.threads
     tune_s = time.perf_counter() - t0
     stream = torch.cuda.current_stream().cuda_stream
     jobs, hosts = [], []
@@ -415,7 +417,7 @@ def run_batched(args):
         check_v, check_t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, n)
         v[:, :check_v.shape[1]] = check_v
         t[:, :check_t.shape[1]] = check_t
-        c = P.Circuit(nl, mark_mode=P.MARK_ROBUST, max_pairs=n, tile_words=tw, threads=args.threads)
+        c = P.Circuit(nl, mark_mode=P.MARK_ROBUST, max_pairs=n, tile_words=tw, threads=threads)
         st = P.State(c)
         dv = torch.from_numpy(v.view(np.int32)).cuda()
         dt = torch.from_numpy(t.view(np.int32)).cuda()
@@ -512,8 +514,9 @@ def run_batched(args):
                                f"({sum(nl.n_gates for nl in nls)} total), depth 20-150, pairs log-uniform "
                                f"1,024-65,536 ({sum(counts)} total), one batched pass per step",
                    "mark_mode": "robust (LUT_R)", "tile_words": tw, "ctas": info.ctas,
-                   "autotune": {"tile_words": tw, "ms_per_pass": tune_ms, "seconds": tune_s} if tune_ms else None,
-                   "threads": args.threads or "piece capacity + 64",
+                   "autotune": {"tile_words": tw, "threads": threads, "ms_per_pass": tune_ms, "seconds": tune_s}
+                   if tune_ms else None,
+                   "threads": threads or "piece capacity + 64",
                    "outputs": "path count and first-detect ids per circuit",
                    "l2": "flushed between timed steps (256 MiB write)"},
         "plain": {"value": units / (min(plain_ms, plain_bt_ms) / 1e3), "ms_per_pass": min(plain_ms, plain_bt_ms),

@@ -682,12 +682,14 @@ class Server:
             pass
 
 
-def batch_autotune(netlists, n_pairs, mark_mode: int = MARK_DEFAULT, reps: int = 3, device: int = 0):
-    """Best tile width for grading these circuits as one batch: (opts, ms per pass)."""
+def batch_autotune(netlists, n_pairs, mark_mode: int = MARK_DEFAULT, reps: int = 3, device: int = 0,
+                   threads: int = 0):
+    """Best tile width and block size for grading these circuits as one batch:
+    (opts, ms per pass); a nonzero `threads` fixes the block size."""
     views = [nl.view() for nl in netlists]
     ptrs = (C.POINTER(Netlist_t) * len(views))(*[C.pointer(v) for v in views])
     npairs = (C.c_uint64 * len(views))(*n_pairs)
-    base = CircuitOpts_t(device, mark_mode, 0, 0, 0)
+    base = CircuitOpts_t(device, mark_mode, 0, 0, threads)
     best = CircuitOpts_t()
     ms = C.c_float()
     check(lib().pdf_batch_autotune(ptrs, npairs, len(views), C.byref(base), reps, C.byref(best), C.byref(ms)),

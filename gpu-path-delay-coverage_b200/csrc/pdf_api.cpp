@@ -1718,11 +1718,20 @@ extern "C" pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, con
     DeviceGuard dg(b0.device);
     if (!dg.ok) return PDF_ECUDA;
     float best_t = 0.0f;
-    uint32_t best_w = 0;
+    uint32_t best_w = 0, best_threads = 0;
     pdf_status last = PDF_OK;
-    for (uint32_t tw : {2u, 4u, 8u}) {
+    // candidates: tile width x block size (the default, piece capacity + 64,
+    // or 256 threads: pieces of 192 gates and more CTAs per SM), unless the
+    // caller fixed the block size
+    std::vector<std::pair<uint32_t, uint32_t>> cand;
+    for (uint32_t tw : {2u, 4u, 8u})
+        for (uint32_t th : {0u, 256u})
+            if (!b0.threads || th == 0) cand.push_back({tw, b0.threads ? b0.threads : th});
+    for (const auto &cw : cand) {
+        const uint32_t tw = cw.first;
         pdf_circuit_opts o = b0;
         o.tile_words = tw;
+        o.threads = cw.second;
         std::vector<pdf_circuit *> cs(n, nullptr);
         std::vector<pdf_state *> ss(n, nullptr);
         std::vector<void *> bufs(n, nullptr);
@@ -1780,11 +1789,13 @@ extern "C" pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, con
         if (!best_w || ms < best_t) {
             best_t = ms;
             best_w = tw;
+            best_threads = cw.second;
         }
     }
     if (!best_w) return last;
     *best = b0;
     best->tile_words = best_w;
+    best->threads = best_threads;
     if (best_ms) *best_ms = best_t;
     return PDF_OK;
 }

@@ -399,12 +399,14 @@ pdf_status pdf_batch_run_async(pdf_batch *b, void *stream);
 pdf_status pdf_batch_run(pdf_batch *b, void *stream);
 
 /*
- * Autotuner of the batch's tile shape: for each candidate tile width (words of
- * 32 pairs per CTA: 2, 4, 8) it builds the circuits, states and pair planes of
- * the given netlists and pair counts (seeded pairs), times `reps` graph
- * replays after a warm-up, and returns the fastest options in *best (the
- * other fields copied from *base) with its milliseconds per run in *best_ms.
- * All it allocates is freed before it returns.
+ * Autotuner of the batch's tile shape: for each candidate (tile width in words
+ * of 32 pairs per CTA: 2, 4, 8; block size: the default, piece capacity + 64,
+ * or 256 threads, pieces of 192 gates; base->threads, when set, fixes the
+ * block size) it builds the circuits, states and pair planes of the given
+ * netlists and pair counts (seeded pairs), times `reps` graph replays after a
+ * warm-up, and returns the fastest options in *best (tile_words and threads;
+ * the other fields copied from *base) with its milliseconds per run in
+ * *best_ms.  All it allocates is freed before it returns.
  */
 pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, const uint64_t *n_pairs, uint32_t n,
                               const pdf_circuit_opts *base, uint32_t reps, pdf_circuit_opts *best,

@@ -121,4 +121,17 @@ def test_batch_rejects_mixed_tiles():
 def test_autotune_picks_a_tile():
     nls = [circuits.random_small(800 + k, n_gates=2000 * (k + 1), n_pi=100, n_po=300, depth=20) for k in range(4)]
     opts, ms = P.batch_autotune(nls, [1024, 3000, 5000, 700], mark_mode=1, reps=2)
-    assert opts.tile_words in (2, 4, 8) and ms > 0
+    assert opts.tile_words in (2, 4, 8) and opts.threads in (0, 256) and ms > 0
+    # the picked shape grades the batch like every circuit alone
+    counts = [1024, 3000, 5000, 700]
+    rng = np.random.default_rng(5)
+    for nl, n in zip(nls, counts):
+        codes = helpers.rand_codes(rng, nl.n_pi, n)
+        c = P.Circuit(nl, mark_mode=1, tile_words=opts.tile_words, threads=opts.threads)
+        s = P.State(c)
+        v, t = P.planes_from_codes(codes)
+        tot = P.grade(c, s, v, t, n)
+        assert tot.value == O.grade(nl, codes, n, mark_mode=1).total
+    # a fixed block size is kept
+    opts2, _ = P.batch_autotune(nls, counts, mark_mode=1, reps=1, threads=384)
+    assert opts2.threads == 384
