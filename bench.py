@@ -337,6 +337,47 @@ def run_ours(args):
             e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_ms_mean = sum(e2e_ms) / len(e2e_ms)
 
+    # e2e, streamed: the same public calls (pdf_grade_async, then
+    # pdf_state_snapshot_on for the count) with each step's pinned host pairs
+    # copied on a second stream into one of two device buffers while the
+    # previous step grades; every step's copy and read-back is inside the
+    # timed region, and every step's count is checked
+    stream_ms, stream_ok = None, True
+    if dist is None:
+        cs = torch.cuda.Stream()
+        comp = torch.cuda.current_stream()
+        bufs = [(torch.empty_like(dv), torch.empty_like(dt_)) for _ in range(2)]
+        copied = [torch.cuda.Event() for _ in range(2)]
+
+        def issue_copy(j):
+            b = j % 2
+            with torch.cuda.stream(cs):
+                bufs[b][0].copy_(hv, non_blocking=True)
+                bufs[b][1].copy_(ht, non_blocking=True)
+                copied[b].record(cs)
+
+        def streamed(k):
+            ok = True
+            issue_copy(0)
+            for i in range(k):
+                b = i % 2
+                comp.wait_event(copied[b])
+                s.reset_async(stream)
+                P.grade_async(c, s, P.make_pairs(bufs[b][0], bufs[b][1], n), base, None, stream)
+                if i + 1 < k:
+                    issue_copy(i + 1)  # buffer (i + 1) % 2 was last read by step i - 1, already read back
+                tot = P.Totals_t()
+                P.check(P.lib().pdf_state_snapshot_on(s.h, None, None, C.byref(tot), C.c_void_p(stream)),
+                        "pdf_state_snapshot_on")
+                ok &= tot.value == ref_total
+            return ok
+
+        streamed(max(3, args.warmup))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        stream_ok = streamed(args.steps)
+        stream_ms = 1e3 * (time.perf_counter() - t0) / args.steps
+
     # max over ranks
     if dist:
         tt = torch.tensor([ms, e2e_ms_mean], dtype=torch.float64, device="cuda")
@@ -364,12 +405,17 @@ def run_ours(args):
                      "kernel_ms": fwd_ms, "cover_ms": prof_ms[1] / max(1, prof_calls),
                      "bytes_per_gate_eval": B, "peak_source": peaks["source"] + " (hbm_gbs)",
                      "traffic": tr.get("dram_bytes_per_launch") if tr else None},
-        "e2e": {"value": units / (e2e_ms_mean / 1e3), "unit": "gate-evals/s",
-                "h2d_bytes_per_step": int(2 * nl.n_pi * W * 4), "d2h_bytes_per_step": 64},
+        "e2e": {"value": units / ((stream_ms or e2e_ms_mean) / 1e3), "unit": "gate-evals/s",
+                "h2d_bytes_per_step": int(2 * nl.n_pi * W * 4), "d2h_bytes_per_step": 64,
+                "mode": ("streamed: pinned host pairs copied on a second stream while the previous step "
+                         "grades (pdf_grade_async + pdf_state_snapshot_on)") if stream_ms else
+                        "one synchronous pdf_grade per step",
+                "value_one_call_per_step": units / (e2e_ms_mean / 1e3),
+                "note": "one call per step: pdf_grade with the host pairs (H2D inside the call), then the next"},
         # k_forward, k_active, k_cover; with segments k_forward, k_seg_merge, k_seg_first, k_cover
         "gpu_launches": (4 if args.segs > 1 else 3) * args.steps,
         "clocks": clocks,
-        "result_stable": bool(totals_ok),
+        "result_stable": bool(totals_ok and stream_ok),
         "batch_count": job_total,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
