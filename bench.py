@@ -655,7 +655,8 @@ def run_served(args):
         v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, per_job)
         jobs.append((nl, v, t))
     units = sum(nl.n_gates * per_job for nl, _, _ in jobs)
-    srv = P.Server(mark_mode=P.MARK_ROBUST, batch_pairs=batch, hbm_budget=int(args.hbm_gb * (1 << 30)))
+    srv = P.Server(mark_mode=P.MARK_ROBUST, batch_pairs=batch, hbm_budget=int(args.hbm_gb * (1 << 30)),
+                   workers=args.workers, tile_words=args.tile_words or 4)
     ids = [None] * n_jobs
     sampler = ClockSampler(gpu_id_for_smi(torch, int(os.environ.get("LOCAL_RANK", "0"))))
     sampler.start()
@@ -693,6 +694,7 @@ def run_served(args):
         "config": {"workload": f"c5: {n_jobs} jobs from the c4 size distribution, Poisson arrivals at "
                                f"{rate:.0f} jobs/s, {batch}-pair appends up to {per_job} pairs per job",
                    "mark_mode": "robust (LUT_R)", "hbm_budget_gib": args.hbm_gb,
+                   "workers": args.workers or "library default", "tile_words": args.tile_words or 4,
                    "outputs": "path count and first-detect ids per job"},
         "latency_ms": {"p50": st.lat_p50_ms, "p99": st.lat_p99_ms, "max": st.lat_max_ms,
                        "per": "job batch, from ready (submission or previous batch) to result"},
@@ -738,6 +740,7 @@ def main():
     ap.add_argument("--circuits", type=int, default=256,
                     help="c4: the first N netlists of the batch (smaller cases for profiling)")
     ap.add_argument("--hbm-gb", type=float, default=64.0, help="c5: device memory for active jobs")
+    ap.add_argument("--workers", type=int, default=0, help="c5: server threads preparing jobs (0 = library default)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

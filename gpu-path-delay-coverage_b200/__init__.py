@@ -635,8 +635,8 @@ class Server:
     netlist and host pair planes alive until its result has been read."""
 
     def __init__(self, mark_mode: int = MARK_DEFAULT, batch_pairs: int = 4096, tile_words: int = 4,
-                 hbm_budget: int = 0, max_jobs: int = 0, device: int = 0):
-        o = ServerOpts_t(device, mark_mode, tile_words, batch_pairs, max_jobs, 0, hbm_budget)
+                 hbm_budget: int = 0, max_jobs: int = 0, device: int = 0, workers: int = 0):
+        o = ServerOpts_t(device, mark_mode, tile_words, batch_pairs, max_jobs, workers, hbm_budget)
         h = C.c_void_p()
         check(lib().pdf_server_create(C.byref(o), C.byref(h)), "pdf_server_create")
         self.h = h

@@ -155,7 +155,8 @@ struct pdf_state {
     pdf_circuit *c = nullptr;
     int device = 0;  // the circuit's device (destroy does not need the circuit)
     DevBuf first_x, first_y, acc;
-    DevAcc *host_acc = nullptr;  // host copy of the accumulators (read after a stream sync)
+    DevAcc *host_acc = nullptr;  // host copy of the accumulators (pinned: read back by DMA, after a
+                                 // stream sync, without the driver's staging of pageable copies)
     Workspace ws;
     std::mutex mu;
     bool profiling = false;
@@ -742,11 +743,13 @@ extern "C" pdf_status pdf_state_create(pdf_circuit *c, pdf_state **out) {
     const size_t G = c->n_first();  // first-detect entries: nets, or segments
     if (s->first_x.ensure(4 * G) != cudaSuccess || s->first_y.ensure(4 * G) != cudaSuccess ||
         s->acc.ensure(sizeof(DevAcc)) != cudaSuccess ||
-        !(s->host_acc = new (std::nothrow) DevAcc())) {
+        cudaHostAlloc(reinterpret_cast<void **>(&s->host_acc), sizeof(DevAcc), cudaHostAllocDefault) != cudaSuccess) {
+        s->host_acc = nullptr;
         (void)cudaGetLastError();
         pdf_state_destroy(s);
         return PDF_ENOMEM;
     }
+    std::memset(s->host_acc, 0, sizeof(DevAcc));
     // cleared on a stream of its own: a device-wide sync here would wait for
     // every other circuit's work in flight (a server creates states while it
     // grades)
@@ -775,7 +778,7 @@ extern "C" void pdf_state_destroy(pdf_state *s) {
     s->first_x.release();
     s->first_y.release();
     s->acc.release();
-    delete s->host_acc;
+    if (s->host_acc && cudaFreeHost(s->host_acc) != cudaSuccess) (void)cudaGetLastError();
     delete s;
 }
 
@@ -1596,7 +1599,8 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     std::memcpy(hbuf + o_c, ca.data(), sizeof(CoverArgs) * n_jobs);
     std::memcpy(hbuf + o_b, bp.data(), 4 * (n_jobs + 1));
     std::memcpy(hbuf + o_g, gp.data(), 4 * (n_jobs + 1));
-    if (b->ctl.ensure(total) != cudaSuccess) return PDF_ENOMEM;
+    // grown geometrically: freeing the old block waits for the whole device
+    if (total > b->ctl.bytes && b->ctl.ensure(std::max(total, 2 * b->ctl.bytes)) != cudaSuccess) return PDF_ENOMEM;
     void *src = nullptr;
     if (!b->up) PDF_CUDA(cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking));
     PDF_CUDA(cudaHostGetDevicePointer(&src, hbuf, 0));
@@ -1703,10 +1707,12 @@ extern "C" pdf_status pdf_batch_run(pdf_batch *b, void *stream) {
     if (st != PDF_OK) return st;
     DeviceGuard dg(b->device);
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    BatchCtl h{};
-    PDF_CUDA(cudaMemcpyAsync(&h, b->ctl.p, sizeof h, cudaMemcpyDeviceToHost, cs));
+    // read back into the pinned staging of the control block (its image is
+    // rewritten at the next rebind): a DMA, not a staged pageable copy
+    BatchCtl *h = reinterpret_cast<BatchCtl *>(b->host_ctl);
+    PDF_CUDA(cudaMemcpyAsync(h, b->ctl.p, sizeof(BatchCtl), cudaMemcpyDeviceToHost, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));
-    return err_status(h.err);
+    return err_status(h->err);
 }
 
 // Autotuner of the batch tile width: times the whole batch at each candidate.

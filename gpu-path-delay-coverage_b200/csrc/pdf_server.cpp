@@ -71,6 +71,11 @@ struct pdf_server {
     cudaStream_t stream = nullptr;
     pdf_server_stats st{};
     std::vector<double> lat_ms;
+    // pinned staging of a retiring job's first-detect ids: read back by DMA,
+    // not through the driver's staging of pageable copies (which the workers'
+    // uploads keep busy)
+    uint32_t *pin = nullptr;
+    size_t pin_words = 0;
     // shared with the worker (under mu)
     std::mutex mu;
     std::condition_variable cv;
@@ -115,9 +120,34 @@ void free_job(Job *j) {
 
 namespace {
 
+// A worker's pinned staging: host-to-device copies from the caller's
+// pageable planes go through two pinned halves, so a copy engine reads them
+// directly; a pageable source would go through the driver's own staging,
+// which the serving step's small copies would then queue behind.
+struct Stage {
+    unsigned char *buf[2] = {};
+    cudaEvent_t ev[2] = {};
+    size_t cap = 0;  // bytes per half
+};
+
+bool upload(void *dst, const void *src, size_t bytes, cudaStream_t up, Stage &sg) {
+    if (!sg.buf[0] || !sg.buf[1]) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, up) == cudaSuccess;
+    int k = 0;
+    for (size_t off = 0; off < bytes; off += sg.cap, k ^= 1) {
+        const size_t n = std::min(sg.cap, bytes - off);
+        if (cudaEventSynchronize(sg.ev[k]) != cudaSuccess) return false;  // this half's last copy is done
+        std::memcpy(sg.buf[k], static_cast<const unsigned char *>(src) + off, n);
+        if (cudaMemcpyAsync(static_cast<unsigned char *>(dst) + off, sg.buf[k], n, cudaMemcpyHostToDevice, up) !=
+                cudaSuccess ||
+            cudaEventRecord(sg.ev[k], up) != cudaSuccess)
+            return false;
+    }
+    return true;
+}
+
 // Circuit, state with its workspace, pair buffers and the job's pairs on the
 // device.  On failure nothing stays allocated and j->prep holds the status.
-void prepare(const pdf_server_opts &o, Job *j, cudaStream_t up) {
+void prepare(const pdf_server_opts &o, Job *j, cudaStream_t up, Stage &sg) {
     pdf_circuit_opts co{};
     co.device = o.device;
     co.mark_mode = o.mark_mode;
@@ -133,8 +163,7 @@ void prepare(const pdf_server_opts &o, Job *j, cudaStream_t up) {
                          cudaMalloc(&j->dall, pairs_bytes(j->view, j->hld)) != cudaSuccess))
         st = PDF_ENOMEM;
     if (st == PDF_OK && (cudaMemsetAsync(j->dv, 0, 2 * npi * j->ld * 4, up) != cudaSuccess ||
-                         cudaMemcpyAsync(j->dall, j->hv, hb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
-                         cudaMemcpyAsync(j->dall + npi * j->hld, j->ht, hb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
+                         !upload(j->dall, j->hv, hb, up, sg) || !upload(j->dall + npi * j->hld, j->ht, hb, up, sg) ||
                          cudaStreamSynchronize(up) != cudaSuccess))
         st = PDF_ECUDA;
     if (st != PDF_OK) {
@@ -157,6 +186,14 @@ void work(pdf_server *srv) {
     cudaSetDevice(srv->o.device);
     cudaStream_t up = nullptr;
     cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+    Stage sg;  // without it (allocation failed) uploads go straight from the caller's planes
+    sg.cap = 4u << 20;
+    for (int k = 0; k < 2; k++)
+        if (cudaHostAlloc(reinterpret_cast<void **>(&sg.buf[k]), sg.cap, cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sg.ev[k], cudaEventDisableTiming) != cudaSuccess) {
+            sg.buf[k] = nullptr;
+            (void)cudaGetLastError();
+        }
     std::unique_lock<std::mutex> lk(srv->mu);
     // cudaFree waits for the whole device, the passes in flight included, so
     // retired jobs are freed only when their memory is needed to admit the
@@ -192,7 +229,7 @@ void work(pdf_server *srv) {
         srv->n_active++;
         srv->preparing++;
         lk.unlock();
-        prepare(srv->o, j, up);
+        prepare(srv->o, j, up, sg);
         lk.lock();
         srv->preparing--;
         srv->ready.push_back(j);
@@ -200,6 +237,10 @@ void work(pdf_server *srv) {
     }
     lk.unlock();
     if (up) cudaStreamDestroy(up);
+    for (int k = 0; k < 2; k++) {
+        if (sg.buf[k]) cudaFreeHost(sg.buf[k]);
+        if (sg.ev[k]) cudaEventDestroy(sg.ev[k]);
+    }
 }
 
 }  // namespace
@@ -248,6 +289,7 @@ extern "C" void pdf_server_destroy(pdf_server *srv) {
     for (Job *j : srv->retired) free_job(j);
     for (Job *j : srv->queue) free_job(j);
     cudaStreamDestroy(srv->stream);
+    if (srv->pin) cudaFreeHost(srv->pin);
     delete srv;
 }
 
@@ -375,11 +417,26 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
             continue;
         }
         Result r;
-        r.fx.resize(j->view.n_gates);
-        r.fy.resize(j->view.n_gates);
+        const size_t G = j->view.n_gates;
+        r.fx.resize(G);
+        r.fy.resize(G);
+        if (srv->pin_words < 2 * G) {  // grown geometrically (freeing pinned memory waits for the device)
+            const size_t want = std::max(2 * G, 2 * srv->pin_words);
+            if (srv->pin) cudaFreeHost(srv->pin);
+            srv->pin = nullptr;
+            srv->pin_words = 0;
+            if (cudaHostAlloc(reinterpret_cast<void **>(&srv->pin), want * 4, cudaHostAllocDefault) != cudaSuccess) {
+                srv->pin = nullptr;
+                (void)cudaGetLastError();
+                return PDF_ENOMEM;
+            }
+            srv->pin_words = want;
+        }
         // ordered on the server's stream: a device-wide sync would also wait
         // for the workers' uploads of arriving jobs
-        if ((st = pdf_state_snapshot_on(j->s, r.fx.data(), r.fy.data(), &r.total, srv->stream)) != PDF_OK) return st;
+        if ((st = pdf_state_snapshot_on(j->s, srv->pin, srv->pin + G, &r.total, srv->stream)) != PDF_OK) return st;
+        std::memcpy(r.fx.data(), srv->pin, 4 * G);
+        std::memcpy(r.fy.data(), srv->pin + G, 4 * G);
         srv->results[j->id] = std::move(r);
         {
             std::lock_guard<std::mutex> lk(srv->mu);
