@@ -1585,7 +1585,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     // transfer would queue behind other host threads' bulk uploads (a
     // server's arriving jobs), which held passes up for hundreds of ms.
     if (b->host_bytes < o_i) {
-        const size_t want = std::max<size_t>(o_i, 2 * b->host_bytes);
+        const size_t want = std::max<size_t>({o_i, 2 * b->host_bytes, (size_t)256 << 10});
         if (b->host_ctl) cudaFreeHost(b->host_ctl);
         b->host_ctl = nullptr;
         b->host_bytes = 0;
@@ -1600,7 +1600,8 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     std::memcpy(hbuf + o_b, bp.data(), 4 * (n_jobs + 1));
     std::memcpy(hbuf + o_g, gp.data(), 4 * (n_jobs + 1));
     // grown geometrically: freeing the old block waits for the whole device
-    if (total > b->ctl.bytes && b->ctl.ensure(std::max(total, 2 * b->ctl.bytes)) != cudaSuccess) return PDF_ENOMEM;
+    if (total > b->ctl.bytes && b->ctl.ensure(std::max<size_t>({total, 2 * b->ctl.bytes, (size_t)1 << 20})) != cudaSuccess)
+        return PDF_ENOMEM;
     void *src = nullptr;
     if (!b->up) PDF_CUDA(cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking));
     PDF_CUDA(cudaHostGetDevicePointer(&src, hbuf, 0));

@@ -268,6 +268,15 @@ extern "C" pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server 
         delete srv;
         return PDF_ECUDA;
     }
+    // the retiring jobs' staging, sized up front for circuits of 256k gates
+    // (pinning memory while the loop runs contends with the workers' calls)
+    if (cudaHostAlloc(reinterpret_cast<void **>(&srv->pin), 2 * (size_t)(256u << 10) * 4, cudaHostAllocDefault) ==
+        cudaSuccess)
+        srv->pin_words = 2 * (size_t)(256u << 10);
+    else {
+        srv->pin = nullptr;
+        (void)cudaGetLastError();
+    }
     for (uint32_t k = 0; k < (o.workers ? o.workers : 4); k++) srv->workers.emplace_back(work, srv);
     *out = srv;
     return PDF_OK;
