@@ -188,12 +188,23 @@ void work(pdf_server *srv) {
     cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
     Stage sg;  // without it (allocation failed) uploads go straight from the caller's planes
     sg.cap = 4u << 20;
-    for (int k = 0; k < 2; k++)
-        if (cudaHostAlloc(reinterpret_cast<void **>(&sg.buf[k]), sg.cap, cudaHostAllocDefault) != cudaSuccess ||
-            cudaEventCreateWithFlags(&sg.ev[k], cudaEventDisableTiming) != cudaSuccess) {
+    for (int k = 0; k < 2; k++) {
+        if (cudaHostAlloc(reinterpret_cast<void **>(&sg.buf[k]), sg.cap, cudaHostAllocDefault) != cudaSuccess) {
             sg.buf[k] = nullptr;
             (void)cudaGetLastError();
         }
+        if (cudaEventCreateWithFlags(&sg.ev[k], cudaEventDisableTiming) != cudaSuccess) {
+            sg.ev[k] = nullptr;
+            (void)cudaGetLastError();
+        }
+    }
+    if (!sg.buf[0] || !sg.buf[1] || !sg.ev[0] || !sg.ev[1]) {  // upload() then copies directly
+        for (int k = 0; k < 2; k++)
+            if (sg.buf[k]) {
+                cudaFreeHost(sg.buf[k]);
+                sg.buf[k] = nullptr;
+            }
+    }
     std::unique_lock<std::mutex> lk(srv->mu);
     // cudaFree waits for the whole device, the passes in flight included, so
     // retired jobs are freed only when their memory is needed to admit the
