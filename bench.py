@@ -409,7 +409,8 @@ def run_ours(args):
                 "h2d_bytes_per_step": int(2 * nl.n_pi * W * 4), "d2h_bytes_per_step": 64,
                 "mode": ("streamed: pinned host pairs copied on a second stream while the previous step "
                          "grades (pdf_grade_async + pdf_state_snapshot_on)") if stream_ms else
-                        "one synchronous pdf_grade per step",
+                        ("per step: host pairs in, mark, MIN-exchange of first-detect ids across ranks, cover, "
+                         "count back" if dist else "one synchronous pdf_grade per step"),
                 "value_one_call_per_step": units / (e2e_ms_mean / 1e3),
                 "note": "one call per step: pdf_grade with the host pairs (H2D inside the call), then the next"},
         # k_forward, k_active, k_cover; with segments k_forward, k_seg_merge, k_seg_first, k_cover
