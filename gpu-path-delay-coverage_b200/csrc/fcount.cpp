@@ -168,7 +168,7 @@ int main(int argc, char *argv[]) {
         check(pdf_circuit_segments(ckt, seg_list.data()), "pdf_circuit_segments");
     }
     const bool dumps = verbose_flag && (sim_flag || mark_flag || merge_flag);
-    if (verbose_flag && cover_flag) std::clog << "gpucover.log is not written by this build" << std::endl;
+    if (verbose_flag && cover_flag) std::clog << "gpucover.log is not written: per-(input, pair) counts stay inside the cover kernel" << std::endl;
 
     for (const std::string &vector_file : benchmarks) {
         std::cerr << "Vector set " << vector_file << std::endl;

@@ -39,7 +39,7 @@ typedef enum pdf_status {
     PDF_EOVERFLOW = 3,  /* a path count does not fit in 128 bits */
     PDF_ETIMEOUT = 4,   /* a bounded device-side wait gave up */
     PDF_ECUDA = 5,      /* a CUDA runtime call failed */
-    PDF_ENOTSUP = 6,    /* feature not available in this build / on this device */
+    PDF_ENOTSUP = 6,    /* not supported for these options or on this device */
     PDF_EBUSY = 7,      /* resource in use (serving queue full, job still running) */
     PDF_ENODEV = 8,     /* no CUDA device */
     PDF_ELIMIT = 9      /* request larger than the fixed scratch of pdf_cover_noalloc */
