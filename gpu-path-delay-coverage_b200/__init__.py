@@ -21,6 +21,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpdf_b200.so")
+# the seeded workload generator alone (no CUDA): gen_netlist / gen_pairs
+GEN_LIB_PATH = os.path.join(_HERE, "libpdf_gen.so")
 
 # gate codes (pdf.h)
 UNKN, INPT, AND, NAND, OR, NOR, XOR, XNOR, BUFF, NOT, FROM, DFF = range(12)
@@ -156,6 +158,8 @@ ABI = [
     ("pdf_batch_query", C.c_int, [C.c_void_p, C.POINTER(BatchInfo_t)]),
     ("pdf_batch_run_async", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pdf_batch_run", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pdf_batch_profile", C.c_int, [C.c_void_p, C.c_int]),
+    ("pdf_batch_profile_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("pdf_batch_autotune", C.c_int, [C.POINTER(C.POINTER(Netlist_t)), C.POINTER(C.c_uint64), C.c_uint32,
                                      C.POINTER(CircuitOpts_t), C.c_uint32, C.POINTER(CircuitOpts_t),
                                      C.POINTER(C.c_float)]),
@@ -206,10 +210,32 @@ def lib() -> C.CDLL:
     return _lib
 
 
+_gen_lib = None
+GEN_ABI = [("pdf_gen_netlist", C.c_int, [C.POINTER(GenParams_t), C.POINTER(C.c_void_p)]),
+           ("pdf_netbuf_view", None, [C.c_void_p, C.POINTER(Netlist_t)]),
+           ("pdf_netbuf_free", None, [C.c_void_p]),
+           ("pdf_gen_pairs", C.c_int, [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p])]
+
+
+def gen_lib() -> C.CDLL:
+    """The workload generator library (host code only; loads no CUDA code)."""
+    global _gen_lib
+    if _gen_lib is None:
+        if not os.path.exists(GEN_LIB_PATH):
+            raise RuntimeError(f"{GEN_LIB_PATH} is missing: build it with __graft_entry__.build()")
+        L = C.CDLL(GEN_LIB_PATH)
+        for name, res, args in GEN_ABI:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _gen_lib = L
+    return _gen_lib
+
+
 def check(status: int, what: str) -> None:
     if status != 0:
-        if status in (2, 5):  # ENOMEM, ECUDA: name the CUDA call behind it
-            what = f"{what} [{lib().pdf_last_error().decode(errors='replace')}]"
+        if status in (2, 5) and _lib is not None:  # ENOMEM, ECUDA: name the CUDA call behind it
+            what = f"{what} [{_lib.pdf_last_error().decode(errors='replace')}]"
         raise PdfError(status, what)
 
 
@@ -314,13 +340,14 @@ def gen_netlist(p: GenParams) -> Netlist:
     gp = GenParams_t(p.seed, p.n_gates, p.n_pi, p.n_po, p.depth, p.fanin_min, p.fanin_max,
                      p.fanout_dist, p.zipf_s, p.fanout_max, p.type_mask)
     h = C.c_void_p()
-    check(lib().pdf_gen_netlist(C.byref(gp), C.byref(h)), "pdf_gen_netlist")
-    return _take_netbuf(h)
+    check(gen_lib().pdf_gen_netlist(C.byref(gp), C.byref(h)), "pdf_gen_netlist")
+    return _take_netbuf(h, gen_lib())
 
 
-def _take_netbuf(h) -> Netlist:
-    """Copy a library-owned netlist into a Netlist and free it."""
-    L = lib()
+def _take_netbuf(h, L=None) -> Netlist:
+    """Copy a netlist owned by library L (the grader by default) into a
+    Netlist and free it there."""
+    L = L or lib()
     try:
         v = Netlist_t()
         L.pdf_netbuf_view(h, C.byref(v))
@@ -414,7 +441,7 @@ def gen_pairs(seed: int, n_pi: int, n_pairs: int, ld: int | None = None) -> tupl
     ld = ld or words(n_pairs)
     v = np.zeros((n_pi, ld), np.uint32)
     t = np.zeros((n_pi, ld), np.uint32)
-    check(lib().pdf_gen_pairs(seed, n_pi, n_pairs, ld, v.ctypes.data, t.ctypes.data), "pdf_gen_pairs")
+    check(gen_lib().pdf_gen_pairs(seed, n_pi, n_pairs, ld, v.ctypes.data, t.ctypes.data), "pdf_gen_pairs")
     return v, t
 
 
@@ -617,6 +644,15 @@ class Batch:
 
     def run(self, stream: int = 0):
         check(lib().pdf_batch_run(self.h, C.c_void_p(stream)), "pdf_batch_run")
+
+    def profile(self, enable: bool):
+        check(lib().pdf_batch_profile(self.h, int(enable)), "pdf_batch_profile")
+
+    def profile_read(self) -> tuple[float, float]:
+        """(forward ms, cover ms) of the most recent run (waits for it)."""
+        ms = (C.c_double * 2)()
+        check(lib().pdf_batch_profile_read(self.h, ms), "pdf_batch_profile_read")
+        return ms[0], ms[1]
 
     def close(self):
         if self.h:

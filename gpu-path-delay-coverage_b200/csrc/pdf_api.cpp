@@ -127,6 +127,7 @@ struct pdf_circuit {
     size_t fwd_smem = 0;
     uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
     uint32_t occ = 1;  // forward CTAs per SM its registers and shared memory are sized for
+    uint64_t chain = 0;  // length of one CTA's walk (pieces, or gates for the lane kernel)
     Workspace stage;  // scratch of the stage calls
     std::mutex mu;    // serialises the stage scratch
     // segments longer than one net
@@ -384,7 +385,8 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     if (opts) o = *opts;
     if (o.mark_mode < PDF_MARK_DEFAULT || o.mark_mode > PDF_MARK_FIXED_NONROBUST) return PDF_EINVAL;
     if (o.seg_len > 8) return PDF_EINVAL;
-    if (o.tile_words && o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8)
+    if (o.tile_words && o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8 &&
+        o.tile_words != kLaneWords)
         return PDF_EINVAL;
     if (o.threads && (o.threads < 64 || o.threads > 1024 || o.threads % 32)) return PDF_EINVAL;
     int ndev = 0;
@@ -461,7 +463,15 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     const uint64_t max_words = ((o.max_pairs ? o.max_pairs : 65536ull) + 31) / 32;
     c->bw = o.tile_words ? o.tile_words
                          : (max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u);
-    const uint32_t max_threads = c->bw >= 8 ? 512 : 1024;
+    const bool lanes = c->bw == kLaneWords;
+    if (lanes) {
+        // the lane kernel reads every fan-in from its plane row: source words
+        // are the fan-in ids themselves
+        for (uint32_t g = 0; g < G; g++)
+            for (uint32_t q = 0; q < kInlineFanins; q++)
+                recs[g].w[3 + q] = q < nl->nfi[g] ? edges[eoff[g] + q] : 0u;
+    }
+    const uint32_t max_threads = lanes ? kLaneThreads : (c->bw >= 8 ? 512 : 1024);
     uint32_t threads_default = 512;  // set from the piece size below
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
@@ -472,14 +482,14 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     uint32_t widest = 1;
     for (uint32_t l = 1; l < L; l++) widest = std::max(widest, nl->level_offsets[l + 1] - nl->level_offsets[l]);
     if (L == 1) widest = inf.max_level_width;
-    c->cap = std::min<uint32_t>(512, (widest + 31) & ~31u);
+    c->cap = lanes ? 0u : std::min<uint32_t>(512, (widest + 31) & ~31u);
     // one thread per gate of a piece plus two warps that have none: they
     // issue the next piece's far-row copies
-    threads_default = std::min<uint32_t>(max_threads, c->cap + 64);
+    threads_default = lanes ? kLaneThreads : std::min<uint32_t>(max_threads, c->cap + 64);
     c->threads = o.threads ? std::min(o.threads, max_threads) : threads_default;
     // a block size given by the caller also bounds the pieces: threads - 64
     // gates, so two warps stay free for the far-row copies
-    if (o.threads && c->threads >= 128) c->cap = std::min(c->cap, (c->threads - 64) & ~31u);
+    if (!lanes && o.threads && c->threads >= 128) c->cap = std::min(c->cap, (c->threads - 64) & ~31u);
     // CTAs per SM that the registers allow for this block size (at most 4);
     // the dynamic shared memory of the forward kernels is then an equal share
     // of the SM, less 1 KiB per CTA the system keeps and 1 KiB for the
@@ -500,140 +510,153 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
                           1024;
     c->ecap = 2048;
     std::vector<Piece> pieces;
-    auto f4 = [](uint64_t x) { return x & ~(uint64_t)3; };
-    auto c4 = [](uint64_t x) { return (x + 3) & ~(uint64_t)3; };
-    for (uint32_t l = 0; l < L; l++) {
-        const uint32_t s0 = nl->level_offsets[l], e0 = nl->level_offsets[l + 1];
-        for (uint32_t a = s0; a < e0;) {
-            uint32_t b = a + 1;
-            while (b < e0 && b - a < c->cap && c4(eoff[b + 1]) - f4(eoff[a]) <= c->ecap) b++;
-            Piece p{};
-            p.a = a;
-            p.b = b;
-            p.level = l;
-            if (c4(eoff[b]) - f4(eoff[a]) <= c->ecap) {
-                p.ea = (uint32_t)f4(eoff[a]);
-                p.eb = (uint32_t)c4(eoff[b]);
-            } else {
-                p.ea = p.eb = 0xFFFFFFFFu;  // one gate with a huge edge list: read in place
-            }
-            pieces.push_back(p);
-            a = b;
-        }
-    }
-    c->n_pieces = (uint32_t)pieces.size();
-    if (c->n_pieces > 65536) {
-        delete c;
-        return PDF_ENOTSUP;
-    }
-    // Far fan-ins of piece i (ring of R slots): fan-ins 0..3 of its gates
-    // below b_i - R.  Those below a_{i-1} (complete when piece i - 1 starts)
-    // go to the piece's deduplicated far list, up to `limit` entries; the rest
-    // are read from their plane rows.  Fills the source words w[3..6].
     std::vector<uint32_t> far_ids;
-    auto far_lists = [&](uint32_t R, uint32_t limit) -> uint32_t {
-        uint32_t worst = 0;
-        far_ids.clear();
-        std::vector<uint32_t> seen(G, 0xFFFFFFFFu);  // gate -> slot in the current piece's list
-        std::vector<uint32_t> list;
-        for (size_t i = 0; i < pieces.size(); i++) {
-            Piece &p = pieces[i];
-            const uint32_t lo = p.b > R ? p.b - R : 0;
-            const uint32_t done = i ? pieces[i - 1].a : 0;
-            list.clear();
-            for (uint32_t g = p.a; g < p.b; g++) {
-                const uint32_t nq = std::min<uint32_t>(nl->nfi[g], kInlineFanins);
-                for (uint32_t q = 0; q < nq; q++) {
-                    const uint32_t f = edges[eoff[g] + q];
-                    uint32_t sw = f & (R - 1);
-                    if (f < lo) {
-                        sw = SRC_PLANE | f;
-                        if (f < done) {
-                            if (seen[f] == 0xFFFFFFFFu && list.size() < limit) {
-                                seen[f] = (uint32_t)list.size();
-                                list.push_back(f);
-                            }
-                            if (seen[f] != 0xFFFFFFFFu) sw = SRC_FAR | seen[f];
-                        }
-                    }
-                    recs[g].w[3 + q] = sw;
-                    if (sw & SRC_PLANE || sw & SRC_FAR) recs[f].w[0] |= RF_SPILL;
+    if (lanes) {
+        // The lane kernel keeps only the column block's mark bitmap on chip
+        // (in global memory when it does not fit); no pieces, ring or far lists.
+        const size_t bm_bytes = (size_t)bm_words * 4;
+        c->bm_shared = bm_bytes + 2048 <= budget ? 1u : 0u;
+        c->off_bm = 0;
+        c->fwd_smem = c->bm_shared ? al(bm_bytes) : 0;
+        c->n_pieces = 0;
+        c->chain = G;
+        while (far_ids.size() < 4) far_ids.push_back(0);
+    } else {
+        auto f4 = [](uint64_t x) { return x & ~(uint64_t)3; };
+        auto c4 = [](uint64_t x) { return (x + 3) & ~(uint64_t)3; };
+        for (uint32_t l = 0; l < L; l++) {
+            const uint32_t s0 = nl->level_offsets[l], e0 = nl->level_offsets[l + 1];
+            for (uint32_t a = s0; a < e0;) {
+                uint32_t b = a + 1;
+                while (b < e0 && b - a < c->cap && c4(eoff[b + 1]) - f4(eoff[a]) <= c->ecap) b++;
+                Piece p{};
+                p.a = a;
+                p.b = b;
+                p.level = l;
+                if (c4(eoff[b]) - f4(eoff[a]) <= c->ecap) {
+                    p.ea = (uint32_t)f4(eoff[a]);
+                    p.eb = (uint32_t)c4(eoff[b]);
+                } else {
+                    p.ea = p.eb = 0xFFFFFFFFu;  // one gate with a huge edge list: read in place
                 }
-                for (uint32_t q = kInlineFanins; q < nl->nfi[g]; q++) {  // read from edges[] at run time
-                    const uint32_t f = edges[eoff[g] + q];
-                    if (f < lo) recs[f].w[0] |= RF_SPILL;
-                }
+                pieces.push_back(p);
+                a = b;
             }
-            for (uint32_t f : list) seen[f] = 0xFFFFFFFFu;
-            worst = std::max<uint32_t>(worst, (uint32_t)list.size());
-            p.far_off = (uint32_t)far_ids.size();
-            p.far_n = (uint32_t)list.size();
-            far_ids.insert(far_ids.end(), list.begin(), list.end());
-            // lists start on 16-byte boundaries: the kernel stages the next
-            // piece's list by a bulk copy located from this piece's fields
-            while (far_ids.size() & 3) far_ids.push_back(0);
         }
-        for (size_t i = 0; i < pieces.size(); i++) pieces[i].nfar_n = i + 1 < pieces.size() ? pieces[i + 1].far_n : 0;
-        return worst;
-    };
-    // Shared memory of k_forward: 2 record buffers; one region holding the
-    // reverse pass's 2 edge buffers or the forward pass's 2 far buffers;
-    // bitmap; piece bits; barriers; the ring.  The ring: the largest power of
-    // two (>= cap, <= 2 * n_gates) that leaves room for far lists of 64
-    // entries; the far lists then get the rest of the budget.
-    const size_t rec_bytes = al(2 * (size_t)c->cap * sizeof(GateRec));
-    const size_t bm_bytes = (size_t)bm_words * 4 <= 16384 ? al((size_t)bm_words * 4) : 0;
-    const size_t fixed = rec_bytes + bm_bytes + al(((size_t)c->n_pieces + 31) / 32 * 4) + 128;
-    const size_t edge_bytes = 2 * (size_t)c->ecap * 4;
-    const size_t far_entry = (size_t)2 * 3 * c->bw * 4;  // one far slot in both buffers, 3 planes
-    uint32_t rmin = 32;
-    while (rmin < c->cap) rmin *= 2;
-    uint32_t rmax = rmin;
-    while ((uint64_t)rmax < 2 * (uint64_t)G && fixed + (size_t)rmax * 2 * c->bw * 12 <= budget) rmax *= 2;
-    // the ring's memory also holds the reverse pass's row staging buffers
-    const size_t rows_bytes = (size_t)2 * c->cap * 2 * c->bw * 4;
-    auto ring_bytes = [&](size_t R) { return std::max(R * c->bw * 12, rows_bytes); };
-    // The largest ring that fits wins: a smaller ring with longer far lists
-    // was measured slower (1M gates, 5,000-gate levels: 116.8 against 109.9
-    // ms) although it leaves fewer fan-ins to plane-row reads.
-    // far region (far rows of two pieces, or the reverse pass's edges) and
-    // the two staged far-id lists, for lists of n entries
-    auto far_bytes = [&](size_t n) { return al(std::max(edge_bytes, n * far_entry)) + al(2 * n * 4); };
-    uint32_t ring = 0;
-    for (uint32_t R = rmax; R >= rmin && !ring; R /= 2)
-        if (fixed + far_bytes(64) + ring_bytes(R) <= budget) ring = R;
-    if (!ring) {
-        delete c;
-        return PDF_ENOTSUP;
+        c->n_pieces = (uint32_t)pieces.size();
+        if (c->n_pieces > 65536) {
+            delete c;
+            return PDF_ENOTSUP;
+        }
+        // Far fan-ins of piece i (ring of R slots): fan-ins 0..3 of its gates
+        // below b_i - R.  Those below a_{i-1} (complete when piece i - 1 starts)
+        // go to the piece's deduplicated far list, up to `limit` entries; the rest
+        // are read from their plane rows.  Fills the source words w[3..6].
+        auto far_lists = [&](uint32_t R, uint32_t limit) -> uint32_t {
+            uint32_t worst = 0;
+            far_ids.clear();
+            std::vector<uint32_t> seen(G, 0xFFFFFFFFu);  // gate -> slot in the current piece's list
+            std::vector<uint32_t> list;
+            for (size_t i = 0; i < pieces.size(); i++) {
+                Piece &p = pieces[i];
+                const uint32_t lo = p.b > R ? p.b - R : 0;
+                const uint32_t done = i ? pieces[i - 1].a : 0;
+                list.clear();
+                for (uint32_t g = p.a; g < p.b; g++) {
+                    const uint32_t nq = std::min<uint32_t>(nl->nfi[g], kInlineFanins);
+                    for (uint32_t q = 0; q < nq; q++) {
+                        const uint32_t f = edges[eoff[g] + q];
+                        uint32_t sw = f & (R - 1);
+                        if (f < lo) {
+                            sw = SRC_PLANE | f;
+                            if (f < done) {
+                                if (seen[f] == 0xFFFFFFFFu && list.size() < limit) {
+                                    seen[f] = (uint32_t)list.size();
+                                    list.push_back(f);
+                                }
+                                if (seen[f] != 0xFFFFFFFFu) sw = SRC_FAR | seen[f];
+                            }
+                        }
+                        recs[g].w[3 + q] = sw;
+                        if (sw & SRC_PLANE || sw & SRC_FAR) recs[f].w[0] |= RF_SPILL;
+                    }
+                    for (uint32_t q = kInlineFanins; q < nl->nfi[g]; q++) {  // read from edges[] at run time
+                        const uint32_t f = edges[eoff[g] + q];
+                        if (f < lo) recs[f].w[0] |= RF_SPILL;
+                    }
+                }
+                for (uint32_t f : list) seen[f] = 0xFFFFFFFFu;
+                worst = std::max<uint32_t>(worst, (uint32_t)list.size());
+                p.far_off = (uint32_t)far_ids.size();
+                p.far_n = (uint32_t)list.size();
+                far_ids.insert(far_ids.end(), list.begin(), list.end());
+                // lists start on 16-byte boundaries: the kernel stages the next
+                // piece's list by a bulk copy located from this piece's fields
+                while (far_ids.size() & 3) far_ids.push_back(0);
+            }
+            for (size_t i = 0; i < pieces.size(); i++) pieces[i].nfar_n = i + 1 < pieces.size() ? pieces[i + 1].far_n : 0;
+            return worst;
+        };
+        // Shared memory of k_forward: 2 record buffers; one region holding the
+        // reverse pass's 2 edge buffers or the forward pass's 2 far buffers;
+        // bitmap; piece bits; barriers; the ring.  The ring: the largest power of
+        // two (>= cap, <= 2 * n_gates) that leaves room for far lists of 64
+        // entries; the far lists then get the rest of the budget.
+        const size_t rec_bytes = al(2 * (size_t)c->cap * sizeof(GateRec));
+        const size_t bm_bytes = (size_t)bm_words * 4 <= 16384 ? al((size_t)bm_words * 4) : 0;
+        const size_t fixed = rec_bytes + bm_bytes + al(((size_t)c->n_pieces + 31) / 32 * 4) + 128;
+        const size_t edge_bytes = 2 * (size_t)c->ecap * 4;
+        const size_t far_entry = (size_t)2 * 3 * c->bw * 4;  // one far slot in both buffers, 3 planes
+        uint32_t rmin = 32;
+        while (rmin < c->cap) rmin *= 2;
+        uint32_t rmax = rmin;
+        while ((uint64_t)rmax < 2 * (uint64_t)G && fixed + (size_t)rmax * 2 * c->bw * 12 <= budget) rmax *= 2;
+        // the ring's memory also holds the reverse pass's row staging buffers
+        const size_t rows_bytes = (size_t)2 * c->cap * 2 * c->bw * 4;
+        auto ring_bytes = [&](size_t R) { return std::max(R * c->bw * 12, rows_bytes); };
+        // The largest ring that fits wins: a smaller ring with longer far lists
+        // was measured slower (1M gates, 5,000-gate levels: 116.8 against 109.9
+        // ms) although it leaves fewer fan-ins to plane-row reads.
+        // far region (far rows of two pieces, or the reverse pass's edges) and
+        // the two staged far-id lists, for lists of n entries
+        auto far_bytes = [&](size_t n) { return al(std::max(edge_bytes, n * far_entry)) + al(2 * n * 4); };
+        uint32_t ring = 0;
+        for (uint32_t R = rmax; R >= rmin && !ring; R /= 2)
+            if (fixed + far_bytes(64) + ring_bytes(R) <= budget) ring = R;
+        if (!ring) {
+            delete c;
+            return PDF_ENOTSUP;
+        }
+        const size_t far_room = budget - fixed - ring_bytes(ring);
+        uint32_t far_limit = (uint32_t)std::min<size_t>(kMaxFar, far_room / (far_entry + 8)) & ~3u;
+        while (far_limit > 64 && far_bytes(far_limit) > far_room) far_limit -= 4;
+        const uint32_t farcap = std::max<uint32_t>(4, (far_lists(ring, far_limit) + 3) & ~3u);
+        while (far_ids.size() < 4) far_ids.push_back(0);
+        c->ring = ring;
+        c->farcap = farcap;
+        size_t off = 0;
+        c->off_rec = (uint32_t)off;
+        off += rec_bytes;
+        c->off_edge = (uint32_t)off;
+        off += al(std::max(edge_bytes, farcap * far_entry));
+        c->off_fid = (uint32_t)off;
+        off += al(2 * (size_t)farcap * 4);
+        c->bm_shared = bm_bytes ? 1u : 0u;
+        c->off_bm = (uint32_t)off;
+        off += bm_bytes;
+        c->off_pbits = (uint32_t)off;
+        off += al(((size_t)c->n_pieces + 31) / 32 * 4);
+        c->off_mbar = (uint32_t)off;
+        off += 128;
+        c->off_ring = (uint32_t)off;
+        // reverse pass: ring2 and the row staging buffers [2][cap][2][bw] share
+        // the ring's memory
+        uint32_t ring2 = 0;
+        for (uint32_t r = 1; (size_t)r * c->bw * 4 + rows_bytes <= ring_bytes(ring); r *= 2) ring2 = r;
+        c->ring2 = ring2;
+        c->fwd_smem = off + ring_bytes(ring);
+        c->chain = c->n_pieces;
     }
-    const size_t far_room = budget - fixed - ring_bytes(ring);
-    uint32_t far_limit = (uint32_t)std::min<size_t>(kMaxFar, far_room / (far_entry + 8)) & ~3u;
-    while (far_limit > 64 && far_bytes(far_limit) > far_room) far_limit -= 4;
-    const uint32_t farcap = std::max<uint32_t>(4, (far_lists(ring, far_limit) + 3) & ~3u);
-    while (far_ids.size() < 4) far_ids.push_back(0);
-    c->ring = ring;
-    c->farcap = farcap;
-    size_t off = 0;
-    c->off_rec = (uint32_t)off;
-    off += rec_bytes;
-    c->off_edge = (uint32_t)off;
-    off += al(std::max(edge_bytes, farcap * far_entry));
-    c->off_fid = (uint32_t)off;
-    off += al(2 * (size_t)farcap * 4);
-    c->bm_shared = bm_bytes ? 1u : 0u;
-    c->off_bm = (uint32_t)off;
-    off += bm_bytes;
-    c->off_pbits = (uint32_t)off;
-    off += al(((size_t)c->n_pieces + 31) / 32 * 4);
-    c->off_mbar = (uint32_t)off;
-    off += 128;
-    c->off_ring = (uint32_t)off;
-    // reverse pass: ring2 and the row staging buffers [2][cap][2][bw] share
-    // the ring's memory
-    uint32_t ring2 = 0;
-    for (uint32_t r = 1; (size_t)r * c->bw * 4 + rows_bytes <= ring_bytes(ring); r *= 2) ring2 = r;
-    c->ring2 = ring2;
-    c->fwd_smem = off + ring_bytes(ring);
     // nets one pair may mark in the cover: as many as its shared memory holds
     c->hash_cap = 4096;
     while (c->hash_cap > 256 && cover_smem_bytes(c->hash_cap) > (size_t)prop.sharedMemPerBlockOptin) c->hash_cap -= 256;
@@ -652,6 +675,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         delete c;
         return st2;
     };
+    if (pieces.empty()) pieces.push_back(Piece{});  // (the lane kernel has none)
     if (c->rec.ensure(sizeof(GateRec) * G) != cudaSuccess ||
         c->edges.ensure(sizeof(uint32_t) * edges.size()) != cudaSuccess ||
         c->level_off.ensure(sizeof(uint32_t) * (L + 1)) != cudaSuccess ||
@@ -1434,12 +1458,23 @@ struct pdf_batch {
     cudaGraphExec_t exec = nullptr;
     bool use_graph = true;
     // side streams and fork/join events of the forward launches per class
-    cudaStream_t side[3] = {};
-    cudaEvent_t fork = nullptr, join[3] = {};
+    cudaStream_t side[kMaxBatchClasses - 1] = {};
+    cudaEvent_t fork = nullptr, join[kMaxBatchClasses - 1] = {};
     cudaStream_t up = nullptr;  // uploads of the control block
     unsigned char *host_ctl = nullptr;  // mapped pinned staging of the control block
     size_t host_bytes = 0;
+    cudaEvent_t prof[3] = {};  // pdf_batch_profile: pass start, forward joined, pass end
+    bool profiling = false;
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
     void release() {
+        for (auto &x : prof)
+            if (x) cudaEventDestroy(x);
+        for (auto &x : prof) x = nullptr;
         if (host_ctl) cudaFreeHost(host_ctl);
         host_ctl = nullptr;
         host_bytes = 0;
@@ -1474,7 +1509,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     for (uint32_t i = 0; i < n_jobs; i++) {
         const pdf_batch_job &j = jobs[i];
         if (!j.circuit || !j.state || j.state->c != j.circuit || j.circuit->device != c0->device ||
-            j.circuit->bw != c0->bw || j.circuit->mark_mode != c0->mark_mode)
+            j.circuit->mark_mode != c0->mark_mode)
             return PDF_EINVAL;
         if (j.circuit->seg_len > 1) return PDF_ENOTSUP;  // batches grade segments of one net
         const uint64_t n = j.pairs.n_pairs, W = (n + 31) / 32;
@@ -1482,10 +1517,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
             !planes_fit(j.circuit, W, j.pairs.ld, {j.pairs.v, j.pairs.t}))
             return PDF_EINVAL;
     }
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
+    b->drop_graph();
     b->device = c0->device;
     b->circuits.clear();
     b->states.clear();
@@ -1496,19 +1528,20 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     uint64_t items = 0;
     BatchLaunch &L = b->L;
     L = BatchLaunch{};
-    L.bw = c0->bw;
     L.sem = (uint32_t)c0->mark_mode;
     L.hash_cap = c0->hash_cap;
-    // Jobs in classes of equal CTAs per SM (1, 2, 4), each class one forward
-    // launch sized for its members, so the CTAs of narrow circuits share SMs
+    // Jobs in classes of equal tile width and CTAs per SM (1, 2, 4), each
+    // class one forward launch (its kernel, block size and shared memory
+    // sized for its members), so the CTAs of narrow circuits share SMs
     // instead of holding the shared memory of the widest member; within a
-    // class the longest level chains go first.
+    // class the longest CTA walks go first.
     std::vector<uint32_t> order(n_jobs);
     for (uint32_t i = 0; i < n_jobs; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
         const pdf_circuit *cx = jobs[x].circuit, *cy = jobs[y].circuit;
+        if (cx->bw != cy->bw) return cx->bw > cy->bw;
         if (cx->occ != cy->occ) return cx->occ < cy->occ;
-        return cx->n_pieces > cy->n_pieces;
+        return cx->chain > cy->chain;
     });
     for (uint32_t k = 0; k < n_jobs; k++) {
         const pdf_batch_job &j = jobs[order[k]];
@@ -1545,8 +1578,10 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         L.threads = std::max(L.threads, c->threads);
         L.fwd_smem = std::max(L.fwd_smem, c->fwd_smem);
         L.cover_grid = std::max(L.cover_grid, c->cover_grid);
-        if (!L.n_class || L.cls[L.n_class - 1].occ != c->occ) {
+        if (!L.n_class || L.cls[L.n_class - 1].occ != c->occ || L.cls[L.n_class - 1].bw != c->bw) {
+            if (L.n_class == kMaxBatchClasses) return PDF_ENOTSUP;
             BatchClass &k2 = L.cls[L.n_class++];
+            k2.bw = c->bw;
             k2.occ = c->occ;
             k2.blk0 = bp[i];
         }
@@ -1563,11 +1598,13 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         if (!b->side[k - 1]) PDF_CUDA(cudaStreamCreateWithFlags(&b->side[k - 1], cudaStreamNonBlocking));
         if (!b->join[k - 1]) PDF_CUDA(cudaEventCreateWithFlags(&b->join[k - 1], cudaEventDisableTiming));
     }
-    for (uint32_t k = 0; k < 3; k++) {
+    for (uint32_t k = 0; k + 1 < kMaxBatchClasses; k++) {
         L.side[k] = b->side[k];
         L.join[k] = b->join[k];
     }
     L.fork = b->fork;
+    for (uint32_t k = 0; k < 3; k++) L.prof[k] = b->profiling ? b->prof[k] : nullptr;
+    L.prof_external = b->use_graph ? 1u : 0u;
     L.n = n_jobs;
     L.total_blocks = bp[n_jobs];
     for (uint32_t k = 0; k < L.n_class; k++)
@@ -1666,7 +1703,7 @@ extern "C" void pdf_batch_destroy(pdf_batch *b) {
 extern "C" pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info) {
     if (!b || !info) return PDF_EINVAL;
     info->n_jobs = b->L.n;
-    info->tile_words = b->L.bw;
+    info->tile_words = b->L.n_class ? b->L.cls[0].bw : 0;  // of the first forward class
     info->threads = b->L.threads;
     info->ctas = b->L.total_blocks;
     info->gate_evals = b->gate_evals;
@@ -1703,6 +1740,31 @@ extern "C" pdf_status pdf_batch_run_async(pdf_batch *b, void *stream) {
     return PDF_OK;
 }
 
+extern "C" pdf_status pdf_batch_profile(pdf_batch *b, int enable) {
+    if (!b) return PDF_EINVAL;
+    DeviceGuard dg(b->device);
+    if (!dg.ok) return PDF_ECUDA;
+    if (enable && !b->prof[0])
+        for (auto &e : b->prof) PDF_CUDA(cudaEventCreate(&e));
+    b->profiling = enable != 0;
+    for (uint32_t k = 0; k < 3; k++) b->L.prof[k] = b->profiling ? b->prof[k] : nullptr;
+    b->drop_graph();  // captured again at the next run, with or without the events
+    return PDF_OK;
+}
+
+extern "C" pdf_status pdf_batch_profile_read(pdf_batch *b, double *ms) {
+    if (!b || !ms || !b->profiling) return PDF_EINVAL;
+    DeviceGuard dg(b->device);
+    if (!dg.ok) return PDF_ECUDA;
+    float f = 0.0f, c = 0.0f;
+    PDF_CUDA(cudaEventSynchronize(b->prof[2]));
+    PDF_CUDA(cudaEventElapsedTime(&f, b->prof[0], b->prof[1]));
+    PDF_CUDA(cudaEventElapsedTime(&c, b->prof[1], b->prof[2]));
+    ms[0] = f;
+    ms[1] = c;
+    return PDF_OK;
+}
+
 extern "C" pdf_status pdf_batch_run(pdf_batch *b, void *stream) {
     pdf_status st = pdf_batch_run_async(b, stream);
     if (st != PDF_OK) return st;
@@ -1734,6 +1796,7 @@ extern "C" pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, con
     for (uint32_t tw : {2u, 4u, 8u})
         for (uint32_t th : {0u, 256u})
             if (!b0.threads || th == 0) cand.push_back({tw, b0.threads ? b0.threads : th});
+    if (!b0.threads) cand.push_back({kLaneWords, 0u});  // the lane kernel (1,024 threads)
     for (const auto &cw : cand) {
         const uint32_t tw = cw.first;
         pdf_circuit_opts o = b0;

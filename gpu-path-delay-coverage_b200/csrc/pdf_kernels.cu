@@ -692,6 +692,283 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
 }
 
 // ---------------------------------------------------------------------------
+// Lane forward kernel (tile of 32 words, 1,024 pairs per CTA): the same
+// stages as forward_cta (sim, forward mark, prune, merge) with the roles of
+// threads turned around.  Lane j of every warp carries word w0 + j of the
+// column block, and a warp evaluates one gate at a time for all 32 words, so
+// every instruction of a gate is uniform across the warp (no divergence on
+// gate type or fan-in count), a gate's record is decoded once per 1,024
+// pairs, and every plane-row access is one coalesced 128-byte line.  Warps
+// take the gates of a level in turn; the gates of a level depend only on
+// lower levels, so a CTA needs one barrier per level (not per piece of a
+// level), and every fan-in is read from its plane row (L1/L2), which is what
+// wide levels need: nothing of the circuit is kept on chip except the
+// block's mark bitmap.  Two gates per warp are in flight at a time (their
+// records, then their fan-in rows are loaded before either is evaluated).
+//
+// Every gate with fan-outs writes its V and T rows (its readers load them);
+// a gate writes its M row only when it holds a mark (every reader of a mark
+// row tests the gate's bitmap bit first), or when the caller asked for the
+// planes (store_all).
+// ---------------------------------------------------------------------------
+
+// Fan-in rows of one gate, loaded before it is evaluated.
+struct LaneIn {
+    GateRec r;
+    uint32_t fv[kInlineFanins], ft[kInlineFanins];
+    uint32_t m0;                 // mark row of fan-in 0 (when its bitmap bit is set)
+    uint32_t fm[kInlineFanins];  // FIXED modes: mark rows of fan-ins 0..3 with their bits set
+    uint32_t sv, st;             // stage call pdf_mark: the gate's own given V and T
+    bool bit0;                   // fan-in 0 holds a mark in this column block
+};
+
+template <int SEM, int MODE>
+__device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, uint32_t g, uint32_t w, bool live,
+                                          LaneIn &x) {
+    constexpr bool FIX = SEM >= 2;
+    const uint32_t h = x.r.w[0], nfi = rec_nfi(x.r);
+    const size_t o = (size_t)g * a.ld + w;
+#pragma unroll
+    for (int q = 0; q < kInlineFanins; q++) {
+        x.fv[q] = 0;
+        x.ft[q] = 0;
+        x.fm[q] = 0;
+    }
+    x.m0 = 0;
+    x.sv = 0;
+    x.st = 0;
+    x.bit0 = false;
+    if (h & RF_INPT) {
+        if (MODE == FWD_MARK) {
+            x.fv[0] = live ? a.V[o] : 0u;
+            x.ft[0] = live ? a.T[o] : 0u;
+        } else {
+            const size_t po = (size_t)g * a.pi_ld + w;
+            x.fv[0] = live ? __ldg(a.pi_v + po) : 0u;
+            x.ft[0] = live ? __ldg(a.pi_t + po) : 0u;
+        }
+        return;
+    }
+    if (MODE == FWD_MARK) {  // the gate's own values are given; fan-ins feed the side test only
+        x.sv = live ? a.V[o] : 0u;
+        x.st = live ? a.T[o] : 0u;
+    }
+    // a killed gate's value is S0 whatever its fan-ins (and it cannot mark)
+    const uint32_t nl = (h & RF_KILL) ? 0u : min(nfi, (uint32_t)kInlineFanins);
+    if (MODE != FWD_SIM) x.bit0 = bit_test(bm, x.r.w[7]);
+#pragma unroll
+    for (int q = 0; q < kInlineFanins; q++) {
+        if ((uint32_t)q < nl && live) {
+            const size_t fo = (size_t)x.r.w[3 + q] * a.ld + w;
+            x.fv[q] = a.V[fo];
+            x.ft[q] = a.T[fo];
+            if (FIX && MODE != FWD_SIM && bit_test(bm, x.r.w[3 + q])) x.fm[q] = a.M[fo];
+        }
+    }
+    if (!FIX && MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live)
+        x.m0 = a.M[(size_t)x.r.w[7] * a.ld + w];
+}
+
+// Evaluate, mark and store one gate; returns whether it holds a mark in the
+// block (warp-uniform).
+template <int SEM, int MODE>
+__device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, uint32_t g, uint32_t w, bool live,
+                                          uint32_t wmask, const LaneIn &x) {
+    constexpr bool FIX = SEM >= 2;
+    const GateRec &r = x.r;
+    const uint32_t h = r.w[0], nfi = rec_nfi(r);
+    const size_t o = (size_t)g * a.ld + w;
+    auto row = [&](const uint32_t *pl, uint32_t f) -> uint32_t { return live ? pl[(size_t)f * a.ld + w] : 0u; };
+    uint32_t V, T, M = 0;
+    if (h & RF_INPT) {
+        V = x.fv[0] & wmask;
+        T = x.ft[0] & wmask;
+    } else if (MODE == FWD_MARK) {
+        V = x.sv & wmask;
+        T = x.st & wmask;
+    } else {
+        uint32_t v1;
+        eval_first(h, x.fv[0], x.ft[0], V, v1);
+        const uint32_t nfold = hdr_nfold(h);
+#pragma unroll
+        for (int q = 1; q < kInlineFanins; q++)
+            if ((uint32_t)q <= nfold) eval_fold<FIX>(h, V, v1, x.fv[q], x.ft[q]);
+        for (uint32_t q = kInlineFanins; q <= nfold; q++) {
+            const uint32_t f = __ldg(a.c.edges + r.w[2] + q);
+            eval_fold<FIX>(h, V, v1, row(a.V, f), row(a.T, f));
+        }
+        eval_finish<FIX>(h, V, v1, T);
+        V &= wmask;
+        T &= wmask;
+    }
+    if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
+        const bool anyT = __any_sync(0xFFFFFFFFu, T != 0);
+        if (h & RF_INPT) {
+            M = T;
+        } else if (!FIX && (h & RF_MARKF0) && x.bit0 && anyT) {
+            // fan-in 0 (gate w[7]) holds a mark: its bitmap bit is set
+            M = T & x.m0;
+            if ((h & RF_SENS) && __any_sync(0xFFFFFFFFu, M != 0)) {
+                // the side test over the fan-in rows already loaded (past the
+                // fourth, read here)
+                SensAcc s;
+                sens_init(s);
+                const bool or_like = (h & RF_IM) != 0;
+#pragma unroll
+                for (int q = 0; q < kInlineFanins; q++)
+                    if ((uint32_t)q < nfi) sens_step<SEM & 1>(s, or_like, x.fv[q], x.ft[q]);
+                for (uint32_t q = kInlineFanins; q < nfi; q++) {
+                    const uint32_t f = __ldg(a.c.edges + r.w[2] + q);
+                    sens_step<SEM & 1>(s, or_like, row(a.V, f), row(a.T, f));
+                }
+                M &= sens_result<SEM & 1>(s);
+            }
+        } else if (FIX && (h & RF_MANY) && anyT) {
+            // any fan-in may carry the path: its own mark enters the side test
+            const uint32_t mor = flagmask(h, RF_IM), mxor = flagmask(h, RF_XOR), mand = ~(mor | mxor);
+            SensAcc s;
+            sens_init(s);
+#pragma unroll
+            for (int q = 0; q < kInlineFanins; q++)
+                if ((uint32_t)q < nfi)
+                    sens_step_fixed<SEM == PDF_MARK_FIXED_NONROBUST>(s, mand, mor, mxor, x.fv[q], x.ft[q], x.fm[q]);
+            for (uint32_t q = kInlineFanins; q < nfi; q++) {
+                const uint32_t f = __ldg(a.c.edges + r.w[2] + q);
+                const uint32_t fm = bit_test(bm, f) ? row(a.M, f) : 0u;
+                sens_step_fixed<SEM == PDF_MARK_FIXED_NONROBUST>(s, mand, mor, mxor, row(a.V, f), row(a.T, f), fm);
+            }
+            M = T & sens_result<SEM == PDF_MARK_FIXED_NONROBUST>(s);
+        }
+    }
+    const bool marked = MODE != FWD_SIM && __any_sync(0xFFFFFFFFu, M != 0);
+    if (live) {
+        if (MODE != FWD_MARK && (a.store_all || r.w[1] || marked)) {
+            a.V[o] = V;
+            a.T[o] = T;
+        }
+        if (MODE != FWD_SIM && (a.store_all || marked)) a.M[o] = M;
+    }
+    if (marked && (threadIdx.x & 31) == 0) atomicOr(bm + (g >> 5), 1u << (g & 31));
+    return marked;
+}
+
+template <int SEM, int MODE>
+__device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32_t blk) {
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
+    const uint32_t w0 = blk * 32, w = w0 + lane;
+    const bool live = w < a.W;
+    const uint32_t wmask = !live ? 0u
+                                 : (w + 1 < a.W ? 0xFFFFFFFFu
+                                                : ((a.n_pairs & 31) ? (1u << (a.n_pairs & 31)) - 1u : 0xFFFFFFFFu));
+    uint32_t *bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
+    uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
+    const uint32_t *lo = a.c.level_off;
+    const uint32_t L = a.c.n_levels;
+
+    if (MODE != FWD_SIM)
+        for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) bm[q] = 0;
+    if (MODE == FWD_FUSED) {  // the batch's cover state (the cover kernels run after this one)
+        if (a.active && threadIdx.x < 32 && w0 + threadIdx.x <= a.W) a.active[w0 + threadIdx.x] = 0;
+        if (a.active && blk == 0 && threadIdx.x == 0) a.active[a.W] = 0;
+        if (a.acc && blk == 0 && threadIdx.x == 0) {
+            a.acc->batch_lo = 0;
+            a.acc->batch_hi = 0;
+            a.acc->batch_flags = 0;
+            a.acc->done = 0;
+        }
+    }
+    __syncthreads();
+
+    // ------------------------------------------------------------- forward
+    uint32_t top = 0;  // levels below `top` may hold a forward mark
+    for (uint32_t l = 0; l < L; l++) {
+        const uint32_t ga = __ldg(lo + l), gb = __ldg(lo + l + 1);
+        bool any = false;
+        for (uint32_t g = ga + warp; g < gb; g += 2 * NW) {
+            const uint32_t g1 = g + NW;
+            const bool two = g1 < gb;
+            LaneIn x0, x1;
+            x0.r = load_rec(a.c.rec + g);
+            if (two) x1.r = load_rec(a.c.rec + g1);
+            lane_load<SEM, MODE>(a, bm, g, w, live, x0);
+            if (two) lane_load<SEM, MODE>(a, bm, g1, w, live, x1);
+            any |= lane_gate<SEM, MODE>(a, bm, g, w, live, wmask, x0);
+            if (two) any |= lane_gate<SEM, MODE>(a, bm, g1, w, live, wmask, x1);
+        }
+        if (__syncthreads_or(any)) top = l + 1;
+    }
+    if constexpr (MODE == FWD_SIM) {
+        return;
+    } else {
+        if (MODE == FWD_MARK && a.no_prune) return;
+        // ------------------------------------------------- prune and merge
+        // (markkernel.cuh:271-293, mergekernel.cuh:116-198) levels descending;
+        // a warp takes 32-gate words of the bitmap and visits their marked
+        // gates; a gate's pruned mark is final once its fan-outs' are.
+        uint32_t maxlvl = 0;
+        for (int l = (int)top - 1; l >= 0; l--) {
+            const uint32_t ga = __ldg(lo + l), gb = __ldg(lo + l + 1);
+            bool any = false;
+            for (uint32_t q = (ga >> 5) + warp; q < (gb + 31) >> 5; q += NW) {
+                uint32_t bits = bm[q];
+                if (q == ga >> 5 && (ga & 31)) bits &= ~((1u << (ga & 31)) - 1u);
+                if (q == (gb - 1) >> 5 && (gb & 31)) bits &= (1u << (gb & 31)) - 1u;
+                while (bits) {
+                    const uint32_t g = q * 32 + (__ffs(bits) - 1);
+                    bits &= bits - 1;
+                    const GateRec r = load_rec(a.c.rec + g);
+                    const size_t o = (size_t)g * a.ld + w;
+                    const uint32_t mk = live ? a.M[o] : 0u;
+                    uint32_t keep = rec_po(r) ? 0xFFFFFFFFu : 0u;
+                    if (!rec_po(r)) {
+                        const uint32_t nfo = r.w[1], base = r.w[2] + rec_nfi(r);
+                        for (uint32_t k = 0; k < nfo; k += 4) {  // four fan-out rows in flight
+                            uint32_t fo[4], m[4];
+#pragma unroll
+                            for (int u = 0; u < 4; u++) fo[u] = k + u < nfo ? __ldg(a.c.edges + base + k + u) : kEmpty;
+#pragma unroll
+                            for (int u = 0; u < 4; u++)
+                                m[u] = fo[u] != kEmpty && live && bit_test(bm, fo[u]) ? a.M[(size_t)fo[u] * a.ld + w]
+                                                                                       : 0u;
+                            keep |= m[0] | m[1] | m[2] | m[3];
+                        }
+                    }
+                    const uint32_t nm = mk & keep;
+                    if (live && nm != mk) a.M[o] = nm;
+                    const bool nz = __any_sync(0xFFFFFFFFu, nm != 0);
+                    if (!nz) {
+                        if (lane == 0) atomicAnd(bm + (g >> 5), ~(1u << (g & 31)));
+                    } else if (MODE == FWD_FUSED && a.first_x) {  // merge: first falling / rising pair
+                        const uint32_t v = live ? a.V[o] : 0u;
+                        const uint32_t x = nm & ~v, y = nm & v;
+                        uint32_t cx = x ? w * 32 + (__ffs(x) - 1) : kEmpty;
+                        uint32_t cy = y ? w * 32 + (__ffs(y) - 1) : kEmpty;
+                        cx = __reduce_min_sync(0xFFFFFFFFu, cx);
+                        cy = __reduce_min_sync(0xFFFFFFFFu, cy);
+                        if (lane == 0) {
+                            if (cx != kEmpty) atomicMin(a.first_x + g, a.pair_base + cx);
+                            if (cy != kEmpty) atomicMin(a.first_y + g, a.pair_base + cy);
+                        }
+                    }
+                    any |= nz;
+                }
+            }
+            if (__syncthreads_or(any) && !maxlvl) maxlvl = (uint32_t)l + 1;
+        }
+        // publish the bitmap of surviving marks for the cover kernels
+        if (a.bm_shared && gbm)
+            for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) gbm[q] = bm[q];
+        if (threadIdx.x == 0) a.blk_maxlvl[blk] = maxlvl;
+    }
+}
+
+template <int SEM, int MODE>
+__global__ void __launch_bounds__(kLaneThreads, 1) k_forward_lanes(const FwdArgs a) {
+    forward_lanes_cta<SEM, MODE>(a, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
 // Cover.
 // ---------------------------------------------------------------------------
 
@@ -1193,6 +1470,27 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
     forward_cta<BW, SEM, FWD_FUSED>(s_a, s_blk);
 }
 
+// The same for the circuits of a batch that take the lane kernel.
+template <int SEM>
+__global__ void __launch_bounds__(kLaneThreads, 1)
+    k_batch_forward_lanes(const FwdArgs *args, const uint32_t *bpref, uint32_t n, BatchCtl *ctl, uint32_t blk0) {
+    __shared__ FwdArgs s_a;
+    __shared__ uint32_t s_blk;
+    if (threadIdx.x == 0) {
+        const uint32_t gb = blk0 + blockIdx.x;
+        const uint32_t ci = prefix_find(bpref, n, gb);
+        s_a = args[ci];
+        s_blk = gb - __ldg(bpref + ci);
+        if (gb == 0) {
+            ctl->n_items = 0;
+            ctl->done = 0;
+            ctl->err = 0;
+        }
+    }
+    __syncthreads();
+    forward_lanes_cta<SEM, FWD_FUSED>(s_a, s_blk);
+}
+
 __global__ void k_batch_active(const CoverArgs *args, const uint32_t *gpref, uint32_t n, uint2 *items,
                                BatchCtl *ctl) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1304,6 +1602,36 @@ cudaError_t launch_fwd_t(const FwdArgs &a, uint32_t threads, size_t smem, cudaSt
     return cudaGetLastError();
 }
 
+template <int SEM, int MODE>
+cudaError_t launch_lanes_t(const FwdArgs &a, uint32_t threads, size_t smem, cudaStream_t st) {
+    auto kern = k_forward_lanes<SEM, MODE>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = (a.W + kLaneWords - 1) / kLaneWords;
+    if (blocks == 0 || threads % 32 || threads > kLaneThreads) return cudaErrorInvalidValue;
+    kern<<<blocks, threads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int SEM>
+cudaError_t launch_lanes_sem(const FwdArgs &a, int mode, uint32_t threads, size_t smem, cudaStream_t st) {
+    switch (mode) {
+        case FWD_FUSED: return launch_lanes_t<SEM, FWD_FUSED>(a, threads, smem, st);
+        case FWD_SIM: return launch_lanes_t<SEM, FWD_SIM>(a, threads, smem, st);
+        default: return launch_lanes_t<SEM, FWD_MARK>(a, threads, smem, st);
+    }
+}
+
+cudaError_t launch_lanes(const FwdArgs &a, int mode, int sem, uint32_t threads, size_t smem, cudaStream_t st) {
+    switch (sem) {
+        case 0: return launch_lanes_sem<0>(a, mode, threads, smem, st);
+        case 1: return launch_lanes_sem<1>(a, mode, threads, smem, st);
+        case 2: return launch_lanes_sem<2>(a, mode, threads, smem, st);
+        case 3: return launch_lanes_sem<3>(a, mode, threads, smem, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 template <int BW, int SEM>
 cudaError_t launch_fwd_sem(const FwdArgs &a, int mode, uint32_t threads, size_t smem, cudaStream_t st) {
     switch (mode) {
@@ -1348,9 +1676,28 @@ int regs_bw(int sem) {
         default: return -1;
     }
 }
+template <int SEM>
+int regs_lanes_t() {
+    cudaFuncAttributes fa{}, fb{};
+    if (cudaFuncGetAttributes(&fa, k_forward_lanes<SEM, FWD_FUSED>) != cudaSuccess ||
+        cudaFuncGetAttributes(&fb, k_batch_forward_lanes<SEM>) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return -1;
+    }
+    return std::max(fa.numRegs, fb.numRegs);
+}
 }  // namespace
 
 int forward_kernel_regs(int bw, int sem) {
+    if (bw == (int)kLaneWords) {
+        switch (sem) {
+            case 0: return regs_lanes_t<0>();
+            case 1: return regs_lanes_t<1>();
+            case 2: return regs_lanes_t<2>();
+            case 3: return regs_lanes_t<3>();
+            default: return -1;
+        }
+    }
     switch (bw) {
         case 1: return regs_bw<1>(sem);
         case 2: return regs_bw<2>(sem);
@@ -1362,6 +1709,7 @@ int forward_kernel_regs(int bw, int sem) {
 
 cudaError_t launch_forward(const FwdArgs &a, int mode, int sem, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st) {
+    if (bw == kLaneWords) return launch_lanes(a, mode, sem, threads, smem, st);
     switch (bw) {
         case 1: return launch_fwd_bw<1>(a, mode, sem, threads, smem, st);
         case 2: return launch_fwd_bw<2>(a, mode, sem, threads, smem, st);
@@ -1394,13 +1742,63 @@ cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bo
     return cudaGetLastError();
 }
 
-template <int BW, int SEM>
-cudaError_t prepare_batch_t(const BatchLaunch &b) {
-    size_t smem = 0;
-    for (uint32_t k = 0; k < b.n_class; k++) smem = std::max(smem, b.cls[k].smem);
-    cudaError_t e = cudaFuncSetAttribute(k_batch_forward<BW, SEM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
+namespace {
+// Kernel attributes and launch of one forward class (tile width, semantics).
+template <int SEM>
+cudaError_t prepare_class_sem(uint32_t bw, size_t smem) {
+    const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    switch (bw) {
+        case 1: return cudaFuncSetAttribute(k_batch_forward<1, SEM>, attr, (int)smem);
+        case 2: return cudaFuncSetAttribute(k_batch_forward<2, SEM>, attr, (int)smem);
+        case 4: return cudaFuncSetAttribute(k_batch_forward<4, SEM>, attr, (int)smem);
+        case 8: return cudaFuncSetAttribute(k_batch_forward<8, SEM>, attr, (int)smem);
+        case kLaneWords: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM>, attr, (int)smem);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int SEM>
+cudaError_t launch_class_sem(const BatchLaunch &b, const BatchClass &c, cudaStream_t s) {
+    switch (c.bw) {
+        case 1: k_batch_forward<1, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0); break;
+        case 2: k_batch_forward<2, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0); break;
+        case 4: k_batch_forward<4, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0); break;
+        case 8: k_batch_forward<8, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0); break;
+        case kLaneWords:
+            k_batch_forward_lanes<SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
+            break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+cudaError_t prepare_class(uint32_t sem, uint32_t bw, size_t smem) {
+    switch (sem) {
+        case 0: return prepare_class_sem<0>(bw, smem);
+        case 1: return prepare_class_sem<1>(bw, smem);
+        case 2: return prepare_class_sem<2>(bw, smem);
+        case 3: return prepare_class_sem<3>(bw, smem);
+        default: return cudaErrorInvalidValue;
+    }
+}
+cudaError_t launch_class(const BatchLaunch &b, const BatchClass &c, cudaStream_t s) {
+    switch (b.sem) {
+        case 0: return launch_class_sem<0>(b, c, s);
+        case 1: return launch_class_sem<1>(b, c, s);
+        case 2: return launch_class_sem<2>(b, c, s);
+        case 3: return launch_class_sem<3>(b, c, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
+
+cudaError_t prepare_batch(const BatchLaunch &b) {
+    for (uint32_t k = 0; k < b.n_class; k++) {
+        // every class of one tile width shares its kernel: the largest request wins
+        size_t smem = 0;
+        for (uint32_t j = 0; j < b.n_class; j++)
+            if (b.cls[j].bw == b.cls[k].bw) smem = std::max(smem, b.cls[j].smem);
+        const cudaError_t e = prepare_class(b.sem, b.cls[k].bw, smem);
+        if (e != cudaSuccess) return e;
+    }
     return cudaFuncSetAttribute(k_batch_cover, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)cover_smem_bytes(b.hash_cap));
 }
@@ -1410,9 +1808,11 @@ cudaError_t prepare_batch_t(const BatchLaunch &b) {
 // wait for `st` and that `st` waits for before the cover.  Run one after
 // another, a class's last CTAs held the GPU alone (its longest level chain)
 // before the next class could start.
-template <int BW, int SEM>
-cudaError_t launch_batch_t(const BatchLaunch &b, cudaStream_t st) {
+cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
+    if (!b.n || !b.total_blocks) return cudaErrorInvalidValue;
     cudaError_t e = cudaSuccess;
+    const unsigned pflag = b.prof_external ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (b.prof[0] && (e = cudaEventRecordWithFlags(b.prof[0], st, pflag)) != cudaSuccess) return e;
     bool fork = false;  // recorded before the first class's launch, which it must not wait for
     for (uint32_t k = 1; k < b.n_class; k++) fork |= b.cls[k].blocks && b.side[k - 1];
     if (fork && (e = cudaEventRecord(b.fork, st)) != cudaSuccess) return e;
@@ -1424,45 +1824,20 @@ cudaError_t launch_batch_t(const BatchLaunch &b, cudaStream_t st) {
             s = b.side[k - 1];
             if ((e = cudaStreamWaitEvent(s, b.fork, 0)) != cudaSuccess) return e;
         }
-        k_batch_forward<BW, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = launch_class(b, c, s)) != cudaSuccess) return e;
         if (s != st) {
             if ((e = cudaEventRecord(b.join[k - 1], s)) != cudaSuccess) return e;
             if ((e = cudaStreamWaitEvent(st, b.join[k - 1], 0)) != cudaSuccess) return e;
         }
     }
+    if (b.prof[1] && (e = cudaEventRecordWithFlags(b.prof[1], st, pflag)) != cudaSuccess) return e;
     k_batch_active<<<(b.total_gates + 255) / 256, 256, 0, st>>>(b.cargs, b.gpref, b.n, b.items, b.ctl);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_batch_cover<<<b.cover_grid, 256, cover_smem_bytes(b.hash_cap), st>>>(b.cargs, b.fargs, b.n, b.items, b.ctl,
                                                                          b.append);
-    return cudaGetLastError();
-}
-
-// (tile words, semantics) -> the instantiation; `prep` selects prepare or launch
-template <int BW>
-cudaError_t batch_bw(const BatchLaunch &b, cudaStream_t st, bool prep) {
-    switch (b.sem) {
-        case 0: return prep ? prepare_batch_t<BW, 0>(b) : launch_batch_t<BW, 0>(b, st);
-        case 1: return prep ? prepare_batch_t<BW, 1>(b) : launch_batch_t<BW, 1>(b, st);
-        case 2: return prep ? prepare_batch_t<BW, 2>(b) : launch_batch_t<BW, 2>(b, st);
-        case 3: return prep ? prepare_batch_t<BW, 3>(b) : launch_batch_t<BW, 3>(b, st);
-        default: return cudaErrorInvalidValue;
-    }
-}
-cudaError_t batch_dispatch(const BatchLaunch &b, cudaStream_t st, bool prep) {
-    switch (b.bw) {
-        case 1: return batch_bw<1>(b, st, prep);
-        case 2: return batch_bw<2>(b, st, prep);
-        case 4: return batch_bw<4>(b, st, prep);
-        case 8: return batch_bw<8>(b, st, prep);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
-cudaError_t prepare_batch(const BatchLaunch &b) { return batch_dispatch(b, nullptr, true); }
-cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
-    if (!b.n || !b.total_blocks) return cudaErrorInvalidValue;
-    return batch_dispatch(b, st, false);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (b.prof[2] && (e = cudaEventRecordWithFlags(b.prof[2], st, pflag)) != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 cudaError_t launch_seg_merge(const SegMergeArgs &a, uint32_t n_blocks, cudaStream_t st) {

@@ -117,6 +117,14 @@ struct SegMergeArgs {
     uint32_t *first_x, *first_y;  // [S]
 };
 
+// Tile width of the lane forward kernel (k_forward_lanes): one warp lane per
+// word, so a column block is 32 words (1,024 pairs) and a CTA 1,024 threads.
+constexpr uint32_t kLaneWords = 32;
+constexpr uint32_t kLaneThreads = 1024;
+// Forward launches of a batch at most: tile widths 1, 2, 4, 8 at 1, 2, 4
+// CTAs per SM, and the lane kernel.
+constexpr uint32_t kMaxBatchClasses = 8;
+
 // Batched grading (k_batch_forward, k_batch_active, k_batch_cover).
 struct BatchCtl {
     unsigned int n_items;  // first-detecting (circuit, pair) items of this pass
@@ -124,9 +132,9 @@ struct BatchCtl {
     unsigned int err;      // OR of every circuit's device error word after the pass
     unsigned int pad;
 };
-// One forward launch of a batch: jobs of equal CTAs per SM.
+// One forward launch of a batch: jobs of equal tile width and CTAs per SM.
 struct BatchClass {
-    uint32_t occ, blk0, blocks, threads;
+    uint32_t bw, occ, blk0, blocks, threads;
     size_t smem;
 };
 struct BatchLaunch {
@@ -137,14 +145,19 @@ struct BatchLaunch {
     uint2 *items;          // [sum of min(n_pairs, 2 n_gates)]
     BatchCtl *ctl;
     uint32_t n, total_blocks, total_gates;
-    uint32_t bw, sem, threads, cover_grid, hash_cap, append;  // sem: PDF_MARK_*
+    uint32_t sem, threads, cover_grid, hash_cap, append;  // sem: PDF_MARK_*
     size_t fwd_smem;
-    uint32_t n_class;      // forward launches: classes of jobs (at most 3: 1, 2, 4 CTAs per SM)
-    BatchClass cls[4];
+    uint32_t n_class;      // forward launches: classes of jobs (tile width x CTAs per SM)
+    BatchClass cls[kMaxBatchClasses];
     // classes after the first run on side streams, forked from and joined
     // back to the launching stream (parallel branches when captured)
-    cudaStream_t side[3];
-    cudaEvent_t fork, join[3];
+    cudaStream_t side[kMaxBatchClasses - 1];
+    cudaEvent_t fork, join[kMaxBatchClasses - 1];
+    // profiling (optional): events recorded on the launching stream before
+    // the forward launches, after they have all joined, and after the cover;
+    // prof_external: recorded as event nodes of a captured graph
+    cudaEvent_t prof[3];
+    uint32_t prof_external;
 };
 // Registers per thread of the fused forward kernel for (tile words, mode); <= 0 on error.
 int forward_kernel_regs(int bw, int sem);

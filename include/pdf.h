@@ -397,6 +397,15 @@ pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info);
 pdf_status pdf_batch_run_async(pdf_batch *b, void *stream);
 /* pdf_batch_run_async, then wait; reports a device-side error of any job. */
 pdf_status pdf_batch_run(pdf_batch *b, void *stream);
+/* Timing of a batch's passes (no reference counterpart).  With enable != 0
+ * every later run records CUDA events on the run's stream (as event nodes of
+ * the captured graph) before the forward launches, after they have all
+ * joined, and after the cover; pdf_batch_profile_read waits for the most
+ * recent run and returns ms[0] = its forward span (every class's forward
+ * launch, side by side) and ms[1] = its cover (k_batch_active + k_batch_cover).
+ * Switching profiling on or off recaptures the graph at the next run. */
+pdf_status pdf_batch_profile(pdf_batch *b, int enable);
+pdf_status pdf_batch_profile_read(pdf_batch *b, double ms[2]);
 
 /*
  * Autotuner of the batch's tile shape: for each candidate (tile width in words

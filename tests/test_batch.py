@@ -14,7 +14,8 @@ O = helpers.oracle()
 
 
 def _jobs(mode, tile=4, seed=0):
-    """Circuits of many shapes and pair counts (including ragged tails)."""
+    """Circuits of many shapes and pair counts (including ragged tails).
+    tile: one tile width for every job, or a list of widths taken in turn."""
     import torch
     shapes = [s[1] for s in circuits.small_suite()[:6]]
     shapes += [circuits.random_small(500 + seed, n_gates=3000, n_pi=120, n_po=400, depth=25),
@@ -24,11 +25,13 @@ def _jobs(mode, tile=4, seed=0):
     counts = [33, 1000, 1, 2500, 64, 777, 4096, 700, 3001, 900, 40]
     rng = np.random.default_rng(11 + seed)
     jobs, want = [], []
-    for nl, n in zip(shapes, counts):
+    tiles = tile if isinstance(tile, list) else [tile]
+    for k, (nl, n) in enumerate(zip(shapes, counts)):
+        tw = tiles[k % len(tiles)]
         codes = helpers.rand_codes(rng, nl.n_pi, n)
-        ld = (P.words(n) + tile - 1) // tile * tile
+        ld = (P.words(n) + tw - 1) // tw * tw
         v, t = P.planes_from_codes(codes, ld)
-        c = P.Circuit(nl, mark_mode=mode, tile_words=tile)
+        c = P.Circuit(nl, mark_mode=mode, tile_words=tw)
         s = P.State(c)
         dv = torch.from_numpy(v.view(np.int32)).cuda()
         dt = torch.from_numpy(t.view(np.int32)).cuda()
@@ -37,9 +40,12 @@ def _jobs(mode, tile=4, seed=0):
     return jobs, want
 
 
+@pytest.mark.parametrize("tile", [4, 32, [32, 4, 8, 2]], ids=["walk4", "lanes", "mixed"])
 @pytest.mark.parametrize("mode", [0, 1, 2, 3])
-def test_batch_equals_each_job_alone(mode):
-    jobs, want = _jobs(mode)
+def test_batch_equals_each_job_alone(mode, tile):
+    """Every tile width in one batch (mixed: one forward launch per class of
+    tile width and CTAs per SM)."""
+    jobs, want = _jobs(mode, tile)
     b = P.Batch(jobs)
     b.run()
     info = b.info()
@@ -109,19 +115,48 @@ def test_batch_rebind_to_other_jobs():
         np.testing.assert_array_equal(fx, w.first_x)
 
 
-def test_batch_rejects_mixed_tiles():
+def test_batch_rejects_mixed_mark_modes():
     jobs, _ = _jobs(0)
     c, s, dv, dt, n, base = jobs[0]
-    c8 = P.Circuit(c.netlist, tile_words=8)
-    s8 = P.State(c8)
+    c1 = P.Circuit(c.netlist, mark_mode=1)
+    s1 = P.State(c1)
     with pytest.raises(P.PdfError):
-        P.Batch([jobs[1], (c8, s8, dv, dt, n, base)])
+        P.Batch([jobs[1], (c1, s1, dv, dt, n, base)])
+
+
+def test_batch_append_mixed_tiles():
+    """Appending runs over a batch whose jobs take different kernels."""
+    jobs, want = _jobs(1, [32, 4], seed=4)
+    b = P.Batch(jobs, append=True)
+    b.run()
+    b.run()  # the same planes again: pairs [n, 2n) repeat pairs [0, n)
+    for (c, s, *_), (nl, codes, n) in zip(jobs, want):
+        w = O.grade(nl, np.concatenate([codes, codes], axis=1), 2 * n, mark_mode=1, chunk=n)
+        fx, fy, tot = s.snapshot()
+        np.testing.assert_array_equal(fx, w.first_x)
+        np.testing.assert_array_equal(fy, w.first_y)
+        assert tot.value == w.total and tot.pairs == 2 * n
+
+
+def test_batch_profile_times_the_pass():
+    """pdf_batch_profile: forward span and cover of the latest pass, from
+    events inside the replayed graph; results unchanged."""
+    jobs, want = _jobs(1, [32, 4], seed=5)
+    b = P.Batch(jobs)
+    b.profile(True)
+    b.run()
+    fwd, cov = b.profile_read()
+    assert fwd > 0 and cov > 0
+    b.profile(False)
+    b.run()
+    for (c, s, *_), (nl, codes, n) in zip(jobs, want):
+        assert s.snapshot()[2].value == 2 * O.grade(nl, codes, n, mark_mode=1).total
 
 
 def test_autotune_picks_a_tile():
     nls = [circuits.random_small(800 + k, n_gates=2000 * (k + 1), n_pi=100, n_po=300, depth=20) for k in range(4)]
     opts, ms = P.batch_autotune(nls, [1024, 3000, 5000, 700], mark_mode=1, reps=2)
-    assert opts.tile_words in (2, 4, 8) and opts.threads in (0, 256) and ms > 0
+    assert opts.tile_words in (2, 4, 8, 32) and opts.threads in (0, 256) and ms > 0
     # the picked shape grades the batch like every circuit alone
     counts = [1024, 3000, 5000, 700]
     rng = np.random.default_rng(5)
