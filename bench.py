@@ -3,17 +3,22 @@
 
 One gate-eval is one (vector pair x gate) through the whole pipeline:
 two-pattern simulation, robust marking, pruning, first-detect merge and
-exact path counting.  A step grades one batch of synthetic pairs as a fresh
-job (the state is reset inside the step).  The default workload is the plain
-drop-in configuration: a 20,000-gate synthetic netlist (1,500 PI, 1,500 PO,
-depth 60) and 32,768 random vector pairs.
+exact path counting.  The default workload is the mixed-size batch (c4):
+256 synthetic netlists of 500-200,000 gates (depth 20-150) with 1,024-65,536
+vector pairs each, graded in one batched pass per step (a CUDA graph of one
+forward launch per class of circuits, then the cover), beside the same
+circuits graded one after another with the plain call.  Other workloads:
+c1 (2,000 gates, 1,024 pairs), c2 (20,000 gates, 32,768 pairs), c3
+(1,000,000 gates, Zipf fan-out, 262,144 pairs) and c5 (a Poisson stream of
+c4-sized jobs served with continuous batching).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c1|c2|c3|c4|c5]
 
-Prints one JSON line (rank 0).  For N > 1 (torchrun), each rank grades its
-own 32,768 pairs of the same circuit; the ranks exchange first-detect ids
-(all-reduce MIN) before counting, so the job equals one grading of all
-N x 32,768 pairs (weak scaling).
+Prints one JSON line (rank 0).  For N > 1 (torchrun) on c1-c3, each rank
+grades its own pairs of the same circuit; the ranks exchange first-detect ids
+(all-reduce MIN) before counting, so the job equals one grading of all ranks'
+pairs (weak scaling).
 """
 from __future__ import annotations
 
@@ -51,59 +56,100 @@ def oracle():
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled every 20 ms by
+    NVML (nvidia-smi at 200 ms when NVML is missing); only the samples taken
+    inside the timed region (mark_start .. mark_end) are reported."""
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("hw_power_brake_slowdown", 0x80), ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_id: str):
-        self.gpu_id = gpu_id
-        self.proc = None
-        self.lines: list[str] = []
+    def __init__(self, pci_bus_id: str | None, smi_index: str):
+        self.pci = pci_bus_id
+        self.smi_index = smi_index
+        self.samples: list[tuple[float, float, float, int]] = []  # (t, sm MHz, max MHz, reason bits)
+        self.stop_flag = threading.Event()
         self.thread = None
+        self.proc = None
+        self.t0 = self.t1 = None
+        self.source = "nvml"
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu_id}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByPciBusId(self.pci.encode()) if self.pci else \
+                N.nvmlDeviceGetHandleByIndex(int(self.smi_index))
+            smax = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+
+            def loop():
+                while not self.stop_flag.is_set():
+                    try:
+                        sm = float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+                        rs = int(N.nvmlDeviceGetCurrentClocksEventReasons(h))
+                        self.samples.append((time.perf_counter(), sm, smax, rs))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.02)
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.source = "nvidia-smi"
+        Q = "clocks.sm,clocks.max.sm,clocks_event_reasons.active"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.smi_index}", f"--query-gpu={Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+
+        def read():
+            for line in self.proc.stdout:
+                f = [x.strip() for x in line.split(",")]
+                try:
+                    self.samples.append((time.perf_counter(), float(f[0]), float(f[1]), int(f[2], 16)))
+                except (ValueError, IndexError):
+                    pass
+        self.thread = threading.Thread(target=read, daemon=True)
         self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self.stop_flag.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 8:
-                continue
-            try:
-                sm.append(float(f[0]))
-                smax.append(float(f[1]))
-            except ValueError:
-                continue
-            for n, val in zip(names, f[4:8]):
-                if val.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        t0 = self.t0 if self.t0 is not None else 0.0
+        t1 = self.t1 if self.t1 is not None else float("inf")
+        inside = [x for x in self.samples if t0 <= x[0] <= t1]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock sample in the timed region"],
+                    "samples": 0, "source": self.source}
+        reasons = sorted({n for _, _, _, r in inside for n, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(x[1] for x in inside), "sm_max_mhz": max(x[2] for x in inside),
+                "reasons": reasons, "samples": len(inside), "source": self.source,
+                "timed_region_s": round(t1 - t0, 3)}
+
+
+def clock_sampler(torch, dev: int) -> ClockSampler:
+    pci = None
+    try:
+        pr = torch.cuda.get_device_properties(dev)
+        pci = f"{int(pr.pci_domain_id):08x}:{int(pr.pci_bus_id):02x}:{int(pr.pci_device_id):02x}.0"
+    except Exception:
+        pass
+    return ClockSampler(pci, gpu_id_for_smi(torch, dev))
 
 
 def gpu_id_for_smi(torch, dev: int) -> str:
@@ -135,12 +181,47 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def traffic_summary(workload: str):
-    p = os.path.join(ROOT, "profiles", f"k_forward_{workload}.json")
+def profile_summary(name: str):
+    """A committed summary of an ncu capture (profiles/<name>.json), or None."""
+    p = os.path.join(ROOT, "profiles", f"{name}.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
     return None
+
+
+def alg_bytes(nl, n_pairs: int) -> float:
+    """Algorithmic bytes of grading n_pairs pairs on netlist nl: the 2-bit
+    transition code and the 1-bit mark of every (net, pair), written once
+    (0.375 B per gate-eval), and the 2-bit codes of the primary inputs read
+    (0.25 B per PI and pair)."""
+    return 0.375 * nl.n_gates * n_pairs + 0.25 * nl.n_pi * n_pairs
+
+
+def roofline(alg: float, kernel_ms: float, kernel: str, prof: dict | None, units: float,
+             sm_count: int, sm_mhz) -> dict:
+    """HBM roofline of the forward kernel: algorithmic bytes per launch over
+    its CUDA-event duration, against the measured copy bandwidth.  With an
+    ncu summary of the same launch: its DRAM traffic (scaled to a full
+    launch when the capture was a slice) and the issue slots its warp
+    instructions fill at the sampled SM clock."""
+    peaks = measured_peaks()
+    achieved = alg / (kernel_ms / 1e3) / 1e9
+    out = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": kernel, "kernel_ms": kernel_ms,
+           "bytes_per_gate_eval": alg / units, "peak_source": peaks["source"] + " (hbm_gbs)"}
+    if prof:
+        scale = prof.get("scale", 1.0)
+        if prof.get("dram_bytes_per_launch") is not None:
+            out["traffic"] = prof["dram_bytes_per_launch"] * scale
+            out["traffic_source"] = prof.get("source")
+        if prof.get("warp_inst_per_launch") and sm_mhz:
+            wi = prof["warp_inst_per_launch"] * scale
+            slots = sm_count * 4 * sm_mhz * 1e6 * kernel_ms / 1e3
+            out["issue_slots_frac"] = wi / slots
+            out["issue_note"] = ("warp instructions per launch (ncu smsp__inst_executed.sum) over "
+                                 "SMs x 4 schedulers x sampled SM clock x kernel time")
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -156,60 +237,136 @@ def oracle_grade(O, nl, codes, n, mode: int, segs: int, threads: int):
     return O.grade(nl, codes, n, mark_mode=mode, threads=threads)
 
 
-def cpu_baseline(P, O, nl, v, t, n_sample: int, threads: int, mode: int = 1, segs: int = 1) -> dict:
-    """The oracle (a restatement of the reference algorithm; the reference has
-    no CPU implementation) on a prefix of the workload's pairs."""
-    codes = P.codes_from_planes(v[:, :P.words(n_sample)], t[:, :P.words(n_sample)], n_sample)
-    t0 = time.perf_counter()
-    r = oracle_grade(O, nl, codes, n_sample, mode, segs, threads)
-    dt = time.perf_counter() - t0
-    return {"value": nl.n_gates * n_sample / dt, "unit": "gate-evals/s", "cores": threads, "kind": "port",
-            "sample": f"first {n_sample} of the workload's pairs, {nl.n_gates} gates, "
-                      f"{dt:.2f} s, count {r.total}"}
+def cpu_sample(P, O, members, target_evals: float, threads: int, mode: int = 1, segs: int = 1,
+               reps: int = 1, stride: int = 1) -> dict:
+    """The CPU path (the oracle: a restatement of the reference algorithm;
+    the reference has no CPU implementation) on a bounded sample of a
+    workload: every `stride`-th member circuit graded on the same fraction of
+    its pairs (a prefix of at least 32 pairs; the pair generator is
+    prefix-stable), so the sample keeps the workload's mix of circuit sizes.
+    A circuit whose sample is at least 1/threads of the whole runs on all
+    threads (split over its pairs); the others run concurrently, one circuit
+    per thread, largest first.  Returns the summed gate-evals over the wall
+    seconds (input generation excluded).
+    members: (netlist, GenParams, n_pairs)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    members = members[::stride]
+    total = sum(nl.n_gates * n for nl, _, n in members)
+    f = min(1.0, target_evals / total)
+    jobs = []
+    for nl, g, n in members:
+        k = min(n, max(32, -(-int(f * n) // 32) * 32))
+        v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, k)
+        jobs.append((nl, P.codes_from_planes(v, t, k), k))
+    jobs.sort(key=lambda j: -j[0].n_gates * j[2])
+    evals = sum(nl.n_gates * k for nl, _, k in jobs)
+    secs, count = [], 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        big = [j for j in jobs if threads == 1 or j[0].n_gates * j[2] * threads >= evals]
+        rest = [j for j in jobs if not (threads == 1 or j[0].n_gates * j[2] * threads >= evals)]
+        for nl, codes, k in big:
+            count += oracle_grade(O, nl, codes, k, mode, segs, threads).total
+        if rest:  # ctypes releases the GIL during each oracle call
+            with ThreadPoolExecutor(max_workers=threads) as ex:
+                count += sum(ex.map(lambda j: oracle_grade(O, j[0], j[1], j[2], mode, segs, 1).total, rest))
+        secs.append(time.perf_counter() - t0)
+    dt = sum(secs) / len(secs)
+    what = (f"the circuit on its first {jobs[0][2]} of {members[0][2]} pairs" if len(members) == 1 else
+            f"{'every' if stride == 1 else f'every {stride}th'} circuit of the batch ({len(members)}), each on "
+            f"the first {100 * f:.2g}% of its pairs (at least 32)"
+            f"{'; small circuits one per thread' if threads > 1 else ''}")
+    return {"value": evals / dt, "unit": "gate-evals/s", "cores": threads, "kind": "port",
+            "sample": f"{what}: {evals:.3g} gate-evals in {dt:.2f} s", "seconds": dt, "gate_evals": evals,
+            "count": count}
+
+
+def cpu_baselines(P, members, args):
+    """The CPU path on all host cores (about 1e9 gate-evals) and on one core
+    (about 6e7, every 16th circuit of a batch), each on the workload's own
+    mix of circuits."""
+    O = oracle()
+    mode = MARK_MODES[args.mark_mode][0]
+    allc = cpu_sample(P, O, members, args.cpu_sample or 1e9, os.cpu_count() or 1, mode, args.segs)
+    one = cpu_sample(P, O, members, (args.cpu_sample or 1e9) / 16, 1, mode, args.segs,
+                     stride=16 if len(members) >= 64 else 1)
+    for r in (allc, one):
+        for k in ("seconds", "gate_evals", "count"):
+            r.pop(k)
+    return allc, one
+
+
+def workload_members(P, args):
+    """(netlist, GenParams, n_pairs) of every circuit of the workload."""
+    if args.workload in ("c4", "c5"):
+        spec = P.batch_workload()[:args.circuits]
+        return [(P.gen_netlist(g), g, n) for g, n in spec]
+    w = P.WORKLOADS[args.workload]
+    return [(P.gen_netlist(w["gen"]), w["gen"], args.pairs or w["pairs"])]
 
 
 def run_reference(args):
-    """--impl reference: the CPU path (the oracle port) on the host cores."""
+    """--impl reference: the CPU path (the oracle port; the reference has no
+    CPU implementation and its GPU code needs a Fermi toolchain) on the host
+    cores, over a bounded sample of the same workload per step.  Loads the
+    workload generator and the oracle, never the grader library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     P, O = pkg(), oracle()
-    if args.workload in ("c4", "c5"):  # the batch's circuit nearest 20,000 gates stands for it
-        spec = P.batch_workload()
-        g, n = min(spec, key=lambda x: abs(x[0].n_gates - 20000))
-        w = {"gen": g, "pairs": n}
-    else:
-        w = P.WORKLOADS[args.workload]
-    nl = P.gen_netlist(w["gen"])
-    n = w["pairs"]
-    v, t = P.gen_pairs(P.pair_seed(w["gen"].seed), nl.n_pi, n)
+    members = workload_members(P, args)
     threads = os.cpu_count() or 1
-    G = nl.n_gates
-    n_sample = min(n, args.ref_sample or (n if G * n <= 2e9 else max(32, int(6.5e8 / G) // 32 * 32)))
-    codes = P.codes_from_planes(v[:, :P.words(n_sample)], t[:, :P.words(n_sample)], n_sample)
     mode = MARK_MODES[args.mark_mode][0]
+    target = args.ref_sample or 1e9  # gate-evals per step: a few seconds on 16 cores
     for _ in range(args.warmup):
-        oracle_grade(O, nl, codes, n_sample, mode, args.segs, threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        oracle_grade(O, nl, codes, n_sample, mode, args.segs, threads)
-        times.append(time.perf_counter() - t0)
-    ms = 1e3 * sum(times) / len(times)
-    val = nl.n_gates * n_sample / (ms / 1e3)
+        cpu_sample(P, O, members, target, threads, mode, args.segs)
+    runs = [cpu_sample(P, O, members, target, threads, mode, args.segs) for _ in range(args.steps)]
+    secs = sum(r["seconds"] for r in runs)
+    evals = sum(r["gate_evals"] for r in runs)
+    val = evals / secs
+    nl = members[0][0]
     line = {
         "impl": "reference", "metric": "gate-evals/s", "value": val, "unit": "gate-evals/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded)",
-        "config": workload_config(P, args.workload if args.workload not in ("c4", "c5") else args.workload + "-member",
-                                  nl, n_sample, args),
+        "config": (batch_config(members, args) if args.workload in ("c4", "c5")
+                   else workload_config(P, args.workload, nl, members[0][2], args)),
         "cpu_baseline": {"value": val, "unit": "gate-evals/s", "cores": threads, "kind": "port",
-                         "sample": f"first {n_sample} of {n} pairs per step"},
+                         "sample": runs[0]["sample"] + " per step"},
         "e2e": {"value": val, "unit": "gate-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "native_libraries": loaded_libraries(),
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def loaded_libraries() -> list[str]:
+    """This repository's shared libraries mapped into the process."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                path = ln.split()[-1] if ln.strip() else ""
+                if path.startswith(ROOT) and path.endswith(".so"):
+                    out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def batch_config(members, args) -> dict:
+    gates = sum(nl.n_gates for nl, _, _ in members)
+    pairs = sum(n for _, _, n in members)
+    return {"workload": f"c4: {len(members)} netlists, gates log-uniform 500-200,000 ({gates} total), "
+                        f"depth 20-150, pairs log-uniform 1,024-65,536 ({pairs} total), one batched pass "
+                        f"per step",
+            "netlists": len(members), "gates": gates, "pairs": pairs,
+            "gate_evals_per_pass": sum(nl.n_gates * n for nl, _, n in members),
+            "mark_mode": MARK_MODES[args.mark_mode][1],
+            "outputs": "path count and first-detect ids per circuit",
+            "l2": "flushed between timed steps (256 MiB write); the pass's planes (GBs) exceed L2"}
 
 
 def workload_config(P, name, nl, n_pairs, args=None) -> dict:
@@ -217,7 +374,9 @@ def workload_config(P, name, nl, n_pairs, args=None) -> dict:
                        f"depth {nl.n_levels - 1}, {n_pairs} pairs/rank",
            "gates": nl.n_gates, "pairs_per_rank": n_pairs,
            "mark_mode": MARK_MODES[args.mark_mode][1] if args else "robust (LUT_R)",
-           "outputs": "path count and first-detect ids (sim/mark planes not requested)",
+           "outputs": ("path count, first-detect ids, and the sim and mark planes of every (net, pair) "
+                       "written to device memory" if args and args.planes else
+                       "path count and first-detect ids (sim/mark planes not requested)"),
            "l2": "flushed between timed steps (256 MiB write)"}
     if args and args.segs > 1:
         cfg["segments"] = args.segs
@@ -266,15 +425,22 @@ def run_ours(args):
     fy_t = torch.empty(c.n_first, dtype=torch.int32, device="cuda")
 
     # The graded quantities are the path count and the first-detect ids (what
-    # fcount reports); the sim and mark planes stay inside the call.
+    # fcount reports); with --planes the sim and mark planes are written to
+    # device memory as well (every (net, pair) code and mark, 3 bits each).
+    outs = None
+    if args.planes:
+        tile = c.info().tile_words
+        planes = [torch.empty((G, -(-W // tile) * tile), dtype=torch.int32, device="cuda") for _ in range(3)]
+        outs = P.make_outputs(*planes)
+
     def step():
         s.reset_async(stream)
         if dist is None:
-            P.grade_async(c, s, pairs, base, None, stream)
+            P.grade_async(c, s, pairs, base, outs, stream)
             return
         # pairs sharded over ranks: mark locally, MIN-reduce the first-detect
         # ids over NVLink (NCCL), then count locally
-        P.grade_mark_async(c, s, pairs, base, None, stream)
+        P.grade_mark_async(c, s, pairs, base, outs, stream)
         P.first_copy(s, fx_t, fy_t, False, stream)
         D.exchange_first_(fx_t, fy_t)
         P.first_copy(s, fx_t, fy_t, True, stream)
@@ -287,19 +453,21 @@ def run_ours(args):
     job_total = D.sum_u128(ref_total, "cuda") if dist else ref_total
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    sampler = ClockSampler(gpu_id_for_smi(torch, local))
+    sampler = clock_sampler(torch, local)
     sampler.start()
-    time.sleep(0.3)
+    time.sleep(0.1)
     s.profile(True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    sampler.mark_start()
     for i in range(args.steps):
         flush.fill_(i & 0xFF)
         ev[i][0].record()
         step()
         ev[i][1].record()
     torch.cuda.synchronize()
+    sampler.mark_end()
     if dist:
         dist.barrier()
     clocks = sampler.stop()
@@ -324,10 +492,10 @@ def run_ours(args):
         s.reset_async(stream)
         tot = P.Totals_t()
         if dist is None:
-            P.check(P.lib().pdf_grade(c.h, s.h, C.byref(hpairs), base, None, C.byref(tot),
-                                      C.c_void_p(stream)), "pdf_grade")
+            P.check(P.lib().pdf_grade(c.h, s.h, C.byref(hpairs), base, C.byref(outs) if outs else None,
+                                      C.byref(tot), C.c_void_p(stream)), "pdf_grade")
         else:
-            P.grade_mark_async(c, s, hpairs, base, None, stream)
+            P.grade_mark_async(c, s, hpairs, base, outs, stream)
             P.first_copy(s, fx_t, fy_t, False, stream)
             D.exchange_first_(fx_t, fy_t)
             P.first_copy(s, fx_t, fy_t, True, stream)
@@ -363,7 +531,7 @@ def run_ours(args):
                 b = i % 2
                 comp.wait_event(copied[b])
                 s.reset_async(stream)
-                P.grade_async(c, s, P.make_pairs(bufs[b][0], bufs[b][1], n), base, None, stream)
+                P.grade_async(c, s, P.make_pairs(bufs[b][0], bufs[b][1], n), base, outs, stream)
                 if i + 1 < k:
                     issue_copy(i + 1)  # buffer (i + 1) % 2 was last read by step i - 1, already read back
                 tot = P.Totals_t()
@@ -386,25 +554,19 @@ def run_ours(args):
 
     units = world * G * n
     value = units / (ms / 1e3)
-    peaks = measured_peaks()
-    # Algorithmic bytes per gate-eval: the pairs read (2 bits per PI and pair)
-    # and the first-detect ids written (8 bytes per gate per call); the planes
-    # of intermediate values never leave the chip except for rows re-read
-    # later, which is traffic, not algorithm.
-    B = 0.25 * nl.n_pi / G + 8.0 / n
     fwd_ms = prof_ms[0] / max(1, prof_calls)
-    achieved = B * G * n / (fwd_ms / 1e3) / 1e9
-    tr = traffic_summary(args.workload)
+    tile = c.info().tile_words
+    kname = "k_forward_lanes" if tile == 32 else "k_forward"
+    prof = profile_summary(f"{kname}_{args.workload}") if not args.planes and args.segs == 1 and \
+        args.mark_mode == "robust" and not args.pairs else None
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     line = {
         "metric": "gate-evals/s", "value": value, "unit": "gate-evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
         "config": workload_config(P, args.workload, nl, n, args),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "kernel": "k_forward",
-                     "kernel_ms": fwd_ms, "cover_ms": prof_ms[1] / max(1, prof_calls),
-                     "bytes_per_gate_eval": B, "peak_source": peaks["source"] + " (hbm_gbs)",
-                     "traffic": tr.get("dram_bytes_per_launch") if tr else None},
+        "roofline": dict(roofline(alg_bytes(nl, n), fwd_ms, f"{kname} (tile {tile} words)", prof, G * n,
+                                  sm_count, clocks.get("sm_mhz")), cover_ms=prof_ms[1] / max(1, prof_calls)),
         "e2e": {"value": units / ((stream_ms or e2e_ms_mean) / 1e3), "unit": "gate-evals/s",
                 "h2d_bytes_per_step": int(2 * nl.n_pi * W * 4), "d2h_bytes_per_step": 64,
                 "mode": ("streamed: pinned host pairs copied on a second stream while the previous step "
@@ -420,9 +582,7 @@ def run_ours(args):
         "batch_count": job_total,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        O = oracle()
-        sample = args.cpu_sample or (n if G * n <= 2e9 else max(32, int(1.3e9 / G) // 32 * 32))
-        line["cpu_baseline"] = cpu_baseline(P, O, nl, v, t, min(n, sample), os.cpu_count() or 1, mode, args.segs)
+        line["cpu_baseline"], line["cpu_baseline_1core"] = cpu_baselines(P, [(nl, w["gen"], n)], args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -432,9 +592,10 @@ def run_ours(args):
 
 
 def run_batched(args):
-    """--workload c4: the mixed-size batch graded in one pass per step (the
-    autotuned tile, replayed from a CUDA graph) against the same circuits
-    graded one after another with the plain call."""
+    """--workload c4: the mixed-size batch graded in one pass per step (one
+    forward launch per class of circuits and the cover, replayed from a CUDA
+    graph) against the same circuits graded one after another with the
+    plain call (pdf_grade_async each)."""
     import ctypes as C
 
     import numpy as np
@@ -442,10 +603,11 @@ def run_batched(args):
 
     P = pkg()
     rank = int(os.environ.get("RANK", "0"))
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    spec = P.batch_workload()[:args.circuits]
-    nls = [P.gen_netlist(g) for g, _ in spec]
-    counts = [n for _, n in spec]
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    members = workload_members(P, args)
+    nls = [m[0] for m in members]
+    counts = [m[2] for m in members]
     t0 = time.perf_counter()
     threads = args.threads
     if args.tile_words:
@@ -457,32 +619,31 @@ def run_batched(args):
     tune_s = time.perf_counter() - t0
     stream = torch.cuda.current_stream().cuda_stream
     jobs, hosts = [], []
-    for k, (nl, (g, n)) in enumerate(zip(nls, spec)):
-        ld = (P.words(n) + tw - 1) // tw * tw
-        v = np.zeros((nl.n_pi, ld), np.uint32)
-        t = np.zeros((nl.n_pi, ld), np.uint32)
-        check_v, check_t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, n)
-        v[:, :check_v.shape[1]] = check_v
-        t[:, :check_t.shape[1]] = check_t
-        c = P.Circuit(nl, mark_mode=P.MARK_ROBUST, max_pairs=n, tile_words=tw, threads=threads)
+    for nl, g, n in members:
+        ld = (P.words(n) + 31) // 32 * 32  # a pitch every tile width divides
+        v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, n, ld)
+        c = P.Circuit(nl, device=local, mark_mode=P.MARK_ROBUST, max_pairs=n, tile_words=tw, threads=threads)
         st = P.State(c)
-        dv = torch.from_numpy(v.view(np.int32)).cuda()
-        dt = torch.from_numpy(t.view(np.int32)).cuda()
-        jobs.append((c, st, dv, dt, n, 0))
-        hosts.append((torch.from_numpy(v.view(np.int32)).pin_memory(), torch.from_numpy(t.view(np.int32)).pin_memory()))
+        hv = torch.from_numpy(v.view(np.int32)).pin_memory()
+        ht = torch.from_numpy(t.view(np.int32)).pin_memory()
+        jobs.append((c, st, hv.cuda(), ht.cuda(), n, 0))
+        hosts.append((hv, ht))
     units = sum(nl.n_gates * n for nl, n in zip(nls, counts))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     # the plain call as a user makes it: each circuit at its own default tile
-    # (the batch's pair planes, whose pitch is a multiple of every tile)
     plain_jobs = []
     for (c, st, dv, dt, n, _), nl in zip(jobs, nls):
-        c0 = P.Circuit(nl, mark_mode=P.MARK_ROBUST, max_pairs=n)
+        c0 = P.Circuit(nl, device=local, mark_mode=P.MARK_ROBUST, max_pairs=n)
         plain_jobs.append((c0, P.State(c0), dv, dt, n, 0))
 
-    def plain_pass(js):
-        for c, st, dv, dt, n, _ in js:
+    def plain_pass(js, marks=None):
+        for k, (c, st, dv, dt, n, _) in enumerate(js):
+            if marks:
+                marks[k].record()
             st.reset_async(stream)
             P.grade_async(c, st, P.make_pairs(dv, dt, n), 0, None, stream)
+        if marks:
+            marks[len(js)].record()
 
     def results(js=jobs):
         return [st.snapshot() for _, st, *_ in js]
@@ -504,6 +665,15 @@ def run_batched(args):
     # plain: every circuit alone, one after another
     plain_ms, plain_res = time_plain(plain_jobs)
     plain_bt_ms, plain_bt_res = time_plain(jobs)
+    if args.timeline:  # per-circuit duration of one plain pass (fill of the GPU against time)
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(jobs) + 1)]
+        plain_pass(plain_jobs, marks)
+        torch.cuda.synchronize()
+        rows = [{"gates": nl.n_gates, "depth": nl.n_levels - 1, "pairs": n, "tile_words": c.info().tile_words,
+                 "ctas": -(-P.words(n) // c.info().tile_words), "ms": marks[k].elapsed_time(marks[k + 1])}
+                for k, ((c, _, _, _, n, _), nl) in enumerate(zip(plain_jobs, nls))]
+        with open(args.timeline, "w") as f:
+            json.dump({"plain_pass_ms": plain_ms, "circuits": rows}, f)
 
     # batched: one graph replay per pass
     b = P.Batch(jobs)
@@ -516,22 +686,32 @@ def run_batched(args):
     for c0, st0, *_ in plain_jobs:
         st0.close()
         c0.close()
+    b.profile(True)  # forward span and cover of every timed pass, from events inside the graph
     for _ in range(max(3, args.warmup)):
         b.run_async(stream)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    sampler = ClockSampler(gpu_id_for_smi(torch, int(os.environ.get("LOCAL_RANK", "0"))))
+    fwd_ms, cov_ms = [], []
+    sampler = clock_sampler(torch, local)
     sampler.start()
-    time.sleep(0.3)
+    time.sleep(0.1)
     torch.cuda.synchronize()
+    sampler.mark_start()
     for i in range(args.steps):
         flush.fill_(i & 0xFF)
         ev[i][0].record()
         b.run_async(stream)
         ev[i][1].record()
+        f, cv = b.profile_read()  # waits for this pass
+        fwd_ms.append(f)
+        cov_ms.append(cv)
     torch.cuda.synchronize()
+    sampler.mark_end()
     clocks = sampler.stop()
+    b.profile(False)
     ms = sum(x.elapsed_time(y) for x, y in ev) / args.steps
+    passes_run = 1 + max(3, args.warmup) + args.steps
+    stable = all(a[2].value == passes_run * x[2].value for a, x in zip(results(), batch_res))
 
     # e2e: host pairs in (pinned), one pass, every job's count back
     tot = P.Totals_t()
@@ -586,47 +766,41 @@ def run_batched(args):
     streamed(args.steps)
     stream_ms = 1e3 * (time.perf_counter() - t1) / args.steps
     b2.close()
-    peaks = measured_peaks()
-    alg = sum(2 * nl.n_pi * P.words(n) * 4 + 8 * nl.n_gates for nl, n in zip(nls, counts))
-    achieved = alg / (ms / 1e3) / 1e9
     info = b.info()
+    kernel_ms = sum(fwd_ms) / len(fwd_ms)
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    prof = profile_summary(f"k_batch_forward_c4_tile{tw}") if args.circuits == 256 else None
+    plain_best = min(plain_ms, plain_bt_ms)
     line = {
         "metric": "gate-evals/s", "value": units / (ms / 1e3), "unit": "gate-evals/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
-        "config": {"workload": f"c4: {len(nls)} netlists, gates log-uniform 500-200,000 "
-                               f"({sum(nl.n_gates for nl in nls)} total), depth 20-150, pairs log-uniform "
-                               f"1,024-65,536 ({sum(counts)} total), one batched pass per step",
-                   "mark_mode": "robust (LUT_R)", "tile_words": tw, "ctas": info.ctas,
-                   "autotune": {"tile_words": tw, "threads": threads, "ms_per_pass": tune_ms, "seconds": tune_s}
-                   if tune_ms else None,
-                   "threads": threads or "piece capacity + 64",
-                   "outputs": "path count and first-detect ids per circuit",
-                   "l2": "flushed between timed steps (256 MiB write)"},
-        "plain": {"value": units / (min(plain_ms, plain_bt_ms) / 1e3), "ms_per_pass": min(plain_ms, plain_bt_ms),
+        "config": dict(batch_config(members, args), tile_words=tw, threads=threads or "default",
+                       ctas=info.ctas, forward_launches=int(info.launches) - 2,
+                       autotune={"tile_words": tw, "threads": threads, "ms_per_pass": tune_ms,
+                                 "seconds": round(tune_s, 1)} if tune_ms else None),
+        "plain": {"value": units / (plain_best / 1e3), "ms_per_pass": plain_best,
                   "ms_per_pass_default_tiles": plain_ms, "ms_per_pass_batch_tile": plain_bt_ms,
                   "note": "the same circuits graded one after another (pdf_grade_async each), at each "
                           "circuit's default tile and at the batch's tile; the faster of the two"},
-        "batched_vs_plain": min(plain_ms, plain_bt_ms) / ms,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "kernel": "k_batch_forward + k_batch_active + k_batch_cover",
-                     "peak_source": peaks["source"] + " (hbm_gbs)", "traffic": None},
+        "batched_vs_plain": plain_best / ms,
+        "roofline": dict(roofline(sum(alg_bytes(nl, n) for nl, n in zip(nls, counts)), kernel_ms,
+                                  f"forward span of the pass (k_batch_forward{'_lanes' if tw == 32 else ''}, "
+                                  f"every class)", prof, units, sm_count, clocks.get("sm_mhz")),
+                         cover_ms=sum(cov_ms) / len(cov_ms)),
         "e2e": {"value": units / (stream_ms / 1e3), "unit": "gate-evals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": 64 * len(jobs),
                 "mode": "streamed: pinned host pairs of the next pass copied on a second stream while this "
                         "pass grades (two buffer sets, two batches)",
                 "value_one_pass_per_step": units / (e2e_ms / 1e3)},
-        "gpu_launches": int(info.launches) * args.steps,  # forward per occupancy class, active, cover
+        "gpu_launches": int(info.launches) * args.steps,  # forward per class, active, cover
         "clocks": clocks,
-        "result_stable": bool(same),
+        "same_config": True,
+        "result_stable": bool(same and stable),
+        "native_libraries": loaded_libraries(),
     }
-    if not args.no_cpu:
-        O = oracle()
-        k = int(np.argmin([abs(nl.n_gates - 20000) for nl in nls]))
-        nl, (g, n) = nls[k], spec[k]
-        v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, n)
-        line["cpu_baseline"] = cpu_baseline(P, O, nl, v, t, min(n, max(32, int(1.3e9 / nl.n_gates) // 32 * 32)),
-                                            os.cpu_count() or 1)
+    if not args.no_cpu and rank == 0:
+        line["cpu_baseline"], line["cpu_baseline_1core"] = cpu_baselines(P, members, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     b.close()
@@ -659,9 +833,10 @@ def run_served(args):
     srv = P.Server(mark_mode=P.MARK_ROBUST, batch_pairs=batch, hbm_budget=int(args.hbm_gb * (1 << 30)),
                    workers=args.workers, tile_words=args.tile_words or 4)
     ids = [None] * n_jobs
-    sampler = ClockSampler(gpu_id_for_smi(torch, int(os.environ.get("LOCAL_RANK", "0"))))
+    sampler = clock_sampler(torch, int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
-    time.sleep(0.3)
+    time.sleep(0.1)
+    sampler.mark_start()
     t0 = time.perf_counter()
     k = 0
     while k < n_jobs or srv.stats().jobs_done < n_jobs:
@@ -675,6 +850,7 @@ def run_served(args):
             continue
         srv.step()
     wall = time.perf_counter() - t0
+    sampler.mark_end()
     clocks = sampler.stop()
     st = srv.stats()
     # every served result against the job graded offline in one call
@@ -721,7 +897,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--mark-mode", choices=sorted(MARK_MODES), default="robust",
                     help="c1-c3: sensitisation table and gate semantics")
     ap.add_argument("--segs", type=int, default=1, help="c1-c3: path segments of this many nets (1-8)")
@@ -731,13 +907,17 @@ def main():
                     help="threads per CTA, pieces of threads - 64 gates (0 = default; c4: the batch's circuits)")
     ap.add_argument("--pairs", type=int, default=0,
                     help="c1-c3: pairs per rank instead of the workload's (small cases for profiling)")
-    # CPU samples: pairs per timed CPU run (0 = the whole workload up to 2e9
-    # gate-evals, else about 1.3e9 gate-evals for the baseline and 6.5e8 per
-    # reference-arm step: a few seconds on the host cores)
-    ap.add_argument("--cpu-sample", type=int, default=0)
-    ap.add_argument("--ref-sample", type=int, default=0)
+    # CPU samples, in gate-evals per timed CPU run (0: about 1e9 for the
+    # baseline and per reference-arm step, 6e7 for the one-core figure; a
+    # few seconds on the host cores)
+    ap.add_argument("--cpu-sample", type=float, default=0)
+    ap.add_argument("--ref-sample", type=float, default=0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--jobs", type=int, default=64, help="c5: jobs in the arrival stream")
+    ap.add_argument("--jobs", type=int, default=512, help="c5: jobs in the arrival stream")
+    ap.add_argument("--planes", action="store_true",
+                    help="c1-c3: also write the sim and mark planes of every (net, pair) to device memory")
+    ap.add_argument("--timeline", default="",
+                    help="c4: write the per-circuit durations of one plain pass to this JSON file")
     ap.add_argument("--circuits", type=int, default=256,
                     help="c4: the first N netlists of the batch (smaller cases for profiling)")
     ap.add_argument("--hbm-gb", type=float, default=64.0, help="c5: device memory for active jobs")
