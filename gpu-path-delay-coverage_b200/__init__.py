@@ -30,6 +30,7 @@ S0, S1, T0, T1 = range(4)
 MARK_DEFAULT, MARK_ROBUST, MARK_FIXED_ROBUST, MARK_FIXED_NONROBUST = 0, 1, 2, 3
 FLAG_OVERFLOW = 1
 BATCH_APPEND, BATCH_NO_GRAPH = 1, 2
+INJECT_DEVICE_ALLOC, INJECT_HOST_ALLOC = 1, 2
 BENCH_BRANCHES = 1
 NONE = 0xFFFFFFFF
 
@@ -73,7 +74,7 @@ class Totals_t(C.Structure):
 class CircuitOpts_t(C.Structure):
     _fields_ = [("device", C.c_int), ("mark_mode", C.c_int), ("max_pairs", C.c_uint32),
                 ("tile_words", C.c_uint32), ("threads", C.c_uint32), ("seg_len", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("wait_polls", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class BatchJob_t(C.Structure):
@@ -122,6 +123,7 @@ ABI = [
     ("pdf_abi_version", C.c_int, []),
     ("pdf_last_error", C.c_char_p, []),
     ("pdf_netlist_check", C.c_int, [C.POINTER(Netlist_t), C.c_char_p, C.c_size_t]),
+    ("pdf_test_inject", C.c_int, [C.c_int, C.c_uint32]),
     ("pdf_circuit_create", C.c_int, [C.POINTER(Netlist_t), C.POINTER(CircuitOpts_t), C.POINTER(C.c_void_p)]),
     ("pdf_circuit_destroy", None, [C.c_void_p]),
     ("pdf_circuit_query", C.c_int, [C.c_void_p, C.POINTER(CircuitInfo_t)]),
@@ -432,6 +434,11 @@ def dump_segments(path: str, segs: np.ndarray, first_x: np.ndarray, first_y: np.
                                   fy.ctypes.data), "pdf_dump_segments")
 
 
+def inject_failures(site: int, count: int) -> None:
+    """The next `count` allocations of kind `site` (INJECT_*) fail (pdf_test_inject)."""
+    check(lib().pdf_test_inject(site, count), "pdf_test_inject")
+
+
 def words(n_pairs: int) -> int:
     return (n_pairs + 31) // 32
 
@@ -489,11 +496,12 @@ class Circuit:
     """A netlist uploaded to one device (pdf_circuit_create)."""
 
     def __init__(self, nl: Netlist, device: int = 0, mark_mode: int = MARK_DEFAULT,
-                 max_pairs: int = 0, tile_words: int = 0, threads: int = 0, seg_len: int = 1):
+                 max_pairs: int = 0, tile_words: int = 0, threads: int = 0, seg_len: int = 1,
+                 wait_polls: int = 0):
         self.h = None
         self.netlist = nl
         self.mark_mode = mark_mode
-        o = CircuitOpts_t(device, mark_mode, max_pairs, tile_words, threads, seg_len)
+        o = CircuitOpts_t(device, mark_mode, max_pairs, tile_words, threads, seg_len, wait_polls)
         h = C.c_void_p()
         check(lib().pdf_circuit_create(C.byref(nl.view()), C.byref(o), C.byref(h)), "pdf_circuit_create")
         self.h = h

@@ -14,8 +14,43 @@
 #include <vector>
 
 #include "pdf.h"
+#include "pdf_inject.h"
 #include "pdf_internal.h"
 #include "pdf_kernels.cuh"
+
+#include <atomic>
+
+namespace {
+std::atomic<uint32_t> g_inject[3];
+}  // namespace
+
+bool inject_fail(int site) {
+    if (site < 1 || site > 2) return false;
+    uint32_t n = g_inject[site].load();
+    while (n > 0)
+        if (g_inject[site].compare_exchange_weak(n, n - 1)) return true;
+    return false;
+}
+cudaError_t dev_alloc(void **p, size_t bytes) {
+    if (inject_fail(PDF_INJECT_DEVICE_ALLOC)) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+cudaError_t host_alloc(void **p, size_t bytes) {
+    if (inject_fail(PDF_INJECT_HOST_ALLOC)) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+}
+
+extern "C" pdf_status pdf_test_inject(int site, uint32_t count) {
+    if (site < 1 || site > 2) return PDF_EINVAL;
+    g_inject[site].store(count);
+    return PDF_OK;
+}
 
 namespace {
 
@@ -60,7 +95,7 @@ struct DevBuf {
     cudaError_t ensure(size_t need) {
         if (bytes >= need) return cudaSuccess;
         release();
-        cudaError_t e = cudaMalloc(&p, need ? need : 16);
+        cudaError_t e = dev_alloc(&p, need ? need : 16);
         if (e == cudaSuccess) bytes = need;
         return e;
     }
@@ -126,6 +161,7 @@ struct pdf_circuit {
     uint32_t off_ring = 0, off_rec = 0, off_edge = 0, off_fid = 0, off_bm = 0, off_pbits = 0, off_mbar = 0;
     size_t fwd_smem = 0;
     uint32_t hash_cap = 4096, cover_threads = 256, cover_grid = 0;
+    uint32_t wait_polls = 0;  // bound of the forward kernels' waits (0 = the default)
     uint32_t occ = 1;  // forward CTAs per SM its registers and shared memory are sized for
     uint64_t chain = 0;  // length of one CTA's walk (pieces, or gates for the lane kernel)
     Workspace stage;  // scratch of the stage calls
@@ -404,6 +440,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     if (!c) return PDF_ENOMEM;
     c->device = o.device;
     c->mark_mode = o.mark_mode;
+    c->wait_polls = o.wait_polls;
     const uint32_t G = nl->n_gates, L = nl->n_levels;
     pdf_circuit_info &inf = c->info;
     inf.n_gates = G;
@@ -985,7 +1022,22 @@ FwdArgs base_fwd(pdf_circuit *c, uint64_t n_pairs) {
     a.off_pbits = c->off_pbits;
     a.off_mbar = c->off_mbar;
     a.err = c->err.as<uint32_t>();
+    a.wait_polls = c->wait_polls;
     return a;
+}
+
+// The device error word of the circuit's stage calls (pdf_sim, pdf_mark):
+// read after the call's work is done, then cleared, so that an expired wait
+// is reported by the call that met it and by no later one.
+pdf_status take_circuit_err(pdf_circuit *c, cudaStream_t cs) {
+    unsigned int e = 0;
+    PDF_CUDA(cudaMemcpyAsync(&e, c->err.p, sizeof e, cudaMemcpyDeviceToHost, cs));
+    PDF_CUDA(cudaStreamSynchronize(cs));
+    if (e) {
+        PDF_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof e, cs));
+        PDF_CUDA(cudaStreamSynchronize(cs));
+    }
+    return err_status(e);
 }
 
 CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t ld, uint64_t n_pairs,
@@ -1279,7 +1331,7 @@ extern "C" pdf_status pdf_sim(pdf_circuit *c, const pdf_pairs *pr, uint32_t *sim
         PDF_CUDA(cudaMemcpy2DAsync(sim_t, ld * 4, a.T, a.ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
     }
     PDF_CUDA(cudaStreamSynchronize(cs));  // the stage scratch is reused by the next stage call
-    return PDF_OK;
+    return take_circuit_err(c, cs);
 }
 
 namespace {
@@ -1315,7 +1367,7 @@ pdf_status mark_planes(pdf_circuit *c, const uint32_t *sim_v, const uint32_t *si
     if (!direct)
         PDF_CUDA(cudaMemcpy2DAsync(mark, ld * 4, a.M, a.ld * 4, W * 4, G, cudaMemcpyDeviceToDevice, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));
-    return PDF_OK;
+    return take_circuit_err(c, cs);
 }
 
 }  // namespace
@@ -1373,10 +1425,7 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
         chunk->flags = h.batch_flags;
         chunk->reserved = 0;
     }
-    unsigned int cerr = 0;
-    PDF_CUDA(cudaMemcpy(&cerr, c->err.p, sizeof cerr, cudaMemcpyDeviceToHost));
-    pdf_status st2 = err_status(h.err | cerr);
-    return st2;
+    return err_status(h.err);
 }
 
 // Allocation-free variant of pdf_cover: the same kernels, with their scratch

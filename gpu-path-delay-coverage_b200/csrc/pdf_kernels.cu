@@ -86,9 +86,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *m, uint32_t phase) {
         : "memory");
     return ok != 0;
 }
-// Every wait is bounded: on expiry the caller reports PDF_ETIMEOUT.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *m, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Every wait is bounded: on expiry the caller reports PDF_ETIMEOUT.  polls =
+// 0: up to kSpinLimit blocking polls (try_wait may suspend the thread until
+// the phase completes); polls > 0: that many non-blocking polls, a bound
+// small enough to run out (tests of the timeout path).
 constexpr uint32_t kSpinLimit = 1u << 24;
-__device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t phase) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t phase, uint32_t polls = 0) {
+    if (polls) {
+        for (uint32_t i = 0; i < polls; i++)
+            if (mbar_test_wait(m, phase)) return true;
+        return false;
+    }
     for (uint32_t i = 0; i < kSpinLimit; i++)
         if (mbar_try_wait(m, phase)) return true;
     return false;
@@ -347,10 +364,13 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
         const int nxt2 = nxt >= 0 ? prev_marked(nxt) : -1;
         Piece Pn2{};
         if (nxt2 >= 0) Pn2 = a.pieces[nxt2];
-        const bool ok = mbar_wait(S.mbar + sbuf, (phase >> sbuf) & 1u);
+        const bool ok = mbar_wait(S.mbar + sbuf, (phase >> sbuf) & 1u, a.wait_polls);
         phase ^= 1u << sbuf;
         if (__syncthreads_or(!ok)) {
+            // no CTA leaves with a copy in flight: wait (at the full bound)
+            // for this piece's copy and the next one's, then report
             failed = true;
+            (void)mbar_wait(S.mbar + sbuf, ((phase >> sbuf) & 1u) ^ 1u);
             if (nxt >= 0) (void)mbar_wait(S.mbar + (sbuf ^ 1), (phase >> (sbuf ^ 1)) & 1u);
             cp_async_wait_all();
             break;
@@ -541,7 +561,7 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
         if (threadIdx.x == stager && has_next) stage_piece(a, S, P1, buf ^ 1, false);
         // every thread waits for the records itself; the piece's only
         // barrier is at its end
-        const bool ok = mbar_wait(S.mbar + buf, (phase >> buf) & 1u);
+        const bool ok = mbar_wait(S.mbar + buf, (phase >> buf) & 1u, a.wait_polls);
         phase ^= 1u << buf;
         if (!ok) s_fail = 1;
         if (has_next && ok) prefetch(P.nfar_n, buf ^ 1, S.fid + (size_t)buf * a.farcap);
@@ -673,7 +693,9 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
         cp_async_wait_all();  // this thread's copies for piece i + 1
         if (__syncthreads_or(any) && threadIdx.x == 0) S.pbits[i >> 5] |= 1u << (i & 31);
         if (s_fail) {
-            // the record copy still in flight, then report
+            // no CTA leaves with a copy in flight: wait (at the full bound)
+            // for this piece's record copy and the next one's, then report
+            (void)mbar_wait(S.mbar + buf, ((phase >> buf) & 1u) ^ 1u);
             if (has_next) (void)mbar_wait(S.mbar + (buf ^ 1), (phase >> (buf ^ 1)) & 1u);
             if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
             return;
@@ -765,8 +787,7 @@ __device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, 
             if (FIX && MODE != FWD_SIM && bit_test(bm, x.r.w[3 + q])) x.fm[q] = a.M[fo];
         }
     }
-    if (!FIX && MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live)
-        x.m0 = a.M[(size_t)x.r.w[7] * a.ld + w];
+    if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live) x.m0 = a.M[(size_t)x.r.w[7] * a.ld + w];
 }
 
 // Evaluate, mark and store one gate; returns whether it holds a mark in the
@@ -805,7 +826,7 @@ __device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, uint32
         const bool anyT = __any_sync(0xFFFFFFFFu, T != 0);
         if (h & RF_INPT) {
             M = T;
-        } else if (!FIX && (h & RF_MARKF0) && x.bit0 && anyT) {
+        } else if ((h & RF_MARKF0) && x.bit0 && anyT) {
             // fan-in 0 (gate w[7]) holds a mark: its bitmap bit is set
             M = T & x.m0;
             if ((h & RF_SENS) && __any_sync(0xFFFFFFFFu, M != 0)) {

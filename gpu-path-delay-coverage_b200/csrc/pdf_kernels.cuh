@@ -57,6 +57,8 @@ struct FwdArgs {
     DevAcc *acc;                  // FWD_FUSED: the batch count, zeroed by block 0 (may be null)
     uint32_t *active;             // FWD_FUSED: the cover's active-pair bitmap [W] + count, zeroed (may be null)
     uint32_t *err;                // device error word (PDF_ETIMEOUT on a wait that expired)
+    uint32_t wait_polls;          // bound of the record waits: 0 = kSpinLimit blocking polls,
+                                  // n = n non-blocking polls (tests of the timeout path)
     uint64_t n_pairs;
     uint32_t W;                   // ceil(n_pairs / 32)
     uint32_t pair_base;

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "pdf.h"
+#include "pdf_inject.h"
 
 namespace {
 
@@ -281,7 +282,7 @@ extern "C" pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server 
     }
     // the retiring jobs' staging, sized up front for circuits of 256k gates
     // (pinning memory while the loop runs contends with the workers' calls)
-    if (cudaHostAlloc(reinterpret_cast<void **>(&srv->pin), 2 * (size_t)(256u << 10) * 4, cudaHostAllocDefault) ==
+    if (host_alloc(reinterpret_cast<void **>(&srv->pin), 2 * (size_t)(256u << 10) * 4) ==
         cudaSuccess)
         srv->pin_words = 2 * (size_t)(256u << 10);
     else {
@@ -422,17 +423,31 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
     pdf_batch_info bi{};
     if (pdf_batch_query(srv->batch, &bi) == PDF_OK) srv->st.launches += bi.launches;
-    const double t1 = now_s();
-    srv->st.steps++;
-    // account, advance, retire
-    std::vector<Job *> keep;
+    // Retire the jobs whose pairs are all graded.  Nothing about a job changes
+    // (and no job is handed to the workers, who free retired jobs) until
+    // every fallible call of this step has succeeded: a failing step leaves
+    // every job active and unchanged on the host.  First the pinned staging
+    // of the retiring jobs' first-detect ids, grown geometrically (freeing
+    // pinned memory waits for the device).
+    size_t gmax = 0;
+    for (Job *j : srv->active)
+        if (j->done + j->cur >= j->n_pairs) gmax = std::max<size_t>(gmax, j->view.n_gates);
+    if (srv->pin_words < 2 * gmax) {
+        const size_t want = std::max(2 * gmax, 2 * srv->pin_words);
+        if (srv->pin) cudaFreeHost(srv->pin);
+        srv->pin = nullptr;
+        srv->pin_words = 0;
+        if (host_alloc(reinterpret_cast<void **>(&srv->pin), want * 4) != cudaSuccess) {
+            srv->pin = nullptr;
+            (void)cudaGetLastError();
+            return PDF_ENOMEM;
+        }
+        srv->pin_words = want;
+    }
+    std::vector<Job *> keep, gone;
+    std::vector<Result> res;
     for (Job *j : srv->active) {
-        srv->lat_ms.push_back(1e3 * (t1 - j->t_ready));
-        j->t_ready = t1;
-        srv->st.batches++;
-        srv->st.gate_evals += (uint64_t)j->view.n_gates * j->cur;
-        j->done += j->cur;
-        if (j->done < j->n_pairs) {
+        if (j->done + j->cur < j->n_pairs) {
             keep.push_back(j);
             continue;
         }
@@ -440,32 +455,34 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         const size_t G = j->view.n_gates;
         r.fx.resize(G);
         r.fy.resize(G);
-        if (srv->pin_words < 2 * G) {  // grown geometrically (freeing pinned memory waits for the device)
-            const size_t want = std::max(2 * G, 2 * srv->pin_words);
-            if (srv->pin) cudaFreeHost(srv->pin);
-            srv->pin = nullptr;
-            srv->pin_words = 0;
-            if (cudaHostAlloc(reinterpret_cast<void **>(&srv->pin), want * 4, cudaHostAllocDefault) != cudaSuccess) {
-                srv->pin = nullptr;
-                (void)cudaGetLastError();
-                return PDF_ENOMEM;
-            }
-            srv->pin_words = want;
-        }
         // ordered on the server's stream: a device-wide sync would also wait
         // for the workers' uploads of arriving jobs
         if ((st = pdf_state_snapshot_on(j->s, srv->pin, srv->pin + G, &r.total, srv->stream)) != PDF_OK) return st;
         std::memcpy(r.fx.data(), srv->pin, 4 * G);
         std::memcpy(r.fy.data(), srv->pin + G, 4 * G);
-        srv->results[j->id] = std::move(r);
+        res.push_back(std::move(r));
+        gone.push_back(j);
+    }
+    // account and advance
+    const double t1 = now_s();
+    srv->st.steps++;
+    for (Job *j : srv->active) {
+        srv->lat_ms.push_back(1e3 * (t1 - j->t_ready));
+        j->t_ready = t1;
+        srv->st.batches++;
+        srv->st.gate_evals += (uint64_t)j->view.n_gates * j->cur;
+        j->done += j->cur;
+    }
+    for (size_t k = 0; k < gone.size(); k++) srv->results[gone[k]->id] = std::move(res[k]);
+    if (!gone.empty()) {
         {
             std::lock_guard<std::mutex> lk(srv->mu);
-            srv->retired.push_back(j);
+            for (Job *j : gone) srv->retired.push_back(j);
         }
         srv->cv.notify_all();
-        srv->st.jobs_done++;
+        srv->st.jobs_done += gone.size();
         srv->dirty = true;
-        if (retired) (*retired)++;
+        if (retired) *retired = (uint32_t)gone.size();
     }
     srv->active.swap(keep);
     srv->st.busy_s += now_s() - t0;

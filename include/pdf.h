@@ -171,7 +171,12 @@ typedef struct pdf_circuit_opts {
                             of 32; from 128 up, pieces then hold at most threads - 64 gates */
     uint32_t seg_len;    /* path segments of this many nets, 0 or 1 = single nets; up to 8
                             (fcount --segs N, main.cu:76-81,185-223) */
-    uint32_t reserved[2];
+    uint32_t wait_polls; /* bound on each device-side wait of the forward kernels for its staged
+                            copy: 0 = 2^24 blocking polls (the default); n > 0 = n non-blocking
+                            polls, after which the call reports PDF_ETIMEOUT (small values
+                            exist to test that path).  The lane kernel (tile_words 32) waits
+                            for nothing. */
+    uint32_t reserved;
 } pdf_circuit_opts;
 
 typedef struct pdf_circuit_info {
@@ -192,6 +197,16 @@ const char *pdf_status_string(int status);
  * CUDA error name and number and the failing call ("" if none yet). */
 const char *pdf_last_error(void);
 int pdf_abi_version(void);
+
+/* Host-side fault injection, for tests of the error paths (no reference
+ * counterpart).  The next `count` allocations of the given kind made by this
+ * library fail as if memory were exhausted (count 0 clears it):
+ * PDF_INJECT_DEVICE_ALLOC  device memory of circuits, states and workspaces;
+ * PDF_INJECT_HOST_ALLOC    the pinned read-back staging of the server.
+ * Process-wide; calls that then fail return PDF_ENOMEM and leave their
+ * objects usable. */
+enum { PDF_INJECT_DEVICE_ALLOC = 1, PDF_INJECT_HOST_ALLOC = 2 };
+pdf_status pdf_test_inject(int site, uint32_t count);
 
 /* Host-side structural check of a netlist (no device needed).  On failure a
  * one-line reason is written to msg (if msg_len > 0). */
@@ -334,7 +349,9 @@ pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark,
  * that loads the library until the process exits; a chunk needs
  * 4 * (ceil(ceil(n_pairs/32)/tile_words) * ceil(n_gates/32)
  *      + ceil(n_pairs/32) + min(n_pairs, 2 * n_gates)) bytes of it plus about
- * 1 KiB, and larger requests return PDF_ELIMIT.  The caller passes the
+ * 1 KiB, and larger requests return PDF_ELIMIT (a circuit with segments of
+ * more than one net gets PDF_ENOTSUP before any size check: the fixed array
+ * holds no (net, pair) set).  The caller passes the
  * pruned mark plane (as pdf_cover) and the first-detect ids as device arrays
  * of n_gates uint32 (for example copied out with pdf_state_first_copy); the
  * chunk's count is returned in *chunk_total (the call waits for it).

@@ -110,6 +110,37 @@ def test_netlist_check_rejects_malformed():
     assert _mutated(nl, level_offsets=lo).check()[0] == 1
     nfi0 = nl.nfi.copy(); nfi0[nl.n_pi] = 0
     assert _mutated(nl, nfi=nfi0).check()[0] == 1
+    # a fan-in id out of range
+    e = nl.edges.copy(); g = int(nl.level_offsets[2]); e[int(nl.edge_offset[g])] = nl.n_gates + 5
+    st, msg = _mutated(nl, edges=e).check()
+    assert st == 1 and "fan-in" in msg
+    # a fan-in on a higher level (a cycle through the level order)
+    e = nl.edges.copy(); g = int(nl.level_offsets[2]); e[int(nl.edge_offset[g])] = int(nl.level_offsets[-2])
+    st, msg = _mutated(nl, edges=e).check()
+    assert st == 1 and "fan-in" in msg
+    # level offsets out of order
+    lo = nl.level_offsets.copy(); lo[2], lo[3] = lo[3], lo[2]
+    assert _mutated(nl, level_offsets=lo).check()[0] == 1
+
+
+def test_fault_injection_entry_point():
+    L = P.lib()
+    assert L.pdf_test_inject(0, 1) == 1 and L.pdf_test_inject(3, 1) == 1  # PDF_EINVAL
+    assert L.pdf_test_inject(P.INJECT_DEVICE_ALLOC, 0) == 0
+
+
+def test_generator_library_is_host_only():
+    """The workload generator is its own library (no CUDA): a CPU baseline
+    can build its inputs without loading the grader."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, 'tests'); import helpers; P = helpers._load('pdf_b200', "
+            "helpers.PKG_DIR / '__init__.py'); nl = P.gen_netlist(P.WORKLOADS['c1']['gen']); "
+            "v, t = P.gen_pairs(1, nl.n_pi, 100); maps = open('/proc/self/maps').read(); "
+            "assert 'libpdf_gen.so' in maps and 'libpdf_b200.so' not in maps and 'libcudart' not in maps, maps; "
+            "print(nl.n_gates)")
+    out = subprocess.run([sys.executable, "-c", code], cwd=helpers.ROOT, capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip() == "2000", out.stderr
 
 
 def test_circuit_create_without_gpu_fails_cleanly():
