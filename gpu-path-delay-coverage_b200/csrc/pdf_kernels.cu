@@ -306,6 +306,15 @@ __device__ __forceinline__ Vec<BW> sens_any_fixed(const GateRec &r, uint32_t nfi
     return out;
 }
 
+// A CTA that gave up on an expired wait publishes an empty column block (no
+// marked net, no marked level), so the kernels that run after it (cover,
+// segment merge) read nothing the CTA did not finish.
+__device__ __forceinline__ void empty_block(const FwdArgs &a, uint32_t blk, uint32_t *gbm) {
+    if (gbm)
+        for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) gbm[q] = 0;
+    if (a.blk_maxlvl && threadIdx.x == 0) a.blk_maxlvl[blk] = 0;
+}
+
 // Reverse pass (prune, markkernel.cuh:271-293) and first-detect merge
 // (mergekernel.cuh:116-198) of k_forward, after its forward pass: only
 // pieces that hold a forward mark, descending, only gates whose bitmap bit is
@@ -435,6 +444,7 @@ __device__ __forceinline__ void prune_and_merge(const FwdArgs &a, const FwdSmem 
         sbuf ^= 1;
     }
     if (failed) {
+        empty_block(a, blk, gbm);
         if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
         return;
     }
@@ -697,6 +707,7 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
             // for this piece's record copy and the next one's, then report
             (void)mbar_wait(S.mbar + buf, ((phase >> buf) & 1u) ^ 1u);
             if (has_next) (void)mbar_wait(S.mbar + (buf ^ 1), (phase >> (buf ^ 1)) & 1u);
+            if (MODE != FWD_SIM) empty_block(a, blk, gbm);
             if (threadIdx.x == 0) atomicOr(a.err, kErrTimeout);
             return;
         }
