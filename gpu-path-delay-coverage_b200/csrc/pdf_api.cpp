@@ -502,11 +502,20 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
                          : (max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u);
     const bool lanes = c->bw == kLaneWords;
     if (lanes) {
-        // the lane kernel reads every fan-in from its plane row: source words
-        // are the fan-in ids themselves
+        // The lane kernel reads every fan-in from its plane row: source words
+        // are the fan-in ids themselves, flagged SRC_ZERO when the fan-in is
+        // a killed gate (S0 whatever its inputs); a gate writes its rows
+        // (RF_SPILL) only when some gate reads them.
+        std::vector<uint8_t> read(G, 0);
         for (uint32_t g = 0; g < G; g++)
-            for (uint32_t q = 0; q < kInlineFanins; q++)
-                recs[g].w[3 + q] = q < nl->nfi[g] ? edges[eoff[g] + q] : 0u;
+            for (uint32_t q = 0; q < nl->nfi[g]; q++) {
+                const uint32_t f = edges[eoff[g] + q];
+                const bool zero = q < kInlineFanins && (recs[f].w[0] & RF_KILL);
+                if (q < kInlineFanins) recs[g].w[3 + q] = f | (zero ? SRC_ZERO : 0u);
+                if (!zero) read[f] = 1;
+            }
+        for (uint32_t g = 0; g < G; g++)
+            if (read[g]) recs[g].w[0] |= RF_SPILL;
     }
     const uint32_t max_threads = lanes ? kLaneThreads : (c->bw >= 8 ? 512 : 1024);
     uint32_t threads_default = 512;  // set from the piece size below
@@ -549,13 +558,24 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     std::vector<Piece> pieces;
     std::vector<uint32_t> far_ids;
     if (lanes) {
-        // The lane kernel keeps only the column block's mark bitmap on chip
-        // (in global memory when it does not fit); no pieces, ring or far lists.
+        // The lane kernel keeps on chip two buffers of staged gate records
+        // and the column block's mark bitmap (in global memory when it does
+        // not fit); its pieces are runs of one level of <= kLaneRecs gates.
+        for (uint32_t l = 0; l < L; l++)
+            for (uint32_t a = nl->level_offsets[l]; a < nl->level_offsets[l + 1]; a += kLaneRecs) {
+                Piece p{};
+                p.a = a;
+                p.b = std::min(a + kLaneRecs, nl->level_offsets[l + 1]);
+                p.level = l;
+                pieces.push_back(p);
+            }
+        c->n_pieces = (uint32_t)pieces.size();
+        const size_t rec_bytes = 2 * (size_t)kLaneRecs * sizeof(GateRec);
         const size_t bm_bytes = (size_t)bm_words * 4;
-        c->bm_shared = bm_bytes + 2048 <= budget ? 1u : 0u;
-        c->off_bm = 0;
-        c->fwd_smem = c->bm_shared ? al(bm_bytes) : 0;
-        c->n_pieces = 0;
+        c->off_rec = 0;
+        c->off_bm = (uint32_t)rec_bytes;
+        c->bm_shared = rec_bytes + bm_bytes + 2048 <= budget ? 1u : 0u;
+        c->fwd_smem = rec_bytes + (c->bm_shared ? al(bm_bytes) : 0);
         c->chain = G;
         while (far_ids.size() < 4) far_ids.push_back(0);
     } else {
@@ -712,7 +732,6 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         delete c;
         return st2;
     };
-    if (pieces.empty()) pieces.push_back(Piece{});  // (the lane kernel has none)
     if (c->rec.ensure(sizeof(GateRec) * G) != cudaSuccess ||
         c->edges.ensure(sizeof(uint32_t) * edges.size()) != cudaSuccess ||
         c->level_off.ensure(sizeof(uint32_t) * (L + 1)) != cudaSuccess ||

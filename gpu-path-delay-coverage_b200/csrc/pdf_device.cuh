@@ -38,6 +38,13 @@ struct __align__(16) GateRec {
 };
 static constexpr int kInlineFanins = 4;
 static constexpr uint32_t SRC_PLANE = 0x80000000u, SRC_FAR = 0x40000000u, SRC_IDX = 0x3FFFFFFFu;
+// Lane kernel (tile of 32 words): w[3..6] hold the fan-in ids, with this bit
+// set when the fan-in is a killed gate (RF_KILL: its value is S0 and it never
+// marks), whose row is then neither read nor, unless someone else reads it,
+// written.
+static constexpr uint32_t SRC_ZERO = 0x80000000u;
+// Gate records per piece of the lane kernel (staged in shared memory).
+static constexpr uint32_t kLaneRecs = 1024;
 static constexpr uint32_t kMaxFar = 1024;  // far-buffer slots per piece at most
 
 // Per-gate evaluation flags, derived once from (type, nfi) so that the
@@ -53,6 +60,7 @@ enum : uint32_t {
     RF_MARKF0 = 1u << 21,  // mark = transition & mark of fan-in 0
     RF_INPT = 1u << 22,    // primary input: mark = transition
     RF_SPILL = 1u << 23,   // a later gate reads this gate's plane rows from global memory
+                           // (lane kernel: some gate reads its rows at all)
     // true n-input semantics (PDF_MARK_FIXED_*)
     RF_XOR = 1u << 5,      // fold steps are XOR (XOR, XNOR)
     RF_OINV = 1u << 6,     // the folded value is inverted under both vectors (NAND, NOR, XNOR)

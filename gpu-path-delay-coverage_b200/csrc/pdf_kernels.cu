@@ -791,11 +791,14 @@ __device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, 
     if (MODE != FWD_SIM) x.bit0 = bit_test(bm, x.r.w[7]);
 #pragma unroll
     for (int q = 0; q < kInlineFanins; q++) {
-        if ((uint32_t)q < nl && live) {
-            const size_t fo = (size_t)x.r.w[3 + q] * a.ld + w;
+        const uint32_t sw = x.r.w[3 + q], f = sw & ~SRC_ZERO;
+        // a killed fan-in is S0 (its row is not written), except in the stage
+        // call pdf_mark, whose given planes are read as they are
+        if ((uint32_t)q < nl && live && (MODE == FWD_MARK || !(sw & SRC_ZERO))) {
+            const size_t fo = (size_t)f * a.ld + w;
             x.fv[q] = a.V[fo];
             x.ft[q] = a.T[fo];
-            if (FIX && MODE != FWD_SIM && bit_test(bm, x.r.w[3 + q])) x.fm[q] = a.M[fo];
+            if (FIX && MODE != FWD_SIM && bit_test(bm, f)) x.fm[q] = a.M[fo];
         }
     }
     if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live) x.m0 = a.M[(size_t)x.r.w[7] * a.ld + w];
@@ -874,7 +877,7 @@ __device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, uint32
     }
     const bool marked = MODE != FWD_SIM && __any_sync(0xFFFFFFFFu, M != 0);
     if (live) {
-        if (MODE != FWD_MARK && (a.store_all || r.w[1] || marked)) {
+        if (MODE != FWD_MARK && (a.store_all || (h & RF_SPILL) || marked)) {
             a.V[o] = V;
             a.T[o] = T;
         }
@@ -895,8 +898,8 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
                                                 : ((a.n_pairs & 31) ? (1u << (a.n_pairs & 31)) - 1u : 0xFFFFFFFFu));
     uint32_t *bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
     uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
+    GateRec *recs = reinterpret_cast<GateRec *>(smraw + a.off_rec);  // [2][kLaneRecs]
     const uint32_t *lo = a.c.level_off;
-    const uint32_t L = a.c.n_levels;
 
     if (MODE != FWD_SIM)
         for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) bm[q] = 0;
@@ -913,23 +916,57 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
     __syncthreads();
 
     // ------------------------------------------------------------- forward
+    // Pieces (runs of one level, <= kLaneRecs gates) in level order; each
+    // piece's gate records are copied into shared memory (cp.async, 16 bytes
+    // per thread and copy) while the piece before it is evaluated, and its
+    // descriptor is loaded a piece earlier still.  One barrier per piece.
+    const auto stage = [&](uint32_t ga, uint32_t gb, int buf) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(a.c.rec + ga);
+        uint4 *dst = reinterpret_cast<uint4 *>(recs + (size_t)buf * kLaneRecs);
+        for (uint32_t i = threadIdx.x; i < 2 * (gb - ga); i += blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + i)), "l"(src + i) : "memory");
+    };
+    // gates [pa, pb) of level pl: the next piece to evaluate; (na, nb, nlv):
+    // the one after it, loaded a piece ahead
     uint32_t top = 0;  // levels below `top` may hold a forward mark
-    for (uint32_t l = 0; l < L; l++) {
-        const uint32_t ga = __ldg(lo + l), gb = __ldg(lo + l + 1);
-        bool any = false;
+    uint32_t pa = a.pieces[0].a, pb = a.pieces[0].b, pl = a.pieces[0].level, na = 0, nb = 0, nlv = 0;
+    if (a.n_pieces > 1) {
+        na = a.pieces[1].a;
+        nb = a.pieces[1].b;
+        nlv = a.pieces[1].level;
+    }
+    stage(pa, pb, 0);
+    bool any = false;
+    uint32_t prev_level = 0;
+    for (uint32_t i = 0; i < a.n_pieces; i++) {
+        cp_async_wait_all();  // this thread's copies of piece i's records
+        if (__syncthreads_or(any) && i) top = max(top, prev_level + 1);
+        any = false;
+        if (i + 1 < a.n_pieces) stage(na, nb, (i + 1) & 1);  // into the buffer of piece i - 1, which every warp has left
+        const uint32_t ga = pa, gb = pb;
+        prev_level = pl;
+        pa = na;
+        pb = nb;
+        pl = nlv;
+        if (i + 2 < a.n_pieces) {
+            na = __ldg(&a.pieces[i + 2].a);
+            nb = __ldg(&a.pieces[i + 2].b);
+            nlv = __ldg(&a.pieces[i + 2].level);
+        }
+        const GateRec *rb = recs + (size_t)(i & 1) * kLaneRecs;
         for (uint32_t g = ga + warp; g < gb; g += 2 * NW) {
             const uint32_t g1 = g + NW;
             const bool two = g1 < gb;
             LaneIn x0, x1;
-            x0.r = load_rec(a.c.rec + g);
-            if (two) x1.r = load_rec(a.c.rec + g1);
+            x0.r = rb[g - ga];
+            if (two) x1.r = rb[g1 - ga];
             lane_load<SEM, MODE>(a, bm, g, w, live, x0);
             if (two) lane_load<SEM, MODE>(a, bm, g1, w, live, x1);
             any |= lane_gate<SEM, MODE>(a, bm, g, w, live, wmask, x0);
             if (two) any |= lane_gate<SEM, MODE>(a, bm, g1, w, live, wmask, x1);
         }
-        if (__syncthreads_or(any)) top = l + 1;
     }
+    if (__syncthreads_or(any)) top = max(top, prev_level + 1);
     if constexpr (MODE == FWD_SIM) {
         return;
     } else {
