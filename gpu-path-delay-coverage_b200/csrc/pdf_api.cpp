@@ -133,6 +133,8 @@ struct DeviceGuard {
 // stage calls).
 struct Workspace {
     DevBuf nzb, maxlvl, active, active_list;
+    DevBuf over_list, spill;  // pairs for the spill cover and its per-net (h, c) slots
+    uint32_t spill_slots = 0;
     DevBuf seg_first;  // (net, pair) hash set of the cover with segments
     uint64_t seg_first_mask = 0;
     DevBuf planes;   // internal V, T, M planes when the caller gives none
@@ -143,6 +145,9 @@ struct Workspace {
         maxlvl.release();
         active.release();
         active_list.release();
+        over_list.release();
+        spill.release();
+        spill_slots = 0;
         seg_first.release();
         seg_first_mask = 0;
         planes.release();
@@ -995,7 +1000,19 @@ pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes
     PDF_CUDA(ws.maxlvl.ensure(n_blocks * 4));
     // active bitmap [W], then the count; the list holds <= 2 pairs per gate
     PDF_CUDA(ws.active.ensure(W * 4 + 16));
-    PDF_CUDA(ws.active_list.ensure(std::min<uint64_t>(W * 32, 2 * std::max<uint64_t>(c->n_first(), c->info.n_gates)) * 4));
+    const uint64_t list = std::min<uint64_t>(W * 32, 2 * std::max<uint64_t>(c->n_first(), c->info.n_gates));
+    PDF_CUDA(ws.active_list.ensure(list * 4));
+    // A pair can mark more nets than the cover's table holds only when the
+    // circuit has more gates than that; its count then goes through the
+    // spill cover, whose slots of 2 x n_gates u128 take up to 16 MiB (at
+    // least one slot).
+    if (c->info.n_gates > c->hash_cap) {
+        const uint64_t slot = 2 * (uint64_t)c->info.n_gates * 16;
+        const uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(16, (16ull << 20) / slot));
+        PDF_CUDA(ws.over_list.ensure(list * 4));
+        PDF_CUDA(ws.spill.ensure(slots * slot));
+        ws.spill_slots = slots;
+    }
     if (c->seg_len > 1) {
         // (net, pair) entries: at most N per first pair of a segment, two per
         // segment, and one per (net, pair); a table at least twice that
@@ -1078,6 +1095,9 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
     a.active_list = ws.active_list.as<uint32_t>();
     a.acc = acc;
     a.hash_cap = c->hash_cap;
+    a.over_list = ws.over_list.as<uint32_t>();
+    a.spill = ws.spill.as<unsigned char>();
+    a.spill_slots = ws.spill_slots;
     a.seg = c->seg_args();
     if (c->seg_len > 1) {
         a.seg_first = ws.seg_first.as<unsigned long long>();
@@ -1684,7 +1704,13 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t o_f = a256(sizeof(BatchCtl)), o_c = o_f + a256(sizeof(FwdArgs) * n_jobs),
                  o_b = o_c + a256(sizeof(CoverArgs) * n_jobs), o_g = o_b + a256(4 * (n_jobs + 1)),
-                 o_i = o_g + a256(4 * (n_jobs + 1)), total = o_i + sizeof(uint2) * std::max<uint64_t>(items, 1);
+                 o_i = o_g + a256(4 * (n_jobs + 1)), o_o = o_i + a256(sizeof(uint2) * std::max<uint64_t>(items, 1)),
+                 total = o_o + sizeof(uint2) * std::max<uint64_t>(items, 1);
+    // the spill cover: as many CTAs as the spilling circuit with the fewest
+    // slots has (circuits without slots cannot spill)
+    L.spill_grid = 0;
+    for (uint32_t i = 0; i < n_jobs; i++)
+        if (ca[i].spill_slots) L.spill_grid = L.spill_grid ? std::min(L.spill_grid, ca[i].spill_slots) : ca[i].spill_slots;
     // The block is written into mapped pinned host memory and pulled to the
     // device by a small kernel on the batch's own stream: a copy-engine
     // transfer would queue behind other host threads' bulk uploads (a
@@ -1723,6 +1749,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     L.bpref = reinterpret_cast<const uint32_t *>(base + o_b);
     L.gpref = reinterpret_cast<const uint32_t *>(base + o_g);
     L.items = reinterpret_cast<uint2 *>(base + o_i);
+    L.over_items = reinterpret_cast<uint2 *>(base + o_o);
     b->bytes = b->ctl.bytes;
     PDF_CUDA(prepare_batch(L));
     if (b->use_graph && !b->cap_stream &&
@@ -1776,7 +1803,7 @@ extern "C" pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info) 
     info->ctas = b->L.total_blocks;
     info->gate_evals = b->gate_evals;
     info->device_bytes = b->bytes;
-    info->launches = 2;
+    info->launches = b->L.spill_grid ? 3 : 2;
     for (uint32_t k = 0; k < b->L.n_class; k++) info->launches += b->L.cls[k].blocks ? 1u : 0u;
     info->reserved = 0;
     return PDF_OK;

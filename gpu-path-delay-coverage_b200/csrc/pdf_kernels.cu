@@ -527,6 +527,8 @@ __device__ __forceinline__ void forward_cta(const FwdArgs &a, const uint32_t blk
             a.acc->batch_hi = 0;
             a.acc->batch_flags = 0;
             a.acc->done = 0;
+            a.acc->n_over = 0;
+            a.acc->done_over = 0;
         }
     }
     __shared__ uint32_t s_fail;
@@ -911,6 +913,8 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
             a.acc->batch_hi = 0;
             a.acc->batch_flags = 0;
             a.acc->done = 0;
+            a.acc->n_over = 0;
+            a.acc->done_over = 0;
         }
     }
     __syncthreads();
@@ -1289,8 +1293,10 @@ __device__ __forceinline__ uint32_t level_of(const uint32_t *lo_tab, uint32_t n_
 //   H = [po] + sum h(fo);  C = sum c(fo);  first = pid is first_x or first_y
 //   c = C + (first ? H : 0);  h = first ? 0 : H;  h = 0 on INPT
 // (a net the pair does not mark has h = c = 0).  Level-0 INPT c values are
-// the pair's count.  A pair marking more than net_cap nets reports
-// kErrHashFull; fan-out lists past the adjacency buffer are read in place.
+// the pair's count.  A pair marking more than net_cap nets is counted by
+// nothing here: cover_pair returns true and the caller queues the pair for
+// the spill cover (spill_pair); fan-out lists past the adjacency buffer are
+// read in place.
 constexpr uint32_t kCoverCand = 4096;   // candidates per chunk (128 bitmap words)
 constexpr uint32_t kCoverLevels = 2048; // level table entries kept in shared memory
 constexpr uint32_t kNetPo = 1u << 31, kNetInpt = 1u << 30, kNetFirst = 1u << 29, kNetLevel = (1u << 29) - 1;
@@ -1301,9 +1307,16 @@ __host__ __device__ constexpr size_t cover_smem_lvt(uint32_t cap) {
     return (size_t)cap * (2 * sizeof(pdf_u128) + 4 * 4 + 4 * 4) + (size_t)kCoverCand * 4;
 }
 
+// Each thread of the candidate test below takes up to kCoverCand / blockDim
+// candidates in registers: the cover kernels run 256 threads.
+constexpr uint32_t kCoverThreads = 256;
+static_assert(kCoverCand / kCoverThreads <= 16, "cover_pair keeps 16 candidate mark words per thread");
+
 // The cover of pair p (index within the batch) of the circuit in `a`;
-// lo_tab is its level table (shared or global memory).
-__device__ __forceinline__ void cover_pair(const CoverArgs &a, const uint32_t p, const uint32_t *lo_tab) {
+// lo_tab is its level table (shared or global memory).  Returns true (the
+// same in every thread) when the pair marks more nets than the table holds:
+// then nothing is counted.
+__device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p, const uint32_t *lo_tab) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const uint32_t cap = a.hash_cap, acap = 4 * cap;
     pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw);
@@ -1376,10 +1389,9 @@ __device__ __forceinline__ void cover_pair(const CoverArgs &a, const uint32_t p,
         __syncthreads();
         if (s_over) break;
     }
-    if (s_over) {
-        if (threadIdx.x == 0) atomicOr(&a.acc->err, kErrHashFull);  // more nets than the list holds
+    if (s_over) {  // more nets than the list holds
         __syncthreads();
-        return;
+        return true;
     }
     const uint32_t n = s_n;
     // ---- C: records, first ids, levels, listed fan-outs
@@ -1473,9 +1485,80 @@ __device__ __forceinline__ void cover_pair(const CoverArgs &a, const uint32_t p,
         }
     }
     __syncthreads();
+    return false;
 }
 
-__global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
+// The same recurrence for a pair that marks more nets than cover_pair's
+// table holds, with every net's (h, c) in global memory: slot = [2][n_gates]
+// u128, indexed by gate.  Levels descending from the column block's highest
+// marked level; a net takes part when its bitmap bit is set and the pair
+// marks it (the mark bit read from the plane).
+__device__ void spill_pair(const CoverArgs &a, const uint32_t p, pdf_u128 *Hs) {
+    __shared__ pdf_u128 s_red[8];
+    __shared__ unsigned int s_flags;
+    pdf_u128 *Cs = Hs + a.c.n_gates;
+    const uint32_t pid = a.pair_base + p;
+    const uint32_t wp = p >> 5, bit = p & 31, blk = wp / a.bw;
+    const uint32_t *nzb = a.nzb + (size_t)blk * a.bm_words;
+    const uint32_t top = a.blk_maxlvl[blk];
+    if (threadIdx.x == 0) s_flags = 0;
+    __syncthreads();
+    auto marks = [&](uint32_t g) { return bit_test(nzb, g) && ((a.M[(size_t)g * a.ld + wp] >> bit) & 1u); };
+    pdf_u128 total = 0;
+    bool ovf = false;
+    for (int lv = (int)top - 1; lv >= 0; lv--) {
+        const uint32_t g1 = __ldg(a.c.level_off + lv + 1);
+        for (uint32_t g = __ldg(a.c.level_off + lv) + threadIdx.x; g < g1; g += blockDim.x) {
+            if (!marks(g)) continue;
+            const GateRec r = load_rec(a.c.rec + g);
+            pdf_u128 H = rec_po(r) ? 1 : 0, C = 0;
+            bool dummy = false;
+            const uint32_t nfo = r.w[1], eb = r.w[2] + rec_nfi(r);
+            for (uint32_t k = 0; k < nfo; k++) {
+                const uint32_t fo = __ldg(a.c.edges + eb + k);
+                if (!marks(fo)) continue;
+                C = add_sat(C, Cs[fo], ovf);
+                H = add_sat(H, Hs[fo], dummy);
+            }
+            const bool first = a.seg.N > 1
+                                   ? first_set_find(a.seg_first, a.seg_first_mask, ((unsigned long long)g << 32) | p)
+                                   : (a.first_x[g] == pid || a.first_y[g] == pid);
+            pdf_u128 c = C, h = H;
+            if (first) {
+                c = add_sat(C, H, ovf);
+                h = 0;
+            }
+            if (c == ~(pdf_u128)0) ovf = true;
+            if (rec_type(r) == PDF_INPT) {
+                h = 0;
+                if (lv == 0) total = add_sat(total, c, ovf);
+            }
+            Hs[g] = h;
+            Cs[g] = c;
+        }
+        __syncthreads();
+    }
+    for (int d = 16; d > 0; d >>= 1) total = add_sat(total, shfl_down_u128(total, d), ovf);
+    if (ovf) atomicOr(&s_flags, PDF_FLAG_OVERFLOW);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = total;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        pdf_u128 t = threadIdx.x < (blockDim.x + 31) / 32 ? s_red[threadIdx.x] : 0;
+        bool o2 = false;
+        for (int d = 16; d > 0; d >>= 1) t = add_sat(t, shfl_down_u128(t, d), o2);
+        if (threadIdx.x == 0) {
+            if (o2 || s_flags) atomicOr(&a.acc->batch_flags, PDF_FLAG_OVERFLOW);
+            if (t) atomic_add_u128(&a.acc->batch_lo, &a.acc->batch_hi, &a.acc->batch_flags, t);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ pdf_u128 *spill_slot(const CoverArgs &a, uint32_t k) {
+    return reinterpret_cast<pdf_u128 *>(a.spill) + (size_t)k * 2 * a.c.n_gates;
+}
+
+__global__ void __launch_bounds__(kCoverThreads) k_cover(const CoverArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     uint32_t *lvt = reinterpret_cast<uint32_t *>(smraw + cover_smem_lvt(a.hash_cap));  // [kCoverLevels] level_off
     const uint32_t L = a.c.n_levels;
@@ -1485,14 +1568,37 @@ __global__ void __launch_bounds__(256) k_cover(const CoverArgs a) {
     const uint32_t *lo_tab = lv_shared ? lvt : a.c.level_off;
     __syncthreads();
     const uint32_t n_active = *a.active_count;
-    for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) cover_pair(a, a.active_list[ai], lo_tab);
-    // the last CTA to finish closes the batch
+    for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) {
+        const uint32_t p = a.active_list[ai];
+        if (cover_pair(a, p, lo_tab) && threadIdx.x == 0) {
+            if (a.spill_slots) a.over_list[atomicAdd(&a.acc->n_over, 1u)] = p;  // for k_cover_spill
+            else atomicOr(&a.acc->err, kErrHashFull);
+        }
+    }
+    // the last CTA to finish closes the batch, unless pairs wait for the spill cover
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(&a.acc->done, 1u) == gridDim.x - 1) {
             __threadfence();
-            batch_close(a.acc, a.n_pairs);
+            if (!a.acc->n_over) batch_close(a.acc, a.n_pairs);
             a.acc->done = 0;
+        }
+    }
+}
+
+// After k_cover: the pairs it queued, one per CTA at a time (CTA k uses
+// spill slot k); the last CTA closes the batch.
+__global__ void __launch_bounds__(kCoverThreads) k_cover_spill(const CoverArgs a) {
+    const uint32_t n_over = a.acc->n_over;
+    if (!n_over) return;  // k_cover closed the batch
+    for (uint32_t j = blockIdx.x; j < n_over; j += gridDim.x) spill_pair(a, a.over_list[j], spill_slot(a, blockIdx.x));
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&a.acc->done_over, 1u) == gridDim.x - 1) {
+            __threadfence();
+            batch_close(a.acc, a.n_pairs);
+            a.acc->n_over = 0;
+            a.acc->done_over = 0;
         }
     }
 }
@@ -1533,6 +1639,8 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
             ctl->n_items = 0;
             ctl->done = 0;
             ctl->err = 0;
+            ctl->n_over = 0;
+            ctl->done_over = 0;
         }
     }
     __syncthreads();
@@ -1554,6 +1662,8 @@ __global__ void __launch_bounds__(kLaneThreads, 1)
             ctl->n_items = 0;
             ctl->done = 0;
             ctl->err = 0;
+            ctl->n_over = 0;
+            ctl->done_over = 0;
         }
     }
     __syncthreads();
@@ -1570,25 +1680,8 @@ __global__ void k_batch_active(const CoverArgs *args, const uint32_t *gpref, uin
                 [&](uint32_t d) { items[atomicAdd(&ctl->n_items, 1u)] = make_uint2(ci, d); });
 }
 
-__global__ void __launch_bounds__(256) k_batch_cover(CoverArgs *args, FwdArgs *fargs, uint32_t n, const uint2 *items,
-                                                     BatchCtl *ctl, uint32_t append) {
-    __shared__ CoverArgs s_a;
-    __shared__ uint32_t s_last;
-    const uint32_t n_items = ctl->n_items;
-    for (uint32_t ai = blockIdx.x; ai < n_items; ai += gridDim.x) {
-        const uint2 it = items[ai];
-        if (threadIdx.x == 0) s_a = args[it.x];
-        __syncthreads();
-        cover_pair(s_a, it.y, s_a.c.level_off);  // ends with a barrier
-    }
-    // the last CTA to finish closes every circuit's batch
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = atomicAdd(&ctl->done, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
+// Close every circuit's batch (by the last CTA of a batch's cover).
+__device__ void batch_close_all(CoverArgs *args, FwdArgs *fargs, uint32_t n, BatchCtl *ctl, uint32_t append) {
     unsigned int err = 0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint64_t np = args[i].n_pairs;
@@ -1601,7 +1694,64 @@ __global__ void __launch_bounds__(256) k_batch_cover(CoverArgs *args, FwdArgs *f
     }
     err = __reduce_or_sync(0xFFFFFFFFu, err);
     if ((threadIdx.x & 31) == 0 && err) atomicOr(&ctl->err, err);
+}
+
+__global__ void __launch_bounds__(kCoverThreads) k_batch_cover(CoverArgs *args, FwdArgs *fargs, uint32_t n,
+                                                               const uint2 *items, uint2 *over_items, BatchCtl *ctl,
+                                                               uint32_t append) {
+    __shared__ CoverArgs s_a;
+    __shared__ uint32_t s_last;
+    const uint32_t n_items = ctl->n_items;
+    for (uint32_t ai = blockIdx.x; ai < n_items; ai += gridDim.x) {
+        const uint2 it = items[ai];
+        if (threadIdx.x == 0) s_a = args[it.x];
+        __syncthreads();
+        if (cover_pair(s_a, it.y, s_a.c.level_off) && threadIdx.x == 0) {  // ends with a barrier
+            if (s_a.spill_slots) over_items[atomicAdd(&ctl->n_over, 1u)] = it;  // for k_batch_cover_spill
+            else atomicOr(&s_a.acc->err, kErrHashFull);
+        }
+        __syncthreads();
+    }
+    // the last CTA to finish closes every circuit's batch, unless items wait
+    // for the spill cover
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ctl->done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (!ctl->n_over) batch_close_all(args, fargs, n, ctl, append);
     if (threadIdx.x == 0) ctl->done = 0;
+}
+
+// After k_batch_cover: the items it queued (CTA k uses spill slot k of the
+// item's circuit; every spilling circuit has at least gridDim slots).
+__global__ void __launch_bounds__(kCoverThreads) k_batch_cover_spill(CoverArgs *args, FwdArgs *fargs, uint32_t n,
+                                                                     const uint2 *over_items, BatchCtl *ctl,
+                                                                     uint32_t append) {
+    __shared__ CoverArgs s_a;
+    __shared__ uint32_t s_last;
+    const uint32_t n_over = ctl->n_over;
+    if (!n_over) return;  // k_batch_cover closed the batch
+    for (uint32_t j = blockIdx.x; j < n_over; j += gridDim.x) {
+        const uint2 it = over_items[j];
+        if (threadIdx.x == 0) s_a = args[it.x];
+        __syncthreads();
+        spill_pair(s_a, it.y, spill_slot(s_a, blockIdx.x));  // ends with a barrier
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ctl->done_over, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    batch_close_all(args, fargs, n, ctl, append);
+    if (threadIdx.x == 0) {
+        ctl->n_over = 0;
+        ctl->done_over = 0;
+    }
 }
 
 // Dense first-detect merge over given planes (stage call pdf_merge): one warp
@@ -1658,6 +1808,8 @@ __global__ void k_batch_begin(DevAcc *acc) {
     acc->batch_hi = 0;
     acc->batch_flags = 0;
     acc->done = 0;
+    acc->n_over = 0;
+    acc->done_over = 0;
 }
 
 template <int BW, int SEM, int MODE>
@@ -1804,10 +1956,15 @@ cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bo
     } else {
         k_active<<<(a.c.n_gates + 255) / 256, 256, 0, st>>>(a);
     }
+    if (threads != kCoverThreads) return cudaErrorInvalidValue;
     const size_t smem = cover_smem_bytes(a.hash_cap);
     cudaError_t e = cudaFuncSetAttribute(k_cover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_cover<<<grid, threads, smem, st>>>(a);
+    if (a.spill_slots) {
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        k_cover_spill<<<a.spill_slots, kCoverThreads, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -1902,9 +2059,14 @@ cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
     if (b.prof[1] && (e = cudaEventRecordWithFlags(b.prof[1], st, pflag)) != cudaSuccess) return e;
     k_batch_active<<<(b.total_gates + 255) / 256, 256, 0, st>>>(b.cargs, b.gpref, b.n, b.items, b.ctl);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_batch_cover<<<b.cover_grid, 256, cover_smem_bytes(b.hash_cap), st>>>(b.cargs, b.fargs, b.n, b.items, b.ctl,
-                                                                         b.append);
+    k_batch_cover<<<b.cover_grid, kCoverThreads, cover_smem_bytes(b.hash_cap), st>>>(b.cargs, b.fargs, b.n, b.items,
+                                                                                   b.over_items, b.ctl, b.append);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (b.spill_grid) {
+        k_batch_cover_spill<<<b.spill_grid, kCoverThreads, 0, st>>>(b.cargs, b.fargs, b.n, b.over_items, b.ctl,
+                                                                    b.append);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (b.prof[2] && (e = cudaEventRecordWithFlags(b.prof[2], st, pflag)) != cudaSuccess) return e;
     return cudaSuccess;
 }

@@ -31,7 +31,8 @@ struct DevAcc {
     unsigned int batch_flags;
     unsigned int err;                       // device-side error code (0 = none)
     unsigned int done;                      // cover CTAs finished (the last one closes the batch)
-    unsigned int pad[2];
+    unsigned int n_over;                    // pairs queued for the spill cover (more nets than the table)
+    unsigned int done_over;                 // spill-cover CTAs finished
 };
 
 struct FwdArgs {
@@ -101,6 +102,13 @@ struct CoverArgs {
     uint32_t *active_count;       // [1]
     DevAcc *acc;
     uint32_t hash_cap;            // nets one pair may mark (the cover's shared-memory net list)
+    // pairs that mark more nets than hash_cap: queued here (count in
+    // acc->n_over) and counted by k_cover_spill with per-net values in global
+    // memory, slot k ([2][n_gates] u128) for its CTA k; spill_slots = 0: no
+    // spill scratch (such a pair reports kErrHashFull)
+    uint32_t *over_list;          // [min(n_pairs, 2 * n_gates)]
+    unsigned char *spill;
+    uint32_t spill_slots;
     // segments longer than one net: first_x / first_y are per segment, and
     // the (net, pair) pairs where a pair is first are a hash set built by
     // k_seg_first (keys net << 32 | pair index, ~0 = empty)
@@ -132,7 +140,9 @@ struct BatchCtl {
     unsigned int n_items;  // first-detecting (circuit, pair) items of this pass
     unsigned int done;     // cover CTAs finished
     unsigned int err;      // OR of every circuit's device error word after the pass
-    unsigned int pad;
+    unsigned int n_over;   // items queued for the spill cover
+    unsigned int done_over;
+    unsigned int pad[3];
 };
 // One forward launch of a batch: jobs of equal tile width and CTAs per SM.
 struct BatchClass {
@@ -145,6 +155,8 @@ struct BatchLaunch {
     const uint32_t *bpref; // [n + 1] first forward CTA of each circuit
     const uint32_t *gpref; // [n + 1] first gate of each circuit
     uint2 *items;          // [sum of min(n_pairs, 2 n_gates)]
+    uint2 *over_items;     // [same]: items whose pair marks more nets than the cover's table
+    uint32_t spill_grid;   // CTAs of the batch's spill cover (<= every spilling circuit's slots)
     BatchCtl *ctl;
     uint32_t n, total_blocks, total_gates;
     uint32_t sem, threads, cover_grid, hash_cap, append;  // sem: PDF_MARK_*
