@@ -185,17 +185,27 @@ struct segment {
     T pattern;
 };
 
-// One segment per net (N = 1), indexed by gate id, terminated by a sentinel
-// whose key is not a gate (mergekernel.cuh:215).
+// The segment list the harness was given ([S][N] gate ids: the reference's
+// generator lives in its missing util/segment.cuh, so the harness feeds the
+// list of the build under test); empty: one segment per net.
+inline std::vector<int> &harness_segments() {
+    static std::vector<int> v;
+    return v;
+}
+
+// The segment list, terminated by a sentinel whose key is not a gate
+// (mergekernel.cuh:215): for N = 1 without a given list, one segment per
+// net, indexed by gate id.
 template <int N>
 void generateSegmentList(segment<N, int2> **out, const GPU_Circuit &ckt) {
-    static_assert(N == 1, "the harness builds segments of length 1 only");
-    segment<N, int2> *l = new segment<N, int2>[ckt.size() + 1];
-    for (size_t g = 0; g < ckt.size(); g++) {
-        l[g].key.num[0] = (int)g;
-        l[g].pattern = make_int2(-1, -1);
+    const std::vector<int> &src = harness_segments();
+    const size_t S = src.empty() ? (N == 1 ? ckt.size() : 0) : src.size() / N;
+    segment<N, int2> *l = new segment<N, int2>[S + 1];
+    for (size_t s = 0; s < S; s++) {
+        for (int i = 0; i < N; i++) l[s].key.num[i] = src.empty() ? (int)s : src[s * N + i];
+        l[s].pattern = make_int2(-1, -1);
     }
-    l[ckt.size()].key.num[0] = -1;
+    for (int i = 0; i < N; i++) l[S].key.num[i] = -1;
     *out = l;
 }
 

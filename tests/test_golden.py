@@ -30,6 +30,12 @@ def load(path):
     return z, nl, n_vec, chunk, robust, v, t
 
 
+def seg_len(z) -> int:
+    """Segments of this many nets (fixtures of gpuMergeSegments<N> /
+    gpuCountPaths<N>); 1: single nets."""
+    return int(z["seg_len"]) if "seg_len" in z else 1
+
+
 def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a, np.uint8).tobytes()).hexdigest()
 
@@ -42,12 +48,27 @@ def test_fixtures_present():
 def test_oracle_matches_reference_kernels(path):
     z, nl, n, chunk, robust, v, t = load(path)
     codes = P.codes_from_planes(v, t, n)
+    N = seg_len(z)
+    if N > 1:  # the segment list given to the reference is the oracle's, and so are the results
+        np.testing.assert_array_equal(O.segments(nl, N), z["segments"])
+        fx = fy = None
+        counts = []
+        for a in range(0, n, chunk):
+            r = O.grade_seg(nl, codes[:, a:a + chunk], min(chunk, n - a), N, pair_base=a, mark_mode=robust,
+                            first_x=fx, first_y=fy)
+            fx, fy = r.first_x, r.first_y
+            counts.append(r.total)
+        np.testing.assert_array_equal(fx, z["ref_first_x"])
+        np.testing.assert_array_equal(fy, z["ref_first_y"])
+        assert counts == [int(x) for x in z["ref_chunk_counts"]]
     r = O.grade(nl, codes, n, mark_mode=robust, chunk=chunk, want_planes=True)
+    assert sha(r.sim) == str(z["ref_sim_sha256"])
+    assert sha(r.mark) == str(z["ref_mark_sha256"])
+    if N > 1:
+        return
     np.testing.assert_array_equal(r.first_x, z["ref_first_x"])
     np.testing.assert_array_equal(r.first_y, z["ref_first_y"])
     assert r.chunk_totals == [int(x) for x in z["ref_chunk_counts"]]
-    assert sha(r.sim) == str(z["ref_sim_sha256"])
-    assert sha(r.mark) == str(z["ref_mark_sha256"])
     if "ref_mark" in z:
         np.testing.assert_array_equal(P.codes_from_planes(z["ref_sim_v"], z["ref_sim_t"], n), r.sim)
         np.testing.assert_array_equal(P.bits_from_plane(z["ref_mark"], n), r.mark)
@@ -59,7 +80,10 @@ def test_cuda_path_matches_reference_kernels(path):
     """The CUDA path through the C ABI, batch by batch as the reference's
     chunks, against the reference's own outputs."""
     z, nl, n, chunk, robust, v, t = load(path)
-    c = P.Circuit(nl, mark_mode=robust)
+    N = seg_len(z)
+    c = P.Circuit(nl, mark_mode=robust, seg_len=N)
+    if N > 1:
+        np.testing.assert_array_equal(c.segments(), z["segments"])
     s = P.State(c)
     sim = np.zeros((nl.n_gates, n), np.uint8)
     mark = np.zeros((nl.n_gates, n), np.uint8)
