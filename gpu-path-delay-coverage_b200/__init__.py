@@ -152,6 +152,8 @@ ABI = [
                             C.c_uint64, C.c_void_p]),
     ("pdf_cover", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,
                             C.POINTER(Totals_t), C.c_void_p]),
+    ("pdf_cover_counts", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,
+                                   C.c_void_p, C.POINTER(Totals_t), C.c_void_p]),
     ("pdf_cover_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_void_p, C.POINTER(Totals_t), C.c_void_p]),
     ("pdf_batch_create", C.c_int, [C.POINTER(BatchJob_t), C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
@@ -192,6 +194,7 @@ ABI = [
     ("pdf_dump_mark", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64,
                                 C.c_int]),
     ("pdf_dump_merge", C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    ("pdf_dump_cover", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_int]),
     ("pdf_dump_segments", C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("pdf_circuit_segments", C.c_int, [C.c_void_p, C.c_void_p]),
 ]
@@ -800,6 +803,23 @@ def stage_cover(c: Circuit, s: State, mark, n_pairs, pair_base, stream: int = 0)
     check(lib().pdf_cover(c.h, s.h, _addr(mark), n_pairs, mark.shape[1], pair_base, C.byref(tot),
                           C.c_void_p(stream)), "pdf_cover")
     return tot
+
+
+def stage_cover_counts(c: Circuit, s: State, mark, n_pairs, pair_base, stream: int = 0):
+    """pdf_cover_counts: the chunk count and the paths each primary input
+    credits to each pair, as Python ints [n_pi][n_pairs]."""
+    tot = Totals_t()
+    raw = np.zeros((c.netlist.n_pi, n_pairs, 2), np.uint64)
+    check(lib().pdf_cover_counts(c.h, s.h, _addr(mark), n_pairs, mark.shape[1], pair_base, raw.ctypes.data,
+                                 C.byref(tot), C.c_void_p(stream)), "pdf_cover_counts")
+    return tot, raw
+
+
+def dump_cover(path: str, raw_counts: np.ndarray, pair_base: int = 0, append: bool = False) -> None:
+    """gpucover.log layout from pdf_cover_counts' array [n_pi][n_pairs][2] (pdf_dump_cover)."""
+    raw = np.ascontiguousarray(raw_counts, np.uint64)
+    check(lib().pdf_dump_cover(os.fsencode(path), raw.ctypes.data, raw.shape[0], raw.shape[1], pair_base,
+                               int(append)), "pdf_dump_cover")
 
 
 def stage_cover_noalloc(c: Circuit, mark, n_pairs, pair_base, first_x, first_y, stream: int = 0) -> Totals_t:

@@ -2,7 +2,7 @@
 // (main.cu:24-235), on the C ABI of libpdf_b200.
 //
 //   fcount --bench CIRCUIT [--robust] [--fixed] [--segs 1] [--num_patterns N]
-//          [--verbose [--sim] [--mark] [--merge]] [--branches] [--device D]
+//          [--verbose [--sim] [--mark] [--merge] [--cover]] [--branches] [--device D]
 //          VECTORS...
 //
 // For each vector file: one line on stdout,
@@ -68,8 +68,8 @@ void usage(const char *argv0) {
     std::printf("\t--segs N : Run fault grading over segments of length N, where 1 <= N <= 8\n");
     std::printf("\t--robust : robust sensitisation table (LUT_R) instead of the default (LUT_NR)\n");
     std::printf("\t--num_patterns N : vector pairs per pass (rounded up to a multiple of 32)\n");
-    std::printf("\t--verbose with --sim / --mark / --merge : write gpusim-p2.log / gpumark-full.log and\n"
-                "\t                       gpumark.log / gpumerge.log\n");
+    std::printf("\t--verbose with --sim / --mark / --merge / --cover : write gpusim-p2.log /\n"
+                "\t                       gpumark-full.log and gpumark.log / gpumerge.log / gpucover.log\n");
     std::printf("\t--branches : .bench only, a FROM gate on every fan-out branch\n");
     std::printf("\t--fixed : true n-input gates and textbook side conditions (non-robust; robust\n"
                 "\t          with --robust) instead of the reference's semantics\n");
@@ -167,8 +167,7 @@ int main(int argc, char *argv[]) {
         seg_list.resize(n_first * segs);
         check(pdf_circuit_segments(ckt, seg_list.data()), "pdf_circuit_segments");
     }
-    const bool dumps = verbose_flag && (sim_flag || mark_flag || merge_flag);
-    if (verbose_flag && cover_flag) std::clog << "gpucover.log is not written: per-(input, pair) counts stay inside the cover kernel" << std::endl;
+    const bool dumps = verbose_flag && (sim_flag || mark_flag || merge_flag || cover_flag);
 
     for (const std::string &vector_file : benchmarks) {
         std::cerr << "Vector set " << vector_file << std::endl;
@@ -247,8 +246,16 @@ int main(int argc, char *argv[]) {
                 const double t_merge =
                     timed([&] { check(pdf_merge(ckt, st, dv.p, dm.p, n, cw, p0, nullptr), "pdf_merge"); });
                 pdf_totals batch{};
-                const double t_cover =
-                    timed([&] { check(pdf_cover(ckt, st, dm.p, n, cw, p0, &batch, nullptr), "pdf_cover"); });
+                const double t_cover = timed([&] {
+                    if (cover_flag) {  // gpucover.log: the paths each input credits to each pair
+                        std::vector<uint64_t> counts((size_t)n_pi * n * 2);
+                        check(pdf_cover_counts(ckt, st, dm.p, n, cw, p0, counts.data(), &batch, nullptr),
+                              "pdf_cover_counts");
+                        check(pdf_dump_cover("gpucover.log", counts.data(), n_pi, n, p0, app), "pdf_dump_cover");
+                    } else {
+                        check(pdf_cover(ckt, st, dm.p, n, cw, p0, &batch, nullptr), "pdf_cover");
+                    }
+                });
                 sim += t_sim;
                 mark += t_mark;
                 merge += t_merge;

@@ -134,6 +134,7 @@ struct DeviceGuard {
 struct Workspace {
     DevBuf nzb, maxlvl, active, active_list;
     DevBuf over_list, spill;  // pairs for the spill cover and its per-net (h, c) slots
+    DevBuf pi_counts;         // pdf_cover_counts: paths per (primary input, pair)
     uint32_t spill_slots = 0;
     DevBuf seg_first;  // (net, pair) hash set of the cover with segments
     uint64_t seg_first_mask = 0;
@@ -147,6 +148,7 @@ struct Workspace {
         active_list.release();
         over_list.release();
         spill.release();
+        pi_counts.release();
         spill_slots = 0;
         seg_first.release();
         seg_first_mask = 0;
@@ -1437,24 +1439,31 @@ extern "C" pdf_status pdf_merge(pdf_circuit *c, pdf_state *s, const uint32_t *si
     return PDF_OK;
 }
 
-extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark, uint64_t n_pairs,
-                                uint64_t ld, uint64_t pair_base, pdf_totals *chunk, void *stream) {
-    if (!c || !s || s->c != c || !mark || n_pairs == 0 || ld < (n_pairs + 31) / 32) return PDF_EINVAL;
-    if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
-    DeviceGuard dg(c->device);
-    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+namespace {
+
+// pdf_cover, and with `counts` (host) the paths each primary input credits to
+// each pair of the chunk.
+pdf_status cover_chunk(pdf_circuit *c, pdf_state *s, const uint32_t *mark, uint64_t n_pairs, uint64_t ld,
+                       uint64_t pair_base, uint64_t *counts, pdf_totals *chunk, cudaStream_t cs) {
     std::lock_guard<std::mutex> lk(s->mu);
     const uint64_t W = (n_pairs + 31) / 32;
     pdf_status st = ensure_ws(c, s->ws, W, false);
     if (st != PDF_OK) return st;
+    const size_t count_bytes = (size_t)c->info.n_pi * n_pairs * 16;
+    if (counts) {
+        PDF_CUDA(s->ws.pi_counts.ensure(count_bytes));
+        PDF_CUDA(cudaMemsetAsync(s->ws.pi_counts.p, 0, count_bytes, cs));
+    }
     DevAcc *acc = s->acc.as<DevAcc>();
     PDF_CUDA(launch_batch_begin(acc, cs));
     PDF_CUDA(launch_bitmap_from_marks(c->dc, mark, ld, n_pairs, c->bw, s->ws.nzb.as<uint32_t>(),
                                       s->ws.maxlvl.as<uint32_t>(), (c->info.n_gates + 31) / 32, cs));
     CoverArgs ca = base_cover(c, s->ws, mark, ld, n_pairs, (uint32_t)pair_base, s->first_x.as<uint32_t>(),
                               s->first_y.as<uint32_t>(), acc);
+    if (counts) ca.pi_counts = s->ws.pi_counts.as<unsigned long long>();
     PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, true, cs));  // closes the batch
     PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
+    if (counts) PDF_CUDA(cudaMemcpyAsync(counts, s->ws.pi_counts.p, count_bytes, cudaMemcpyDeviceToHost, cs));
     PDF_CUDA(cudaStreamSynchronize(cs));
     const DevAcc &h = *s->host_acc;
     if (chunk) {
@@ -1465,6 +1474,27 @@ extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *ma
         chunk->reserved = 0;
     }
     return err_status(h.err);
+}
+
+}  // namespace
+
+extern "C" pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark, uint64_t n_pairs,
+                                uint64_t ld, uint64_t pair_base, pdf_totals *chunk, void *stream) {
+    if (!c || !s || s->c != c || !mark || n_pairs == 0 || ld < (n_pairs + 31) / 32) return PDF_EINVAL;
+    if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    return cover_chunk(c, s, mark, n_pairs, ld, pair_base, nullptr, chunk, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" pdf_status pdf_cover_counts(pdf_circuit *c, pdf_state *s, const uint32_t *mark, uint64_t n_pairs,
+                                       uint64_t ld, uint64_t pair_base, uint64_t *counts, pdf_totals *chunk,
+                                       void *stream) {
+    if (!c || !s || s->c != c || !mark || !counts || n_pairs == 0 || ld < (n_pairs + 31) / 32) return PDF_EINVAL;
+    if (pair_base + n_pairs > 0xFFFFFFFFull) return PDF_EINVAL;
+    DeviceGuard dg(c->device);
+    if (!dg.ok) return PDF_ECUDA;
+    return cover_chunk(c, s, mark, n_pairs, ld, pair_base, counts, chunk, static_cast<cudaStream_t>(stream));
 }
 
 // Allocation-free variant of pdf_cover: the same kernels, with their scratch

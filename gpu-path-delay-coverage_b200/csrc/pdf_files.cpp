@@ -541,6 +541,17 @@ void dump_header(std::ofstream &o, uint32_t n_gates) {
 
 inline uint32_t bit_at(const uint32_t *row, uint64_t p) { return (row[p >> 5] >> (p & 31)) & 1u; }
 
+// Decimal digits of the 128-bit value hi:lo.
+std::string u128_decimal(uint64_t hi, uint64_t lo) {
+    unsigned __int128 v = ((unsigned __int128)hi << 64) | lo;
+    std::string d;
+    do {
+        d.insert(d.begin(), char('0' + (int)(v % 10)));
+        v /= 10;
+    } while (v);
+    return d;
+}
+
 }  // namespace
 
 extern "C" pdf_status pdf_dump_sim(const char *path, const uint32_t *sim_v, const uint32_t *sim_t,
@@ -571,6 +582,23 @@ extern "C" pdf_status pdf_dump_mark(const char *path, const uint32_t *mark, uint
     for (uint64_t p = 0; p < n_pairs; p++) {
         o << "Vector " << p + pair_base << ":\t";
         for (uint32_t g = 0; g < n_gates; g++) o << std::setw(4) << (bit_at(mark + (uint64_t)g * ld, p) ? "Y" : "N") << " ";
+        o << "\n";
+    }
+    return o.good() ? PDF_OK : PDF_EINVAL;
+}
+
+extern "C" pdf_status pdf_dump_cover(const char *path, const uint64_t *counts, uint32_t n_pi, uint64_t n_pairs,
+                                     uint64_t pair_base, int append) {
+    if (!path || !counts || !n_pi) return PDF_EINVAL;
+    std::ofstream o(path, append ? std::ios::out | std::ios::app : std::ios::out);
+    if (!o) return PDF_EINVAL;
+    if (!append) dump_header(o, n_pi);  // the primary inputs are gates 0 .. n_pi - 1
+    for (uint64_t p = 0; p < n_pairs; p++) {
+        o << "Vector " << p + pair_base << ":\t";
+        for (uint32_t i = 0; i < n_pi; i++) {
+            const uint64_t *c = counts + ((uint64_t)i * n_pairs + p) * 2;
+            o << std::setw(4) << u128_decimal(c[1], c[0]) << " ";
+        }
         o << "\n";
     }
     return o.good() ? PDF_OK : PDF_EINVAL;

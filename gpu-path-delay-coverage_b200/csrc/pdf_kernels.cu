@@ -1312,6 +1312,14 @@ __host__ __device__ constexpr size_t cover_smem_lvt(uint32_t cap) {
 constexpr uint32_t kCoverThreads = 256;
 static_assert(kCoverCand / kCoverThreads <= 16, "cover_pair keeps 16 candidate mark words per thread");
 
+// Paths primary input g credits to pair p (the values the reference dumps to
+// gpucover.log, coverkernel.cuh:44-66).
+__device__ __forceinline__ void put_pi_count(const CoverArgs &a, uint32_t g, uint32_t p, pdf_u128 c) {
+    unsigned long long *d = a.pi_counts + ((size_t)g * a.n_pairs + p) * 2;
+    d[0] = (unsigned long long)c;
+    d[1] = (unsigned long long)(c >> 64);
+}
+
 // The cover of pair p (index within the batch) of the circuit in `a`;
 // lo_tab is its level table (shared or global memory).  Returns true (the
 // same in every thread) when the pair marks more nets than the table holds:
@@ -1463,7 +1471,10 @@ __device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p,
             if (c == ~(pdf_u128)0) ovf = true;
             if (inf & kNetInpt) {
                 h = 0;
-                if (lv == 0) total = add_sat(total, c, ovf);
+                if (lv == 0) {
+                    total = add_sat(total, c, ovf);
+                    if (a.pi_counts) put_pi_count(a, lid[i], p, c);
+                }
             }
             hv[i] = h;
             cv[i] = c;
@@ -1531,7 +1542,10 @@ __device__ void spill_pair(const CoverArgs &a, const uint32_t p, pdf_u128 *Hs) {
             if (c == ~(pdf_u128)0) ovf = true;
             if (rec_type(r) == PDF_INPT) {
                 h = 0;
-                if (lv == 0) total = add_sat(total, c, ovf);
+                if (lv == 0) {
+                    total = add_sat(total, c, ovf);
+                    if (a.pi_counts) put_pi_count(a, g, p, c);
+                }
             }
             Hs[g] = h;
             Cs[g] = c;

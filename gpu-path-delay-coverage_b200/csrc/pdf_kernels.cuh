@@ -109,6 +109,9 @@ struct CoverArgs {
     uint32_t *over_list;          // [min(n_pairs, 2 * n_gates)]
     unsigned char *spill;
     uint32_t spill_slots;
+    // optional: the paths each primary input credits to each pair,
+    // [n_pi][n_pairs] u128 as (low, high) u64 pairs, zeroed by the caller
+    unsigned long long *pi_counts;
     // segments longer than one net: first_x / first_y are per segment, and
     // the (net, pair) pairs where a pair is first are a hash set built by
     // k_seg_first (keys net << 32 | pair index, ~0 = empty)

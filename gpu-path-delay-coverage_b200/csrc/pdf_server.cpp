@@ -85,6 +85,7 @@ struct pdf_server {
     std::deque<Job *> retired;   // results taken, device memory still to free (by a worker)
     uint64_t used = 0;           // footprint of prepared + active jobs
     uint64_t n_active = 0;       // jobs prepared or active (retired ones until freed)
+    size_t graded_n = 0;         // jobs the batch is bound to
     uint64_t preparing = 0;      // jobs a worker is preparing now
     bool stop = false;
     std::vector<std::thread> workers;
@@ -379,12 +380,17 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         }
     }
     if (srv->active.empty()) return PDF_OK;
-    // the next batch of every active job: read in place from the job's
-    // pairs (rows of words done/32 .. on) when their pitch keeps the kernels'
-    // alignment, which moves the job's view every batch; else copied into the
-    // job's batch buffer (device to device)
+    // The jobs to grade: every active job with pairs left (a job whose pairs
+    // are all graded but whose retirement failed in an earlier step only
+    // waits to retire).  Their next batch is read in place from the job's
+    // pairs (rows of words done/32 .. on) when their pitch keeps the
+    // kernels' alignment, which moves the job's view every batch; else
+    // copied into the job's batch buffer (device to device).
     const uint64_t tw = srv->o.tile_words;
+    std::vector<Job *> grading;
     for (Job *j : srv->active) {
+        if (j->done >= j->n_pairs) continue;
+        grading.push_back(j);
         const uint64_t n = std::min<uint64_t>(srv->o.batch_pairs, j->n_pairs - j->done);
         if (n != j->cur) srv->dirty = true;
         j->cur = n;
@@ -405,33 +411,49 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
             return PDF_ECUDA;
         }
     }
-    if (srv->dirty) {
-        std::vector<pdf_batch_job> jobs;
-        for (Job *j : srv->active) {
-            const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32;
-            const pdf_pairs p = j->in_place
-                                    ? pdf_pairs{j->dall + w0, j->dall + npi * j->hld + w0, j->cur, j->hld, 1}
-                                    : pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1};
-            jobs.push_back(pdf_batch_job{j->c, j->s, p, j->done});
+    if (grading.size() != srv->graded_n) srv->dirty = true;
+    if (!grading.empty()) {
+        if (srv->dirty) {
+            std::vector<pdf_batch_job> jobs;
+            for (Job *j : grading) {
+                const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32;
+                const pdf_pairs p = j->in_place
+                                        ? pdf_pairs{j->dall + w0, j->dall + npi * j->hld + w0, j->cur, j->hld, 1}
+                                        : pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1};
+                jobs.push_back(pdf_batch_job{j->c, j->s, p, j->done});
+            }
+            const uint32_t fl = PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH;
+            st = srv->batch ? pdf_batch_rebind(srv->batch, jobs.data(), (uint32_t)jobs.size(), fl)
+                            : pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), fl, &srv->batch);
+            if (st != PDF_OK) return st;
+            srv->dirty = false;
+            srv->graded_n = grading.size();
         }
-        const uint32_t fl = PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH;
-        st = srv->batch ? pdf_batch_rebind(srv->batch, jobs.data(), (uint32_t)jobs.size(), fl)
-                        : pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), fl, &srv->batch);
-        if (st != PDF_OK) return st;
-        srv->dirty = false;
+        if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
+        pdf_batch_info bi{};
+        if (pdf_batch_query(srv->batch, &bi) == PDF_OK) srv->st.launches += bi.launches;
+        // the pass has graded (and, on the device, appended) every job's
+        // batch: account for it now, whatever happens below
+        const double t1 = now_s();
+        srv->st.steps++;
+        for (Job *j : grading) {
+            srv->lat_ms.push_back(1e3 * (t1 - j->t_ready));
+            j->t_ready = t1;
+            srv->st.batches++;
+            srv->st.gate_evals += (uint64_t)j->view.n_gates * j->cur;
+            j->done += j->cur;
+            if (j->done >= j->n_pairs) srv->dirty = true;  // leaves the batch
+        }
     }
-    if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
-    pdf_batch_info bi{};
-    if (pdf_batch_query(srv->batch, &bi) == PDF_OK) srv->st.launches += bi.launches;
-    // Retire the jobs whose pairs are all graded.  Nothing about a job changes
-    // (and no job is handed to the workers, who free retired jobs) until
-    // every fallible call of this step has succeeded: a failing step leaves
-    // every job active and unchanged on the host.  First the pinned staging
-    // of the retiring jobs' first-detect ids, grown geometrically (freeing
-    // pinned memory waits for the device).
+    // Retire the jobs whose pairs are all graded.  No job is handed to the
+    // workers (who free retired jobs) or leaves the active list until every
+    // read-back of this step has succeeded; after a failure here those jobs
+    // stay active, are not graded again, and retire at a later step.  First
+    // the pinned staging of their first-detect ids, grown geometrically
+    // (freeing pinned memory waits for the device).
     size_t gmax = 0;
     for (Job *j : srv->active)
-        if (j->done + j->cur >= j->n_pairs) gmax = std::max<size_t>(gmax, j->view.n_gates);
+        if (j->done >= j->n_pairs) gmax = std::max<size_t>(gmax, j->view.n_gates);
     if (srv->pin_words < 2 * gmax) {
         const size_t want = std::max(2 * gmax, 2 * srv->pin_words);
         if (srv->pin) cudaFreeHost(srv->pin);
@@ -447,7 +469,7 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     std::vector<Job *> keep, gone;
     std::vector<Result> res;
     for (Job *j : srv->active) {
-        if (j->done + j->cur < j->n_pairs) {
+        if (j->done < j->n_pairs) {
             keep.push_back(j);
             continue;
         }
@@ -462,16 +484,6 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         std::memcpy(r.fy.data(), srv->pin + G, 4 * G);
         res.push_back(std::move(r));
         gone.push_back(j);
-    }
-    // account and advance
-    const double t1 = now_s();
-    srv->st.steps++;
-    for (Job *j : srv->active) {
-        srv->lat_ms.push_back(1e3 * (t1 - j->t_ready));
-        j->t_ready = t1;
-        srv->st.batches++;
-        srv->st.gate_evals += (uint64_t)j->view.n_gates * j->cur;
-        j->done += j->cur;
     }
     for (size_t k = 0; k < gone.size(); k++) srv->results[gone[k]->id] = std::move(res[k]);
     if (!gone.empty()) {

@@ -336,6 +336,16 @@ pdf_status pdf_cover(pdf_circuit *c, pdf_state *s, const uint32_t *mark,
                      uint64_t n_pairs, uint64_t ld, uint64_t pair_base,
                      pdf_totals *chunk_total, void *stream);
 
+/* pdf_cover that also returns, in host memory, the paths each primary input
+ * credits to each pair of the chunk: counts[(i * n_pairs + p) * 2] and
+ * [... + 1] are the low and high 64 bits of input i's count for pair p
+ * (n_pi x n_pairs x 16 bytes).  These are the per-(input, pair) values the
+ * reference writes to gpucover.log in debug builds (debugCover,
+ * coverkernel.cuh:44-66,242-248), here exact; their sum is the chunk count. */
+pdf_status pdf_cover_counts(pdf_circuit *c, pdf_state *s, const uint32_t *mark, uint64_t n_pairs,
+                            uint64_t ld, uint64_t pair_base, uint64_t *counts, pdf_totals *chunk_total,
+                            void *stream);
+
 /*
  * pdf_cover without any allocation.  No counterpart in the reference (whose
  * gpuCountPaths allocates per chunk, coverkernel.cuh:256-275).
@@ -570,6 +580,11 @@ pdf_status pdf_dump_sim(const char *path, const uint32_t *sim_v, const uint32_t 
 pdf_status pdf_dump_mark(const char *path, const uint32_t *mark, uint32_t n_gates, uint64_t n_pairs,
                          uint64_t ld, uint64_t pair_base, int append);
 pdf_status pdf_dump_merge(const char *path, const uint32_t *first_x, const uint32_t *first_y, uint32_t n_gates);
+/* gpucover.log (debugCover, coverkernel.cuh:44-66): a header of the primary
+ * inputs' gate ids, then per pair "Vector <pair_base + p>:" and the paths
+ * each input credits to it, from pdf_cover_counts (exact decimal). */
+pdf_status pdf_dump_cover(const char *path, const uint64_t *counts, uint32_t n_pi, uint64_t n_pairs,
+                          uint64_t pair_base, int append);
 /* Segments longer than one net: "Segment <s>(g_0,...,g_{N-1}): x,y" per
  * segment, ids signed (debugSegmentList, mergekernel.cuh:25-46). */
 pdf_status pdf_dump_segments(const char *path, const uint32_t *gates, uint32_t seg_len, uint64_t n_segments,

@@ -41,6 +41,8 @@ def lib() -> C.CDLL:
         L.pdfo_mark.argtypes = [P, P, C.c_uint64, C.c_int, P, C.c_int, C.c_int]
         L.pdfo_merge.argtypes = [P, P, P, C.c_uint64, C.c_uint64, P, P, C.c_int]
         L.pdfo_cover.argtypes = [P, P, C.c_uint64, C.c_uint64, P, P, P, P, P, C.c_int]
+        L.pdfo_cover_counts.argtypes = [P, P, C.c_uint64, C.c_uint64, P, P, P, P, P, P, C.c_int]
+        L.pdfo_cover_counts.restype = C.c_int
         L.pdfo_grade.argtypes = [P, P, C.c_uint64, C.c_uint64, C.c_int, C.c_uint64, P, P, P, P, P, P, P,
                                  P, C.c_int]
         L.pdfo_segments.restype = C.c_uint64
@@ -157,14 +159,24 @@ def merge(nl, sim_codes, mark_bits, n_pairs: int, pair_base: int, first_x, first
                      first_y.ctypes.data, 0)
 
 
-def cover(nl, mark_bits, n_pairs: int, pair_base: int, first_x, first_y, threads: int = 0):
-    """kernCover<1> + kernSumSingle restated: returns (count, flags) of one chunk."""
+def cover(nl, mark_bits, n_pairs: int, pair_base: int, first_x, first_y, threads: int = 0,
+          want_counts: bool = False):
+    """kernCover<1> + kernSumSingle restated: returns (count, flags) of one
+    chunk; with want_counts also the c value of every primary input for every
+    pair (what debugCover writes to gpucover.log) as [n_pi][n_pairs][2] u64."""
     m = np.ascontiguousarray(mark_bits, dtype=np.uint8)
     fx = np.ascontiguousarray(first_x, dtype=np.uint32)
     fy = np.ascontiguousarray(first_y, dtype=np.uint32)
     lo, hi, fl = C.c_uint64(0), C.c_uint64(0), C.c_uint32(0)
-    rc = lib().pdfo_cover(_nl(nl), m.ctypes.data, n_pairs, pair_base, fx.ctypes.data, fy.ctypes.data,
-                          C.addressof(lo), C.addressof(hi), C.addressof(fl), threads)
+    counts = np.zeros((nl.n_pi, n_pairs, 2), np.uint64) if want_counts else None
+    if want_counts:
+        rc = lib().pdfo_cover_counts(_nl(nl), m.ctypes.data, n_pairs, pair_base, fx.ctypes.data, fy.ctypes.data,
+                                     counts.ctypes.data, C.addressof(lo), C.addressof(hi), C.addressof(fl), threads)
+    else:
+        rc = lib().pdfo_cover(_nl(nl), m.ctypes.data, n_pairs, pair_base, fx.ctypes.data, fy.ctypes.data,
+                              C.addressof(lo), C.addressof(hi), C.addressof(fl), threads)
     if rc:
         raise MemoryError("oracle allocation failed")
+    if want_counts:
+        return (hi.value << 64) | lo.value, fl.value, counts
     return (hi.value << 64) | lo.value, fl.value

@@ -358,12 +358,21 @@ static inline u128 sat_add(u128 a, u128 b, int *ovf) {
  */
 static int cover_impl(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
                       const uint32_t *first_x, const uint32_t *first_y, const uint8_t *first_plane,
-                      uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads);
+                      uint64_t *pi_counts, uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads);
 
 int pdfo_cover(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
                const uint32_t *first_x, const uint32_t *first_y, uint64_t *lo, uint64_t *hi,
                uint32_t *flags, int threads) {
-    return cover_impl(nl, mark, n_pairs, pair_base, first_x, first_y, NULL, lo, hi, flags, threads);
+    return cover_impl(nl, mark, n_pairs, pair_base, first_x, first_y, NULL, NULL, lo, hi, flags, threads);
+}
+
+/* pdfo_cover, also writing the c value of every primary input i for every
+ * pair p to pi_counts[(i * n_pairs + p) * 2 + {0, 1}] (low, high 64 bits):
+ * what debugCover prints to gpucover.log (coverkernel.cuh:44-66). */
+int pdfo_cover_counts(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
+                      const uint32_t *first_x, const uint32_t *first_y, uint64_t *pi_counts, uint64_t *lo,
+                      uint64_t *hi, uint32_t *flags, int threads) {
+    return cover_impl(nl, mark, n_pairs, pair_base, first_x, first_y, NULL, pi_counts, lo, hi, flags, threads);
 }
 
 /* first_plane (segments longer than one net): byte [g][p] = 1 when pair p of
@@ -371,7 +380,7 @@ int pdfo_cover(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uin
  * test (coverkernel.cuh:115-170 finds those pairs per gate). */
 static int cover_impl(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
                       const uint32_t *first_x, const uint32_t *first_y, const uint8_t *first_plane,
-                      uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads) {
+                      uint64_t *pi_counts, uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads) {
     const uint32_t G = nl->n_gates;
     const uint32_t lvl0 = nl->level_offsets[1];
     const int nt = nthreads(threads);
@@ -421,7 +430,13 @@ static int cover_impl(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pai
                     if (nl->type[g] == PDF_INPT) h[g] = 0; /* :221-223 */
                 }
                 for (uint32_t g = 0; g < lvl0; g++) /* kernSumSingle :83-92 */
-                    if (nl->type[g] == PDF_INPT) local = sat_add(local, c[g], &ovf);
+                    if (nl->type[g] == PDF_INPT) {
+                        local = sat_add(local, c[g], &ovf);
+                        if (pi_counts) {
+                            pi_counts[((uint64_t)g * n_pairs + p) * 2] = (uint64_t)c[g];
+                            pi_counts[((uint64_t)g * n_pairs + p) * 2 + 1] = (uint64_t)(c[g] >> 64);
+                        }
+                    }
             }
         }
 #pragma omp critical
@@ -603,7 +618,7 @@ int pdfo_cover_seg(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs,
             for (uint32_t i = 0; i < N; i++) fp[(uint64_t)segs[s * N + i] * n_pairs + (f[k] - pair_base)] = 1;
         }
     }
-    const int rc = cover_impl(nl, mark, n_pairs, pair_base, NULL, NULL, fp, lo, hi, flags, threads);
+    const int rc = cover_impl(nl, mark, n_pairs, pair_base, NULL, NULL, fp, NULL, lo, hi, flags, threads);
     free(fp);
     return rc;
 }

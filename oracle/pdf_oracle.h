@@ -49,6 +49,11 @@ int pdfo_merge(const pdf_netlist *nl, const uint8_t *sim, const uint8_t *mark,
 int pdfo_cover(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs,
                uint64_t pair_base, const uint32_t *first_x, const uint32_t *first_y,
                uint64_t *lo, uint64_t *hi, uint32_t *flags, int threads);
+/* pdfo_cover, also writing every primary input's count for every pair to
+ * pi_counts[(i * n_pairs + p) * 2 + {0, 1}] (low, high 64 bits). */
+int pdfo_cover_counts(const pdf_netlist *nl, const uint8_t *mark, uint64_t n_pairs, uint64_t pair_base,
+                      const uint32_t *first_x, const uint32_t *first_y, uint64_t *pi_counts, uint64_t *lo,
+                      uint64_t *hi, uint32_t *flags, int threads);
 
 /*
  * The reference's chunk loop (main.cu:171-231) over pi_codes [n_pi][n_pairs]:

@@ -108,7 +108,7 @@ def cases():
         # segments of 2, 3 and 4 nets (gpuMergeSegments<N>, gpuCountPaths<N>)
         ("seg2_mix", with_segments(0x601D0101, 2, 200, 16, 60, 8), 4096, 4096, 0, False, 2),
         ("seg3_marking", with_segments(0x601D0201, 3, 300, 20, 120, 9, mask=MARKING), 4096, 1024, 1, False, 3),
-        ("seg4_deep", with_segments(0x601D0301, 4, 300, 12, 150, 20), 4096, 2048, 0, False, 4),
+        ("seg4_marking", with_segments(0x601D0501, 4, 300, 20, 120, 9, mask=MARKING), 4096, 2048, 0, False, 4),
     ]
 
 

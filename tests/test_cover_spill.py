@@ -99,6 +99,13 @@ def test_stage_cover_spills():
     P.stage_merge(c, s, sv, mk, n, 0)
     tot = P.stage_cover(c, s, mk, n, 0)
     assert tot.value == want.total
+    # the spill cover also reports every input's count for every pair
+    s2 = P.State(c)
+    P.stage_merge(c, s2, sv, mk, n, 0)
+    tot2, raw = P.stage_cover_counts(c, s2, mk, n, 0)
+    _, _, counts = O.cover(nl, want.mark, n, 0, want.first_x, want.first_y, want_counts=True)
+    np.testing.assert_array_equal(raw, counts)
+    assert tot2.value == want.total
 
 
 def test_fixed_robust_on_c2():

@@ -265,8 +265,8 @@ def test_cli_logs_equal_oracle_planes(tmp_path):
     P.write_bench(nl, bench)
     back = P.read_bench(bench)
     vec, vpath = _vectors(tmp_path, nl.n_pi, 100, 3)
-    (m,) = _run(["--verbose", "--sim", "--mark", "--merge", "--num_patterns", "64", "--bench", bench, vpath],
-                cwd=str(tmp_path))
+    (m,) = _run(["--verbose", "--sim", "--mark", "--merge", "--cover", "--num_patterns", "64", "--bench", bench,
+                 vpath], cwd=str(tmp_path))
     n = vec.shape[1]
     v, t = P.pairs_from_vectors(vec)
     codes = P.codes_from_planes(v, t, n)
@@ -291,6 +291,42 @@ def test_cli_logs_equal_oracle_planes(tmp_path):
     merge = [ln.split("\t")[1].split(",") for ln in (tmp_path / "gpumerge.log").read_text().splitlines()]
     np.testing.assert_array_equal([int(x) & 0xFFFFFFFF for x, _ in merge], w.first_x)
     np.testing.assert_array_equal([int(y) & 0xFFFFFFFF for _, y in merge], w.first_y)
+    # gpucover.log: per pair, the paths each primary input credits to it,
+    # against the oracle's cover of each chunk with the first ids after it
+    lines = (tmp_path / "gpucover.log").read_text().splitlines()
+    assert lines[0].split() == ["Gate:"] + [str(i) for i in range(back.n_pi)]
+    body = [ln.split("\t", 1) for ln in lines[1:]]
+    assert [b[0] for b in body] == [f"Vector {p}:" for p in range(n)]
+    got = np.array([[int(x) for x in b[1].split()] for b in body], dtype=object).T
+    for a in range(0, n, 64):
+        b = min(n, a + 64)
+        wk = O.grade(back, codes[:, :b], b, chunk=64)
+        _, _, want = O.cover(back, w.mark[:, a:b], b - a, a, wk.first_x, wk.first_y, want_counts=True)
+        want = want[:, :, 0].astype(object) + (want[:, :, 1].astype(object) << 64)
+        np.testing.assert_array_equal(got[:, a:b], want)
+    assert int(got.sum()) == w.total
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tile", [0, 32])
+def test_cover_counts_equal_oracle(tile):
+    """pdf_cover_counts: every primary input's count for every pair, and
+    their sum the chunk's count."""
+    import torch
+    nl = circuits.random_small(79, n_gates=600, n_pi=24, n_po=80, depth=10, mask=circuits.MARKING_TYPES)
+    n = 1500
+    codes = helpers.rand_codes(np.random.default_rng(2), nl.n_pi, n)
+    w = O.grade(nl, codes, n, want_planes=True)
+    c = P.Circuit(nl, tile_words=tile)
+    s = P.State(c)
+    mk = torch.from_numpy(_planes(w.mark).view(np.int32)).cuda()
+    sv = torch.from_numpy(_planes(w.sim & 1).view(np.int32)).cuda()
+    P.stage_merge(c, s, sv, mk, n, 0)
+    tot, raw = P.stage_cover_counts(c, s, mk, n, 0)
+    _, _, want = O.cover(nl, w.mark, n, 0, w.first_x, w.first_y, want_counts=True)
+    np.testing.assert_array_equal(raw, want)
+    assert tot.value == w.total > 0
+    assert int(raw[:, :, 0].astype(object).sum()) == w.total
 
 
 @pytest.mark.gpu
