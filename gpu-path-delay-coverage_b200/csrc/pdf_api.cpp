@@ -134,6 +134,7 @@ struct DeviceGuard {
 struct Workspace {
     DevBuf nzb, maxlvl, active, active_list;
     DevBuf over_list, spill;  // pairs for the spill cover and its per-net (h, c) slots
+    DevBuf nzb_fine, maxlvl_fine;  // lane circuits: the cover's bitmaps per quarter column block
     DevBuf pi_counts;         // pdf_cover_counts: paths per (primary input, pair)
     uint32_t spill_slots = 0;
     DevBuf seg_first;  // (net, pair) hash set of the cover with segments
@@ -148,6 +149,8 @@ struct Workspace {
         active_list.release();
         over_list.release();
         spill.release();
+        nzb_fine.release();
+        maxlvl_fine.release();
         pi_counts.release();
         spill_slots = 0;
         seg_first.release();
@@ -1000,6 +1003,10 @@ pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes
     const uint64_t bm_words = (c->info.n_gates + 31) / 32;
     PDF_CUDA(ws.nzb.ensure(n_blocks * bm_words * 4));
     PDF_CUDA(ws.maxlvl.ensure(n_blocks * 4));
+    if (c->bw == kLaneWords) {  // the cover's bitmaps per quarter column block
+        PDF_CUDA(ws.nzb_fine.ensure(4 * n_blocks * bm_words * 4));
+        PDF_CUDA(ws.maxlvl_fine.ensure(4 * n_blocks * 4));
+    }
     // active bitmap [W], then the count; the list holds <= 2 pairs per gate
     PDF_CUDA(ws.active.ensure(W * 4 + 16));
     const uint64_t list = std::min<uint64_t>(W * 32, 2 * std::max<uint64_t>(c->n_first(), c->info.n_gates));
@@ -1084,10 +1091,13 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
     a.c = c->dc;
     a.M = M;
     a.ld = ld;
-    a.nzb = ws.nzb.as<uint32_t>();
-    a.blk_maxlvl = ws.maxlvl.as<uint32_t>();
+    // a lane circuit's cover reads bitmaps per quarter of its column blocks
+    // (fewer candidate nets per pair than the 1,024-pair block's)
+    const bool fine = c->bw == kLaneWords;
+    a.nzb = fine ? ws.nzb_fine.as<uint32_t>() : ws.nzb.as<uint32_t>();
+    a.blk_maxlvl = fine ? ws.maxlvl_fine.as<uint32_t>() : ws.maxlvl.as<uint32_t>();
     a.bm_words = (c->info.n_gates + 31) / 32;
-    a.bw = c->bw;
+    a.bw = fine ? kLaneCoverWords : c->bw;
     a.first_x = fx;
     a.first_y = fy;
     a.n_pairs = n_pairs;
@@ -1193,6 +1203,8 @@ pdf_status grade_mark_locked(pdf_circuit *c, pdf_state *s, const pdf_pairs *pr, 
     }
     a.nzb = s->ws.nzb.as<uint32_t>();
     a.blk_maxlvl = s->ws.maxlvl.as<uint32_t>();
+    a.nzb_fine = s->ws.nzb_fine.as<uint32_t>();
+    a.maxlvl_fine = s->ws.maxlvl_fine.as<uint32_t>();
     // with segments the state holds per-segment ids, merged after the kernel
     a.first_x = c->seg_len > 1 ? nullptr : s->first_x.as<uint32_t>();
     a.first_y = c->seg_len > 1 ? nullptr : s->first_y.as<uint32_t>();
@@ -1456,10 +1468,11 @@ pdf_status cover_chunk(pdf_circuit *c, pdf_state *s, const uint32_t *mark, uint6
     }
     DevAcc *acc = s->acc.as<DevAcc>();
     PDF_CUDA(launch_batch_begin(acc, cs));
-    PDF_CUDA(launch_bitmap_from_marks(c->dc, mark, ld, n_pairs, c->bw, s->ws.nzb.as<uint32_t>(),
-                                      s->ws.maxlvl.as<uint32_t>(), (c->info.n_gates + 31) / 32, cs));
     CoverArgs ca = base_cover(c, s->ws, mark, ld, n_pairs, (uint32_t)pair_base, s->first_x.as<uint32_t>(),
                               s->first_y.as<uint32_t>(), acc);
+    // the bitmaps the cover reads, at its granularity, from the given marks
+    PDF_CUDA(launch_bitmap_from_marks(c->dc, mark, ld, n_pairs, ca.bw, const_cast<uint32_t *>(ca.nzb),
+                                      const_cast<uint32_t *>(ca.blk_maxlvl), ca.bm_words, cs));
     if (counts) ca.pi_counts = s->ws.pi_counts.as<unsigned long long>();
     PDF_CUDA(launch_cover(ca, c->cover_grid, c->cover_threads, true, cs));  // closes the batch
     PDF_CUDA(cudaMemcpyAsync(s->host_acc, s->acc.p, sizeof(DevAcc), cudaMemcpyDeviceToHost, cs));
@@ -1679,6 +1692,8 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         a.M = a.T + G * a.ld;
         a.nzb = s->ws.nzb.as<uint32_t>();
         a.blk_maxlvl = s->ws.maxlvl.as<uint32_t>();
+        a.nzb_fine = s->ws.nzb_fine.as<uint32_t>();
+        a.maxlvl_fine = s->ws.maxlvl_fine.as<uint32_t>();
         a.first_x = s->first_x.as<uint32_t>();
         a.first_y = s->first_y.as<uint32_t>();
         a.pair_base = (uint32_t)j.pair_base;
@@ -1921,7 +1936,7 @@ extern "C" pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, con
     for (uint32_t tw : {2u, 4u, 8u})
         for (uint32_t th : {0u, 256u})
             if (!b0.threads || th == 0) cand.push_back({tw, b0.threads ? b0.threads : th});
-    if (!b0.threads) cand.push_back({kLaneWords, 0u});  // the lane kernel (1,024 threads)
+    if (!b0.threads) cand.push_back({kLaneWords, 0u});  // the lane kernel
     for (const auto &cw : cand) {
         const uint32_t tw = cw.first;
         pdf_circuit_opts o = b0;

@@ -738,8 +738,8 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
 // lower levels, so a CTA needs one barrier per level (not per piece of a
 // level), and every fan-in is read from its plane row (L1/L2), which is what
 // wide levels need: nothing of the circuit is kept on chip except the
-// block's mark bitmap.  Two gates per warp are in flight at a time (their
-// records, then their fan-in rows are loaded before either is evaluated).
+// block's mark bitmap and the staged records.  Several gates per warp are in
+// flight at a time (their fan-in rows are loaded before any is evaluated).
 //
 // Every gate with fan-outs writes its V and T rows (its readers load them);
 // a gate writes its M row only when it holds a mark (every reader of a mark
@@ -747,9 +747,9 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
 // planes (store_all).
 // ---------------------------------------------------------------------------
 
-// Fan-in rows of one gate, loaded before it is evaluated.
+// Fan-in rows of one gate, loaded before it is evaluated (its record stays
+// in shared memory and is read there by both phases).
 struct LaneIn {
-    GateRec r;
     uint32_t fv[kInlineFanins], ft[kInlineFanins];
     uint32_t m0;                 // mark row of fan-in 0 (when its bitmap bit is set)
     uint32_t fm[kInlineFanins];  // FIXED modes: mark rows of fan-ins 0..3 with their bits set
@@ -758,10 +758,10 @@ struct LaneIn {
 };
 
 template <int SEM, int MODE>
-__device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, uint32_t g, uint32_t w, bool live,
-                                          LaneIn &x) {
+__device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, const GateRec &r, uint32_t g,
+                                          uint32_t w, bool live, LaneIn &x) {
     constexpr bool FIX = SEM >= 2;
-    const uint32_t h = x.r.w[0], nfi = rec_nfi(x.r);
+    const uint32_t h = r.w[0], nfi = rec_nfi(r);
     const size_t o = (size_t)g * a.ld + w;
 #pragma unroll
     for (int q = 0; q < kInlineFanins; q++) {
@@ -790,10 +790,10 @@ __device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, 
     }
     // a killed gate's value is S0 whatever its fan-ins (and it cannot mark)
     const uint32_t nl = (h & RF_KILL) ? 0u : min(nfi, (uint32_t)kInlineFanins);
-    if (MODE != FWD_SIM) x.bit0 = bit_test(bm, x.r.w[7]);
+    if (MODE != FWD_SIM) x.bit0 = bit_test(bm, r.w[7]);
 #pragma unroll
     for (int q = 0; q < kInlineFanins; q++) {
-        const uint32_t sw = x.r.w[3 + q], f = sw & ~SRC_ZERO;
+        const uint32_t sw = r.w[3 + q], f = sw & ~SRC_ZERO;
         // a killed fan-in is S0 (its row is not written), except in the stage
         // call pdf_mark, whose given planes are read as they are
         if ((uint32_t)q < nl && live && (MODE == FWD_MARK || !(sw & SRC_ZERO))) {
@@ -803,16 +803,15 @@ __device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, 
             if (FIX && MODE != FWD_SIM && bit_test(bm, f)) x.fm[q] = a.M[fo];
         }
     }
-    if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live) x.m0 = a.M[(size_t)x.r.w[7] * a.ld + w];
+    if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live) x.m0 = a.M[(size_t)r.w[7] * a.ld + w];
 }
 
 // Evaluate, mark and store one gate; returns whether it holds a mark in the
 // block (warp-uniform).
 template <int SEM, int MODE>
-__device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, uint32_t g, uint32_t w, bool live,
-                                          uint32_t wmask, const LaneIn &x) {
+__device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, const GateRec &r, uint32_t g, uint32_t w,
+                                          bool live, uint32_t wmask, const LaneIn &x) {
     constexpr bool FIX = SEM >= 2;
-    const GateRec &r = x.r;
     const uint32_t h = r.w[0], nfi = rec_nfi(r);
     const size_t o = (size_t)g * a.ld + w;
     auto row = [&](const uint32_t *pl, uint32_t f) -> uint32_t { return live ? pl[(size_t)f * a.ld + w] : 0u; };
@@ -889,7 +888,9 @@ __device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, uint32
     return marked;
 }
 
-template <int SEM, int MODE>
+// U: gates per warp in flight (their fan-in rows are loaded before any of
+// them is evaluated), as many as the registers hold.
+template <int SEM, int MODE, int U>
 __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32_t blk) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
@@ -905,6 +906,9 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
 
     if (MODE != FWD_SIM)
         for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) bm[q] = 0;
+    uint32_t *fine = MODE == FWD_FUSED && a.nzb_fine ? a.nzb_fine + (size_t)blk * 4 * a.bm_words : nullptr;
+    if (fine)
+        for (uint32_t q = threadIdx.x; q < 4 * a.bm_words; q += blockDim.x) fine[q] = 0;
     if (MODE == FWD_FUSED) {  // the batch's cover state (the cover kernels run after this one)
         if (a.active && threadIdx.x < 32 && w0 + threadIdx.x <= a.W) a.active[w0 + threadIdx.x] = 0;
         if (a.active && blk == 0 && threadIdx.x == 0) a.active[a.W] = 0;
@@ -958,16 +962,18 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
             nlv = __ldg(&a.pieces[i + 2].level);
         }
         const GateRec *rb = recs + (size_t)(i & 1) * kLaneRecs;
-        for (uint32_t g = ga + warp; g < gb; g += 2 * NW) {
-            const uint32_t g1 = g + NW;
-            const bool two = g1 < gb;
-            LaneIn x0, x1;
-            x0.r = rb[g - ga];
-            if (two) x1.r = rb[g1 - ga];
-            lane_load<SEM, MODE>(a, bm, g, w, live, x0);
-            if (two) lane_load<SEM, MODE>(a, bm, g1, w, live, x1);
-            any |= lane_gate<SEM, MODE>(a, bm, g, w, live, wmask, x0);
-            if (two) any |= lane_gate<SEM, MODE>(a, bm, g1, w, live, wmask, x1);
+        for (uint32_t g = ga + warp; g < gb; g += U * NW) {
+            LaneIn x[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const uint32_t gu = g + u * NW;
+                if (gu < gb) lane_load<SEM, MODE>(a, bm, rb[gu - ga], gu, w, live, x[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const uint32_t gu = g + u * NW;
+                if (gu < gb) any |= lane_gate<SEM, MODE>(a, bm, rb[gu - ga], gu, w, live, wmask, x[u]);
+            }
         }
     }
     if (__syncthreads_or(any)) top = max(top, prev_level + 1);
@@ -1009,10 +1015,14 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
                     }
                     const uint32_t nm = mk & keep;
                     if (live && nm != mk) a.M[o] = nm;
-                    const bool nz = __any_sync(0xFFFFFFFFu, nm != 0);
+                    const uint32_t nzl = __ballot_sync(0xFFFFFFFFu, nm != 0);  // words (lanes) still marked
+                    const bool nz = nzl != 0;
                     if (!nz) {
                         if (lane == 0) atomicAnd(bm + (g >> 5), ~(1u << (g & 31)));
-                    } else if (MODE == FWD_FUSED && a.first_x) {  // merge: first falling / rising pair
+                    } else if (fine && lane < 4 && ((nzl >> (8 * lane)) & 0xFFu)) {
+                        atomicOr(fine + (size_t)lane * a.bm_words + (g >> 5), 1u << (g & 31));  // quarter `lane`
+                    }
+                    if (nz && MODE == FWD_FUSED && a.first_x) {  // merge: first falling / rising pair
                         const uint32_t v = live ? a.V[o] : 0u;
                         const uint32_t x = nm & ~v, y = nm & v;
                         uint32_t cx = x ? w * 32 + (__ffs(x) - 1) : kEmpty;
@@ -1033,12 +1043,13 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
         if (a.bm_shared && gbm)
             for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) gbm[q] = bm[q];
         if (threadIdx.x == 0) a.blk_maxlvl[blk] = maxlvl;
+        if (fine && threadIdx.x < 4) a.maxlvl_fine[blk * 4 + threadIdx.x] = maxlvl;
     }
 }
 
 template <int SEM, int MODE>
 __global__ void __launch_bounds__(kLaneThreads, 1) k_forward_lanes(const FwdArgs a) {
-    forward_lanes_cta<SEM, MODE>(a, blockIdx.x);
+    forward_lanes_cta<SEM, MODE, (SEM >= 2 || MODE == FWD_MARK) ? 4 : 8>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1681,7 +1692,7 @@ __global__ void __launch_bounds__(kLaneThreads, 1)
         }
     }
     __syncthreads();
-    forward_lanes_cta<SEM, FWD_FUSED>(s_a, s_blk);
+    forward_lanes_cta<SEM, FWD_FUSED, SEM >= 2 ? 4 : 6>(s_a, s_blk);  // arguments in shared memory take registers
 }
 
 __global__ void k_batch_active(const CoverArgs *args, const uint32_t *gpref, uint32_t n, uint2 *items,

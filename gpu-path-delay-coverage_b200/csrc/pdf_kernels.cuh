@@ -52,6 +52,10 @@ struct FwdArgs {
     uint32_t no_prune;            // FWD_MARK: stop after the forward marks (no removal pass)
     uint32_t *nzb;                // [n_blocks][bm_words] gates with a nonzero mark
     uint32_t *blk_maxlvl;         // [n_blocks] highest level holding a mark (+1), 0 = none
+    // lane kernel, fused: the same after the prune for each quarter (8 words)
+    // of a column block, [n_blocks * 4][bm_words] and [n_blocks * 4] (the
+    // cover's bitmaps; a bound for the level), or null
+    uint32_t *nzb_fine, *maxlvl_fine;
     uint32_t bm_words;
     uint32_t bm_shared;           // 1: the bitmap lives in shared memory during the kernel
     uint32_t *first_x, *first_y;  // [n_gates] (FWD_FUSED only)
@@ -131,9 +135,12 @@ struct SegMergeArgs {
 };
 
 // Tile width of the lane forward kernel (k_forward_lanes): one warp lane per
-// word, so a column block is 32 words (1,024 pairs) and a CTA 1,024 threads.
+// word, so a column block is 32 words (1,024 pairs); a CTA of 512 threads
+// (16 warps, up to 128 registers each: room for 8 gates in flight per warp).
 constexpr uint32_t kLaneWords = 32;
-constexpr uint32_t kLaneThreads = 1024;
+constexpr uint32_t kLaneThreads = 512;
+// Words per cover bitmap of a lane circuit (a quarter of its column block).
+constexpr uint32_t kLaneCoverWords = 8;
 // Forward launches of a batch at most: tile widths 1, 2, 4, 8 at 1, 2, 4
 // CTAs per SM, and the lane kernel.
 constexpr uint32_t kMaxBatchClasses = 8;
