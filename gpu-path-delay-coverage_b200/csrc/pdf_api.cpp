@@ -503,13 +503,23 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         delete c;
         return PDF_ECUDA;
     }
-    // Default tile: 4 words (128 pairs) per CTA; 8 when the circuit's largest
-    // batch still gives at least two 8-word CTAs per SM, which halves the
-    // per-gate work of record decode and staging per pair (1M gates at
-    // 262,144 pairs: 137 ms per batch at 8 words against 165 ms at 4).
+    // Default tile: the lane kernel (32 words, a warp per gate) when the
+    // circuit's largest batch gives it at least one 1,024-pair column block
+    // per SM and its levels average 1,024 gates or more (1M gates, 5,000-gate
+    // levels, 262,144 pairs: 70 ms per batch against 106 ms at 8 words; on
+    // narrower or smaller jobs its few CTAs leave SMs idle: 20,000 gates,
+    // 32,768 pairs, 0.92 against 0.25 ms).  Otherwise 4 words (128 pairs) per
+    // CTA, or 8 when the largest batch still gives at least two 8-word CTAs
+    // per SM, which halves the per-gate work of record decode and staging per
+    // pair (1M gates: 137 ms at 8 words against 165 ms at 4).
     const uint64_t max_words = ((o.max_pairs ? o.max_pairs : 65536ull) + 31) / 32;
-    c->bw = o.tile_words ? o.tile_words
-                         : (max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u);
+    const uint64_t mean_width = L > 1 ? (G - inf.n_pi) / (L - 1) : G;
+    if (o.tile_words)
+        c->bw = o.tile_words;
+    else if (max_words / kLaneWords >= (uint64_t)prop.multiProcessorCount && mean_width >= 1024)
+        c->bw = kLaneWords;
+    else
+        c->bw = max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u;
     const bool lanes = c->bw == kLaneWords;
     if (lanes) {
         // The lane kernel reads every fan-in from its plane row: source words

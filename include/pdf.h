@@ -165,8 +165,11 @@ typedef struct pdf_circuit_opts {
     int device;          /* CUDA device ordinal */
     int mark_mode;       /* PDF_MARK_* */
     uint32_t max_pairs;  /* largest batch this circuit will grade (sizes scratch); 0 = 65536 */
-    uint32_t tile_words; /* 0 = by batch size (8 when max_pairs gives >= 2 such CTAs per SM,
-                            else 4); else words (32 pairs) per CTA column block: 1,2,4,8 */
+    uint32_t tile_words; /* words (32 pairs) per CTA column block: 1, 2, 4, 8 (a thread per gate)
+                            or 32 (the lane kernel: a warp per gate, for wide levels);
+                            0 = chosen: 32 when max_pairs gives >= 1 such block per SM and the
+                            levels average >= 1,024 gates, else 8 when max_pairs gives >= 2
+                            8-word CTAs per SM, else 4 */
     uint32_t threads;    /* 0 = piece capacity + 64; else threads per CTA: 64..1024, a multiple
                             of 32; from 128 up, pieces then hold at most threads - 64 gates */
     uint32_t seg_len;    /* path segments of this many nets, 0 or 1 = single nets; up to 8
