@@ -620,7 +620,7 @@ def run_batched(args):
     stream = torch.cuda.current_stream().cuda_stream
     jobs, hosts = [], []
     for nl, g, n in members:
-        ld = (P.words(n) + 31) // 32 * 32  # a pitch every tile width divides
+        ld = (P.words(n) + 127) // 128 * 128  # a pitch every tile width divides
         v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, n, ld)
         c = P.Circuit(nl, device=local, mark_mode=P.MARK_ROBUST, max_pairs=n, tile_words=tw, threads=threads)
         st = P.State(c)

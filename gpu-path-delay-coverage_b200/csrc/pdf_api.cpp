@@ -432,7 +432,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     if (o.mark_mode < PDF_MARK_DEFAULT || o.mark_mode > PDF_MARK_FIXED_NONROBUST) return PDF_EINVAL;
     if (o.seg_len > 8) return PDF_EINVAL;
     if (o.tile_words && o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8 &&
-        o.tile_words != kLaneWords)
+        !lane_tile(o.tile_words))
         return PDF_EINVAL;
     if (o.threads && (o.threads < 64 || o.threads > 1024 || o.threads % 32)) return PDF_EINVAL;
     int ndev = 0;
@@ -503,24 +503,39 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         delete c;
         return PDF_ECUDA;
     }
-    // Default tile: the lane kernel (32 words, a warp per gate) when the
-    // circuit's largest batch gives it at least one 1,024-pair column block
-    // per SM and its levels average 1,024 gates or more (1M gates, 5,000-gate
-    // levels, 262,144 pairs: 70 ms per batch against 106 ms at 8 words; on
-    // narrower or smaller jobs its few CTAs leave SMs idle: 20,000 gates,
-    // 32,768 pairs, 0.92 against 0.25 ms).  Otherwise 4 words (128 pairs) per
-    // CTA, or 8 when the largest batch still gives at least two 8-word CTAs
-    // per SM, which halves the per-gate work of record decode and staging per
-    // pair (1M gates: 137 ms at 8 words against 165 ms at 4).
+    // Default tile.  The lane kernel (a warp per gate) when the circuit's
+    // largest batch gives it at least one 1,024-pair column block per SM and
+    // its levels average 1,024 gates or more; of its tiles the one with the
+    // least modelled time, waves of CTAs (one per SM) x words per CTA x the
+    // tile's time per word relative to 32 words, measured on a batch that
+    // fills the GPU: 1.0, 0.67, 0.52 at 32, 64, 128 words.  (1M gates, 5,000-
+    // gate levels, 262,144 pairs: 61, 36 and 58 ms at 32, 64, 128 words, 128
+    // CTAs being one wave at 64 words and 64 CTAs leaving half the SMs idle
+    // at 128.)  On narrower or smaller jobs the lane kernel's few CTAs leave
+    // SMs idle (20,000 gates, 32,768 pairs: 0.92 against 0.25 ms): 4 words
+    // (128 pairs) per CTA, or 8 when the largest batch still gives at least
+    // two 8-word CTAs per SM, which halves the per-gate work of record decode
+    // and staging per pair (1M gates: 137 ms at 8 words against 165 ms at 4).
     const uint64_t max_words = ((o.max_pairs ? o.max_pairs : 65536ull) + 31) / 32;
     const uint64_t mean_width = L > 1 ? (G - inf.n_pi) / (L - 1) : G;
-    if (o.tile_words)
+    const uint64_t sms = (uint64_t)prop.multiProcessorCount;
+    if (o.tile_words) {
         c->bw = o.tile_words;
-    else if (max_words / kLaneWords >= (uint64_t)prop.multiProcessorCount && mean_width >= 1024)
-        c->bw = kLaneWords;
-    else
-        c->bw = max_words / 8 >= 2ull * (uint64_t)prop.multiProcessorCount ? 8u : 4u;
-    const bool lanes = c->bw == kLaneWords;
+    } else if (max_words / kLaneWords >= sms && mean_width >= 1024) {
+        double best = 0;
+        for (const auto &t : {std::make_pair(kLaneWords, 1.0), std::make_pair(kLaneWords2, 0.67),
+                              std::make_pair(kLaneWords4, 0.52)}) {
+            const uint64_t ctas = (max_words + t.first - 1) / t.first;
+            const double cost = (double)((ctas + sms - 1) / sms) * t.first * t.second;
+            if (!best || cost < best) {
+                best = cost;
+                c->bw = t.first;
+            }
+        }
+    } else {
+        c->bw = max_words / 8 >= 2ull * sms ? 8u : 4u;
+    }
+    const bool lanes = lane_tile(c->bw);
     if (lanes) {
         // The lane kernel reads every fan-in from its plane row: source words
         // are the fan-in ids themselves, flagged SRC_ZERO when the fan-in is
@@ -537,7 +552,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
         for (uint32_t g = 0; g < G; g++)
             if (read[g]) recs[g].w[0] |= RF_SPILL;
     }
-    const uint32_t max_threads = lanes ? kLaneThreads : (c->bw >= 8 ? 512 : 1024);
+    const uint32_t max_threads = lanes ? lane_threads(c->bw) : (c->bw >= 8 ? 512 : 1024);
     uint32_t threads_default = 512;  // set from the piece size below
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     const uint32_t bm_words = (G + 31) / 32;
@@ -551,7 +566,7 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     c->cap = lanes ? 0u : std::min<uint32_t>(512, (widest + 31) & ~31u);
     // one thread per gate of a piece plus two warps that have none: they
     // issue the next piece's far-row copies
-    threads_default = lanes ? kLaneThreads : std::min<uint32_t>(max_threads, c->cap + 64);
+    threads_default = lanes ? lane_threads(c->bw) : std::min<uint32_t>(max_threads, c->cap + 64);
     c->threads = o.threads ? std::min(o.threads, max_threads) : threads_default;
     // a block size given by the caller also bounds the pieces: threads - 64
     // gates, so two warps stay free for the far-row copies
@@ -1013,9 +1028,10 @@ pdf_status ensure_ws(pdf_circuit *c, Workspace &ws, uint64_t W, bool need_planes
     const uint64_t bm_words = (c->info.n_gates + 31) / 32;
     PDF_CUDA(ws.nzb.ensure(n_blocks * bm_words * 4));
     PDF_CUDA(ws.maxlvl.ensure(n_blocks * 4));
-    if (c->bw == kLaneWords) {  // the cover's bitmaps per quarter column block
-        PDF_CUDA(ws.nzb_fine.ensure(4 * n_blocks * bm_words * 4));
-        PDF_CUDA(ws.maxlvl_fine.ensure(4 * n_blocks * 4));
+    if (lane_tile(c->bw)) {  // the cover's bitmaps per kLaneCoverWords words of a column block
+        const uint64_t nf = c->bw / kLaneCoverWords;
+        PDF_CUDA(ws.nzb_fine.ensure(nf * n_blocks * bm_words * 4));
+        PDF_CUDA(ws.maxlvl_fine.ensure(nf * n_blocks * 4));
     }
     // active bitmap [W], then the count; the list holds <= 2 pairs per gate
     PDF_CUDA(ws.active.ensure(W * 4 + 16));
@@ -1101,9 +1117,9 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
     a.c = c->dc;
     a.M = M;
     a.ld = ld;
-    // a lane circuit's cover reads bitmaps per quarter of its column blocks
-    // (fewer candidate nets per pair than the 1,024-pair block's)
-    const bool fine = c->bw == kLaneWords;
+    // a lane circuit's cover reads bitmaps per 8 words of its column blocks
+    // (fewer candidate nets per pair than the whole block's)
+    const bool fine = lane_tile(c->bw);
     a.nzb = fine ? ws.nzb_fine.as<uint32_t>() : ws.nzb.as<uint32_t>();
     a.blk_maxlvl = fine ? ws.maxlvl_fine.as<uint32_t>() : ws.maxlvl.as<uint32_t>();
     a.bm_words = (c->info.n_gates + 31) / 32;
@@ -1130,11 +1146,12 @@ CoverArgs base_cover(pdf_circuit *c, Workspace &ws, const uint32_t *M, uint64_t 
 
 // Device pointers of the pairs (staging host pairs through the workspace).
 // True when (ptr, ld) can be used by the kernels directly: rows of ld words,
-// ld a multiple of the tile width, every row long enough for whole tiles, and
-// 16-byte aligned base addresses.
+// ld a multiple of the tile width and below 2^30 (row pitches in bytes fit
+// 32 bits), every row long enough for whole tiles, and 16-byte aligned base
+// addresses.
 bool planes_fit(const pdf_circuit *c, uint64_t W, uint64_t ld, std::initializer_list<const void *> ptrs) {
     const uint64_t Wp = (W + c->bw - 1) / c->bw * c->bw;
-    if (ld < Wp || ld % c->bw) return false;
+    if (ld < Wp || ld % c->bw || ld >= (1ull << 30)) return false;
     for (const void *p : ptrs)
         if (!p || (reinterpret_cast<uintptr_t>(p) & 15)) return false;
     return true;
@@ -1946,7 +1963,11 @@ extern "C" pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, con
     for (uint32_t tw : {2u, 4u, 8u})
         for (uint32_t th : {0u, 256u})
             if (!b0.threads || th == 0) cand.push_back({tw, b0.threads ? b0.threads : th});
-    if (!b0.threads) cand.push_back({kLaneWords, 0u});  // the lane kernel
+    if (!b0.threads) {  // the lane tiles
+        cand.push_back({kLaneWords, 0u});
+        cand.push_back({kLaneWords2, 0u});
+        cand.push_back({kLaneWords4, 0u});
+    }
     for (const auto &cw : cand) {
         const uint32_t tw = cw.first;
         pdf_circuit_opts o = b0;

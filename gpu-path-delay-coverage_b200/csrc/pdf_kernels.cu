@@ -727,162 +727,284 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024) k_forward(const FwdArgs 
 }
 
 // ---------------------------------------------------------------------------
-// Lane forward kernel (tile of 32 words, 1,024 pairs per CTA): the same
-// stages as forward_cta (sim, forward mark, prune, merge) with the roles of
-// threads turned around.  Lane j of every warp carries word w0 + j of the
-// column block, and a warp evaluates one gate at a time for all 32 words, so
-// every instruction of a gate is uniform across the warp (no divergence on
-// gate type or fan-in count), a gate's record is decoded once per 1,024
-// pairs, and every plane-row access is one coalesced 128-byte line.  Warps
-// take the gates of a level in turn; the gates of a level depend only on
-// lower levels, so a CTA needs one barrier per level (not per piece of a
-// level), and every fan-in is read from its plane row (L1/L2), which is what
-// wide levels need: nothing of the circuit is kept on chip except the
-// block's mark bitmap and the staged records.  Several gates per warp are in
-// flight at a time (their fan-in rows are loaded before any is evaluated).
+// Lane forward kernel (tiles of 32 x LW words, LW = 1 or 2): the same stages
+// as forward_cta (sim, forward mark, prune, merge) with the roles of threads
+// turned around.  Lane j of every warp carries words w0 + LW j .. + LW - 1 of
+// the column block, and a warp evaluates one gate at a time for the whole
+// block, so every instruction of a gate is uniform across the warp (no
+// divergence on gate type or fan-in count), a gate's record is decoded once
+// per 1,024 LW pairs, and every plane-row access is one coalesced line of
+// 128 LW bytes.  Warps take the gates of a level in turn; the gates of a
+// level depend only on lower levels, so a CTA needs one barrier per level
+// (not per piece of a level), and every fan-in is read from its plane row
+// (L1/L2), which is what wide levels need: nothing of the circuit is kept on
+// chip except the block's mark bitmap and the staged records.  Several gates
+// per warp are in flight at a time (their fan-in rows are loaded before any
+// is evaluated).
 //
 // Every gate with fan-outs writes its V and T rows (its readers load them);
 // a gate writes its M row only when it holds a mark (every reader of a mark
 // row tests the gate's bitmap bit first), or when the caller asked for the
-// planes (store_all).
+// planes (store_all).  Words past the last pair of a row are read (rows are
+// padded to whole blocks) but masked, and never written.
 // ---------------------------------------------------------------------------
 
+// A lane's view of the planes: its first word in row 0 of each plane, and
+// the row pitch in bytes (below 2^32: planes_fit), so that a row address is
+// one wide multiply-add.
+struct LanePlanes {
+    char *V, *T, *M;
+    uint32_t ld4;
+};
+template <typename P>
+__device__ __forceinline__ uint32_t *lrow(P *base, uint32_t f, uint32_t ld4) {
+    return reinterpret_cast<uint32_t *>(const_cast<char *>(base) + (size_t)f * ld4);
+}
+template <int LW>
+__device__ __forceinline__ void lload(const uint32_t *p, uint32_t (&d)[LW]) {
+    if constexpr (LW == 4) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(p);
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
+    } else if constexpr (LW == 2) {
+        const uint2 v = *reinterpret_cast<const uint2 *>(p);
+        d[0] = v.x;
+        d[1] = v.y;
+    } else {
+        d[0] = *p;
+    }
+}
+template <int LW>
+__device__ __forceinline__ void lload_nc(const uint32_t *p, uint32_t (&d)[LW]) {
+    if constexpr (LW == 4) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p));
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
+    } else if constexpr (LW == 2) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2 *>(p));
+        d[0] = v.x;
+        d[1] = v.y;
+    } else {
+        d[0] = __ldg(p);
+    }
+}
+// nw: the lane's words that hold pairs (1..LW); the others are not written
+template <int LW>
+__device__ __forceinline__ void lstore(uint32_t *p, const uint32_t (&s)[LW], uint32_t nw) {
+    if constexpr (LW == 4) {
+        if (nw == 4) {
+            *reinterpret_cast<uint4 *>(p) = make_uint4(s[0], s[1], s[2], s[3]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                if ((uint32_t)j < nw) p[j] = s[j];
+        }
+    } else if constexpr (LW == 2) {
+        if (nw == 2) *reinterpret_cast<uint2 *>(p) = make_uint2(s[0], s[1]);
+        else p[0] = s[0];
+    } else {
+        p[0] = s[0];
+    }
+}
+template <int LW>
+__device__ __forceinline__ void lzero(uint32_t (&d)[LW]) {
+#pragma unroll
+    for (int j = 0; j < LW; j++) d[j] = 0;
+}
+template <int LW>
+__device__ __forceinline__ bool lany(const uint32_t (&d)[LW]) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int j = 0; j < LW; j++) o |= d[j];
+    return o != 0;
+}
+
 // Fan-in rows of one gate, loaded before it is evaluated (its record stays
-// in shared memory and is read there by both phases).
+// in shared memory; the header travels here).
+template <int LW>
 struct LaneIn {
-    uint32_t fv[kInlineFanins], ft[kInlineFanins];
-    uint32_t m0;                 // mark row of fan-in 0 (when its bitmap bit is set)
-    uint32_t fm[kInlineFanins];  // FIXED modes: mark rows of fan-ins 0..3 with their bits set
-    uint32_t sv, st;             // stage call pdf_mark: the gate's own given V and T
-    bool bit0;                   // fan-in 0 holds a mark in this column block
+    uint32_t h;                          // record header
+    uint32_t fv[kInlineFanins][LW], ft[kInlineFanins][LW];
+    uint32_t m0[LW];                     // mark row of fan-in 0 (when its bitmap bit is set)
+    uint32_t fm[kInlineFanins][LW];      // FIXED modes: mark rows of fan-ins 0..3 with their bits set
+    uint32_t sv[LW], st[LW];             // stage call pdf_mark: the gate's own given V and T
+    bool bit0;                           // fan-in 0 holds a mark in this column block
 };
 
-template <int SEM, int MODE>
-__device__ __forceinline__ void lane_load(const FwdArgs &a, const uint32_t *bm, const GateRec &r, uint32_t g,
-                                          uint32_t w, bool live, LaneIn &x) {
+template <int SEM, int MODE, int LW>
+__device__ __forceinline__ void lane_load(const FwdArgs &a, const LanePlanes &P, const uint32_t *bm,
+                                          const GateRec *rp, uint32_t g, uint32_t w, bool live, LaneIn<LW> &x) {
     constexpr bool FIX = SEM >= 2;
-    const uint32_t h = r.w[0], nfi = rec_nfi(r);
-    const size_t o = (size_t)g * a.ld + w;
+    const uint4 r0 = reinterpret_cast<const uint4 *>(rp)[0], r1 = reinterpret_cast<const uint4 *>(rp)[1];
+    const uint32_t h = r0.x, nfi = (h >> 8) & 0xFFu;
+    const uint32_t src[kInlineFanins] = {r0.w, r1.x, r1.y, r1.z};  // w[3..6]
+    x.h = h;
 #pragma unroll
     for (int q = 0; q < kInlineFanins; q++) {
-        x.fv[q] = 0;
-        x.ft[q] = 0;
-        x.fm[q] = 0;
+        lzero<LW>(x.fv[q]);
+        lzero<LW>(x.ft[q]);
+        lzero<LW>(x.fm[q]);
     }
-    x.m0 = 0;
-    x.sv = 0;
-    x.st = 0;
+    lzero<LW>(x.m0);
+    lzero<LW>(x.sv);
+    lzero<LW>(x.st);
     x.bit0 = false;
     if (h & RF_INPT) {
+        if (!live) return;
         if (MODE == FWD_MARK) {
-            x.fv[0] = live ? a.V[o] : 0u;
-            x.ft[0] = live ? a.T[o] : 0u;
+            lload<LW>(lrow(P.V, g, P.ld4), x.fv[0]);
+            lload<LW>(lrow(P.T, g, P.ld4), x.ft[0]);
         } else {
-            const size_t po = (size_t)g * a.pi_ld + w;
-            x.fv[0] = live ? __ldg(a.pi_v + po) : 0u;
-            x.ft[0] = live ? __ldg(a.pi_t + po) : 0u;
+            const uint32_t pld4 = (uint32_t)(a.pi_ld * 4);
+            lload_nc<LW>(lrow(reinterpret_cast<const char *>(a.pi_v + w), g, pld4), x.fv[0]);
+            lload_nc<LW>(lrow(reinterpret_cast<const char *>(a.pi_t + w), g, pld4), x.ft[0]);
         }
         return;
     }
-    if (MODE == FWD_MARK) {  // the gate's own values are given; fan-ins feed the side test only
-        x.sv = live ? a.V[o] : 0u;
-        x.st = live ? a.T[o] : 0u;
+    if (MODE == FWD_MARK && live) {  // the gate's own values are given; fan-ins feed the side test only
+        lload<LW>(lrow(P.V, g, P.ld4), x.sv);
+        lload<LW>(lrow(P.T, g, P.ld4), x.st);
     }
     // a killed gate's value is S0 whatever its fan-ins (and it cannot mark)
     const uint32_t nl = (h & RF_KILL) ? 0u : min(nfi, (uint32_t)kInlineFanins);
-    if (MODE != FWD_SIM) x.bit0 = bit_test(bm, r.w[7]);
+    if (MODE != FWD_SIM) x.bit0 = bit_test(bm, r1.w);
 #pragma unroll
     for (int q = 0; q < kInlineFanins; q++) {
-        const uint32_t sw = r.w[3 + q], f = sw & ~SRC_ZERO;
+        const uint32_t sw = src[q], f = sw & ~SRC_ZERO;
         // a killed fan-in is S0 (its row is not written), except in the stage
         // call pdf_mark, whose given planes are read as they are
         if ((uint32_t)q < nl && live && (MODE == FWD_MARK || !(sw & SRC_ZERO))) {
-            const size_t fo = (size_t)f * a.ld + w;
-            x.fv[q] = a.V[fo];
-            x.ft[q] = a.T[fo];
-            if (FIX && MODE != FWD_SIM && bit_test(bm, f)) x.fm[q] = a.M[fo];
+            lload<LW>(lrow(P.V, f, P.ld4), x.fv[q]);
+            lload<LW>(lrow(P.T, f, P.ld4), x.ft[q]);
+            if (FIX && MODE != FWD_SIM && bit_test(bm, f)) lload<LW>(lrow(P.M, f, P.ld4), x.fm[q]);
         }
     }
-    if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live) x.m0 = a.M[(size_t)r.w[7] * a.ld + w];
+    if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live) lload<LW>(lrow(P.M, r1.w, P.ld4), x.m0);
 }
 
 // Evaluate, mark and store one gate; returns whether it holds a mark in the
-// block (warp-uniform).
-template <int SEM, int MODE>
-__device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, const GateRec &r, uint32_t g, uint32_t w,
-                                          bool live, uint32_t wmask, const LaneIn &x) {
+// block (warp-uniform).  wm: the lane's word masks (pairs present).
+template <int SEM, int MODE, int LW>
+__device__ __forceinline__ bool lane_gate(const FwdArgs &a, const LanePlanes &P, uint32_t *bm, const GateRec *rp,
+                                          uint32_t g, bool live, uint32_t nw, const uint32_t (&wm)[LW],
+                                          const LaneIn<LW> &x) {
     constexpr bool FIX = SEM >= 2;
-    const uint32_t h = r.w[0], nfi = rec_nfi(r);
-    const size_t o = (size_t)g * a.ld + w;
-    auto row = [&](const uint32_t *pl, uint32_t f) -> uint32_t { return live ? pl[(size_t)f * a.ld + w] : 0u; };
-    uint32_t V, T, M = 0;
+    const uint32_t h = x.h, nfi = (h >> 8) & 0xFFu;
+    // fan-in q > 3 of the gate (its id from the edge array), read from its rows
+    const auto far_row = [&](uint32_t q, uint32_t (&v)[LW], uint32_t (&t)[LW]) {
+        const uint32_t f = __ldg(a.c.edges + rp->w[2] + q);
+        lzero<LW>(v);
+        lzero<LW>(t);
+        if (live) {
+            lload<LW>(lrow(P.V, f, P.ld4), v);
+            lload<LW>(lrow(P.T, f, P.ld4), t);
+        }
+        return f;
+    };
+    uint32_t V[LW], T[LW], M[LW];
+    lzero<LW>(M);
     if (h & RF_INPT) {
-        V = x.fv[0] & wmask;
-        T = x.ft[0] & wmask;
+#pragma unroll
+        for (int j = 0; j < LW; j++) {
+            V[j] = x.fv[0][j] & wm[j];
+            T[j] = x.ft[0][j] & wm[j];
+        }
     } else if (MODE == FWD_MARK) {
-        V = x.sv & wmask;
-        T = x.st & wmask;
+#pragma unroll
+        for (int j = 0; j < LW; j++) {
+            V[j] = x.sv[j] & wm[j];
+            T[j] = x.st[j] & wm[j];
+        }
     } else {
-        uint32_t v1;
-        eval_first(h, x.fv[0], x.ft[0], V, v1);
+        uint32_t v1[LW];
+#pragma unroll
+        for (int j = 0; j < LW; j++) eval_first(h, x.fv[0][j], x.ft[0][j], V[j], v1[j]);
         const uint32_t nfold = hdr_nfold(h);
 #pragma unroll
         for (int q = 1; q < kInlineFanins; q++)
-            if ((uint32_t)q <= nfold) eval_fold<FIX>(h, V, v1, x.fv[q], x.ft[q]);
+            if ((uint32_t)q <= nfold)
+#pragma unroll
+                for (int j = 0; j < LW; j++) eval_fold<FIX>(h, V[j], v1[j], x.fv[q][j], x.ft[q][j]);
         for (uint32_t q = kInlineFanins; q <= nfold; q++) {
-            const uint32_t f = __ldg(a.c.edges + r.w[2] + q);
-            eval_fold<FIX>(h, V, v1, row(a.V, f), row(a.T, f));
+            uint32_t rv[LW], rt[LW];
+            far_row(q, rv, rt);
+#pragma unroll
+            for (int j = 0; j < LW; j++) eval_fold<FIX>(h, V[j], v1[j], rv[j], rt[j]);
         }
-        eval_finish<FIX>(h, V, v1, T);
-        V &= wmask;
-        T &= wmask;
+#pragma unroll
+        for (int j = 0; j < LW; j++) {
+            eval_finish<FIX>(h, V[j], v1[j], T[j]);
+            V[j] &= wm[j];
+            T[j] &= wm[j];
+        }
     }
     if (MODE != FWD_SIM) {  // markkernel.cuh:226-267
-        const bool anyT = __any_sync(0xFFFFFFFFu, T != 0);
+        const bool anyT = __any_sync(0xFFFFFFFFu, lany<LW>(T));
         if (h & RF_INPT) {
-            M = T;
+#pragma unroll
+            for (int j = 0; j < LW; j++) M[j] = T[j];
         } else if ((h & RF_MARKF0) && x.bit0 && anyT) {
             // fan-in 0 (gate w[7]) holds a mark: its bitmap bit is set
-            M = T & x.m0;
-            if ((h & RF_SENS) && __any_sync(0xFFFFFFFFu, M != 0)) {
+#pragma unroll
+            for (int j = 0; j < LW; j++) M[j] = T[j] & x.m0[j];
+            if ((h & RF_SENS) && __any_sync(0xFFFFFFFFu, lany<LW>(M))) {
                 // the side test over the fan-in rows already loaded (past the
                 // fourth, read here)
-                SensAcc s;
-                sens_init(s);
+                SensAcc s[LW];
                 const bool or_like = (h & RF_IM) != 0;
 #pragma unroll
+                for (int j = 0; j < LW; j++) sens_init(s[j]);
+#pragma unroll
                 for (int q = 0; q < kInlineFanins; q++)
-                    if ((uint32_t)q < nfi) sens_step<SEM & 1>(s, or_like, x.fv[q], x.ft[q]);
+                    if ((uint32_t)q < nfi)
+#pragma unroll
+                        for (int j = 0; j < LW; j++) sens_step<SEM & 1>(s[j], or_like, x.fv[q][j], x.ft[q][j]);
                 for (uint32_t q = kInlineFanins; q < nfi; q++) {
-                    const uint32_t f = __ldg(a.c.edges + r.w[2] + q);
-                    sens_step<SEM & 1>(s, or_like, row(a.V, f), row(a.T, f));
+                    uint32_t rv[LW], rt[LW];
+                    far_row(q, rv, rt);
+#pragma unroll
+                    for (int j = 0; j < LW; j++) sens_step<SEM & 1>(s[j], or_like, rv[j], rt[j]);
                 }
-                M &= sens_result<SEM & 1>(s);
+#pragma unroll
+                for (int j = 0; j < LW; j++) M[j] &= sens_result<SEM & 1>(s[j]);
             }
         } else if (FIX && (h & RF_MANY) && anyT) {
             // any fan-in may carry the path: its own mark enters the side test
             const uint32_t mor = flagmask(h, RF_IM), mxor = flagmask(h, RF_XOR), mand = ~(mor | mxor);
-            SensAcc s;
-            sens_init(s);
+            SensAcc s[LW];
+#pragma unroll
+            for (int j = 0; j < LW; j++) sens_init(s[j]);
 #pragma unroll
             for (int q = 0; q < kInlineFanins; q++)
                 if ((uint32_t)q < nfi)
-                    sens_step_fixed<SEM == PDF_MARK_FIXED_NONROBUST>(s, mand, mor, mxor, x.fv[q], x.ft[q], x.fm[q]);
+#pragma unroll
+                    for (int j = 0; j < LW; j++)
+                        sens_step_fixed<SEM == PDF_MARK_FIXED_NONROBUST>(s[j], mand, mor, mxor, x.fv[q][j],
+                                                                         x.ft[q][j], x.fm[q][j]);
             for (uint32_t q = kInlineFanins; q < nfi; q++) {
-                const uint32_t f = __ldg(a.c.edges + r.w[2] + q);
-                const uint32_t fm = bit_test(bm, f) ? row(a.M, f) : 0u;
-                sens_step_fixed<SEM == PDF_MARK_FIXED_NONROBUST>(s, mand, mor, mxor, row(a.V, f), row(a.T, f), fm);
+                uint32_t rv[LW], rt[LW], rm[LW];
+                const uint32_t f = far_row(q, rv, rt);
+                lzero<LW>(rm);
+                if (live && bit_test(bm, f)) lload<LW>(lrow(P.M, f, P.ld4), rm);
+#pragma unroll
+                for (int j = 0; j < LW; j++)
+                    sens_step_fixed<SEM == PDF_MARK_FIXED_NONROBUST>(s[j], mand, mor, mxor, rv[j], rt[j], rm[j]);
             }
-            M = T & sens_result<SEM == PDF_MARK_FIXED_NONROBUST>(s);
+#pragma unroll
+            for (int j = 0; j < LW; j++) M[j] = T[j] & sens_result<SEM == PDF_MARK_FIXED_NONROBUST>(s[j]);
         }
     }
-    const bool marked = MODE != FWD_SIM && __any_sync(0xFFFFFFFFu, M != 0);
+    const bool marked = MODE != FWD_SIM && __any_sync(0xFFFFFFFFu, lany<LW>(M));
     if (live) {
         if (MODE != FWD_MARK && (a.store_all || (h & RF_SPILL) || marked)) {
-            a.V[o] = V;
-            a.T[o] = T;
+            lstore<LW>(lrow(P.V, g, P.ld4), V, nw);
+            lstore<LW>(lrow(P.T, g, P.ld4), T, nw);
         }
-        if (MODE != FWD_SIM && (a.store_all || marked)) a.M[o] = M;
+        if (MODE != FWD_SIM && (a.store_all || marked)) lstore<LW>(lrow(P.M, g, P.ld4), M, nw);
     }
     if (marked && (threadIdx.x & 31) == 0) atomicOr(bm + (g >> 5), 1u << (g & 31));
     return marked;
@@ -890,15 +1012,27 @@ __device__ __forceinline__ bool lane_gate(const FwdArgs &a, uint32_t *bm, const 
 
 // U: gates per warp in flight (their fan-in rows are loaded before any of
 // them is evaluated), as many as the registers hold.
-template <int SEM, int MODE, int U>
+template <int SEM, int MODE, int U, int LW>
 __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32_t blk) {
     extern __shared__ __align__(128) unsigned char smraw[];
+    constexpr uint32_t BWL = 32 * LW;                    // words per column block
+    constexpr uint32_t NF = BWL / kLaneCoverWords;       // cover bitmaps per block
+    constexpr uint32_t SUBL = kLaneCoverWords / LW;      // lanes per cover bitmap
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
-    const uint32_t w0 = blk * 32, w = w0 + lane;
+    const uint32_t w0 = blk * BWL, w = w0 + lane * LW;
     const bool live = w < a.W;
-    const uint32_t wmask = !live ? 0u
-                                 : (w + 1 < a.W ? 0xFFFFFFFFu
+    const uint32_t nw = live ? min((uint32_t)LW, a.W - w) : 0u;  // words of the lane that hold pairs
+    uint32_t wm[LW];
+#pragma unroll
+    for (int j = 0; j < LW; j++)
+        wm[j] = w + j >= a.W ? 0u
+                             : (w + j + 1 < a.W ? 0xFFFFFFFFu
                                                 : ((a.n_pairs & 31) ? (1u << (a.n_pairs & 31)) - 1u : 0xFFFFFFFFu));
+    LanePlanes P;
+    P.ld4 = (uint32_t)(a.ld * 4);
+    P.V = reinterpret_cast<char *>(a.V + w);
+    P.T = reinterpret_cast<char *>(a.T + w);
+    P.M = reinterpret_cast<char *>(a.M + w);
     uint32_t *bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
     uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
     GateRec *recs = reinterpret_cast<GateRec *>(smraw + a.off_rec);  // [2][kLaneRecs]
@@ -906,11 +1040,11 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
 
     if (MODE != FWD_SIM)
         for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) bm[q] = 0;
-    uint32_t *fine = MODE == FWD_FUSED && a.nzb_fine ? a.nzb_fine + (size_t)blk * 4 * a.bm_words : nullptr;
+    uint32_t *fine = MODE == FWD_FUSED && a.nzb_fine ? a.nzb_fine + (size_t)blk * NF * a.bm_words : nullptr;
     if (fine)
-        for (uint32_t q = threadIdx.x; q < 4 * a.bm_words; q += blockDim.x) fine[q] = 0;
+        for (uint32_t q = threadIdx.x; q < NF * a.bm_words; q += blockDim.x) fine[q] = 0;
     if (MODE == FWD_FUSED) {  // the batch's cover state (the cover kernels run after this one)
-        if (a.active && threadIdx.x < 32 && w0 + threadIdx.x <= a.W) a.active[w0 + threadIdx.x] = 0;
+        if (a.active && threadIdx.x < BWL && w0 + threadIdx.x <= a.W) a.active[w0 + threadIdx.x] = 0;
         if (a.active && blk == 0 && threadIdx.x == 0) a.active[a.W] = 0;
         if (a.acc && blk == 0 && threadIdx.x == 0) {
             a.acc->batch_lo = 0;
@@ -963,16 +1097,16 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
         }
         const GateRec *rb = recs + (size_t)(i & 1) * kLaneRecs;
         for (uint32_t g = ga + warp; g < gb; g += U * NW) {
-            LaneIn x[U];
+            LaneIn<LW> x[U];
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const uint32_t gu = g + u * NW;
-                if (gu < gb) lane_load<SEM, MODE>(a, bm, rb[gu - ga], gu, w, live, x[u]);
+                if (gu < gb) lane_load<SEM, MODE, LW>(a, P, bm, rb + (gu - ga), gu, w, live, x[u]);
             }
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const uint32_t gu = g + u * NW;
-                if (gu < gb) any |= lane_gate<SEM, MODE>(a, bm, rb[gu - ga], gu, w, live, wmask, x[u]);
+                if (gu < gb) any |= lane_gate<SEM, MODE, LW>(a, P, bm, rb + (gu - ga), gu, live, nw, wm, x[u]);
             }
         }
     }
@@ -997,36 +1131,55 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
                     const uint32_t g = q * 32 + (__ffs(bits) - 1);
                     bits &= bits - 1;
                     const GateRec r = load_rec(a.c.rec + g);
-                    const size_t o = (size_t)g * a.ld + w;
-                    const uint32_t mk = live ? a.M[o] : 0u;
-                    uint32_t keep = rec_po(r) ? 0xFFFFFFFFu : 0u;
+                    uint32_t *mrow = lrow(P.M, g, P.ld4);
+                    uint32_t mk[LW], keep[LW], nm[LW];
+                    lzero<LW>(mk);
+                    if (live) lload<LW>(mrow, mk);
+#pragma unroll
+                    for (int j = 0; j < LW; j++) {
+                        mk[j] &= wm[j];  // words past the last pair hold no mark
+                        keep[j] = rec_po(r) ? 0xFFFFFFFFu : 0u;
+                    }
                     if (!rec_po(r)) {
                         const uint32_t nfo = r.w[1], base = r.w[2] + rec_nfi(r);
                         for (uint32_t k = 0; k < nfo; k += 4) {  // four fan-out rows in flight
-                            uint32_t fo[4], m[4];
+                            uint32_t fo[4], m[4][LW];
 #pragma unroll
                             for (int u = 0; u < 4; u++) fo[u] = k + u < nfo ? __ldg(a.c.edges + base + k + u) : kEmpty;
 #pragma unroll
-                            for (int u = 0; u < 4; u++)
-                                m[u] = fo[u] != kEmpty && live && bit_test(bm, fo[u]) ? a.M[(size_t)fo[u] * a.ld + w]
-                                                                                       : 0u;
-                            keep |= m[0] | m[1] | m[2] | m[3];
+                            for (int u = 0; u < 4; u++) {
+                                lzero<LW>(m[u]);
+                                if (fo[u] != kEmpty && live && bit_test(bm, fo[u])) lload<LW>(lrow(P.M, fo[u], P.ld4), m[u]);
+                            }
+#pragma unroll
+                            for (int j = 0; j < LW; j++) keep[j] |= m[0][j] | m[1][j] | m[2][j] | m[3][j];
                         }
                     }
-                    const uint32_t nm = mk & keep;
-                    if (live && nm != mk) a.M[o] = nm;
-                    const uint32_t nzl = __ballot_sync(0xFFFFFFFFu, nm != 0);  // words (lanes) still marked
+                    bool changed = false;
+#pragma unroll
+                    for (int j = 0; j < LW; j++) {
+                        nm[j] = mk[j] & keep[j];
+                        changed |= nm[j] != mk[j];
+                    }
+                    if (live && changed) lstore<LW>(mrow, nm, nw);
+                    const uint32_t nzl = __ballot_sync(0xFFFFFFFFu, lany<LW>(nm));  // lanes still marked
                     const bool nz = nzl != 0;
                     if (!nz) {
                         if (lane == 0) atomicAnd(bm + (g >> 5), ~(1u << (g & 31)));
-                    } else if (fine && lane < 4 && ((nzl >> (8 * lane)) & 0xFFu)) {
-                        atomicOr(fine + (size_t)lane * a.bm_words + (g >> 5), 1u << (g & 31));  // quarter `lane`
+                    } else if (fine && lane < NF && ((nzl >> (SUBL * lane)) & ((1u << SUBL) - 1u))) {
+                        atomicOr(fine + (size_t)lane * a.bm_words + (g >> 5), 1u << (g & 31));  // bitmap `lane`
                     }
                     if (nz && MODE == FWD_FUSED && a.first_x) {  // merge: first falling / rising pair
-                        const uint32_t v = live ? a.V[o] : 0u;
-                        const uint32_t x = nm & ~v, y = nm & v;
-                        uint32_t cx = x ? w * 32 + (__ffs(x) - 1) : kEmpty;
-                        uint32_t cy = y ? w * 32 + (__ffs(y) - 1) : kEmpty;
+                        uint32_t v[LW];
+                        lzero<LW>(v);
+                        if (live) lload<LW>(lrow(P.V, g, P.ld4), v);
+                        uint32_t cx = kEmpty, cy = kEmpty;
+#pragma unroll
+                        for (int j = LW - 1; j >= 0; j--) {  // the lowest word last
+                            const uint32_t x = nm[j] & ~v[j], y = nm[j] & v[j];
+                            if (x) cx = (w + j) * 32 + (__ffs(x) - 1);
+                            if (y) cy = (w + j) * 32 + (__ffs(y) - 1);
+                        }
                         cx = __reduce_min_sync(0xFFFFFFFFu, cx);
                         cy = __reduce_min_sync(0xFFFFFFFFu, cy);
                         if (lane == 0) {
@@ -1043,13 +1196,23 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
         if (a.bm_shared && gbm)
             for (uint32_t q = threadIdx.x; q < a.bm_words; q += blockDim.x) gbm[q] = bm[q];
         if (threadIdx.x == 0) a.blk_maxlvl[blk] = maxlvl;
-        if (fine && threadIdx.x < 4) a.maxlvl_fine[blk * 4 + threadIdx.x] = maxlvl;
+        if (fine && threadIdx.x < NF) a.maxlvl_fine[blk * NF + threadIdx.x] = maxlvl;
     }
 }
 
-template <int SEM, int MODE>
-__global__ void __launch_bounds__(kLaneThreads, 1) k_forward_lanes(const FwdArgs a) {
-    forward_lanes_cta<SEM, MODE, (SEM >= 2 || MODE == FWD_MARK) ? 4 : 8>(a, blockIdx.x);
+// Gates per warp in flight, by tile and semantics (the FIXED modes and the
+// stage call pdf_mark carry more rows per gate).  More warps beat more gates
+// per warp: on a 1M-gate circuit at 64 words, 1,024 threads with one gate
+// each took 36 ms against 46 ms for 512 threads with three or four.
+template <int SEM, int MODE, int LW>
+struct LaneU {
+    static constexpr bool heavy = SEM >= 2 || MODE == FWD_MARK;
+    static constexpr int value = LW == 1 ? (heavy ? 2 : 2) : LW == 2 ? (heavy ? 1 : 1) : (heavy ? 1 : 1);
+};
+
+template <int SEM, int MODE, int LW>
+__global__ void __launch_bounds__(lane_threads(32 * LW), 1) k_forward_lanes(const FwdArgs a) {
+    forward_lanes_cta<SEM, MODE, LaneU<SEM, MODE, LW>::value, LW>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1365,25 +1528,38 @@ __device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p,
         s_flags = 0;
     }
     __syncthreads();
-    // ---- A, B: the pair's nets, in gate order
-    for (uint32_t q0 = 0; q0 < nwords; q0 += kCoverCand / 32) {
-        const uint32_t q = q0 + threadIdx.x;
-        uint32_t bits = 0;
-        if (threadIdx.x < kCoverCand / 32 && q < nwords) {
-            bits = nzb[q];
-            if (q == nwords - 1 && (gend & 31)) bits &= (1u << (gend & 31)) - 1u;
-        }
-        uint32_t nc;
-        uint32_t pos = block_scan_excl(__popc(bits), s_warp, &nc);
-        while (bits) {
-            cand[pos++] = q * 32 + (__ffs(bits) - 1);
-            bits &= bits - 1;
+    // ---- A: every thread counts the candidates (nets with a surviving mark in
+    // the block: bitmap bits) of its own run of bitmap words; one scan orders
+    // them
+    const uint32_t per_w = (nwords + blockDim.x - 1) / blockDim.x;
+    const uint32_t q_lo = min(nwords, threadIdx.x * per_w), q_hi = min(nwords, q_lo + per_w);
+    auto word = [&](uint32_t q) {
+        uint32_t b = nzb[q];
+        if (q == nwords - 1 && (gend & 31)) b &= (1u << (gend & 31)) - 1u;
+        return b;
+    };
+    uint32_t mine = 0;
+    for (uint32_t q = q_lo; q < q_hi; q++) mine += __popc(word(q));
+    uint32_t total_c;
+    const uint32_t first_c = block_scan_excl(mine, s_warp, &total_c);
+    // ---- B: in windows of kCoverCand candidates, those the pair marks (one
+    // mark word each) join the pair's list, in gate order
+    for (uint32_t c_lo = 0; c_lo < total_c; c_lo += kCoverCand) {
+        const uint32_t c_hi = min(total_c, c_lo + kCoverCand);
+        if (first_c < c_hi && first_c + mine > c_lo) {  // this thread's candidates in the window
+            uint32_t idx = first_c;
+            for (uint32_t q = q_lo; q < q_hi && idx < c_hi; q++) {
+                uint32_t b = word(q);
+                for (; b && idx < c_hi; idx++, b &= b - 1)
+                    if (idx >= c_lo) cand[idx - c_lo] = q * 32 + (__ffs(b) - 1);
+            }
         }
         __syncthreads();
+        const uint32_t nc = c_hi - c_lo;
         // each thread tests a contiguous run of candidates (order kept)
         const uint32_t per = (nc + blockDim.x - 1) / blockDim.x;
         const uint32_t c0 = min(nc, threadIdx.x * per), c1 = min(nc, c0 + per);
-        uint32_t keep = 0, nk = 0;  // per <= kCoverCand / 256 = 16: one bit each
+        uint32_t keep = 0, nk = 0;  // per <= kCoverCand / kCoverThreads = 16: one bit each
         uint32_t mw[16];
 #pragma unroll
         for (int k = 0; k < 16; k++) mw[k] = c0 + k < c1 ? a.M[(size_t)cand[c0 + k] * a.ld + wp] : 0u;
@@ -1450,12 +1626,32 @@ __device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p,
         }
     }
     __syncthreads();
-    // ---- the recurrence, levels descending
+    // ---- the recurrence, levels descending.  The list is in gate order, so
+    // each level's nets are one run of it: bnd[l] = the first listed net of
+    // level >= l (binary searches, in parallel), and a level without nets
+    // costs neither a pass over the list nor a barrier.
     pdf_u128 total = 0;
     bool ovf = false;
     const uint32_t lv_hi = n ? (info[n - 1] & kNetLevel) : 0;
+    uint32_t *bnd = cand;  // [lv_hi + 2] (the candidates are no longer needed)
+    const bool runs = lv_hi + 2 <= kCoverCand;
+    if (runs) {
+        for (uint32_t l = threadIdx.x; l <= lv_hi + 1; l += blockDim.x) {
+            const uint32_t g0 = lo_tab[l];
+            uint32_t lo = 0, hi = n;  // first index with lid >= g0
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (lid[mid] < g0) lo = mid + 1;
+                else hi = mid;
+            }
+            bnd[l] = lo;
+        }
+        __syncthreads();
+    }
     for (int lv = (int)lv_hi; lv >= 0 && n; lv--) {
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t i0 = runs ? bnd[lv] : 0, i1 = runs ? bnd[lv + 1] : n;
+        if (i0 == i1) continue;  // the same in every thread
+        for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
             const uint32_t inf = info[i];
             if ((inf & kNetLevel) != (uint32_t)lv) continue;
             pdf_u128 H = (inf & kNetPo) ? 1 : 0, C = 0;
@@ -1672,9 +1868,9 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
     forward_cta<BW, SEM, FWD_FUSED>(s_a, s_blk);
 }
 
-// The same for the circuits of a batch that take the lane kernel.
-template <int SEM>
-__global__ void __launch_bounds__(kLaneThreads, 1)
+// The same for the circuits of a batch that take a lane tile.
+template <int SEM, int LW>
+__global__ void __launch_bounds__(lane_threads(32 * LW), 1)
     k_batch_forward_lanes(const FwdArgs *args, const uint32_t *bpref, uint32_t n, BatchCtl *ctl, uint32_t blk0) {
     __shared__ FwdArgs s_a;
     __shared__ uint32_t s_blk;
@@ -1692,7 +1888,7 @@ __global__ void __launch_bounds__(kLaneThreads, 1)
         }
     }
     __syncthreads();
-    forward_lanes_cta<SEM, FWD_FUSED, SEM >= 2 ? 4 : 6>(s_a, s_blk);  // arguments in shared memory take registers
+    forward_lanes_cta<SEM, FWD_FUSED, LaneU<SEM, FWD_FUSED, LW>::value, LW>(s_a, s_blk);
 }
 
 __global__ void k_batch_active(const CoverArgs *args, const uint32_t *gpref, uint32_t n, uint2 *items,
@@ -1848,32 +2044,33 @@ cudaError_t launch_fwd_t(const FwdArgs &a, uint32_t threads, size_t smem, cudaSt
     return cudaGetLastError();
 }
 
-template <int SEM, int MODE>
+template <int SEM, int MODE, int LW>
 cudaError_t launch_lanes_t(const FwdArgs &a, uint32_t threads, size_t smem, cudaStream_t st) {
-    auto kern = k_forward_lanes<SEM, MODE>;
+    auto kern = k_forward_lanes<SEM, MODE, LW>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const uint32_t blocks = (a.W + kLaneWords - 1) / kLaneWords;
-    if (blocks == 0 || threads % 32 || threads > kLaneThreads) return cudaErrorInvalidValue;
+    const uint32_t blocks = (a.W + 32 * LW - 1) / (32 * LW);
+    if (blocks == 0 || threads % 32 || threads > lane_threads(32 * LW)) return cudaErrorInvalidValue;
     kern<<<blocks, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-template <int SEM>
+template <int SEM, int LW>
 cudaError_t launch_lanes_sem(const FwdArgs &a, int mode, uint32_t threads, size_t smem, cudaStream_t st) {
     switch (mode) {
-        case FWD_FUSED: return launch_lanes_t<SEM, FWD_FUSED>(a, threads, smem, st);
-        case FWD_SIM: return launch_lanes_t<SEM, FWD_SIM>(a, threads, smem, st);
-        default: return launch_lanes_t<SEM, FWD_MARK>(a, threads, smem, st);
+        case FWD_FUSED: return launch_lanes_t<SEM, FWD_FUSED, LW>(a, threads, smem, st);
+        case FWD_SIM: return launch_lanes_t<SEM, FWD_SIM, LW>(a, threads, smem, st);
+        default: return launch_lanes_t<SEM, FWD_MARK, LW>(a, threads, smem, st);
     }
 }
 
+template <int LW>
 cudaError_t launch_lanes(const FwdArgs &a, int mode, int sem, uint32_t threads, size_t smem, cudaStream_t st) {
     switch (sem) {
-        case 0: return launch_lanes_sem<0>(a, mode, threads, smem, st);
-        case 1: return launch_lanes_sem<1>(a, mode, threads, smem, st);
-        case 2: return launch_lanes_sem<2>(a, mode, threads, smem, st);
-        case 3: return launch_lanes_sem<3>(a, mode, threads, smem, st);
+        case 0: return launch_lanes_sem<0, LW>(a, mode, threads, smem, st);
+        case 1: return launch_lanes_sem<1, LW>(a, mode, threads, smem, st);
+        case 2: return launch_lanes_sem<2, LW>(a, mode, threads, smem, st);
+        case 3: return launch_lanes_sem<3, LW>(a, mode, threads, smem, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1922,41 +2119,47 @@ int regs_bw(int sem) {
         default: return -1;
     }
 }
-template <int SEM>
+template <int SEM, int LW>
 int regs_lanes_t() {
     cudaFuncAttributes fa{}, fb{};
-    if (cudaFuncGetAttributes(&fa, k_forward_lanes<SEM, FWD_FUSED>) != cudaSuccess ||
-        cudaFuncGetAttributes(&fb, k_batch_forward_lanes<SEM>) != cudaSuccess) {
+    if (cudaFuncGetAttributes(&fa, k_forward_lanes<SEM, FWD_FUSED, LW>) != cudaSuccess ||
+        cudaFuncGetAttributes(&fb, k_batch_forward_lanes<SEM, LW>) != cudaSuccess) {
         (void)cudaGetLastError();
         return -1;
     }
     return std::max(fa.numRegs, fb.numRegs);
 }
+template <int LW>
+int regs_lanes(int sem) {
+    switch (sem) {
+        case 0: return regs_lanes_t<0, LW>();
+        case 1: return regs_lanes_t<1, LW>();
+        case 2: return regs_lanes_t<2, LW>();
+        case 3: return regs_lanes_t<3, LW>();
+        default: return -1;
+    }
+}
 }  // namespace
 
 int forward_kernel_regs(int bw, int sem) {
-    if (bw == (int)kLaneWords) {
-        switch (sem) {
-            case 0: return regs_lanes_t<0>();
-            case 1: return regs_lanes_t<1>();
-            case 2: return regs_lanes_t<2>();
-            case 3: return regs_lanes_t<3>();
-            default: return -1;
-        }
-    }
     switch (bw) {
         case 1: return regs_bw<1>(sem);
         case 2: return regs_bw<2>(sem);
         case 4: return regs_bw<4>(sem);
         case 8: return regs_bw<8>(sem);
+        case kLaneWords: return regs_lanes<1>(sem);
+        case kLaneWords2: return regs_lanes<2>(sem);
+        case kLaneWords4: return regs_lanes<4>(sem);
         default: return -1;
     }
 }
 
 cudaError_t launch_forward(const FwdArgs &a, int mode, int sem, uint32_t bw, uint32_t threads,
                            size_t smem, cudaStream_t st) {
-    if (bw == kLaneWords) return launch_lanes(a, mode, sem, threads, smem, st);
     switch (bw) {
+        case kLaneWords: return launch_lanes<1>(a, mode, sem, threads, smem, st);
+        case kLaneWords2: return launch_lanes<2>(a, mode, sem, threads, smem, st);
+        case kLaneWords4: return launch_lanes<4>(a, mode, sem, threads, smem, st);
         case 1: return launch_fwd_bw<1>(a, mode, sem, threads, smem, st);
         case 2: return launch_fwd_bw<2>(a, mode, sem, threads, smem, st);
         case 4: return launch_fwd_bw<4>(a, mode, sem, threads, smem, st);
@@ -2003,7 +2206,9 @@ cudaError_t prepare_class_sem(uint32_t bw, size_t smem) {
         case 2: return cudaFuncSetAttribute(k_batch_forward<2, SEM>, attr, (int)smem);
         case 4: return cudaFuncSetAttribute(k_batch_forward<4, SEM>, attr, (int)smem);
         case 8: return cudaFuncSetAttribute(k_batch_forward<8, SEM>, attr, (int)smem);
-        case kLaneWords: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM>, attr, (int)smem);
+        case kLaneWords: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM, 1>, attr, (int)smem);
+        case kLaneWords2: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM, 2>, attr, (int)smem);
+        case kLaneWords4: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM, 4>, attr, (int)smem);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -2015,7 +2220,13 @@ cudaError_t launch_class_sem(const BatchLaunch &b, const BatchClass &c, cudaStre
         case 4: k_batch_forward<4, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0); break;
         case 8: k_batch_forward<8, SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0); break;
         case kLaneWords:
-            k_batch_forward_lanes<SEM><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
+            k_batch_forward_lanes<SEM, 1><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
+            break;
+        case kLaneWords2:
+            k_batch_forward_lanes<SEM, 2><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
+            break;
+        case kLaneWords4:
+            k_batch_forward_lanes<SEM, 4><<<c.blocks, c.threads, c.smem, s>>>(b.fargs, b.bpref, b.n, b.ctl, c.blk0);
             break;
         default: return cudaErrorInvalidValue;
     }

@@ -134,16 +134,31 @@ struct SegMergeArgs {
     uint32_t *first_x, *first_y;  // [S]
 };
 
-// Tile width of the lane forward kernel (k_forward_lanes): one warp lane per
-// word, so a column block is 32 words (1,024 pairs); a CTA of 512 threads
-// (16 warps, up to 128 registers each: room for 8 gates in flight per warp).
+// Tile widths of the lane forward kernel (k_forward_lanes): a warp per gate
+// and LW consecutive words per lane (one 4 LW-byte access per lane and row),
+// so a column block is 32 LW words: 32, 64 or 128 words (1,024, 2,048 or
+// 4,096 pairs).  A gate's record decode, row addressing, votes and branches
+// are paid once per block, so wider lanes spend fewer instructions per pair
+// (9.4e9 warp instructions for a pass at 32 words, 4.1e9 at 64).  CTAs of
+// 1,024 threads (32 warps) at up to 64 registers for LW = 1, 2; of 512
+// threads at up to 128 for LW = 4, whose rows of four words per fan-in
+// spill at 64.
 constexpr uint32_t kLaneWords = 32;
-constexpr uint32_t kLaneThreads = 512;
-// Words per cover bitmap of a lane circuit (a quarter of its column block).
+constexpr uint32_t kLaneWords2 = 64;
+constexpr uint32_t kLaneWords4 = 128;
+constexpr uint32_t kLaneThreads1 = 1024;
+constexpr uint32_t kLaneThreads2 = 1024;
+constexpr uint32_t kLaneThreads4 = 512;
+constexpr bool lane_tile(uint32_t bw) { return bw == kLaneWords || bw == kLaneWords2 || bw == kLaneWords4; }
+constexpr uint32_t lane_threads(uint32_t bw) {
+    return bw == kLaneWords4 ? kLaneThreads4 : bw == kLaneWords2 ? kLaneThreads2 : kLaneThreads1;
+}
+// Words per cover bitmap of a lane circuit (a quarter of a 32-word column
+// block, an eighth of a 64-word one, ...).
 constexpr uint32_t kLaneCoverWords = 8;
-// Forward launches of a batch at most: tile widths 1, 2, 4, 8 at 1, 2, 4
-// CTAs per SM, and the lane kernel.
-constexpr uint32_t kMaxBatchClasses = 8;
+// Forward launches of a batch at most: (tile width, CTAs per SM) classes of
+// the thread-per-gate kernel and the two lane tiles.
+constexpr uint32_t kMaxBatchClasses = 10;
 
 // Batched grading (k_batch_forward, k_batch_active, k_batch_cover).
 struct BatchCtl {

@@ -40,7 +40,7 @@ def _jobs(mode, tile=4, seed=0):
     return jobs, want
 
 
-@pytest.mark.parametrize("tile", [4, 32, [32, 4, 8, 2]], ids=["walk4", "lanes", "mixed"])
+@pytest.mark.parametrize("tile", [4, 32, 64, 128, [32, 4, 64, 8, 128, 2]], ids=["walk4", "lanes", "lanes64", "lanes128", "mixed"])
 @pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_batch_equals_each_job_alone(mode, tile):
     """Every tile width in one batch (mixed: one forward launch per class of
@@ -156,7 +156,7 @@ def test_batch_profile_times_the_pass():
 def test_autotune_picks_a_tile():
     nls = [circuits.random_small(800 + k, n_gates=2000 * (k + 1), n_pi=100, n_po=300, depth=20) for k in range(4)]
     opts, ms = P.batch_autotune(nls, [1024, 3000, 5000, 700], mark_mode=1, reps=2)
-    assert opts.tile_words in (2, 4, 8, 32) and opts.threads in (0, 256) and ms > 0
+    assert opts.tile_words in (2, 4, 8, 32, 64, 128) and opts.threads in (0, 256) and ms > 0
     # the picked shape grades the batch like every circuit alone
     counts = [1024, 3000, 5000, 700]
     rng = np.random.default_rng(5)

@@ -32,7 +32,7 @@ def big():
     return nl, codes, n, O.grade(nl, codes, n, mark_mode=3)
 
 
-@pytest.mark.parametrize("tile", [0, 32])
+@pytest.mark.parametrize("tile", [0, 32, 64, 128])
 def test_every_pair_spills(big, tile):
     nl, codes, n, want = big
     per_pair = O.grade(nl, codes, n, mark_mode=3, want_planes=True).mark.sum(axis=0)
@@ -51,9 +51,9 @@ def test_spill_in_a_batch(big):
     members = [(nl0, codes0, n0, 32)]
     for k in range(3):
         nl = circuits.random_small(50 + k, n_gates=2000, n_pi=60, n_po=300, depth=12)
-        members.append((nl, helpers.rand_codes(np.random.default_rng(k), nl.n_pi, 900), 900, 4))
+        members.append((nl, helpers.rand_codes(np.random.default_rng(k), nl.n_pi, 900), 900, (4, 64, 128)[k]))
     for nl, codes, n, tw in members:
-        ld = (P.words(n) + 31) // 32 * 32
+        ld = (P.words(n) + 127) // 128 * 128
         v, t = P.planes_from_codes(codes, ld)
         c = P.Circuit(nl, mark_mode=3, tile_words=tw)
         s = P.State(c)
@@ -75,7 +75,7 @@ def test_reference_tables_spill_on_a_wide_hub(mode):
     codes = helpers.rand_codes(np.random.default_rng(8), nl.n_pi, n)
     want = O.grade(nl, codes, n, mark_mode=mode, want_planes=True)
     assert want.mark.sum(axis=0).max() > 3072
-    for tile in (0, 32):
+    for tile in (0, 32, 64):
         fx, fy, tot = _grade(nl, codes, n, mode, tile)
         np.testing.assert_array_equal(fx, want.first_x)
         np.testing.assert_array_equal(fy, want.first_y)
@@ -115,7 +115,7 @@ def test_fixed_robust_on_c2():
     v, t = P.gen_pairs(P.pair_seed(w["gen"].seed), nl.n_pi, n)
     codes = P.codes_from_planes(v, t, n)
     want = O.grade(nl, codes, n, mark_mode=2)
-    for tile in (0, 32):
+    for tile in (0, 32, 64):
         fx, fy, tot = _grade(nl, codes, n, 2, tile)
         np.testing.assert_array_equal(fx, want.first_x)
         assert tot.value == want.total

@@ -24,7 +24,7 @@ def c3():
     return nl, v, t, codes, n, O.grade(nl, codes, n, mark_mode=1, chunk=1024)
 
 
-@pytest.mark.parametrize("tile", [0, 8, 32])
+@pytest.mark.parametrize("tile", [0, 8, 32, 64, 128])
 def test_c3_prefix_in_two_batches(c3, tile):
     nl, v, t, codes, n, want = c3
     c = P.Circuit(nl, mark_mode=1, max_pairs=n, tile_words=tile)
@@ -44,7 +44,7 @@ def test_c3_prefix_in_two_batches(c3, tile):
     assert one.value == sum(totals)
 
 
-@pytest.mark.parametrize("tile", [0, 32])
+@pytest.mark.parametrize("tile", [0, 32, 64, 128])
 def test_c4_batch_against_the_oracle(tile):
     """The 256 circuits of the mixed-size batch in one batched pass, each on
     its first min(n, 1024) pairs; every 8th circuit (32 of them, all sizes)
@@ -55,7 +55,7 @@ def test_c4_batch_against_the_oracle(tile):
     for g, n in spec:
         nl = P.gen_netlist(g)
         k = min(n, 1024)
-        v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, k, 32)
+        v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, k, 128)
         c = P.Circuit(nl, mark_mode=1, max_pairs=k, tile_words=tile)
         jobs.append((c, P.State(c), torch.from_numpy(v.view(np.int32)).cuda(),
                      torch.from_numpy(t.view(np.int32)).cuda(), k, 0))
