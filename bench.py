@@ -181,6 +181,9 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+LANE_TILES = (32, 64, 128)  # tile widths of the lane kernel (a warp per gate)
+
+
 def profile_summary(name: str):
     """A committed summary of an ncu capture (profiles/<name>.json), or None."""
     p = os.path.join(ROOT, "profiles", f"{name}.json")
@@ -556,8 +559,8 @@ def run_ours(args):
     value = units / (ms / 1e3)
     fwd_ms = prof_ms[0] / max(1, prof_calls)
     tile = c.info().tile_words
-    kname = "k_forward_lanes" if tile == 32 else "k_forward"
-    prof = profile_summary(f"{kname}_{args.workload}") if not args.planes and args.segs == 1 and \
+    kname = "k_forward_lanes" if tile in LANE_TILES else "k_forward"
+    prof = profile_summary(f"{kname}_{args.workload}_tile{tile}") if not args.planes and args.segs == 1 and \
         args.mark_mode == "robust" and not args.pairs else None
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     line = {
@@ -785,7 +788,7 @@ def run_batched(args):
                           "circuit's default tile and at the batch's tile; the faster of the two"},
         "batched_vs_plain": plain_best / ms,
         "roofline": dict(roofline(sum(alg_bytes(nl, n) for nl, n in zip(nls, counts)), kernel_ms,
-                                  f"forward span of the pass (k_batch_forward{'_lanes' if tw == 32 else ''}, "
+                                  f"forward span of the pass (k_batch_forward{'_lanes' if tw in LANE_TILES else ''}, "
                                   f"every class)", prof, units, sm_count, clocks.get("sm_mhz")),
                          cover_ms=sum(cov_ms) / len(cov_ms)),
         "e2e": {"value": units / (stream_ms / 1e3), "unit": "gate-evals/s", "h2d_bytes_per_step": int(h2d),
@@ -821,13 +824,17 @@ def run_served(args):
     rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     n_jobs, per_job, batch, rate = args.jobs, 65536, 4096, 200.0
-    spec = P.batch_workload()[:n_jobs]
+    # past the 256 circuits of the distribution, the list again with other pairs
+    base = P.batch_workload()
     rng = np.random.default_rng(0x5EED0005)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_jobs))
-    jobs = []
-    for g, _ in spec:
-        nl = P.gen_netlist(g)
-        v, t = P.gen_pairs(P.pair_seed(g.seed), nl.n_pi, per_job)
+    jobs, nls = [], {}
+    for k in range(n_jobs):
+        g = base[k % len(base)][0]
+        if g.seed not in nls:
+            nls[g.seed] = P.gen_netlist(g)
+        nl = nls[g.seed]
+        v, t = P.gen_pairs(P.pair_seed(g.seed) + k // len(base), nl.n_pi, per_job)
         jobs.append((nl, v, t))
     units = sum(nl.n_gates * per_job for nl, _, _ in jobs)
     srv = P.Server(mark_mode=P.MARK_ROBUST, batch_pairs=batch, hbm_budget=int(args.hbm_gb * (1 << 30)),
@@ -868,16 +875,18 @@ def run_served(args):
         "metric": "gate-evals/s", "value": units / wall, "unit": "gate-evals/s", "n_gpus": 1, "steps": int(st.steps),
         "warmup": 0, "ms_per_step": 1e3 * st.busy_s / max(1, st.steps), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
-        "config": {"workload": f"c5: {n_jobs} jobs from the c4 size distribution, Poisson arrivals at "
+        "config": {"workload": f"c5: {n_jobs} jobs from the c4 size distribution (its 256 circuits in turn), "
+                               f"Poisson arrivals at "
                                f"{rate:.0f} jobs/s, {batch}-pair appends up to {per_job} pairs per job",
                    "mark_mode": "robust (LUT_R)", "hbm_budget_gib": args.hbm_gb,
                    "workers": args.workers or "library default", "tile_words": args.tile_words or 4,
                    "outputs": "path count and first-detect ids per job"},
         "latency_ms": {"p50": st.lat_p50_ms, "p99": st.lat_p99_ms, "max": st.lat_max_ms,
                        "per": "job batch, from ready (submission or previous batch) to result"},
-        "wall_s": wall, "busy_s": st.busy_s, "batches": int(st.batches),
+        "wall_s": wall, "busy_s": st.busy_s, "gpu_s": st.gpu_s, "batches": int(st.batches),
         # the arrival stream caps throughput: all the work over the span of the arrivals
         "offered_load": units / float(arrivals[-1]),
+        "served_fraction_of_offered": float(arrivals[-1]) / wall,
         "e2e": {"value": units / wall, "unit": "gate-evals/s",
                 "h2d_bytes_per_step": int(sum(2 * nl.n_pi * (per_job // 32) * 4 for nl, _, _ in jobs) / max(1, st.steps)),
                 "d2h_bytes_per_step": 64},

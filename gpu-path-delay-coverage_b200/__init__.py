@@ -97,7 +97,8 @@ class ServerStats_t(C.Structure):
     _fields_ = [("jobs_done", C.c_uint64), ("jobs_active", C.c_uint64), ("jobs_queued", C.c_uint64),
                 ("batches", C.c_uint64), ("steps", C.c_uint64), ("gate_evals", C.c_uint64),
                 ("busy_s", C.c_double), ("lat_p50_ms", C.c_double), ("lat_p99_ms", C.c_double),
-                ("lat_max_ms", C.c_double), ("bytes_in_use", C.c_uint64), ("launches", C.c_uint64)]
+                ("lat_max_ms", C.c_double), ("bytes_in_use", C.c_uint64), ("launches", C.c_uint64),
+                ("gpu_s", C.c_double)]
 
 
 class CircuitInfo_t(C.Structure):
@@ -622,12 +623,12 @@ class Batch:
     while the batch exists.  append: each run advances every job's pair_base
     by its pair count."""
 
-    def __init__(self, jobs, append: bool = False):
+    def __init__(self, jobs, append: bool = False, graph: bool = True):
         self.h = None
         self.jobs = list(jobs)  # keeps circuits, states and pair tensors alive
         h = C.c_void_p()
-        check(lib().pdf_batch_create(self._arr(self.jobs), len(self.jobs), BATCH_APPEND if append else 0,
-                                     C.byref(h)), "pdf_batch_create")
+        flags = (BATCH_APPEND if append else 0) | (0 if graph else BATCH_NO_GRAPH)
+        check(lib().pdf_batch_create(self._arr(self.jobs), len(self.jobs), flags, C.byref(h)), "pdf_batch_create")
         self.h = h
 
     @staticmethod

@@ -1763,6 +1763,8 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         L.join[k] = b->join[k];
     }
     L.fork = b->fork;
+    b->use_graph = !(flags & PDF_BATCH_NO_GRAPH);
+    // inside a captured graph the events are external nodes; run directly, plain records
     for (uint32_t k = 0; k < 3; k++) L.prof[k] = b->profiling ? b->prof[k] : nullptr;
     L.prof_external = b->use_graph ? 1u : 0u;
     L.n = n_jobs;
@@ -1771,7 +1773,6 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         L.cls[k].blocks = (k + 1 < L.n_class ? L.cls[k + 1].blk0 : L.total_blocks) - L.cls[k].blk0;
     L.total_gates = gp[n_jobs];
     L.append = (flags & PDF_BATCH_APPEND) ? 1u : 0u;
-    b->use_graph = !(flags & PDF_BATCH_NO_GRAPH);
     // one device block: control word, circuit arguments, prefixes, then items
     auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t o_f = a256(sizeof(BatchCtl)), o_c = o_f + a256(sizeof(FwdArgs) * n_jobs),

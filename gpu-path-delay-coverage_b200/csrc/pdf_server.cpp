@@ -265,7 +265,9 @@ extern "C" pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server 
     if (!o.tile_words) o.tile_words = 4;
     if (!o.batch_pairs) o.batch_pairs = 4096;
     if (!o.max_jobs) o.max_jobs = 1024;
-    if (o.batch_pairs % 32 || (o.tile_words != 1 && o.tile_words != 2 && o.tile_words != 4 && o.tile_words != 8) ||
+    const bool tile_ok = o.tile_words == 1 || o.tile_words == 2 || o.tile_words == 4 || o.tile_words == 8 ||
+                         o.tile_words == 32 || o.tile_words == 64 || o.tile_words == 128;
+    if (o.batch_pairs % 32 || !tile_ok ||
         o.mark_mode < PDF_MARK_DEFAULT || o.mark_mode > PDF_MARK_FIXED_NONROBUST)
         return PDF_EINVAL;
     if (cudaSetDevice(o.device) != cudaSuccess) return PDF_ENODEV;
@@ -423,13 +425,18 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
                 jobs.push_back(pdf_batch_job{j->c, j->s, p, j->done});
             }
             const uint32_t fl = PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH;
+            const bool fresh = !srv->batch;
             st = srv->batch ? pdf_batch_rebind(srv->batch, jobs.data(), (uint32_t)jobs.size(), fl)
                             : pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), fl, &srv->batch);
             if (st != PDF_OK) return st;
+            // events around each pass's forward launches and cover: its device time
+            if (fresh && (st = pdf_batch_profile(srv->batch, 1)) != PDF_OK) return st;
             srv->dirty = false;
             srv->graded_n = grading.size();
         }
         if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
+        double ms[2] = {0.0, 0.0};
+        if (pdf_batch_profile_read(srv->batch, ms) == PDF_OK) srv->st.gpu_s += (ms[0] + ms[1]) / 1e3;
         pdf_batch_info bi{};
         if (pdf_batch_query(srv->batch, &bi) == PDF_OK) srv->st.launches += bi.launches;
         // the pass has graded (and, on the device, appended) every job's

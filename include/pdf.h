@@ -166,19 +166,22 @@ typedef struct pdf_circuit_opts {
     int mark_mode;       /* PDF_MARK_* */
     uint32_t max_pairs;  /* largest batch this circuit will grade (sizes scratch); 0 = 65536 */
     uint32_t tile_words; /* words (32 pairs) per CTA column block: 1, 2, 4, 8 (a thread per gate)
-                            or 32 (the lane kernel: a warp per gate, for wide levels);
-                            0 = chosen: 32 when max_pairs gives >= 1 such block per SM and the
-                            levels average >= 1,024 gates, else 8 when max_pairs gives >= 2
-                            8-word CTAs per SM, else 4 */
-    uint32_t threads;    /* 0 = piece capacity + 64; else threads per CTA: 64..1024, a multiple
-                            of 32; from 128 up, pieces then hold at most threads - 64 gates */
+                            or 32, 64, 128 (the lane kernel: a warp per gate, 1, 2 or 4 words
+                            per lane, for wide levels); 0 = chosen: a lane tile when max_pairs
+                            gives >= 1 1,024-pair block per SM and the levels average >= 1,024
+                            gates (the one with the least modelled time), else 8 when max_pairs
+                            gives >= 2 8-word CTAs per SM, else 4 */
+    uint32_t threads;    /* 0 = piece capacity + 64 (lane tiles: 1,024, or 512 at 128 words);
+                            else threads per CTA: 64..1024, a multiple of 32, capped at the
+                            lane tile's default; from 128 up, pieces of the thread-per-gate
+                            tiles then hold at most threads - 64 gates */
     uint32_t seg_len;    /* path segments of this many nets, 0 or 1 = single nets; up to 8
                             (fcount --segs N, main.cu:76-81,185-223) */
     uint32_t wait_polls; /* bound on each device-side wait of the forward kernels for its staged
                             copy: 0 = 2^24 blocking polls (the default); n > 0 = n non-blocking
                             polls, after which the call reports PDF_ETIMEOUT (small values
-                            exist to test that path).  The lane kernel (tile_words 32) waits
-                            for nothing. */
+                            exist to test that path).  The lane kernel (tile_words 32, 64,
+                            128) waits for nothing. */
     uint32_t reserved;
 } pdf_circuit_opts;
 
@@ -472,7 +475,7 @@ typedef struct pdf_server pdf_server;
 typedef struct pdf_server_opts {
     int device;
     int mark_mode;          /* PDF_MARK_* for every job */
-    uint32_t tile_words;    /* 0 = 4 */
+    uint32_t tile_words;    /* as pdf_circuit_opts.tile_words, for every job; 0 = 4 */
     uint32_t batch_pairs;   /* pairs per batch, a multiple of 32 (0 = 4096) */
     uint32_t max_jobs;      /* active jobs at most (0 = 1024) */
     uint32_t workers;       /* host threads preparing admitted jobs (0 = 4) */
@@ -487,6 +490,7 @@ typedef struct pdf_server_stats {
     double lat_p50_ms, lat_p99_ms, lat_max_ms; /* per-batch latency */
     uint64_t bytes_in_use;
     uint64_t launches;      /* kernel launches of the batched passes */
+    double gpu_s;           /* device time of the batched passes (forward launches and cover) */
 } pdf_server_stats;
 pdf_status pdf_server_create(const pdf_server_opts *opts, pdf_server **out);
 void pdf_server_destroy(pdf_server *srv);

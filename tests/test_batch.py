@@ -138,11 +138,13 @@ def test_batch_append_mixed_tiles():
         assert tot.value == w.total and tot.pairs == 2 * n
 
 
-def test_batch_profile_times_the_pass():
+@pytest.mark.parametrize("graph", [True, False], ids=["graph", "direct"])
+def test_batch_profile_times_the_pass(graph):
     """pdf_batch_profile: forward span and cover of the latest pass, from
-    events inside the replayed graph; results unchanged."""
+    events inside the replayed graph or around the direct launches; results
+    unchanged."""
     jobs, want = _jobs(1, [32, 4], seed=5)
-    b = P.Batch(jobs)
+    b = P.Batch(jobs, graph=graph)
     b.profile(True)
     b.run()
     fwd, cov = b.profile_read()

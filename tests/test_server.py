@@ -33,8 +33,8 @@ def _jobs():
     return out
 
 
-def _serve(jobs, budget=0, mode=1, arrive_every=2):
-    srv = P.Server(mark_mode=mode, batch_pairs=BATCH, hbm_budget=budget)
+def _serve(jobs, budget=0, mode=1, arrive_every=2, tile=4):
+    srv = P.Server(mark_mode=mode, batch_pairs=BATCH, hbm_budget=budget, tile_words=tile)
     ids, pending = [], list(jobs)
     steps = 0
     while pending or srv.stats().jobs_done < len(jobs):
@@ -56,6 +56,7 @@ def test_served_results_equal_offline_grading(mode):
     assert st.jobs_done == len(jobs) and st.jobs_active == 0 and st.jobs_queued == 0
     assert st.gate_evals == sum(nl.n_gates * n for nl, _, _, _, n in jobs)
     assert 0 < st.lat_p50_ms <= st.lat_p99_ms <= st.lat_max_ms
+    assert 0 < st.gpu_s <= st.busy_s
     for (nl, codes, v, t, n), (fx, fy, tot) in zip(jobs, res):
         w = O.grade(nl, codes, n, mark_mode=mode, chunk=BATCH)
         np.testing.assert_array_equal(fx, w.first_x)
@@ -80,3 +81,17 @@ def test_admission_by_footprint_queues_jobs():
     assert st.jobs_done == 4
     for (nl, codes, v, t, n), (fx, fy, tot) in zip(jobs, res):
         assert tot.value == O.grade(nl, codes, n, mark_mode=1, chunk=BATCH).total
+
+
+@pytest.mark.parametrize("tile", [32, 128])
+def test_served_on_lane_tiles(tile):
+    """Jobs served with the lane kernel (batches narrower than its column
+    block: one partial block per job and step)."""
+    jobs = _jobs()
+    res, st = _serve(jobs, tile=tile)
+    assert st.jobs_done == len(jobs)
+    for (nl, codes, v, t, n), (fx, fy, tot) in zip(jobs, res):
+        w = O.grade(nl, codes, n, mark_mode=1, chunk=BATCH)
+        np.testing.assert_array_equal(fx, w.first_x)
+        np.testing.assert_array_equal(fy, w.first_y)
+        assert tot.value == w.total and tot.flags == w.flags and tot.pairs == n
