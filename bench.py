@@ -779,7 +779,7 @@ def run_batched(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
         "config": dict(batch_config(members, args), tile_words=tw, threads=threads or "default",
-                       ctas=info.ctas, forward_launches=int(info.launches) - 2,
+                       ctas=info.ctas, forward_launches=int(info.forward_launches),
                        autotune={"tile_words": tw, "threads": threads, "ms_per_pass": tune_ms,
                                  "seconds": round(tune_s, 1)} if tune_ms else None),
         "plain": {"value": units / (plain_best / 1e3), "ms_per_pass": plain_best,
@@ -796,7 +796,7 @@ def run_batched(args):
                 "mode": "streamed: pinned host pairs of the next pass copied on a second stream while this "
                         "pass grades (two buffer sets, two batches)",
                 "value_one_pass_per_step": units / (e2e_ms / 1e3)},
-        "gpu_launches": int(info.launches) * args.steps,  # forward per class, active, cover
+        "gpu_launches": int(info.launches) * args.steps,  # forward per class, active, cover (, spill cover)
         "clocks": clocks,
         "same_config": True,
         "result_stable": bool(same and stable),

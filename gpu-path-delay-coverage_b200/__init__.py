@@ -84,7 +84,7 @@ class BatchJob_t(C.Structure):
 class BatchInfo_t(C.Structure):
     _fields_ = [("n_jobs", C.c_uint32), ("tile_words", C.c_uint32), ("threads", C.c_uint32),
                 ("ctas", C.c_uint32), ("gate_evals", C.c_uint64), ("device_bytes", C.c_uint64),
-                ("launches", C.c_uint32), ("reserved", C.c_uint32)]
+                ("launches", C.c_uint32), ("forward_launches", C.c_uint32)]
 
 
 class ServerOpts_t(C.Structure):

@@ -1876,9 +1876,9 @@ extern "C" pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info) 
     info->ctas = b->L.total_blocks;
     info->gate_evals = b->gate_evals;
     info->device_bytes = b->bytes;
-    info->launches = b->L.spill_grid ? 3 : 2;
-    for (uint32_t k = 0; k < b->L.n_class; k++) info->launches += b->L.cls[k].blocks ? 1u : 0u;
-    info->reserved = 0;
+    info->forward_launches = 0;
+    for (uint32_t k = 0; k < b->L.n_class; k++) info->forward_launches += b->L.cls[k].blocks ? 1u : 0u;
+    info->launches = info->forward_launches + (b->L.spill_grid ? 3 : 2);
     return PDF_OK;
 }
 

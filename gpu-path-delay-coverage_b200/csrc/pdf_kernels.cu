@@ -841,20 +841,15 @@ __device__ __forceinline__ void lane_load(const FwdArgs &a, const LanePlanes &P,
     constexpr bool FIX = SEM >= 2;
     const uint4 r0 = reinterpret_cast<const uint4 *>(rp)[0], r1 = reinterpret_cast<const uint4 *>(rp)[1];
     const uint32_t h = r0.x, nfi = (h >> 8) & 0xFFu;
-    const uint32_t src[kInlineFanins] = {r0.w, r1.x, r1.y, r1.z};  // w[3..6]
     x.h = h;
-#pragma unroll
-    for (int q = 0; q < kInlineFanins; q++) {
-        lzero<LW>(x.fv[q]);
-        lzero<LW>(x.ft[q]);
-        lzero<LW>(x.fm[q]);
-    }
-    lzero<LW>(x.m0);
-    lzero<LW>(x.sv);
-    lzero<LW>(x.st);
-    x.bit0 = false;
+    // Whether fan-in 0 holds a mark in the block: the same on every lane of
+    // the warp (the branch in lane_gate that it guards holds warp votes), so
+    // it is set before any lane leaves.  m0 is read only where bit0 and
+    // RF_MARKF0 had it loaded.
+    x.bit0 = MODE != FWD_SIM && !(h & (RF_INPT | RF_KILL)) && bit_test(bm, r1.w);
+    // A lane past the last pair loads nothing: what it evaluates is masked.
+    if (!live) return;
     if (h & RF_INPT) {
-        if (!live) return;
         if (MODE == FWD_MARK) {
             lload<LW>(lrow(P.V, g, P.ld4), x.fv[0]);
             lload<LW>(lrow(P.T, g, P.ld4), x.ft[0]);
@@ -865,25 +860,42 @@ __device__ __forceinline__ void lane_load(const FwdArgs &a, const LanePlanes &P,
         }
         return;
     }
-    if (MODE == FWD_MARK && live) {  // the gate's own values are given; fan-ins feed the side test only
+    if (MODE == FWD_MARK) {  // the gate's own values are given; fan-ins feed the side test only
         lload<LW>(lrow(P.V, g, P.ld4), x.sv);
         lload<LW>(lrow(P.T, g, P.ld4), x.st);
     }
-    // a killed gate's value is S0 whatever its fan-ins (and it cannot mark)
-    const uint32_t nl = (h & RF_KILL) ? 0u : min(nfi, (uint32_t)kInlineFanins);
-    if (MODE != FWD_SIM) x.bit0 = bit_test(bm, r1.w);
-#pragma unroll
-    for (int q = 0; q < kInlineFanins; q++) {
-        const uint32_t sw = src[q], f = sw & ~SRC_ZERO;
-        // a killed fan-in is S0 (its row is not written), except in the stage
-        // call pdf_mark, whose given planes are read as they are
-        if ((uint32_t)q < nl && live && (MODE == FWD_MARK || !(sw & SRC_ZERO))) {
+    // A killed gate's value is S0 whatever its fan-ins (and it cannot mark):
+    // nothing to load.  Fan-ins 0 .. nl - 1 follow warp-uniform branches on
+    // the count, so absent fan-ins cost no predicated-off slots; a killed
+    // fan-in is S0 (its row is not written), except in the stage call
+    // pdf_mark, whose given planes are read as they are.
+    if (h & RF_KILL) return;
+    const uint32_t nl = min(nfi, (uint32_t)kInlineFanins);
+    const auto fanin = [&](int q, uint32_t sw) {
+        const uint32_t f = sw & ~SRC_ZERO;
+        if (MODE == FWD_MARK || !(sw & SRC_ZERO)) {
             lload<LW>(lrow(P.V, f, P.ld4), x.fv[q]);
             lload<LW>(lrow(P.T, f, P.ld4), x.ft[q]);
-            if (FIX && MODE != FWD_SIM && bit_test(bm, f)) lload<LW>(lrow(P.M, f, P.ld4), x.fm[q]);
+        } else {
+            lzero<LW>(x.fv[q]);
+            lzero<LW>(x.ft[q]);
+        }
+        if (FIX && MODE != FWD_SIM) {
+            if (bit_test(bm, f)) lload<LW>(lrow(P.M, f, P.ld4), x.fm[q]);
+            else lzero<LW>(x.fm[q]);
+        }
+    };
+    if (nl > 0) {
+        fanin(0, r0.w);
+        if (nl > 1) {
+            fanin(1, r1.x);
+            if (nl > 2) {
+                fanin(2, r1.y);
+                if (nl > 3) fanin(3, r1.z);
+            }
         }
     }
-    if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0 && live) lload<LW>(lrow(P.M, r1.w, P.ld4), x.m0);
+    if (MODE != FWD_SIM && (h & RF_MARKF0) && x.bit0) lload<LW>(lrow(P.M, r1.w, P.ld4), x.m0);
 }
 
 // Evaluate, mark and store one gate; returns whether it holds a mark in the
@@ -919,16 +931,30 @@ __device__ __forceinline__ bool lane_gate(const FwdArgs &a, const LanePlanes &P,
             V[j] = x.sv[j] & wm[j];
             T[j] = x.st[j] & wm[j];
         }
+    } else if ((h & RF_KILL) || !live) {
+        lzero<LW>(V);
+        lzero<LW>(T);
+        if (FIX && (h & RF_OINV)) {
+#pragma unroll
+            for (int j = 0; j < LW; j++) V[j] = wm[j];  // S0 inverted under both vectors: S1
+        }
     } else {
         uint32_t v1[LW];
 #pragma unroll
         for (int j = 0; j < LW; j++) eval_first(h, x.fv[0][j], x.ft[0][j], V[j], v1[j]);
+        // fold steps in fan-in order, behind warp-uniform branches on the count
         const uint32_t nfold = hdr_nfold(h);
+        const auto fold = [&](int q) {
 #pragma unroll
-        for (int q = 1; q < kInlineFanins; q++)
-            if ((uint32_t)q <= nfold)
-#pragma unroll
-                for (int j = 0; j < LW; j++) eval_fold<FIX>(h, V[j], v1[j], x.fv[q][j], x.ft[q][j]);
+            for (int j = 0; j < LW; j++) eval_fold<FIX>(h, V[j], v1[j], x.fv[q][j], x.ft[q][j]);
+        };
+        if (nfold >= 1) {
+            fold(1);
+            if (nfold >= 2) {
+                fold(2);
+                if (nfold >= 3) fold(3);
+            }
+        }
         for (uint32_t q = kInlineFanins; q <= nfold; q++) {
             uint32_t rv[LW], rt[LW];
             far_row(q, rv, rt);

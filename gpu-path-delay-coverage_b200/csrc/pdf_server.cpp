@@ -397,12 +397,13 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         if (n != j->cur) srv->dirty = true;
         j->cur = n;
         const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32, W = (n + 31) / 32;
-        j->in_place = j->hld % tw == 0 && (npi * j->hld) % 4 == 0 && w0 % 4 == 0 && w0 % tw == 0 &&
-                      w0 + (W + tw - 1) / tw * tw <= j->hld;
-        if (j->in_place) {
-            srv->dirty = true;
-            continue;
-        }
+        const bool in_place = j->hld % tw == 0 && (npi * j->hld) % 4 == 0 && w0 % 4 == 0 && w0 % tw == 0 &&
+                              w0 + (W + tw - 1) / tw * tw <= j->hld;
+        // a view moves every batch; a job that leaves its view for the batch
+        // buffer (or comes back to it) changes its pairs' address and pitch
+        if (in_place || in_place != j->in_place) srv->dirty = true;
+        j->in_place = in_place;
+        if (in_place) continue;
         uint32_t *dv = j->dv, *dt = j->dv + npi * j->ld;
         const uint32_t *sv = j->dall + w0, *stp = j->dall + npi * j->hld + w0;
         if (cudaMemcpy2DAsync(dv, j->ld * 4, sv, j->hld * 4, W * 4, npi, cudaMemcpyDeviceToDevice, srv->stream) !=

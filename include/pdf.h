@@ -414,8 +414,9 @@ typedef struct pdf_batch_info {
     uint32_t n_jobs, tile_words, threads, ctas;
     uint64_t gate_evals; /* per run: sum over jobs of n_gates * n_pairs */
     uint64_t device_bytes;
-    uint32_t launches;   /* kernel launches per run: one forward launch per occupancy class, then two */
-    uint32_t reserved;
+    uint32_t launches;   /* kernel launches per run: the forward launches, then k_batch_active,
+                            k_batch_cover and (when a circuit may spill) k_batch_cover_spill */
+    uint32_t forward_launches; /* one per class of tile width and CTAs per SM */
 } pdf_batch_info;
 pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out);
 void pdf_batch_destroy(pdf_batch *b);
