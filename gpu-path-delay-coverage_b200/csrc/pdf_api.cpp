@@ -1773,12 +1773,21 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
         L.cls[k].blocks = (k + 1 < L.n_class ? L.cls[k + 1].blk0 : L.total_blocks) - L.cls[k].blk0;
     L.total_gates = gp[n_jobs];
     L.append = (flags & PDF_BATCH_APPEND) ? 1u : 0u;
-    // one device block: control word, circuit arguments, prefixes, then items
+    // the small-table cover that runs first (several CTAs per SM)
+    {
+        uint32_t per_sm = 0;
+        L.small_cap = std::min(cover_small_cap(b->device, &per_sm), L.hash_cap);
+        if (!L.small_cap) return PDF_ECUDA;
+        L.small_grid = L.cover_grid * per_sm;
+    }
+    // one device block: control word, circuit arguments, prefixes, then the
+    // item lists (all items; those passed to the large table; those queued
+    // for the spill cover)
     auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t list = a256(sizeof(uint2) * std::max<uint64_t>(items, 1));
     const size_t o_f = a256(sizeof(BatchCtl)), o_c = o_f + a256(sizeof(FwdArgs) * n_jobs),
                  o_b = o_c + a256(sizeof(CoverArgs) * n_jobs), o_g = o_b + a256(4 * (n_jobs + 1)),
-                 o_i = o_g + a256(4 * (n_jobs + 1)), o_o = o_i + a256(sizeof(uint2) * std::max<uint64_t>(items, 1)),
-                 total = o_o + sizeof(uint2) * std::max<uint64_t>(items, 1);
+                 o_i = o_g + a256(4 * (n_jobs + 1)), o_m = o_i + list, o_o = o_m + list, total = o_o + list;
     // the spill cover: as many CTAs as the spilling circuit with the fewest
     // slots has (circuits without slots cannot spill)
     L.spill_grid = 0;
@@ -1822,6 +1831,7 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     L.bpref = reinterpret_cast<const uint32_t *>(base + o_b);
     L.gpref = reinterpret_cast<const uint32_t *>(base + o_g);
     L.items = reinterpret_cast<uint2 *>(base + o_i);
+    L.mid_items = reinterpret_cast<uint2 *>(base + o_m);
     L.over_items = reinterpret_cast<uint2 *>(base + o_o);
     b->bytes = b->ctl.bytes;
     PDF_CUDA(prepare_batch(L));
@@ -1878,7 +1888,7 @@ extern "C" pdf_status pdf_batch_query(const pdf_batch *b, pdf_batch_info *info) 
     info->device_bytes = b->bytes;
     info->forward_launches = 0;
     for (uint32_t k = 0; k < b->L.n_class; k++) info->forward_launches += b->L.cls[k].blocks ? 1u : 0u;
-    info->launches = info->forward_launches + (b->L.spill_grid ? 3 : 2);
+    info->launches = info->forward_launches + (b->L.spill_grid ? 4 : 3);
     return PDF_OK;
 }
 

@@ -1497,20 +1497,24 @@ __device__ __forceinline__ uint32_t level_of(const uint32_t *lo_tab, uint32_t n_
 // nothing here: cover_pair returns true and the caller queues the pair for
 // the spill cover (spill_pair); fan-out lists past the adjacency buffer are
 // read in place.
-constexpr uint32_t kCoverCand = 4096;   // candidates per chunk (128 bitmap words)
+constexpr uint32_t kCoverCand = 4096;   // candidates per window (k_cover and the large-table batch cover)
+constexpr uint32_t kCoverCandSmall = 2048;  // candidates per window of the small-table batch cover
 constexpr uint32_t kCoverLevels = 2048; // level table entries kept in shared memory
 constexpr uint32_t kNetPo = 1u << 31, kNetInpt = 1u << 30, kNetFirst = 1u << 29, kNetLevel = (1u << 29) - 1;
-// Byte offset of the level table in k_cover's shared memory: after h, c
-// (u128), the net list, flags, adjacency offsets and lengths, 4 cap
-// adjacency entries and the candidates.
-__host__ __device__ constexpr size_t cover_smem_lvt(uint32_t cap) {
-    return (size_t)cap * (2 * sizeof(pdf_u128) + 4 * 4 + 4 * 4) + (size_t)kCoverCand * 4;
+// Shared memory of cover_pair's tables for `cap` nets and a window of
+// `cand` candidates: h, c (u128), the net list, flags, adjacency offsets and
+// lengths, 4 cap adjacency entries and the candidates.
+__host__ __device__ constexpr size_t cover_smem_tables(uint32_t cap, uint32_t cand) {
+    return (size_t)cap * (2 * sizeof(pdf_u128) + 4 * 4 + 4 * 4) + (size_t)cand * 4;
 }
+// Byte offset of the level table in k_cover's shared memory (after the tables).
+__host__ __device__ constexpr size_t cover_smem_lvt(uint32_t cap) { return cover_smem_tables(cap, kCoverCand); }
 
-// Each thread of the candidate test below takes up to kCoverCand / blockDim
+// Each thread of the candidate test below takes up to CAND / blockDim
 // candidates in registers: the cover kernels run 256 threads.
 constexpr uint32_t kCoverThreads = 256;
 static_assert(kCoverCand / kCoverThreads <= 16, "cover_pair keeps 16 candidate mark words per thread");
+static_assert(kCoverCandSmall % kCoverThreads == 0 && kCoverCandSmall <= kCoverCand, "small window");
 
 // Paths primary input g credits to pair p (the values the reference dumps to
 // gpucover.log, coverkernel.cuh:44-66).
@@ -1521,12 +1525,16 @@ __device__ __forceinline__ void put_pi_count(const CoverArgs &a, uint32_t g, uin
 }
 
 // The cover of pair p (index within the batch) of the circuit in `a`;
-// lo_tab is its level table (shared or global memory).  Returns true (the
-// same in every thread) when the pair marks more nets than the table holds:
-// then nothing is counted.
-__device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p, const uint32_t *lo_tab) {
+// lo_tab is its level table (shared or global memory); cap: nets the table
+// holds; CAND: candidates per window.  Returns true (the same in every
+// thread) when the pair marks more nets than the table holds: then nothing
+// is counted.
+template <uint32_t CAND>
+__device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p, const uint32_t *lo_tab,
+                                           const uint32_t cap) {
     extern __shared__ __align__(128) unsigned char smraw[];
-    const uint32_t cap = a.hash_cap, acap = 4 * cap;
+    constexpr uint32_t kPer = CAND / kCoverThreads;  // candidates per thread and window
+    const uint32_t acap = 4 * cap;
     pdf_u128 *hv = reinterpret_cast<pdf_u128 *>(smraw);
     pdf_u128 *cv = hv + cap;
     uint32_t *lid = reinterpret_cast<uint32_t *>(cv + cap);  // [cap] listed nets, ascending
@@ -1534,7 +1542,7 @@ __device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p,
     uint32_t *aoff = info + cap;                              // [cap] adjacency offset, kEmpty: read in place
     uint32_t *acnt = aoff + cap;                              // [cap] adjacency length
     uint32_t *adj = acnt + cap;                               // [4 cap] listed fan-outs (list indices)
-    uint32_t *cand = adj + acap;                              // [kCoverCand]
+    uint32_t *cand = adj + acap;                              // [CAND]
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_n, s_adj, s_over;
     __shared__ pdf_u128 s_red[8];
@@ -1568,10 +1576,10 @@ __device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p,
     for (uint32_t q = q_lo; q < q_hi; q++) mine += __popc(word(q));
     uint32_t total_c;
     const uint32_t first_c = block_scan_excl(mine, s_warp, &total_c);
-    // ---- B: in windows of kCoverCand candidates, those the pair marks (one
+    // ---- B: in windows of CAND candidates, those the pair marks (one
     // mark word each) join the pair's list, in gate order
-    for (uint32_t c_lo = 0; c_lo < total_c; c_lo += kCoverCand) {
-        const uint32_t c_hi = min(total_c, c_lo + kCoverCand);
+    for (uint32_t c_lo = 0; c_lo < total_c; c_lo += CAND) {
+        const uint32_t c_hi = min(total_c, c_lo + CAND);
         if (first_c < c_hi && first_c + mine > c_lo) {  // this thread's candidates in the window
             uint32_t idx = first_c;
             for (uint32_t q = q_lo; q < q_hi && idx < c_hi; q++) {
@@ -1585,12 +1593,12 @@ __device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p,
         // each thread tests a contiguous run of candidates (order kept)
         const uint32_t per = (nc + blockDim.x - 1) / blockDim.x;
         const uint32_t c0 = min(nc, threadIdx.x * per), c1 = min(nc, c0 + per);
-        uint32_t keep = 0, nk = 0;  // per <= kCoverCand / kCoverThreads = 16: one bit each
-        uint32_t mw[16];
+        uint32_t keep = 0, nk = 0;  // per <= kPer <= 16: one bit each
+        uint32_t mw[kPer];
 #pragma unroll
-        for (int k = 0; k < 16; k++) mw[k] = c0 + k < c1 ? a.M[(size_t)cand[c0 + k] * a.ld + wp] : 0u;
+        for (int k = 0; k < (int)kPer; k++) mw[k] = c0 + k < c1 ? a.M[(size_t)cand[c0 + k] * a.ld + wp] : 0u;
 #pragma unroll
-        for (int k = 0; k < 16; k++) {
+        for (int k = 0; k < (int)kPer; k++) {
             const uint32_t m = (mw[k] >> bit) & 1u;
             keep |= m << k;
             nk += m;
@@ -1660,7 +1668,7 @@ __device__ __forceinline__ bool cover_pair(const CoverArgs &a, const uint32_t p,
     bool ovf = false;
     const uint32_t lv_hi = n ? (info[n - 1] & kNetLevel) : 0;
     uint32_t *bnd = cand;  // [lv_hi + 2] (the candidates are no longer needed)
-    const bool runs = lv_hi + 2 <= kCoverCand;
+    const bool runs = lv_hi + 2 <= CAND;
     if (runs) {
         for (uint32_t l = threadIdx.x; l <= lv_hi + 1; l += blockDim.x) {
             const uint32_t g0 = lo_tab[l];
@@ -1817,7 +1825,7 @@ __global__ void __launch_bounds__(kCoverThreads) k_cover(const CoverArgs a) {
     const uint32_t n_active = *a.active_count;
     for (uint32_t ai = blockIdx.x; ai < n_active; ai += gridDim.x) {
         const uint32_t p = a.active_list[ai];
-        if (cover_pair(a, p, lo_tab) && threadIdx.x == 0) {
+        if (cover_pair<kCoverCand>(a, p, lo_tab, a.hash_cap) && threadIdx.x == 0) {
             if (a.spill_slots) a.over_list[atomicAdd(&a.acc->n_over, 1u)] = p;  // for k_cover_spill
             else atomicOr(&a.acc->err, kErrHashFull);
         }
@@ -1888,6 +1896,8 @@ __global__ void __launch_bounds__(BW >= 8 ? 512 : 1024)
             ctl->err = 0;
             ctl->n_over = 0;
             ctl->done_over = 0;
+            ctl->n_mid = 0;
+            ctl->done_mid = 0;
         }
     }
     __syncthreads();
@@ -1911,6 +1921,8 @@ __global__ void __launch_bounds__(lane_threads(32 * LW), 1)
             ctl->err = 0;
             ctl->n_over = 0;
             ctl->done_over = 0;
+            ctl->n_mid = 0;
+            ctl->done_mid = 0;
         }
     }
     __syncthreads();
@@ -1943,33 +1955,47 @@ __device__ void batch_close_all(CoverArgs *args, FwdArgs *fargs, uint32_t n, Bat
     if ((threadIdx.x & 31) == 0 && err) atomicOr(&ctl->err, err);
 }
 
+// The batch's cover in two passes of the same code.  TIER 0 lists at most
+// `cap` nets per pair in a small table, so several CTAs share an SM (the
+// per-pair phases are chains of dependent loads and barriers, which one CTA
+// per SM leaves mostly idle); a pair that marks more nets is passed on
+// (out_items, ctl->n_mid).  TIER 1 counts those with the large table (one
+// CTA per SM) and queues what still does not fit for the spill cover
+// (ctl->n_over).  The last CTA of the last pass that has work closes every
+// circuit's batch.
+template <int TIER>
 __global__ void __launch_bounds__(kCoverThreads) k_batch_cover(CoverArgs *args, FwdArgs *fargs, uint32_t n,
-                                                               const uint2 *items, uint2 *over_items, BatchCtl *ctl,
-                                                               uint32_t append) {
+                                                               const uint2 *in_items, uint2 *out_items, BatchCtl *ctl,
+                                                               uint32_t append, uint32_t cap) {
     __shared__ CoverArgs s_a;
     __shared__ uint32_t s_last;
-    const uint32_t n_items = ctl->n_items;
+    const uint32_t n_items = TIER == 0 ? ctl->n_items : ctl->n_mid;
+    if (TIER == 1 && !n_items) return;  // the small-table pass closed the batch
     for (uint32_t ai = blockIdx.x; ai < n_items; ai += gridDim.x) {
-        const uint2 it = items[ai];
+        const uint2 it = in_items[ai];
         if (threadIdx.x == 0) s_a = args[it.x];
         __syncthreads();
-        if (cover_pair(s_a, it.y, s_a.c.level_off) && threadIdx.x == 0) {  // ends with a barrier
-            if (s_a.spill_slots) over_items[atomicAdd(&ctl->n_over, 1u)] = it;  // for k_batch_cover_spill
+        const bool over = TIER == 0 ? cover_pair<kCoverCandSmall>(s_a, it.y, s_a.c.level_off, cap)
+                                    : cover_pair<kCoverCand>(s_a, it.y, s_a.c.level_off, cap);  // end with a barrier
+        if (over && threadIdx.x == 0) {
+            if (TIER == 0) out_items[atomicAdd(&ctl->n_mid, 1u)] = it;             // for the large table
+            else if (s_a.spill_slots) out_items[atomicAdd(&ctl->n_over, 1u)] = it;  // for k_batch_cover_spill
             else atomicOr(&s_a.acc->err, kErrHashFull);
         }
         __syncthreads();
     }
     // the last CTA to finish closes every circuit's batch, unless items wait
-    // for the spill cover
+    // for the next pass
+    unsigned int *done = TIER == 0 ? &ctl->done : &ctl->done_mid;
     if (threadIdx.x == 0) {
         __threadfence();
-        s_last = atomicAdd(&ctl->done, 1u) == gridDim.x - 1;
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    if (!ctl->n_over) batch_close_all(args, fargs, n, ctl, append);
-    if (threadIdx.x == 0) ctl->done = 0;
+    if (!(TIER == 0 ? ctl->n_mid : ctl->n_over)) batch_close_all(args, fargs, n, ctl, append);
+    if (threadIdx.x == 0) *done = 0;
 }
 
 // After k_batch_cover: the items it queued (CTA k uses spill slot k of the
@@ -2195,6 +2221,28 @@ cudaError_t launch_forward(const FwdArgs &a, int mode, int sem, uint32_t bw, uin
 }
 
 size_t cover_smem_bytes(uint32_t net_cap) { return cover_smem_lvt(net_cap) + (size_t)kCoverLevels * 4; }
+size_t cover_small_smem_bytes(uint32_t cap) { return cover_smem_tables(cap, kCoverCandSmall); }
+
+// CTAs per SM of the batch's small-table cover, and the nets per pair its
+// table then holds: an equal share of the SM's shared memory less what the
+// system keeps per CTA and the kernel's static variables.  Four CTAs of 256
+// threads: the kernel's registers allow five.
+uint32_t cover_small_cap(int device, uint32_t *ctas_per_sm) {
+    constexpr uint32_t kCtas = 4;
+    int per_sm = 0, reserved = 0, optin = 0;
+    cudaFuncAttributes fa{};
+    if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, k_batch_cover<0>) != cudaSuccess)
+        return 0;
+    const int64_t share = std::min<int64_t>(optin, per_sm / kCtas - reserved - (int64_t)fa.sharedSizeBytes);
+    const int64_t room = share - (int64_t)kCoverCandSmall * 4;
+    const uint32_t per_net = (uint32_t)cover_smem_tables(1, 0);
+    if (room < (int64_t)per_net * 32) return 0;
+    if (ctas_per_sm) *ctas_per_sm = kCtas;
+    return (uint32_t)(room / per_net) & ~31u;
+}
 
 cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bool zero_active, cudaStream_t st) {
     const uint32_t W = (uint32_t)((a.n_pairs + 31) / 32);
@@ -2287,8 +2335,11 @@ cudaError_t prepare_batch(const BatchLaunch &b) {
         const cudaError_t e = prepare_class(b.sem, b.cls[k].bw, smem);
         if (e != cudaSuccess) return e;
     }
-    return cudaFuncSetAttribute(k_batch_cover, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)cover_smem_bytes(b.hash_cap));
+    const cudaError_t e = cudaFuncSetAttribute(k_batch_cover<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)cover_small_smem_bytes(b.small_cap));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_batch_cover<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)cover_smem_tables(b.hash_cap, kCoverCand));
 }
 
 // The classes' forward launches are independent (different circuits), so
@@ -2321,8 +2372,11 @@ cudaError_t launch_batch(const BatchLaunch &b, cudaStream_t st) {
     if (b.prof[1] && (e = cudaEventRecordWithFlags(b.prof[1], st, pflag)) != cudaSuccess) return e;
     k_batch_active<<<(b.total_gates + 255) / 256, 256, 0, st>>>(b.cargs, b.gpref, b.n, b.items, b.ctl);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_batch_cover<<<b.cover_grid, kCoverThreads, cover_smem_bytes(b.hash_cap), st>>>(b.cargs, b.fargs, b.n, b.items,
-                                                                                   b.over_items, b.ctl, b.append);
+    k_batch_cover<0><<<b.small_grid, kCoverThreads, cover_small_smem_bytes(b.small_cap), st>>>(
+        b.cargs, b.fargs, b.n, b.items, b.mid_items, b.ctl, b.append, b.small_cap);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_batch_cover<1><<<b.cover_grid, kCoverThreads, cover_smem_tables(b.hash_cap, kCoverCand), st>>>(
+        b.cargs, b.fargs, b.n, b.mid_items, b.over_items, b.ctl, b.append, b.hash_cap);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (b.spill_grid) {
         k_batch_cover_spill<<<b.spill_grid, kCoverThreads, 0, st>>>(b.cargs, b.fargs, b.n, b.over_items, b.ctl,

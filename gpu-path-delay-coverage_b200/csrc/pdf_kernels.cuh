@@ -167,7 +167,9 @@ struct BatchCtl {
     unsigned int err;      // OR of every circuit's device error word after the pass
     unsigned int n_over;   // items queued for the spill cover
     unsigned int done_over;
-    unsigned int pad[3];
+    unsigned int n_mid;    // items the small-table cover passed to the large-table cover
+    unsigned int done_mid;
+    unsigned int pad[1];
 };
 // One forward launch of a batch: jobs of equal tile width and CTAs per SM.
 struct BatchClass {
@@ -180,11 +182,14 @@ struct BatchLaunch {
     const uint32_t *bpref; // [n + 1] first forward CTA of each circuit
     const uint32_t *gpref; // [n + 1] first gate of each circuit
     uint2 *items;          // [sum of min(n_pairs, 2 n_gates)]
+    uint2 *mid_items;      // [same]: items whose pair marks more nets than the small table
     uint2 *over_items;     // [same]: items whose pair marks more nets than the cover's table
     uint32_t spill_grid;   // CTAs of the batch's spill cover (<= every spilling circuit's slots)
     BatchCtl *ctl;
     uint32_t n, total_blocks, total_gates;
     uint32_t sem, threads, cover_grid, hash_cap, append;  // sem: PDF_MARK_*
+    // the small-table cover that runs first: nets per pair, CTAs
+    uint32_t small_cap, small_grid;
     size_t fwd_smem;
     uint32_t n_class;      // forward launches: classes of jobs (tile width x CTAs per SM)
     BatchClass cls[kMaxBatchClasses];
@@ -211,6 +216,10 @@ cudaError_t launch_forward(const FwdArgs &a, int mode, int sem, uint32_t bw, uin
 // must be zero (k_forward clears them; zero_active asks for a memset).
 cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bool zero_active, cudaStream_t st);
 size_t cover_smem_bytes(uint32_t hash_cap);
+// The batch's small-table cover: several CTAs per SM, each listing at most
+// the returned number of nets per pair in shared memory (0 on error).
+uint32_t cover_small_cap(int device, uint32_t *ctas_per_sm);
+size_t cover_small_smem_bytes(uint32_t cap);
 cudaError_t launch_merge_dense(const DevCircuit &c, const uint32_t *V, const uint32_t *M,
                                uint64_t ld, uint64_t n_pairs, uint32_t pair_base,
                                uint32_t *first_x, uint32_t *first_y, cudaStream_t st);

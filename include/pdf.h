@@ -383,7 +383,7 @@ pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, uint64_t n_pa
 
 /*
  * A batch grades the vector pairs of many (circuit, state) jobs in one pass of
- * three kernel launches, captured once as a CUDA graph and replayed by each
+ * a few kernel launches, captured once as a CUDA graph and replayed by each
  * pdf_batch_run.  Each job's result is the same as pdf_grade of that job alone
  * (its state's first-detect ids and totals).  No reference counterpart: the
  * reference grades one circuit per process (main.cu:129-235).
@@ -415,7 +415,8 @@ typedef struct pdf_batch_info {
     uint64_t gate_evals; /* per run: sum over jobs of n_gates * n_pairs */
     uint64_t device_bytes;
     uint32_t launches;   /* kernel launches per run: the forward launches, then k_batch_active,
-                            k_batch_cover and (when a circuit may spill) k_batch_cover_spill */
+                            the small- and large-table passes of k_batch_cover and (when a
+                            circuit may spill) k_batch_cover_spill */
     uint32_t forward_launches; /* one per class of tile width and CTAs per SM */
 } pdf_batch_info;
 pdf_status pdf_batch_create(const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags, pdf_batch **out);

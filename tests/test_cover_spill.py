@@ -119,3 +119,40 @@ def test_fixed_robust_on_c2():
         fx, fy, tot = _grade(nl, codes, n, 2, tile)
         np.testing.assert_array_equal(fx, want.first_x)
         assert tot.value == want.total
+
+
+def test_batch_cover_passes(big):
+    """A batch's cover runs a small table first (several CTAs per SM), then
+    the large table for the pairs that marked more nets, then the spill
+    cover: here a 30,000-gate circuit whose pairs mark 670 to 1,330 nets
+    each (on both sides of the small table's limit) shares a batch with a
+    spilling circuit and a small one; all graded twice, against the oracle."""
+    import torch
+    nl0, codes0, n0, want0 = big
+    mid = P.gen_netlist(P.GenParams(0x5EED0302, 30_000, 700, 700, 40))
+    n1 = 256
+    codes1 = helpers.rand_codes(np.random.default_rng(5), mid.n_pi, n1)
+    want1 = O.grade(mid, codes1, n1, mark_mode=3, want_planes=True)
+    per_pair = want1.mark.sum(axis=0)
+    assert per_pair.min() < 700 and 1000 < per_pair.max() <= 3072
+    small = circuits.random_small(61, n_gates=2000, n_pi=60, n_po=300, depth=12)
+    codes2 = helpers.rand_codes(np.random.default_rng(6), small.n_pi, 700)
+    members = [(nl0, codes0, n0, 32, want0), (mid, codes1, n1, 64, want1), (mid, codes1, n1, 128, want1),
+               (small, codes2, 700, 128, O.grade(small, codes2, 700, mark_mode=3))]
+    jobs, want = [], []
+    for nl, codes, n, tw, w in members:
+        ld = (P.words(n) + 127) // 128 * 128
+        v, t = P.planes_from_codes(codes, ld)
+        c = P.Circuit(nl, mark_mode=3, tile_words=tw)
+        s = P.State(c)
+        jobs.append((c, s, torch.from_numpy(v.view(np.int32)).cuda(), torch.from_numpy(t.view(np.int32)).cuda(), n, 0))
+        want.append(w)
+    b = P.Batch(jobs)
+    assert b.info().launches == b.info().forward_launches + 4  # active, two cover tables, spill
+    b.run()
+    b.run()  # replayed: every pass's queue starts empty again
+    for (c, s, *_), w in zip(jobs, want):
+        fx, fy, tot = s.snapshot()
+        np.testing.assert_array_equal(fx, w.first_x)
+        np.testing.assert_array_equal(fy, w.first_y)
+        assert tot.value == 2 * w.total and tot.flags == w.flags
