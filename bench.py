@@ -668,6 +668,34 @@ def run_batched(args):
     # plain: every circuit alone, one after another
     plain_ms, plain_res = time_plain(plain_jobs)
     plain_bt_ms, plain_bt_res = time_plain(jobs)
+    # and each circuit at the tile that grades it fastest alone (every tile
+    # width timed per circuit): the best the plain call can do
+    sweep_ms, sweep_tiles, sweep_same = 0.0, {}, True
+    if not args.no_tile_sweep:
+        for (c, st, dv, dt, n, _), nl, ref in zip(jobs, nls, plain_res):
+            best = None
+            for tile in (4, 8) + LANE_TILES:
+                c1 = P.Circuit(nl, device=local, mark_mode=P.MARK_ROBUST, max_pairs=n, tile_words=tile)
+                s1 = P.State(c1)
+                pr = P.make_pairs(dv, dt, n)
+                s1.reset_async(stream)
+                P.grade_async(c1, s1, pr, 0, None, stream)
+                got = s1.snapshot()
+                sweep_same &= bool(np.array_equal(got[0], ref[0]) and got[2].value == ref[2].value)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(3):
+                    s1.reset_async(stream)
+                    P.grade_async(c1, s1, pr, 0, None, stream)
+                e1.record()
+                torch.cuda.synchronize()
+                t_ms = e0.elapsed_time(e1) / 3
+                if best is None or t_ms < best[0]:
+                    best = (t_ms, tile)
+                s1.close()
+                c1.close()
+            sweep_ms += best[0]
+            sweep_tiles[best[1]] = sweep_tiles.get(best[1], 0) + 1
     if args.timeline:  # per-circuit duration of one plain pass (fill of the GPU against time)
         marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(jobs) + 1)]
         plain_pass(plain_jobs, marks)
@@ -773,7 +801,7 @@ def run_batched(args):
     kernel_ms = sum(fwd_ms) / len(fwd_ms)
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     prof = profile_summary(f"k_batch_forward_c4_tile{tw}") if args.circuits == 256 else None
-    plain_best = min(plain_ms, plain_bt_ms)
+    plain_best = min(plain_ms, plain_bt_ms, sweep_ms or float("inf"))
     line = {
         "metric": "gate-evals/s", "value": units / (ms / 1e3), "unit": "gate-evals/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -784,8 +812,11 @@ def run_batched(args):
                                  "seconds": round(tune_s, 1)} if tune_ms else None),
         "plain": {"value": units / (plain_best / 1e3), "ms_per_pass": plain_best,
                   "ms_per_pass_default_tiles": plain_ms, "ms_per_pass_batch_tile": plain_bt_ms,
-                  "note": "the same circuits graded one after another (pdf_grade_async each), at each "
-                          "circuit's default tile and at the batch's tile; the faster of the two"},
+                  "ms_per_pass_best_tile_per_circuit": sweep_ms or None,
+                  "best_tiles": {str(k): v for k, v in sorted(sweep_tiles.items())} or None,
+                  "note": "the same circuits graded one after another (pdf_grade_async each): at each "
+                          "circuit's default tile, at the batch's tile, and each at the tile that graded "
+                          "it fastest (every tile timed per circuit, 3 calls each); the fastest of these"},
         "batched_vs_plain": plain_best / ms,
         "roofline": dict(roofline(sum(alg_bytes(nl, n) for nl, n in zip(nls, counts)), kernel_ms,
                                   f"forward span of the pass (k_batch_forward{'_lanes' if tw in LANE_TILES else ''}, "
@@ -799,7 +830,7 @@ def run_batched(args):
         "gpu_launches": int(info.launches) * args.steps,  # forward per class, active, cover (, spill cover)
         "clocks": clocks,
         "same_config": True,
-        "result_stable": bool(same and stable),
+        "result_stable": bool(same and stable and sweep_same),
         "native_libraries": loaded_libraries(),
     }
     if not args.no_cpu and rank == 0:
@@ -925,6 +956,8 @@ def main():
     ap.add_argument("--jobs", type=int, default=512, help="c5: jobs in the arrival stream")
     ap.add_argument("--planes", action="store_true",
                     help="c1-c3: also write the sim and mark planes of every (net, pair) to device memory")
+    ap.add_argument("--no-tile-sweep", action="store_true",
+                    help="c4: skip timing the plain call of each circuit at every tile")
     ap.add_argument("--timeline", default="",
                     help="c4: write the per-circuit durations of one plain pass to this JSON file")
     ap.add_argument("--circuits", type=int, default=256,
