@@ -1606,6 +1606,7 @@ extern "C" pdf_status pdf_cover_noalloc(pdf_circuit *c, const uint32_t *mark, ui
 
 struct pdf_batch {
     int device = 0;
+    uint32_t small_cap = 0, small_per_sm = 0;  // the small-table cover: nets per pair, CTAs per SM
     std::vector<pdf_circuit *> circuits;
     std::vector<pdf_state *> states;
     BatchLaunch L{};
@@ -1660,7 +1661,11 @@ namespace {
 
 // (Re)build batch b for these jobs: per-circuit arguments and prefixes in
 // one device block, which is reused when it is large enough.
-pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags) {
+// up: the stream that uploads the control block, in order before the next
+// pass on it (the caller then must not rebind or destroy the batch before
+// that pass is done); null: uploaded and waited for here.
+pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags,
+                       cudaStream_t up = nullptr) {
     if (!jobs || !n_jobs || (flags & ~(uint32_t)(PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH))) return PDF_EINVAL;
     pdf_circuit *c0 = jobs[0].circuit;
     if (!c0) return PDF_EINVAL;
@@ -1774,12 +1779,12 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     L.total_gates = gp[n_jobs];
     L.append = (flags & PDF_BATCH_APPEND) ? 1u : 0u;
     // the small-table cover that runs first (several CTAs per SM)
-    {
-        uint32_t per_sm = 0;
-        L.small_cap = std::min(cover_small_cap(b->device, &per_sm), L.hash_cap);
-        if (!L.small_cap) return PDF_ECUDA;
-        L.small_grid = L.cover_grid * per_sm;
+    if (!b->small_cap) {  // once per batch (its device does not change)
+        b->small_cap = cover_small_cap(b->device, &b->small_per_sm);
+        if (!b->small_cap) return PDF_ECUDA;
     }
+    L.small_cap = std::min(b->small_cap, L.hash_cap);
+    L.small_grid = L.cover_grid * b->small_per_sm;
     // one device block: control word, circuit arguments, prefixes, then the
     // item lists (all items; those passed to the large table; those queued
     // for the spill cover)
@@ -1816,14 +1821,14 @@ pdf_status batch_build(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs,
     if (total > b->ctl.bytes && b->ctl.ensure(std::max<size_t>({total, 2 * b->ctl.bytes, (size_t)1 << 20})) != cudaSuccess)
         return PDF_ENOMEM;
     void *src = nullptr;
-    if (!b->up) PDF_CUDA(cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking));
+    if (!up && !b->up) PDF_CUDA(cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking));
     PDF_CUDA(cudaHostGetDevicePointer(&src, hbuf, 0));
     // the launch below is checked with cudaGetLastError, which would also
     // report an unchecked failure left on this thread by an earlier call
     // (this library's or the caller's); start from a clean slate
     (void)cudaGetLastError();
-    PDF_CUDA(launch_copy_from_host(b->ctl.p, src, o_i / 16, b->up));
-    PDF_CUDA(cudaStreamSynchronize(b->up));
+    PDF_CUDA(launch_copy_from_host(b->ctl.p, src, o_i / 16, up ? up : b->up));
+    if (!up) PDF_CUDA(cudaStreamSynchronize(b->up));
     unsigned char *base = b->ctl.as<unsigned char>();
     L.ctl = reinterpret_cast<BatchCtl *>(base);
     L.fargs = reinterpret_cast<FwdArgs *>(base + o_f);
@@ -1941,6 +1946,29 @@ extern "C" pdf_status pdf_batch_profile_read(pdf_batch *b, double *ms) {
     ms[0] = f;
     ms[1] = c;
     return PDF_OK;
+}
+
+pdf_status batch_rebind_on(pdf_batch *b, const pdf_batch_job *jobs, uint32_t n_jobs, uint32_t flags,
+                           cudaStream_t stream) {
+    if (!b || !jobs || !n_jobs || !jobs[0].circuit || jobs[0].circuit->device != b->device || !stream)
+        return PDF_EINVAL;
+    DeviceGuard dg(b->device);
+    if (!dg.ok) return PDF_ECUDA;
+    const pdf_status st = batch_build(b, jobs, n_jobs, flags, stream);
+    if (st != PDF_OK) (void)cudaGetLastError();
+    return st;
+}
+
+pdf_status batch_pass_async(pdf_batch *b, cudaStream_t stream) {
+    pdf_status st = pdf_batch_run_async(b, stream);
+    if (st != PDF_OK) return st;
+    DeviceGuard dg(b->device);
+    PDF_CUDA(cudaMemcpyAsync(b->host_ctl, b->ctl.p, sizeof(BatchCtl), cudaMemcpyDeviceToHost, stream));
+    return PDF_OK;
+}
+
+pdf_status batch_pass_status(const pdf_batch *b) {
+    return err_status(reinterpret_cast<const BatchCtl *>(b->host_ctl)->err);
 }
 
 extern "C" pdf_status pdf_batch_run(pdf_batch *b, void *stream) {

@@ -17,6 +17,7 @@
 #include "pdf_kernels.cuh"
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 
 namespace {
@@ -2271,18 +2272,39 @@ cudaError_t launch_cover(const CoverArgs &a, uint32_t grid, uint32_t threads, bo
 }
 
 namespace {
+// The dynamic shared-memory limit of a batch kernel on the current device,
+// raised only when a batch asks for more than any earlier one did: a
+// serving loop rebinds its batch every step, and only these calls set the
+// batch kernels' limits, so the limit never falls below a request.
+cudaError_t raise_smem_limit(const void *fn, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> have;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &h = have[{dev, fn}];
+    if (smem <= h) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) h = smem;
+    return e;
+}
+template <typename F>
+cudaError_t raise_smem(F *fn, size_t smem) {
+    return raise_smem_limit(reinterpret_cast<const void *>(fn), smem);
+}
+
 // Kernel attributes and launch of one forward class (tile width, semantics).
 template <int SEM>
 cudaError_t prepare_class_sem(uint32_t bw, size_t smem) {
-    const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
     switch (bw) {
-        case 1: return cudaFuncSetAttribute(k_batch_forward<1, SEM>, attr, (int)smem);
-        case 2: return cudaFuncSetAttribute(k_batch_forward<2, SEM>, attr, (int)smem);
-        case 4: return cudaFuncSetAttribute(k_batch_forward<4, SEM>, attr, (int)smem);
-        case 8: return cudaFuncSetAttribute(k_batch_forward<8, SEM>, attr, (int)smem);
-        case kLaneWords: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM, 1>, attr, (int)smem);
-        case kLaneWords2: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM, 2>, attr, (int)smem);
-        case kLaneWords4: return cudaFuncSetAttribute(k_batch_forward_lanes<SEM, 4>, attr, (int)smem);
+        case 1: return raise_smem(k_batch_forward<1, SEM>, smem);
+        case 2: return raise_smem(k_batch_forward<2, SEM>, smem);
+        case 4: return raise_smem(k_batch_forward<4, SEM>, smem);
+        case 8: return raise_smem(k_batch_forward<8, SEM>, smem);
+        case kLaneWords: return raise_smem(k_batch_forward_lanes<SEM, 1>, smem);
+        case kLaneWords2: return raise_smem(k_batch_forward_lanes<SEM, 2>, smem);
+        case kLaneWords4: return raise_smem(k_batch_forward_lanes<SEM, 4>, smem);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -2335,11 +2357,9 @@ cudaError_t prepare_batch(const BatchLaunch &b) {
         const cudaError_t e = prepare_class(b.sem, b.cls[k].bw, smem);
         if (e != cudaSuccess) return e;
     }
-    const cudaError_t e = cudaFuncSetAttribute(k_batch_cover<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)cover_small_smem_bytes(b.small_cap));
+    const cudaError_t e = raise_smem(k_batch_cover<0>, cover_small_smem_bytes(b.small_cap));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_batch_cover<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)cover_smem_tables(b.hash_cap, kCoverCand));
+    return raise_smem(k_batch_cover<1>, cover_smem_tables(b.hash_cap, kCoverCand));
 }
 
 // The classes' forward launches are independent (different circuits), so

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "pdf.h"
+#include "pdf_internal.h"
 #include "pdf_inject.h"
 
 namespace {
@@ -48,7 +49,9 @@ struct Job {
     pdf_state *s = nullptr;
     uint32_t *dv = nullptr;  // [2][n_pi][ld] one batch of pairs
     uint64_t ld = 0, cur = 0;  // words per row, pairs of the batch in flight
-    bool in_place = false;     // the batch in flight is read from dall directly
+    bool in_place = false;     // the batch bound last is read from dall directly
+    bool in_flight = false;    // a batch of the job is in the pass in flight
+    uint64_t graded = 0;       // pairs of that batch
     uint32_t *dall = nullptr;  // [2][n_pi][hld] all the job's pairs, on the device while active
     pdf_status prep = PDF_OK;  // outcome of the preparation
     double t_ready = 0.0;
@@ -67,8 +70,15 @@ struct pdf_server {
     uint64_t next_id = 1;
     std::vector<Job *> active;
     std::map<uint64_t, Result> results;
-    pdf_batch *batch = nullptr;
-    bool dirty = true;
+    // two batches, used by alternate passes: one is bound for the next pass
+    // while the other's pass is in flight
+    pdf_batch *batch[2] = {nullptr, nullptr};
+    int cur = 0;                   // the batch of the next pass
+    bool pending = false;          // a pass is in flight (on `stream`, batch pend_b)
+    int pend_b = 0;
+    std::vector<Job *> inflight;   // the jobs it grades
+    cudaEvent_t done_ev[2] = {nullptr, nullptr};  // recorded after each batch's last pass
+    cudaStream_t rstream = nullptr;               // read-back of retiring jobs
     cudaStream_t stream = nullptr;
     pdf_server_stats st{};
     std::vector<double> lat_ms;
@@ -85,7 +95,6 @@ struct pdf_server {
     std::deque<Job *> retired;   // results taken, device memory still to free (by a worker)
     uint64_t used = 0;           // footprint of prepared + active jobs
     uint64_t n_active = 0;       // jobs prepared or active (retired ones until freed)
-    size_t graded_n = 0;         // jobs the batch is bound to
     uint64_t preparing = 0;      // jobs a worker is preparing now
     bool stop = false;
     std::vector<std::thread> workers;
@@ -307,7 +316,10 @@ extern "C" void pdf_server_destroy(pdf_server *srv) {
     for (std::thread &w : srv->workers) w.join();
     cudaSetDevice(srv->o.device);
     cudaStreamSynchronize(srv->stream);
-    pdf_batch_destroy(srv->batch);
+    for (pdf_batch *b : srv->batch) pdf_batch_destroy(b);
+    for (cudaEvent_t e : srv->done_ev)
+        if (e) cudaEventDestroy(e);
+    if (srv->rstream) cudaStreamDestroy(srv->rstream);
     for (Job *j : srv->active) free_job(j);
     for (Job *j : srv->ready) free_job(j);
     for (Job *j : srv->retired) free_job(j);
@@ -348,6 +360,13 @@ extern "C" pdf_status pdf_server_submit(pdf_server *srv, const pdf_netlist *nl, 
     return PDF_OK;
 }
 
+// One step keeps one batched pass in flight: it admits ready jobs, binds the
+// next batch of every job with pairs left to one of two batches, enqueues
+// that pass on the server's stream, and only then waits for the pass the
+// previous step enqueued, accounts for it and retires the jobs it finished.
+// So the host's work of a step (admission, binding, read-back of retiring
+// jobs) runs while the device grades, and a job's batches still follow one
+// another in stream order.
 extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     if (!srv) return PDF_EINVAL;
     if (retired) *retired = 0;
@@ -355,11 +374,12 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     const double t0 = now_s();
     pdf_status st = PDF_OK;
     // admission: the jobs the worker has prepared (in arrival order); with
-    // none active, wait (up to a second) for the first one queued or in
-    // preparation
+    // none active and no pass in flight, wait (up to a second) for the first
+    // one queued or in preparation
     {
         std::unique_lock<std::mutex> lk(srv->mu);
-        if (srv->active.empty() && srv->ready.empty() && (srv->preparing > 0 || !srv->queue.empty()))
+        if (srv->active.empty() && !srv->pending && srv->ready.empty() &&
+            (srv->preparing > 0 || !srv->queue.empty()))
             srv->cv.wait_for(lk, std::chrono::seconds(1), [&] {
                 return !srv->ready.empty() || (srv->preparing == 0 && srv->queue.empty());
             });
@@ -378,32 +398,37 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
                 continue;
             }
             srv->active.push_back(j);
-            srv->dirty = true;
         }
     }
-    if (srv->active.empty()) return PDF_OK;
-    // The jobs to grade: every active job with pairs left (a job whose pairs
-    // are all graded but whose retirement failed in an earlier step only
-    // waits to retire).  Their next batch is read in place from the job's
-    // pairs (rows of words done/32 .. on) when their pitch keeps the
-    // kernels' alignment, which moves the job's view every batch; else
-    // copied into the job's batch buffer (device to device).
+    if (srv->active.empty() && !srv->pending) return PDF_OK;
+    if (!srv->done_ev[0]) {
+        for (int k = 0; k < 2; k++)
+            if (cudaEventCreateWithFlags(&srv->done_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+                (void)cudaGetLastError();
+                return PDF_ECUDA;
+            }
+        if (cudaStreamCreateWithFlags(&srv->rstream, cudaStreamNonBlocking) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return PDF_ECUDA;
+        }
+    }
+    // ---- the next pass: every active job with pairs left that is not in
+    // the pass in flight's last batch (a job's pairs are all accounted for
+    // when its last batch is enqueued).  Its next batch is read in place
+    // from the job's pairs (rows of words done/32 .. on) when their pitch
+    // keeps the kernels' alignment, else copied into the job's batch buffer
+    // (device to device, ordered after the pass in flight, which may read it)
     const uint64_t tw = srv->o.tile_words;
     std::vector<Job *> grading;
     for (Job *j : srv->active) {
         if (j->done >= j->n_pairs) continue;
         grading.push_back(j);
         const uint64_t n = std::min<uint64_t>(srv->o.batch_pairs, j->n_pairs - j->done);
-        if (n != j->cur) srv->dirty = true;
         j->cur = n;
         const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32, W = (n + 31) / 32;
-        const bool in_place = j->hld % tw == 0 && (npi * j->hld) % 4 == 0 && w0 % 4 == 0 && w0 % tw == 0 &&
-                              w0 + (W + tw - 1) / tw * tw <= j->hld;
-        // a view moves every batch; a job that leaves its view for the batch
-        // buffer (or comes back to it) changes its pairs' address and pitch
-        if (in_place || in_place != j->in_place) srv->dirty = true;
-        j->in_place = in_place;
-        if (in_place) continue;
+        j->in_place = j->hld % tw == 0 && (npi * j->hld) % 4 == 0 && w0 % 4 == 0 && w0 % tw == 0 &&
+                      w0 + (W + tw - 1) / tw * tw <= j->hld;
+        if (j->in_place) continue;
         uint32_t *dv = j->dv, *dt = j->dv + npi * j->ld;
         const uint32_t *sv = j->dall + w0, *stp = j->dall + npi * j->hld + w0;
         if (cudaMemcpy2DAsync(dv, j->ld * 4, sv, j->hld * 4, W * 4, npi, cudaMemcpyDeviceToDevice, srv->stream) !=
@@ -414,54 +439,83 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
             return PDF_ECUDA;
         }
     }
-    if (grading.size() != srv->graded_n) srv->dirty = true;
+    bool enqueued = false;
+    const int b_now = srv->cur;
     if (!grading.empty()) {
-        if (srv->dirty) {
-            std::vector<pdf_batch_job> jobs;
-            for (Job *j : grading) {
-                const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32;
-                const pdf_pairs p = j->in_place
-                                        ? pdf_pairs{j->dall + w0, j->dall + npi * j->hld + w0, j->cur, j->hld, 1}
-                                        : pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1};
-                jobs.push_back(pdf_batch_job{j->c, j->s, p, j->done});
-            }
-            const uint32_t fl = PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH;
-            const bool fresh = !srv->batch;
-            st = srv->batch ? pdf_batch_rebind(srv->batch, jobs.data(), (uint32_t)jobs.size(), fl)
-                            : pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), fl, &srv->batch);
-            if (st != PDF_OK) return st;
-            // events around each pass's forward launches and cover: its device time
-            if (fresh && (st = pdf_batch_profile(srv->batch, 1)) != PDF_OK) return st;
-            srv->dirty = false;
-            srv->graded_n = grading.size();
+        // the batch last used two passes ago (done: the previous step waited
+        // for it); its control block is uploaded in order on the stream
+        std::vector<pdf_batch_job> jobs;
+        for (Job *j : grading) {
+            const uint64_t npi = j->view.level_offsets[1], w0 = j->done / 32;
+            const pdf_pairs p = j->in_place ? pdf_pairs{j->dall + w0, j->dall + npi * j->hld + w0, j->cur, j->hld, 1}
+                                            : pdf_pairs{j->dv, j->dv + npi * j->ld, j->cur, j->ld, 1};
+            jobs.push_back(pdf_batch_job{j->c, j->s, p, j->done});
         }
-        if ((st = pdf_batch_run(srv->batch, srv->stream)) != PDF_OK) return st;
-        double ms[2] = {0.0, 0.0};
-        if (pdf_batch_profile_read(srv->batch, ms) == PDF_OK) srv->st.gpu_s += (ms[0] + ms[1]) / 1e3;
+        const uint32_t fl = PDF_BATCH_APPEND | PDF_BATCH_NO_GRAPH;
+        pdf_batch *&b = srv->batch[b_now];
+        if (!b) {
+            if ((st = pdf_batch_create(jobs.data(), (uint32_t)jobs.size(), fl, &b)) != PDF_OK) return st;
+            // events around each pass's forward launches and cover: its device time
+            if ((st = pdf_batch_profile(b, 1)) != PDF_OK) return st;
+        }
+        if ((st = batch_rebind_on(b, jobs.data(), (uint32_t)jobs.size(), fl, srv->stream)) != PDF_OK) return st;
+        if ((st = batch_pass_async(b, srv->stream)) != PDF_OK) return st;
+        if (cudaEventRecord(srv->done_ev[b_now], srv->stream) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return PDF_ECUDA;
+        }
         pdf_batch_info bi{};
-        if (pdf_batch_query(srv->batch, &bi) == PDF_OK) srv->st.launches += bi.launches;
-        // the pass has graded (and, on the device, appended) every job's
-        // batch: account for it now, whatever happens below
+        if (pdf_batch_query(b, &bi) == PDF_OK) srv->st.launches += bi.launches;
+        // the jobs' pairs of this batch are accounted for now: the next step
+        // binds their following batch
+        for (Job *j : grading) j->done += j->cur;
+        enqueued = true;
+    }
+    // ---- the pass the previous step enqueued: wait for it, account for it
+    if (srv->pending) {
+        const int pb = srv->pend_b;
+        if (cudaEventSynchronize(srv->done_ev[pb]) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return PDF_ECUDA;
+        }
+        const pdf_status ps = batch_pass_status(srv->batch[pb]);
+        double ms[2] = {0.0, 0.0};
+        if (pdf_batch_profile_read(srv->batch[pb], ms) == PDF_OK) srv->st.gpu_s += (ms[0] + ms[1]) / 1e3;
         const double t1 = now_s();
         srv->st.steps++;
-        for (Job *j : grading) {
+        for (Job *j : srv->inflight) {
             srv->lat_ms.push_back(1e3 * (t1 - j->t_ready));
             j->t_ready = t1;
             srv->st.batches++;
-            srv->st.gate_evals += (uint64_t)j->view.n_gates * j->cur;
-            j->done += j->cur;
-            if (j->done >= j->n_pairs) srv->dirty = true;  // leaves the batch
+            srv->st.gate_evals += (uint64_t)j->view.n_gates * j->graded;
+            j->in_flight = false;
+        }
+        srv->pending = false;
+        srv->inflight.clear();
+        if (ps != PDF_OK) st = ps;  // reported after the pass enqueued above is recorded
+    }
+    if (enqueued) {
+        srv->pending = true;
+        srv->pend_b = b_now;
+        srv->cur ^= 1;
+        srv->inflight = grading;
+        for (Job *j : grading) {  // after the previous pass's jobs were cleared above
+            j->in_flight = true;
+            j->graded = j->cur;
         }
     }
-    // Retire the jobs whose pairs are all graded.  No job is handed to the
-    // workers (who free retired jobs) or leaves the active list until every
-    // read-back of this step has succeeded; after a failure here those jobs
-    // stay active, are not graded again, and retire at a later step.  First
-    // the pinned staging of their first-detect ids, grown geometrically
-    // (freeing pinned memory waits for the device).
+    if (st != PDF_OK) return st;
+    // ---- retire the jobs whose pairs are all graded and whose last pass is
+    // done.  No job is handed to the workers (who free retired jobs) or
+    // leaves the active list until every read-back of this step has
+    // succeeded; after a failure here those jobs stay active and retire at
+    // a later step.  Read back on a stream of its own: the server's stream
+    // holds the pass just enqueued.  First the pinned staging of their
+    // first-detect ids, grown geometrically (freeing pinned memory waits for
+    // the device).
     size_t gmax = 0;
     for (Job *j : srv->active)
-        if (j->done >= j->n_pairs) gmax = std::max<size_t>(gmax, j->view.n_gates);
+        if (j->done >= j->n_pairs && !j->in_flight) gmax = std::max<size_t>(gmax, j->view.n_gates);
     if (srv->pin_words < 2 * gmax) {
         const size_t want = std::max(2 * gmax, 2 * srv->pin_words);
         if (srv->pin) cudaFreeHost(srv->pin);
@@ -477,7 +531,7 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
     std::vector<Job *> keep, gone;
     std::vector<Result> res;
     for (Job *j : srv->active) {
-        if (j->done < j->n_pairs) {
+        if (j->done < j->n_pairs || j->in_flight) {
             keep.push_back(j);
             continue;
         }
@@ -485,9 +539,7 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         const size_t G = j->view.n_gates;
         r.fx.resize(G);
         r.fy.resize(G);
-        // ordered on the server's stream: a device-wide sync would also wait
-        // for the workers' uploads of arriving jobs
-        if ((st = pdf_state_snapshot_on(j->s, srv->pin, srv->pin + G, &r.total, srv->stream)) != PDF_OK) return st;
+        if ((st = pdf_state_snapshot_on(j->s, srv->pin, srv->pin + G, &r.total, srv->rstream)) != PDF_OK) return st;
         std::memcpy(r.fx.data(), srv->pin, 4 * G);
         std::memcpy(r.fy.data(), srv->pin + G, 4 * G);
         res.push_back(std::move(r));
@@ -501,7 +553,6 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         }
         srv->cv.notify_all();
         srv->st.jobs_done += gone.size();
-        srv->dirty = true;
         if (retired) *retired = (uint32_t)gone.size();
     }
     srv->active.swap(keep);
