@@ -464,11 +464,13 @@ pdf_status pdf_batch_autotune(const pdf_netlist *const *netlists, const uint64_t
  * it is graded in batches of `batch_pairs` pairs that append to the job's
  * device-resident coverage state.  Each pdf_server_step admits queued jobs
  * in arrival order while their device footprint fits `hbm_budget` (and
- * fewer than `max_jobs` are active), grades the next batch of every active
- * job in one batched pass (pdf_batch_*), and retires jobs whose pairs are
- * all graded (their results stay readable).  Jobs that arrive while a step
- * runs join at the next step, so work of jobs of different ages overlaps on
- * the device.  A job's result equals pdf_grade of all its pairs in batches of
+ * fewer than `max_jobs` are active), enqueues the next batch of every active
+ * job as one batched pass (pdf_batch_*), then waits for the pass the step
+ * before enqueued and retires the jobs whose pairs that pass finished
+ * grading (their results stay readable).  So one pass stays in flight while
+ * the caller's thread works between steps, and a job retires at the step
+ * after its last batch was enqueued.  Jobs that arrive meanwhile join at the
+ * next step, so work of jobs of different ages overlaps on the device.  A job's result equals pdf_grade of all its pairs in batches of
  * batch_pairs.  Per-batch latency is the time from the batch being ready
  * (submission, or the previous batch's end) to its result.  No reference
  * counterpart: the reference grades one circuit per process (main.cu).
@@ -499,7 +501,9 @@ void pdf_server_destroy(pdf_server *srv);
 /* Queue a job: v, t are host planes [n_pi][ld] of n_pairs pairs. */
 pdf_status pdf_server_submit(pdf_server *srv, const pdf_netlist *nl, const uint32_t *v, const uint32_t *t,
                              uint64_t ld, uint64_t n_pairs, uint64_t *job_id);
-/* One step; *retired gets the number of jobs that finished in it. */
+/* One step; *retired gets the number of jobs that finished in it.  Call it
+ * until every job has retired: a step with no job to grade still completes
+ * the pass in flight. */
 pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired);
 /* Result of a finished job: its total (and first-detect ids, if non-null, n_gates each).
  * PDF_EINVAL while the job is still queued or active. */
