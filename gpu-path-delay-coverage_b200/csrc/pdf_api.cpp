@@ -595,18 +595,25 @@ extern "C" pdf_status pdf_circuit_create(const pdf_netlist *nl, const pdf_circui
     if (lanes) {
         // The lane kernel keeps on chip two buffers of staged gate records
         // and the column block's mark bitmap (in global memory when it does
-        // not fit); its pieces are runs of one level of <= kLaneRecs gates.
+        // not fit); its pieces are runs of one level of <= cap gates: 2 x
+        // kLaneRecs when those buffers fit beside a shared-memory bitmap (a
+        // barrier per piece, so wide levels take half as many), else
+        // kLaneRecs.
+        const size_t bm_bytes = (size_t)bm_words * 4;
+        c->cap = kLaneRecs;
+        if (widest > kLaneRecs &&
+            2 * 2 * (size_t)kLaneRecs * sizeof(GateRec) + al(bm_bytes) + 2048 <= budget)
+            c->cap = 2 * kLaneRecs;
         for (uint32_t l = 0; l < L; l++)
-            for (uint32_t a = nl->level_offsets[l]; a < nl->level_offsets[l + 1]; a += kLaneRecs) {
+            for (uint32_t a = nl->level_offsets[l]; a < nl->level_offsets[l + 1]; a += c->cap) {
                 Piece p{};
                 p.a = a;
-                p.b = std::min(a + kLaneRecs, nl->level_offsets[l + 1]);
+                p.b = std::min(a + c->cap, nl->level_offsets[l + 1]);
                 p.level = l;
                 pieces.push_back(p);
             }
         c->n_pieces = (uint32_t)pieces.size();
-        const size_t rec_bytes = 2 * (size_t)kLaneRecs * sizeof(GateRec);
-        const size_t bm_bytes = (size_t)bm_words * 4;
+        const size_t rec_bytes = 2 * (size_t)c->cap * sizeof(GateRec);
         c->off_rec = 0;
         c->off_bm = (uint32_t)rec_bytes;
         c->bm_shared = rec_bytes + bm_bytes + 2048 <= budget ? 1u : 0u;

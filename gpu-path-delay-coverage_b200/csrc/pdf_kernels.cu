@@ -1062,7 +1062,7 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
     P.M = reinterpret_cast<char *>(a.M + w);
     uint32_t *bm = a.bm_shared ? reinterpret_cast<uint32_t *>(smraw + a.off_bm) : a.nzb + (size_t)blk * a.bm_words;
     uint32_t *gbm = a.nzb ? a.nzb + (size_t)blk * a.bm_words : nullptr;
-    GateRec *recs = reinterpret_cast<GateRec *>(smraw + a.off_rec);  // [2][kLaneRecs]
+    GateRec *recs = reinterpret_cast<GateRec *>(smraw + a.off_rec);  // [2][a.cap]
     const uint32_t *lo = a.c.level_off;
 
     if (MODE != FWD_SIM)
@@ -1085,13 +1085,13 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
     __syncthreads();
 
     // ------------------------------------------------------------- forward
-    // Pieces (runs of one level, <= kLaneRecs gates) in level order; each
+    // Pieces (runs of one level, <= a.cap gates) in level order; each
     // piece's gate records are copied into shared memory (cp.async, 16 bytes
     // per thread and copy) while the piece before it is evaluated, and its
     // descriptor is loaded a piece earlier still.  One barrier per piece.
     const auto stage = [&](uint32_t ga, uint32_t gb, int buf) {
         const uint4 *src = reinterpret_cast<const uint4 *>(a.c.rec + ga);
-        uint4 *dst = reinterpret_cast<uint4 *>(recs + (size_t)buf * kLaneRecs);
+        uint4 *dst = reinterpret_cast<uint4 *>(recs + (size_t)buf * a.cap);
         for (uint32_t i = threadIdx.x; i < 2 * (gb - ga); i += blockDim.x)
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + i)), "l"(src + i) : "memory");
     };
@@ -1122,7 +1122,7 @@ __device__ __forceinline__ void forward_lanes_cta(const FwdArgs &a, const uint32
             nb = __ldg(&a.pieces[i + 2].b);
             nlv = __ldg(&a.pieces[i + 2].level);
         }
-        const GateRec *rb = recs + (size_t)(i & 1) * kLaneRecs;
+        const GateRec *rb = recs + (size_t)(i & 1) * a.cap;
         for (uint32_t g = ga + warp; g < gb; g += U * NW) {
             LaneIn<LW> x[U];
 #pragma unroll
