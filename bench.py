@@ -607,7 +607,26 @@ def run_batched(args):
     P = pkg()
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        # replicas: every rank grades the whole batch on its own GPU (the
+        # circuits share nothing); the process group only times the ranks
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        args.no_tile_sweep = True  # the plain arm's per-circuit tile sweep runs at N = 1
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     members = workload_members(P, args)
     nls = [m[0] for m in members]
     counts = [m[2] for m in members]
@@ -727,6 +746,8 @@ def run_batched(args):
     sampler.start()
     time.sleep(0.1)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     sampler.mark_start()
     for i in range(args.steps):
         flush.fill_(i & 0xFF)
@@ -737,10 +758,12 @@ def run_batched(args):
         fwd_ms.append(f)
         cov_ms.append(cv)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     sampler.mark_end()
     clocks = sampler.stop()
     b.profile(False)
-    ms = sum(x.elapsed_time(y) for x, y in ev) / args.steps
+    ms = max_over_ranks(sum(x.elapsed_time(y) for x, y in ev) / args.steps)
     passes_run = 1 + max(3, args.warmup) + args.steps
     stable = all(a[2].value == passes_run * x[2].value for a, x in zip(results(), batch_res))
 
@@ -793,9 +816,12 @@ def run_batched(args):
 
     streamed(2)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t1 = time.perf_counter()
     streamed(args.steps)
-    stream_ms = 1e3 * (time.perf_counter() - t1) / args.steps
+    stream_ms = max_over_ranks(1e3 * (time.perf_counter() - t1) / args.steps)
+    e2e_ms = max_over_ranks(e2e_ms)
     b2.close()
     info = b.info()
     kernel_ms = sum(fwd_ms) / len(fwd_ms)
@@ -803,10 +829,11 @@ def run_batched(args):
     prof = profile_summary(f"k_batch_forward_c4_tile{tw}") if args.circuits == 256 else None
     plain_best = min(plain_ms, plain_bt_ms, sweep_ms or float("inf"))
     line = {
-        "metric": "gate-evals/s", "value": units / (ms / 1e3), "unit": "gate-evals/s", "n_gpus": 1,
+        "metric": "gate-evals/s", "value": world * units / (ms / 1e3), "unit": "gate-evals/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
         "config": dict(batch_config(members, args), tile_words=tw, threads=threads or "default",
+                       parallelism=f"replicas x{world}" if world > 1 else "one GPU",
                        ctas=info.ctas, forward_launches=int(info.forward_launches),
                        autotune={"tile_words": tw, "threads": threads, "ms_per_pass": tune_ms,
                                  "seconds": round(tune_s, 1)} if tune_ms else None),
@@ -822,22 +849,25 @@ def run_batched(args):
                                   f"forward span of the pass (k_batch_forward{'_lanes' if tw in LANE_TILES else ''}, "
                                   f"every class)", prof, units, sm_count, clocks.get("sm_mhz")),
                          cover_ms=sum(cov_ms) / len(cov_ms)),
-        "e2e": {"value": units / (stream_ms / 1e3), "unit": "gate-evals/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": 64 * len(jobs),
+        "e2e": {"value": world * units / (stream_ms / 1e3), "unit": "gate-evals/s",
+                "h2d_bytes_per_step": int(world * h2d), "d2h_bytes_per_step": 64 * len(jobs) * world,
                 "mode": "streamed: pinned host pairs of the next pass copied on a second stream while this "
                         "pass grades (two buffer sets, two batches)",
-                "value_one_pass_per_step": units / (e2e_ms / 1e3)},
-        "gpu_launches": int(info.launches) * args.steps,  # forward per class, active, cover (, spill cover)
+                "value_one_pass_per_step": world * units / (e2e_ms / 1e3)},
+        "gpu_launches": int(info.launches) * args.steps * world,  # forward per class, active, covers, spill cover
         "clocks": clocks,
         "same_config": True,
         "result_stable": bool(same and stable and sweep_same),
         "native_libraries": loaded_libraries(),
     }
-    if not args.no_cpu and rank == 0:
+    if not args.no_cpu and rank == 0 and world == 1:
         line["cpu_baseline"], line["cpu_baseline_1core"] = cpu_baselines(P, members, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     b.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
