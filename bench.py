@@ -224,6 +224,11 @@ def roofline(alg: float, kernel_ms: float, kernel: str, prof: dict | None, units
             out["issue_slots_frac"] = wi / slots
             out["issue_note"] = ("warp instructions per launch (ncu smsp__inst_executed.sum) over "
                                  "SMs x 4 schedulers x sampled SM clock x kernel time")
+    # what the numbers say bounds the kernel: HBM or issue when either is
+    # near its peak, else latency (dependent chains per warp, barriers)
+    issue = out.get("issue_slots_frac")
+    out["limiter"] = ("hbm" if out["frac"] >= 0.8 else "issue" if issue is not None and issue >= 0.8 else
+                      "latency" if issue is not None else "unknown (no ncu summary for this kernel)")
     return out
 
 
@@ -979,7 +984,7 @@ def run_served(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
