@@ -460,21 +460,27 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         }
         if ((st = batch_rebind_on(b, jobs.data(), (uint32_t)jobs.size(), fl, srv->stream)) != PDF_OK) return st;
         if ((st = batch_pass_async(b, srv->stream)) != PDF_OK) return st;
-        if (cudaEventRecord(srv->done_ev[b_now], srv->stream) != cudaSuccess) {
-            (void)cudaGetLastError();
-            return PDF_ECUDA;
-        }
-        pdf_batch_info bi{};
-        if (pdf_batch_query(b, &bi) == PDF_OK) srv->st.launches += bi.launches;
-        // the jobs' pairs of this batch are accounted for now: the next step
-        // binds their following batch
+        // the pass is on the stream: the jobs' pairs of this batch are
+        // accounted for now (the next step binds their following batch)
         for (Job *j : grading) j->done += j->cur;
         enqueued = true;
+        pdf_batch_info bi{};
+        if (pdf_batch_query(b, &bi) == PDF_OK) srv->st.launches += bi.launches;
+        if (cudaEventRecord(srv->done_ev[b_now], srv->stream) != cudaSuccess) {
+            // without its event the next step could not wait for this pass:
+            // wait for it here, and report the failure once it is recorded
+            (void)cudaGetLastError();
+            (void)cudaStreamSynchronize(srv->stream);
+            (void)cudaGetLastError();
+            st = PDF_ECUDA;
+        }
     }
     // ---- the pass the previous step enqueued: wait for it, account for it
     if (srv->pending) {
         const int pb = srv->pend_b;
         if (cudaEventSynchronize(srv->done_ev[pb]) != cudaSuccess) {
+            // an error left by the device itself: every later read-back
+            // fails too, so no job can retire with a result read early
             (void)cudaGetLastError();
             return PDF_ECUDA;
         }
@@ -492,7 +498,7 @@ extern "C" pdf_status pdf_server_step(pdf_server *srv, uint32_t *retired) {
         }
         srv->pending = false;
         srv->inflight.clear();
-        if (ps != PDF_OK) st = ps;  // reported after the pass enqueued above is recorded
+        if (ps != PDF_OK && st == PDF_OK) st = ps;  // reported after the pass enqueued above is recorded
     }
     if (enqueued) {
         srv->pending = true;
