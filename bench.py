@@ -18,7 +18,8 @@ c4-sized jobs served with continuous batching).
 Prints one JSON line (rank 0).  For N > 1 (torchrun) on c1-c3, each rank
 grades its own pairs of the same circuit; the ranks exchange first-detect ids
 (all-reduce MIN) before counting, so the job equals one grading of all ranks'
-pairs (weak scaling).
+pairs (weak scaling).  On c4 each rank grades the whole batch (replicas; the
+ranks are timed together and the slowest sets the time).
 """
 from __future__ import annotations
 
