@@ -641,7 +641,8 @@ def run_batched(args):
     if args.tile_words:
         tw, tune_ms = args.tile_words, None
     else:
-        best, tune_ms = P.batch_autotune(nls, counts, mark_mode=P.MARK_ROBUST, reps=2, threads=args.threads)
+        best, tune_ms = P.batch_autotune(nls, counts, mark_mode=P.MARK_ROBUST, reps=2, device=local,
+                                         threads=args.threads)
         tw = best.tile_words
         threads = best.threads
     tune_s = time.perf_counter() - t0
